@@ -1,0 +1,312 @@
+#!/usr/bin/env python
+"""Throughput of the multi-layer XPBD step on B200 (one JSON line on rank 0).
+
+Workload: the plain multi-layer Neo-Hookean block -- 64x16x16 cubes of 0.1 m,
+6 tets per cube (18,785 vertices, 98,304 tets), per-tet E log-uniform in
+[1e4, 1e7] Pa, nu uniform in [0.25, 0.45] (seeded), a coarse layer of fixed
+8^3-cube rigid clusters (5 iterations) then the fine layer (10 iterations),
+dt = 1/60 s, base pinned, seeded surface impulse at t = 0.  Synthetic data.
+
+A step is one xpbdLayer3D.integrate step.  `value` is steps/s of the
+device-resident stepper (state in HBM, one CUDA graph per step) with L2
+flushed between timed steps; `e2e` is steps/s through the public host API
+(XpbdLayer3D.integrate -> mlx_layer_solve with host buffers, every step copies
+its inputs host->device and its positions back).  Multi-GPU runs are
+independent replicas (weak scaling): the step does not shard.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "sim steps/sec & iters to residual 1e-4: learned warm-start vs plain, 1 B200"
+WORKLOAD = ("config2: plain multi-layer Neo-Hookean block 64x16x16 cubes (18785 vertices, 98304 tets), "
+            "coarse 8^3-cube rigid clusters (5 it) + fine layer (10 it), dt=1/60, base pinned, "
+            "seeded surface impulse at t=0")
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            time.sleep(0.3)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peak_hbm():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        if d.get("hbm_gbs"):
+            return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def make_scene():
+    from multilayersolver2024_b200 import scenes
+    return scenes.config2()
+
+
+def make_integrator(scene, precision):
+    from multilayersolver2024_b200 import XpbdLayer3D
+    integ = XpbdLayer3D()
+    integ.Gravity = scene.gravity
+    integ.setLayers(scene.layers)
+    integ.iterations = list(scene.iterations)
+    integ.customRigidSets = scene.custom_sets
+    integ.precision = precision
+    return integ
+
+
+def cpu_port_steps_per_s(nsteps, threads):
+    """The oracle (FP64 C++ restatement of the reference path, all given host
+    threads) on the same workload: steps/s over `nsteps` steps."""
+    from oracle import oracle as O
+    from multilayersolver2024_b200.xpbd_layer3d import ContactSet, StepCache
+    O.load().orc_set_threads(threads)
+    sc = make_scene()
+    integ = make_integrator(sc, 1)
+    m = sc.mesh
+    m.v[sc.impulse[0] - 1] += sc.impulse[1]
+    cache = StepCache()
+    O.integrate(integ, m, sc.h, ContactSet(), cache, 1)  # warm-up (frame 1)
+    t0 = time.perf_counter()
+    for frame in range(2, nsteps + 2):
+        O.integrate(integ, m, sc.h, ContactSet(), cache, frame)
+    dt = time.perf_counter() - t0
+    return nsteps / dt, dt
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    warm = max(args.warmup, 0)
+    # warm-up steps are part of the same run of the port
+    total = warm + args.steps
+    sps, dt = cpu_port_steps_per_s(total, threads)
+    value = sps
+    line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "solver": "plain multi-layer, CPU port"},
+            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "port",
+                             "sample": f"{total} consecutive steps of the full workload (oracle restatement; "
+                                       "MATLAB, the reference's runtime, is not installed)"},
+            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    from multilayersolver2024_b200 import MLX_FP32, StepCache, XpbdLayer3D, load
+    from multilayersolver2024_b200.xpbd_layer3d import ContactSet, ResidentSim, Solver, find_boundary_vertices
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    lib = load()
+    assert lib.mlx_device_count() > 0, "no sm_100 device visible"
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    sc = make_scene()
+    m = sc.mesh
+    integ = make_integrator(sc, MLX_FP32)
+    sets = sc.custom_sets
+    ls = find_boundary_vertices(m, sets, [int(sets[:, c].max(initial=0)) for c in range(sets.shape[1])])
+    solver = Solver(m, precision=MLX_FP32, device=local, material="lame")
+    sim = ResidentSim(solver, integ, ls, sc.h, p0=m.p, v0=np.zeros_like(m.p))
+    sim.add_velocity(sc.impulse[0], sc.impulse[1])
+    sim.sweep_timing(True)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
+    for _ in range(args.warmup):
+        sim.step(1, graph=True)
+    torch.cuda.synchronize()
+    sim.sweep_stats(reset=True)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    total_ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        total_ms += sim.step(1, graph=True, timed=True)
+    torch.cuda.synchronize()
+    barrier()
+    clocks.stop()
+    sweep_ms, sweep_bytes, sweep_launches = sim.sweep_stats(reset=True)
+    max_ms = max_over_ranks(total_ms)
+    value = args.steps * world / (max_ms / 1000.0)
+    launches_per_step = sim.launches_per_step
+    p_gpu, _ = sim.state()
+    finite = bool(np.all(np.isfinite(p_gpu)))
+
+    # ---- e2e: public host API, host buffers, every step copies in and out ----
+    sc2 = make_scene()
+    m2 = sc2.mesh
+    integ2 = make_integrator(sc2, MLX_FP32)
+    cache = StepCache()
+    m2.v[sc2.impulse[0] - 1] += sc2.impulse[1]
+    e2e_steps = max(3, min(args.steps, 20))
+    for frame in range(1, 3):  # warm-up: solver creation and layer caches
+        integ2.integrate(m2, sc2.h, ContactSet(), cache, frame)
+    barrier()
+    e2e_s = 0.0
+    for frame in range(3, 3 + e2e_steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        integ2.integrate(m2, sc2.h, ContactSet(), cache, frame)
+        e2e_s += time.perf_counter() - t0
+    barrier()
+    e2e_s = max_over_ranks(e2e_s)
+    N, T = m2.N, m2.T
+    h2d = 8 * (3 * 3 * N + 6 * T + m2.pinnedDOFs.size)
+    d2h = 8 * 3 * N
+
+    line = None
+    if rank == 0:
+        peak, peak_kind = measured_peak_hbm()
+        achieved = (sweep_bytes / (sweep_ms / 1000.0)) / 1e9 if sweep_ms > 0 else None
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            sps, dt = cpu_port_steps_per_s(args.cpu_steps, threads)
+            cpu = {"value": sps, "unit": "steps/s", "cores": threads, "kind": "port",
+                   "sample": f"{args.cpu_steps} steps of the full workload after 1 warm-up step "
+                             f"({dt:.1f} s, FP64 oracle restatement, OpenMP over the tets of a colour)"}
+        line = {
+            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "solver": "plain multi-layer (no warm-start)",
+                       "iterations_per_step": int(sum(sc.iterations)), "precision": "FP32 bulk, FP64 rigid bodies",
+                       "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}",
+                       "graph": "one CUDA graph per step"},
+            "roofline": {"bound": "hbm", "kernel": "k_project_color (all colours of a sweep)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "peak_kind": peak_kind, "bytes_per_tet": solver_bytes_per_tet(m, MLX_FP32),
+                         "sweep_ms_per_step": sweep_ms / args.steps,
+                         "colour_launches_per_step": sweep_launches / args.steps,
+                         "avg_launch_us": 1000.0 * sweep_ms / max(sweep_launches, 1)},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_steps * world / e2e_s, "unit": "steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "api": "XpbdLayer3D.integrate -> mlx_layer_solve"},
+            "gpu_launches": int(launches_per_step * args.steps),
+            "clocks": clocks.summary(),
+            "state_finite": finite,
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def solver_bytes_per_tet(mesh, precision):
+    """Algorithmic bytes of one tet projection in the device layout: vertex
+    ids (16), DmInv (9 r), volume (r), material (2 r for Neo-Hookean, 3 r for
+    StVK from Lame parameters), lambda read + write (2 x 2 r or 2 x 6 r), four
+    vertex records read and written (8 x 4 r); r = 4 (FP32) or 8 (FP64)."""
+    from multilayersolver2024_b200 import MLX_ENERGY_NEOHOOKEAN
+    r = 4 if precision == 0 else 8
+    nh = mesh.energy_type == MLX_ENERGY_NEOHOOKEAN
+    return 16 + 9 * r + r + (2 if nh else 3) * r + 2 * (2 if nh else 6) * r + 8 * 4 * r
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,250 @@
+/*
+ * mlxpbd.h -- C ABI of the B200 multi-layer XPBD step.
+ *
+ * This is the drop-in boundary for the reference's static
+ * `xpbdLayer3D.layerSolve` (3d/integrator/xpbdLayer3D.m:44-93) and the helpers
+ * `xpbdLayer3D.integrate` calls around it (xpbdLayer3D.m:601-745).  Every entry
+ * point takes plain pointers and sizes, returns an int status (MLX_OK == 0) and
+ * never throws; the message of the last failure on the calling thread is
+ * available from mlx_last_error().
+ *
+ * Array conventions follow the MATLAB caller exactly, so a mex gateway can pass
+ * mxArray data pointers straight through:
+ *   - positions, velocities, forces, masses: 3N doubles, AoS [x1 y1 z1 x2 ...]
+ *     (Mesh3D.p, Mesh3D.m:181);
+ *   - index arrays are 1-based int32 and matrices are column-major
+ *     (Mesh3D.t is T x 4, Mesh3D.m:193);
+ *   - page arrays (DmInv 3x3xT, alpha 6x6xT) are column-major pages;
+ *   - logical masks are one byte per entry (MATLAB `logical`).
+ * The library never keeps a caller pointer beyond the call that received it.
+ */
+#ifndef MLXPBD_H
+#define MLXPBD_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MLX_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  MLX_OK = 0,
+  MLX_ERR_ARGUMENT = 1,     /* bad pointer / size / value                    */
+  MLX_ERR_UNSUPPORTED = 2,  /* valid input this build does not handle        */
+  MLX_ERR_CUDA = 3,         /* a CUDA runtime call failed                     */
+  MLX_ERR_NO_DEVICE = 4,    /* no usable sm_100 device                        */
+  MLX_ERR_NUMERIC = 5,      /* NaN/Inf detected in the state                  */
+  MLX_ERR_LIMIT = 6,        /* an iteration or wait limit was reached         */
+  MLX_ERR_ALLOC = 7         /* device or host allocation failed              */
+};
+
+/* ---- element energies (xpbdLayer3D.energyType, xpbdLayer3D.m:22) -------- */
+enum {
+  MLX_ENERGY_NEOHOOKEAN = 1,   /* stable Neo-Hookean D/H pair per tet; the 3D
+                                  form of 2d/mex/mexNeoHookeanDConstraint.cpp and
+                                  mexNeoHookeanHConstraint.cpp                   */
+  MLX_ENERGY_STVK_VOIGT = 2    /* matStvkVoigtConstraint3D.m:1-45              */
+};
+
+/* ---- arithmetic of the bulk projection ---------------------------------- */
+enum {
+  MLX_FP32 = 0,   /* positions, lambdas and tet rest data in FP32; rigid-body
+                     state, its reductions and the residual norm in FP64      */
+  MLX_FP64 = 1    /* everything in FP64 (the reference's own precision)      */
+};
+
+/* Mesh precompute consumed by layerSolve: the Mesh3D fields of
+ * xpbdLayer3D.m:713-729 (mass, t, pinnedDOFs, DmInv, alpha, beta, colours,
+ * volume).  Compliance is given in ONE of two forms:
+ *   (a) alpha/beta pages exactly as Mesh3D.updateMaterials builds them
+ *       (Mesh3D.m:445-460).  They must be block diagonal (3x3 (+) 3x3 with a
+ *       diagonal lower block) -- which updateMaterials always produces;
+ *   (b) per-tet Lame parameters mu/lambda and Rayleigh alpha1, from which the
+ *       same blocks are formed on the device (TriangleMaterial.m:18-64).
+ * Neo-Hookean meshes need mu/lambda (form b). */
+typedef struct mlx_mesh_desc {
+  int32_t num_vertices;          /* N                                         */
+  int32_t num_tets;              /* T                                         */
+  const int32_t* t;              /* T x 4, column-major, 1-based              */
+  const double* mass;            /* 3N lumped masses (computeMass.m:24-39)    */
+  const double* DmInv;           /* 3 x 3 x T (computeB3D.m:24)               */
+  const double* volume;          /* T (Mesh3D.elV)                            */
+  const int32_t* element_color;  /* T, 1-based (naiveGraphColoring.m)         */
+  int32_t num_colors;            /* max(element_color)                        */
+  const int32_t* pinned_dofs;    /* 1-based DOF ids, sorted (pin.m:8)         */
+  int32_t num_pinned_dofs;
+  int32_t energy_type;           /* MLX_ENERGY_*                              */
+  const double* alpha;           /* form (a): 6 x 6 x T, or NULL              */
+  const double* beta;            /* form (a): 6 x 6 x T, or NULL              */
+  const double* mu;              /* form (b): T, or NULL                      */
+  const double* lambda;          /* form (b): T, or NULL                      */
+  const double* alpha1;          /* form (b): T, or NULL (= 0)                */
+  int32_t precision;             /* MLX_FP32 / MLX_FP64                       */
+  int32_t device;                /* CUDA ordinal                              */
+} mlx_mesh_desc;
+
+/* The layer description of one call (xpbdLayer3D.m:44-49,54,59-60,84),
+ * produced by buildLayers + findBoundaryVertices (xpbdLayer3D.m:646-652).
+ * Per-layer arrays have `num_columns` columns (numel(sortedLayers)); user
+ * layer l (0-based) reads column layers_map[l]-1. */
+typedef struct mlx_layer_desc {
+  int32_t num_layers;                  /* numel(layers)                       */
+  int32_t num_columns;                 /* numel(sortedLayers)                 */
+  const int32_t* layers_map;           /* num_layers, 1-based                 */
+  const int32_t* iterations;           /* num_layers                          */
+  const uint8_t* is_elastic_element;   /* T x num_columns                     */
+  const uint8_t* is_rigid_element;     /* T x num_columns                     */
+  const int32_t* rigid_body_sets;      /* T x num_columns, 0 = elastic        */
+  const int32_t* vertex_rigid_body;    /* N x num_columns, 0 = elastic        */
+  const uint8_t* is_boundary_vertex;   /* N x num_columns                     */
+  const uint8_t* is_rigid_vertex;      /* N x num_columns                     */
+  const int32_t* num_rigids;           /* num_columns                         */
+} mlx_layer_desc;
+
+/* Scalar settings of layerSolve (xpbdLayer3D.m:53-67,85-86,91-92). */
+typedef struct mlx_solve_params {
+  double h;
+  double boundary_compliance;
+  double contact_resistance;
+  double run_until;                    /* runUntilResSmallerThan, <0 = off    */
+  double give_up_threshold;
+  double gravity_compliance;           /* accepted; gravity constraint is
+                                          disabled in the reference (:325-327)*/
+  double gravity;
+  double stop_at_improvement_percent;
+  int32_t compute_residuals;
+  int32_t hanging_stop;                /* <0 = off                            */
+  int32_t give_up_enabled;
+  int32_t last_layer_give_up_enabled;
+  int32_t use_gravity_constraints;
+  int32_t use_rigid_contacts;
+} mlx_solve_params;
+
+/* Step-start contacts (xpbdLayer3D.m:675-681; contactInfo3D.m:32-55). */
+typedef struct mlx_contacts {
+  int32_t num_contacts;                /* K                                   */
+  const double* normals;               /* K x 3, column-major                 */
+  const double* point_colliders;       /* K x 3, column-major                 */
+  const int32_t* vertex_ids;           /* K, 1-based                          */
+  const double* compliance;            /* K (xpbdContactCompliance)           */
+} mlx_contacts;
+
+/* Per-step vectors of layerSolve. */
+typedef struct mlx_solve_inputs {
+  const double* xi;                    /* 3N                                  */
+  const double* lambdai;               /* T x 6 column-major                  */
+  const double* oldp;                  /* 3N                                  */
+  const double* old_oldp;              /* 3N (accepted; unused by the path)   */
+  const double* f;                     /* 3N (accepted; unused by the path)   */
+  const double* residualv;             /* 3N                                  */
+  const double* pinnedx;               /* num_pinned_dofs                     */
+  const double* residual_in;           /* residualArray on entry              */
+  int32_t residual_in_len;
+  double sum_non_monitored_time;
+} mlx_solve_inputs;
+
+typedef struct mlx_solve_outputs {
+  double* xi;                          /* 3N                                  */
+  double* lambdai;                     /* T x 6, optional (NULL = skip)       */
+  double* residual;                    /* residualArray on exit (capacity)    */
+  int32_t residual_capacity;
+  int32_t residual_len;                /* written                             */
+  double run_until;                    /* written                             */
+  double sum_non_monitored_time;       /* written                             */
+  int32_t total_iterations;            /* written: projectGS iterations run   */
+} mlx_solve_outputs;
+
+typedef struct mlx_solver mlx_solver;  /* device-resident mesh + work buffers */
+
+/* ---- library ------------------------------------------------------------ */
+const char* mlx_last_error(void);
+int mlx_abi_version(void);
+/* Number of visible sm_100 devices (0 when none). */
+int mlx_device_count(void);
+
+/* ---- solver (replaces the device residency of layerSolve's runOnGPU path,
+ *      xpbdLayer3D.m:96-103 / 227-231) ------------------------------------ */
+int mlx_create(const mlx_mesh_desc* mesh, mlx_solver** out);
+int mlx_destroy(mlx_solver* solver);
+
+/* xpbdLayer3D.layerSolve (xpbdLayer3D.m:44-232) with host buffers: uploads
+ * the per-step vectors, runs every layer on the device, downloads xi.  The
+ * outputs mirror [xi, sumNonMonitoredTime, residualArray, runUntil]. */
+int mlx_layer_solve(mlx_solver* solver,
+                    const mlx_layer_desc* layers,
+                    const mlx_solve_params* params,
+                    const mlx_contacts* contacts,
+                    const mlx_solve_inputs* in,
+                    mlx_solve_outputs* out);
+
+/* ---- device-resident stepping ------------------------------------------
+ * xpbdLayer3D.integrate (xpbdLayer3D.m:621-745) with the state kept on the
+ * device between steps: one solver holds one resident simulation.  The layer
+ * description is fixed for all steps (fixed rigid clusters, or layers built
+ * once), contacts are not detected, iterations are fixed
+ * (compute_residuals = 0).  Frame 1 semantics: the pinned values are the
+ * initial positions of the pinned DOFs (xpbdLayer3D.m:629-632). */
+int mlx_sim_init(mlx_solver* solver, const mlx_layer_desc* layers,
+                 const mlx_solve_params* params, const double* p0, const double* v0,
+                 double air_drag);
+/* Adds dv to the velocity DOFs `dofs` (1-based), as
+ * VelocityImpulseAnimationScripter.scriptMesh does before a step
+ * (3d/animations/VelocityImpulseAnimationScripter.m:16-30). */
+int mlx_sim_add_velocity(mlx_solver* solver, const int32_t* dofs, const double* dv, int32_t n);
+/* Runs `nsteps` steps; use_graph replays one captured CUDA graph per step.
+ * device_ms (optional) receives the CUDA-event time of the steps. */
+int mlx_sim_step(mlx_solver* solver, int32_t nsteps, int32_t use_graph, double* device_ms);
+/* Copies positions and velocities (3N each, either may be NULL) to the host. */
+int mlx_sim_get_state(mlx_solver* solver, double* p, double* v);
+/* Colour-sweep timing of the resident stepper: with `on`, every iteration's
+ * run of colour-projection kernels is bracketed by a pair of CUDA events on
+ * the solver's stream (recorded inside the captured step).  sweep_stats
+ * returns the summed device time, the algorithmic bytes of the projected tets
+ * and the number of colour kernels since the last reset. */
+int mlx_sim_sweep_timing(mlx_solver* solver, int32_t on);
+int mlx_sim_sweep_stats(mlx_solver* solver, double* ms, double* bytes, long long* launches, int32_t reset);
+/* Kernel launches per step of the resident stepper (after a step ran), and
+ * kernel launches of the last mlx_layer_solve call. */
+long long mlx_sim_launches_per_step(const mlx_solver* solver);
+long long mlx_last_call_launches(const mlx_solver* solver);
+
+/* ---- host-side helpers of the step (run on the CPU in the reference too) */
+
+/* naiveGraphColoring (2d/tools/functionalities/naiveGraphColoring.m:1-19):
+ * greedy first-fit colour per tet in index order.  Returns num_colors. */
+int mlx_greedy_coloring(const int32_t* t, int32_t num_tets, int32_t num_vertices,
+                        int32_t* element_color, int32_t* num_colors);
+
+/* mexEdiffNorm3D applied to F = B*p and B*oldp (xpbdLayer3D.m:606-608,
+ * 3d/mex/mexEdiffNorm3D.cpp:25-61): per-tet strain-rate norm. */
+int mlx_strain_rate_norms(const int32_t* t, int32_t num_tets, const double* DmInv,
+                          const double* p, const double* oldp, double h,
+                          double* norms);
+
+/* buildLayers' ordering + mexUnionFindByVertice (xpbdLayer3D.m:601-619,
+ * 2d/mex/mexUnionFindByVertice.cpp:117-178).  `order` is the 1-based element
+ * order (strain-rate ascending), `sorted_layers` the ascending unique
+ * percentages.  Writes T x num_sorted rigid IDs and num_sorted counts. */
+int mlx_union_find_layers(const int32_t* order, int32_t num_tets,
+                          const double* sorted_layers, int32_t num_sorted,
+                          const uint8_t* forced_elastic, const int32_t* t,
+                          int32_t num_vertices, int32_t* rigid_body_sets,
+                          int32_t* num_rigids);
+
+/* xpbdLayer2D.findBoundaryVertices (2d/integrator/xpbdLayer2D.m:551-569). */
+int mlx_find_boundary_vertices(const int32_t* t, int32_t num_tets,
+                               int32_t num_vertices,
+                               const int32_t* rigid_body_sets, int32_t num_columns,
+                               uint8_t* is_boundary_vertex,
+                               uint8_t* is_elastic_element,
+                               uint8_t* is_rigid_vertex,
+                               int32_t* vertex_rigid_body);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MLXPBD_H */

@@ -1,0 +1,386 @@
+// body_kernels.cuh -- rigid-layer kernels (FP64 body state on every path).
+//
+// One CTA owns one rigid body: its vertex, boundary-vertex and rigid-contact
+// lists are contiguous CSR ranges, the per-body sums of the reference's
+// accumarray calls become fixed-order block reductions (deterministic), and
+// the body update (expRodrigues, R <- dR R, I <- R I0 R') runs on thread 0
+// between two barriers.  Elastic contacts, which touch no body, ride in the
+// extra CTAs of the same launch.
+#pragma once
+
+#include "common.cuh"
+#include "tet_kernels.cuh"
+
+namespace mlx {
+
+// Device description of one layer (built on the host from the layer masks).
+struct LayerDev {
+  int nb;                   // bodies in this layer
+  const int* body_vert_off; // [nb+1] CSR over body_verts
+  const int* body_verts;    // rigid vertices grouped by body, ascending
+  const int* bnd_off;       // [nb+1] CSR over bnd_verts
+  const int* bnd_verts;     // boundary vertices grouped by body, ascending
+  const int* rc_off;        // [nb+1] CSR over rc_ids
+  const int* rc_ids;        // rigid contact ids grouped by body, ascending
+  int any_boundary;         // the layer has at least one boundary vertex
+  int any_rigid_contact;    // the layer has at least one rigid contact
+  const int* vert_body;     // [N] 1-based body of each vertex, 0 = elastic
+  const unsigned char* vert_rigid;  // [N] isRigidVertex
+  int n_ec_groups;          // elastic contacts grouped by vertex
+  const int* ec_off;        // [n_ec_groups+1]
+  const int* ec_ids;        // contact ids, ascending inside a group
+};
+
+__device__ __forceinline__ D3 solve3_piv(const double* Mcm, D3 b) {
+  double A[3][3], bb[3] = {b.x, b.y, b.z}, x[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) A[r][c] = Mcm[r + 3 * c];
+  solve3x3<double>(A, bb, x);
+  return d3(x[0], x[1], x[2]);
+}
+
+__device__ __forceinline__ void mm3(const double* A, const double* B, double* C) {  // C = A*B
+  double t[9];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int r = 0; r < 3; ++r) t[r + 3 * c] = A[r] * B[3 * c] + A[r + 3] * B[1 + 3 * c] + A[r + 6] * B[2 + 3 * c];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) C[i] = t[i];
+}
+__device__ __forceinline__ void mm3_bt(const double* A, const double* B, double* C) {  // C = A*B'
+  double t[9];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int r = 0; r < 3; ++r) t[r + 3 * c] = A[r] * B[c] + A[r + 3] * B[c + 3] + A[r + 6] * B[c + 6];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) C[i] = t[i];
+}
+
+// expRodrigues (3d/tools/math/expRodrigues.m:1-15)
+__device__ __forceinline__ void exp_rodrigues(D3 w, double h, double* R) {
+  double mag = sqrt(w.x * w.x + w.y * w.y + w.z * w.z);
+  double u[3] = {w.x / mag, w.y / mag, w.z / mag};
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+    if (isnan(u[i])) u[i] = 0;
+  double th = h * mag;
+  double K[9] = {0, u[2], -u[1], -u[2], 0, u[0], u[1], -u[0], 0}, K2[9];
+  mm3(K, K, K2);
+  double s = sin(th), c1 = 1 - cos(th);
+#pragma unroll
+  for (int i = 0; i < 9; ++i) R[i] = (i % 4 == 0 ? 1.0 : 0.0) + s * K[i] + c1 * K2[i];
+}
+
+__device__ __forceinline__ D3 body_point(const Body& b, const double4& r) {
+  return mv3(b.R, d3(r.x, r.y, r.z)) + d3(b.com[0], b.com[1], b.com[2]);
+}
+
+template <typename R>
+__device__ __forceinline__ void store_xyz(R4<R>* pos, int v, D3 x) {
+  R4<R> p = pos[v];
+  pos[v] = make_r4<R>((R)x.x, (R)x.y, (R)x.z, p.w);
+}
+
+// AdaptiveMesh3D.makeRigidsFromConnectivity (AdaptiveMesh3D.m:32-43) ->
+// RigidBody3D.matComputeRigidBodyProperties3D (RigidBody3D.m:198-247):
+// mass, COM, COM velocity, inertia, angular momentum and omega = I \ L, with
+// the residual velocity as vertex velocity; writes ri = p - COM.
+template <typename R>
+__global__ void __launch_bounds__(256) k_make_rigids(LayerDev L, Body* __restrict__ bodies,
+                                                     const R4<R>* __restrict__ pos,
+                                                     const R4<R>* __restrict__ resv,
+                                                     const double* __restrict__ vmass,
+                                                     double4* __restrict__ ri) {
+  int b = blockIdx.x;
+  int beg = L.body_vert_off[b], end = L.body_vert_off[b + 1];
+  double s[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+    int v = L.body_verts[i];
+    double m = vmass[v];
+    R4<R> p = pos[v], u = resv[v];
+    s[0] += m;
+    s[1] += (double)p.x * m; s[2] += (double)p.y * m; s[3] += (double)p.z * m;
+    s[4] += (double)u.x * m; s[5] += (double)u.y * m; s[6] += (double)u.z * m;
+  }
+  block_sum<7>(s);
+  double M = s[0];
+  D3 com = d3(s[1] / M, s[2] / M, s[3] / M), cdot = d3(s[4] / M, s[5] / M, s[6] / M);
+  double t[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // Ixx Iyy Izz Ixy Ixz Iyz Lx Ly Lz
+  for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+    int v = L.body_verts[i];
+    double m = vmass[v];
+    R4<R> p = pos[v], u = resv[v];
+    D3 r = d3((double)p.x, (double)p.y, (double)p.z) - com;
+    D3 vd = d3((double)u.x, (double)u.y, (double)u.z) - cdot;
+    ri[v] = make_double4(r.x, r.y, r.z, 0.0);
+    double nm = -m;  // -m .* ([r]x [r]x)  (RigidBody3D.m:251)
+    t[0] += nm * (-(r.z * r.z) - r.y * r.y);
+    t[1] += nm * (-(r.z * r.z) - r.x * r.x);
+    t[2] += nm * (-(r.y * r.y) - r.x * r.x);
+    t[3] += nm * (r.y * r.x);
+    t[4] += nm * (r.z * r.x);
+    t[5] += nm * (r.z * r.y);
+    D3 c = cross(r, vd);
+    t[6] += m * c.x; t[7] += m * c.y; t[8] += m * c.z;
+  }
+  block_sum<9>(t);
+  if (threadIdx.x == 0) {
+    Body& B = bodies[b];
+    double I0[9] = {t[0], t[3], t[4], t[3], t[1], t[5], t[4], t[5], t[2]};
+    D3 w = solve3_piv(I0, d3(t[6], t[7], t[8]));
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      B.I0[i] = I0[i];
+      B.I[i] = I0[i];
+      B.R[i] = (i % 4 == 0) ? 1.0 : 0.0;
+      B.Rstep[i] = B.R[i];
+    }
+    B.com[0] = com.x; B.com[1] = com.y; B.com[2] = com.z;
+    B.comdot[0] = cdot.x; B.comdot[1] = cdot.y; B.comdot[2] = cdot.z;
+    B.omega[0] = w.x; B.omega[1] = w.y; B.omega[2] = w.z;
+    B.mass = M;
+  }
+}
+
+// Release all elastic residual (xpbdLayer3D.m:138-139).
+template <typename R>
+__global__ void k_release_elastic(R4<R>* __restrict__ pos, R4<R>* __restrict__ resv,
+                                  const unsigned char* __restrict__ vert_rigid, int N, R h) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= N || vert_rigid[v]) return;
+  R4<R> p = pos[v], u = resv[v];
+  pos[v] = make_r4<R>(p.x + h * u.x, p.y + h * u.y, p.z + h * u.z, p.w);
+  resv[v] = make_r4<R>(0, 0, 0, 0);
+}
+
+// RigidBody3D.rigidSymplecticImperativeStep (RigidBody3D.m:174-179), the
+// re-placement of rigid vertices (xpbdLayer3D.m:147) and the residual rebase
+// resv = R_step resv - (x - xprev)/h (xpbdLayer3D.m:149-158).
+template <typename R>
+__global__ void __launch_bounds__(256) k_rigid_step(LayerDev L, Body* __restrict__ bodies,
+                                                    R4<R>* __restrict__ pos,
+                                                    const R4<R>* __restrict__ xprev,
+                                                    R4<R>* __restrict__ resv,
+                                                    const double4* __restrict__ ri, double h) {
+  __shared__ Body sb;
+  int b = blockIdx.x;
+  if (threadIdx.x == 0) {
+    Body B = bodies[b];
+    for (int d = 0; d < 3; ++d) B.com[d] += h * B.comdot[d];
+    double dR[9], tmp[9];
+    exp_rodrigues(d3(B.omega[0], B.omega[1], B.omega[2]), h, dR);
+    mm3(dR, B.R, B.R);
+    mm3(B.R, B.I0, tmp);
+    mm3_bt(tmp, B.R, B.I);
+    for (int i = 0; i < 9; ++i) B.Rstep[i] = B.R[i];
+    bodies[b] = B;
+    sb = B;
+  }
+  __syncthreads();
+  int beg = L.body_vert_off[b], end = L.body_vert_off[b + 1];
+  for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+    int v = L.body_verts[i];
+    D3 x = body_point(sb, ri[v]);
+    R4<R> p = pos[v];
+    R4<R> q = make_r4<R>((R)x.x, (R)x.y, (R)x.z, p.w);
+    pos[v] = q;
+    R4<R> u = resv[v], xp = xprev[v];
+    D3 rot = mv3(sb.Rstep, d3((double)u.x, (double)u.y, (double)u.z));
+    double rx = ((double)q.x - (double)xp.x) / h;
+    double ry = ((double)q.y - (double)xp.y) / h;
+    double rz = ((double)q.z - (double)xp.z) / h;
+    resv[v] = make_r4<R>((R)(rot.x - rx), (R)(rot.y - ry), (R)(rot.z - rz), 0);
+  }
+}
+
+// rigidGeneralizedInverseMass (3d/constraints/rigidGeneralizedInverseMass.m)
+__device__ __forceinline__ double gen_inv_mass(double invM, D3 r, const double* I, D3 n) {
+  D3 axis = cross(r, n);
+  D3 ic = solve3_piv(I, axis);
+  return invM + dot(axis, ic);
+}
+
+// Per-body update after an accumulation (xpbdLayer3D.m:401-414, 466-479).
+__device__ __forceinline__ void apply_increments(Body& B, const double* s, double h) {
+  for (int d = 0; d < 3; ++d) B.com[d] += s[d];
+  D3 w = solve3_piv(B.I, d3(s[3], s[4], s[5]));
+  double dR[9], tmp[9];
+  exp_rodrigues(w, h, dR);
+  mm3(dR, B.R, B.R);
+  mm3_bt(B.I0, B.R, tmp);
+  mm3(B.R, tmp, B.I);
+}
+
+// One iteration's rigid-elastic glue (rigidElasticBoundaryAccumulationConstraints,
+// xpbdLayer3D.m:381-420 + rigidBoundaryConstraint.m:4-35), rigid contacts
+// (contactConstraints rigid branch, xpbdLayer3D.m:440-484 +
+// penaltyConstraint.projectRigid :30-63) and elastic contacts
+// (projectElastic :4-28), Jacobi style as in the reference.
+template <typename R>
+__global__ void __launch_bounds__(256) k_iterate_bodies(LayerDev L, Body* __restrict__ bodies,
+                                                        R4<R>* __restrict__ pos,
+                                                        const double4* __restrict__ ri,
+                                                        const double* __restrict__ vmass,
+                                                        double* __restrict__ lamB, ContactData cd,
+                                                        double h, double boundary_compliance,
+                                                        double contact_resistance, int use_rigid_contacts) {
+  __shared__ Body sb;
+  int b = blockIdx.x;
+  if (b >= L.nb) {
+    // elastic contacts: one thread per vertex group, all contacts of the group
+    // read the same step-start position and the last one's result is kept
+    int g = (b - L.nb) * blockDim.x + threadIdx.x;
+    if (g >= L.n_ec_groups) return;
+    double h2 = h * h;
+    int k0 = L.ec_off[g], k1 = L.ec_off[g + 1];
+    int v = cd.vid[L.ec_ids[k0]];
+    R4<R> p = pos[v];
+    D3 x = d3((double)p.x, (double)p.y, (double)p.z);
+    double minv = (double)p.w;
+    D3 xn = x;
+    for (int q = k0; q < k1; ++q) {
+      int k = L.ec_ids[q];
+      D3 n = d3(cd.normal[k], cd.normal[cd.K + k], cd.normal[2 * cd.K + k]);
+      D3 c = d3(cd.point[k], cd.point[cd.K + k], cd.point[2 * cd.K + k]);
+      double phi = dot(n, x - c);
+      if (phi > 0) phi = 0;
+      double C = contact_resistance * phi;
+      double aT = cd.compliance[k] / h2;
+      double dl = (-C - aT * cd.lambda[k]) / (2 * minv + aT);
+      cd.lambda[k] += dl;
+      xn = d3(x.x + minv * (dl * n.x), x.y + minv * (dl * n.y), x.z + minv * (dl * n.z));
+    }
+    pos[v] = make_r4<R>((R)xn.x, (R)xn.y, (R)xn.z, p.w);
+    return;
+  }
+  if (threadIdx.x == 0) sb = bodies[b];
+  __syncthreads();
+  bool dirty = false;
+  if (L.any_boundary) {
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    int beg = L.bnd_off[b], end = L.bnd_off[b + 1];
+    double invM = 1.0 / sb.mass;
+    D3 com = d3(sb.com[0], sb.com[1], sb.com[2]);
+    for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+      int v = L.bnd_verts[i];
+      R4<R> p = pos[v];
+      D3 pE = d3((double)p.x, (double)p.y, (double)p.z);
+      double minvE = 1.0 / vmass[v];
+      D3 pR = body_point(sb, ri[v]);
+      D3 r = pR - com;
+      D3 dir = pR - pE;
+      double C = sqrt(dot(dir, dir));
+      D3 n = d3(dir.x / C, dir.y / C, dir.z / C);
+      if (isnan(n.x)) n.x = 0;
+      if (isnan(n.y)) n.y = 0;
+      if (isnan(n.z)) n.z = 0;
+      double w = gen_inv_mass(invM, r, sb.I, n);
+      double dl = (-C - boundary_compliance * lamB[i]) / ((minvE + w) + boundary_compliance);
+      lamB[i] += dl;
+      D3 pp = dl * n;
+      s[0] += pp.x * invM; s[1] += pp.y * invM; s[2] += pp.z * invM;
+      D3 dw = cross(r, d3(pp.x / h, pp.y / h, pp.z / h));
+      s[3] += dw.x; s[4] += dw.y; s[5] += dw.z;
+    }
+    block_sum<6>(s);
+    if (threadIdx.x == 0) apply_increments(sb, s, h);
+    __syncthreads();
+    for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+      int v = L.bnd_verts[i];
+      store_xyz<R>(pos, v, body_point(sb, ri[v]));
+    }
+    dirty = true;
+  }
+  if (use_rigid_contacts && L.any_rigid_contact) {
+    __syncthreads();
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    int beg = L.rc_off[b], end = L.rc_off[b + 1];
+    double invM = 1.0 / sb.mass, h2 = h * h;
+    D3 com = d3(sb.com[0], sb.com[1], sb.com[2]);
+    for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+      int k = L.rc_ids[i];
+      int v = cd.vid[k];
+      R4<R> p = pos[v];
+      D3 x = d3((double)p.x, (double)p.y, (double)p.z);
+      D3 pR = body_point(sb, ri[v]);
+      D3 r = pR - com;
+      D3 n = d3(cd.normal[k], cd.normal[cd.K + k], cd.normal[2 * cd.K + k]);
+      D3 c = d3(cd.point[k], cd.point[cd.K + k], cd.point[2 * cd.K + k]);
+      double phi = dot(n, x - c);
+      if (phi > 0) phi = 0;
+      double C = contact_resistance * phi;
+      double w = gen_inv_mass(invM, r, sb.I, n);
+      double aT = (2 * cd.compliance[k]) / h2;
+      double dl = (-C - aT * cd.lambda[k]) / (2 * w + aT);
+      cd.lambda[k] += dl;
+      D3 pp = dl * n;
+      s[0] += pp.x * invM; s[1] += pp.y * invM; s[2] += pp.z * invM;
+      D3 cr = cross(r, pp);
+      s[3] += (1 / h) * cr.x; s[4] += (1 / h) * cr.y; s[5] += (1 / h) * cr.z;
+    }
+    block_sum<6>(s);
+    if (threadIdx.x == 0) apply_increments(sb, s, h);
+    __syncthreads();
+    for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+      int v = cd.vid[L.rc_ids[i]];
+      store_xyz<R>(pos, v, body_point(sb, ri[v]));
+    }
+    dirty = true;
+  }
+  if (dirty && threadIdx.x == 0) bodies[b] = sb;
+}
+
+// xi(pinnedDOFs) = pinnedx (xpbdLayer3D.m:333)
+template <typename R>
+__global__ void k_pin(R4<R>* __restrict__ pos, const int* __restrict__ dofs,
+                      const R* __restrict__ vals, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int d = dofs[i];
+  reinterpret_cast<R*>(&pos[d / 3])[d % 3] = vals[i];
+}
+
+// End of projectGS / layer: rotateAllVerts (xpbdLayer3D.m:344, 508-513) and,
+// for a rigid layer, rotateResidual by dR = R_proj R_step' (:217-221, 234-241).
+template <typename R>
+__global__ void __launch_bounds__(256) k_finish_layer(LayerDev L, const Body* __restrict__ bodies,
+                                                      R4<R>* __restrict__ pos, R4<R>* __restrict__ resv,
+                                                      const double4* __restrict__ ri, int rigid_layer) {
+  __shared__ Body sb;
+  __shared__ double dR[9];
+  int b = blockIdx.x;
+  if (threadIdx.x == 0) {
+    sb = bodies[b];
+    mm3_bt(sb.R, sb.Rstep, dR);
+  }
+  __syncthreads();
+  int beg = L.body_vert_off[b], end = L.body_vert_off[b + 1];
+  for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+    int v = L.body_verts[i];
+    store_xyz<R>(pos, v, body_point(sb, ri[v]));
+    if (rigid_layer) {
+      R4<R> u = resv[v];
+      D3 r = mv3(dR, d3((double)u.x, (double)u.y, (double)u.z));
+      resv[v] = make_r4<R>((R)r.x, (R)r.y, (R)r.z, 0);
+    }
+  }
+}
+
+// ||residualv|| partial sums (xpbdLayer3D.m:161), FP64.
+template <typename R>
+__global__ void __launch_bounds__(256) k_norm3_partials(const R4<R>* __restrict__ v, int N,
+                                                        double* __restrict__ partials) {
+  double acc[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    R4<R> u = v[i];
+    acc[0] += (double)u.x * u.x + (double)u.y * u.y + (double)u.z * u.z;
+  }
+  block_sum<1>(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc[0];
+}
+
+}  // namespace mlx

@@ -1,0 +1,58 @@
+// common.cuh -- shared device types and helpers of the B200 XPBD kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mlx {
+
+// Vertex record: position and inverse mass in one 16 B (FP32) or 32 B (FP64)
+// load, so a tet gathers its four vertices with four vector loads.
+template <typename R> struct Vec4;
+template <> struct Vec4<float> { using type = float4; };
+template <> struct Vec4<double> { using type = double4; };
+template <typename R> using R4 = typename Vec4<R>::type;
+
+template <typename R> __host__ __device__ inline R4<R> make_r4(R x, R y, R z, R w);
+template <> __host__ __device__ inline float4 make_r4<float>(float x, float y, float z, float w) {
+  return make_float4(x, y, z, w);
+}
+template <> __host__ __device__ inline double4 make_r4<double>(double x, double y, double z, double w) {
+  return make_double4(x, y, z, w);
+}
+
+// 32-byte aligned double4 loads are split by the compiler into two 16-byte
+// transactions on sm_100; float4 is one 16-byte transaction.
+template <typename R> __device__ __forceinline__ R4<R> ld_r4(const R4<R>* p) { return *p; }
+
+struct D3 { double x, y, z; };
+__host__ __device__ inline D3 d3(double x, double y, double z) { return {x, y, z}; }
+__host__ __device__ inline D3 operator+(D3 a, D3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__host__ __device__ inline D3 operator-(D3 a, D3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__host__ __device__ inline D3 operator*(double s, D3 a) { return {s * a.x, s * a.y, s * a.z}; }
+__host__ __device__ inline double dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__host__ __device__ inline D3 cross(D3 a, D3 b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+// M is a 3x3 column-major matrix
+__host__ __device__ inline D3 mv3(const double* M, D3 v) {
+  return {M[0] * v.x + M[3] * v.y + M[6] * v.z, M[1] * v.x + M[4] * v.y + M[7] * v.z,
+          M[2] * v.x + M[5] * v.y + M[8] * v.z};
+}
+
+// Rigid body state, FP64 (the momentum and rotation accumulation stays in
+// double on every precision path).  One record per body, 256 B aligned so a
+// body's CTA reads it with few sectors.
+struct __align__(16) Body {
+  double R[9];      // current rotation
+  double Rstep[9];  // rotation after the symplectic step (steppedVelocityR)
+  double I0[9];     // body-frame inertia at construction
+  double I[9];      // world inertia R I0 R'
+  double com[3];
+  double comdot[3];
+  double omega[3];
+  double mass;
+  double pad[2];
+};
+
+}  // namespace mlx

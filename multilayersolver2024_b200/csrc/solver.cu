@@ -1,0 +1,1292 @@
+// solver.cu -- device-resident mesh, per-call layer description and the
+// layerSolve orchestration behind the C ABI of include/mlxpbd.h.
+//
+// Data layout in HBM (per solver):
+//   tets, colour-sorted (colour c owns [color_off[c], color_off[c+1])):
+//     vid int4[T], dminv R[9][T], vol R[T], mat R[stride][T], lambda R[6][T]
+//   vertices: pos R4[N] = (x, y, z, 1/m), oldp/xprev/resv R4[N],
+//     vmass double[N], ri double4[N] (FP64 body-frame offsets)
+//   bodies: Body[nb] (FP64)
+// Host-side per-layer preprocessing builds CSR lists (elastic tets per colour,
+// vertices / boundary vertices / rigid contacts per body, elastic contacts per
+// vertex) and caches the contact-independent part across calls.
+#include "../../include/mlxpbd.h"
+#include "common.cuh"
+#include "tet_kernels.cuh"
+#include "body_kernels.cuh"
+#include "solver.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+using namespace mlx;
+
+namespace mlx {
+thread_local std::string g_err;
+int set_error(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+}  // namespace mlx
+
+#define CU(x)                                                                              \
+  do {                                                                                     \
+    cudaError_t e_ = (x);                                                                  \
+    if (e_ != cudaSuccess)                                                                 \
+      return set_error(MLX_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_));    \
+  } while (0)
+#define CHECK(x)           \
+  do {                     \
+    int rc_ = (x);         \
+    if (rc_ != MLX_OK) return rc_; \
+  } while (0)
+
+namespace {
+
+// ---- conversion kernels (MATLAB layout <-> device layout) -----------------
+template <typename R>
+__global__ void k_load_pos(const double* __restrict__ xi, const double* __restrict__ mass,
+                           R4<R>* __restrict__ pos, int N) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= N) return;
+  pos[v] = make_r4<R>((R)xi[3 * v], (R)xi[3 * v + 1], (R)xi[3 * v + 2], (R)(1.0 / mass[3 * v]));
+}
+template <typename R>
+__global__ void k_load_vec(const double* __restrict__ a, R4<R>* __restrict__ out, int N) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= N) return;
+  out[v] = make_r4<R>((R)a[3 * v], (R)a[3 * v + 1], (R)a[3 * v + 2], 0);
+}
+template <typename R>
+__global__ void k_store_pos(const R4<R>* __restrict__ pos, double* __restrict__ xi, int N) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= N) return;
+  R4<R> p = pos[v];
+  xi[3 * v] = p.x; xi[3 * v + 1] = p.y; xi[3 * v + 2] = p.z;
+}
+template <typename R>
+__global__ void k_load_lambda(const double* __restrict__ lam, const int* __restrict__ s2e,
+                              R* __restrict__ out, int T) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= T) return;
+  int e = s2e[s];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) out[(size_t)q * T + s] = (R)lam[e + (size_t)T * q];
+}
+template <typename R>
+__global__ void k_store_lambda(const R* __restrict__ lam, const int* __restrict__ s2e,
+                               double* __restrict__ out, int T) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= T) return;
+  int e = s2e[s];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) out[e + (size_t)T * q] = lam[(size_t)q * T + s];
+}
+template <typename R>
+__global__ void k_cast(const double* __restrict__ a, R* __restrict__ out, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = (R)a[i];
+}
+
+inline int blocks_for(long long n, int b) { return (int)((n + b - 1) / b); }
+
+// ---- buffers ---------------------------------------------------------------
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { if (p) cudaFree(p); }
+  int ensure(size_t n) {
+    if (n <= bytes && p) return MLX_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    size_t want = std::max<size_t>(n, 256);
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) return set_error(MLX_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    bytes = want;
+    return MLX_OK;
+  }
+  template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+struct PinnedBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  PinnedBuf() = default;
+  PinnedBuf(const PinnedBuf&) = delete;
+  PinnedBuf& operator=(const PinnedBuf&) = delete;
+  ~PinnedBuf() { if (p) cudaFreeHost(p); }
+  int ensure(size_t n) {
+    if (n <= bytes && p) return MLX_OK;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    size_t want = std::max<size_t>(n, 256);
+    cudaError_t e = cudaMallocHost(&p, want);
+    if (e != cudaSuccess) return set_error(MLX_ERR_ALLOC, std::string("cudaMallocHost: ") + cudaGetErrorString(e));
+    bytes = want;
+    return MLX_OK;
+  }
+  template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int d) {
+    cudaGetDevice(&prev);
+    if (prev != d) cudaSetDevice(d);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// Contact-independent part of one layer column, cached across calls.
+struct LayerStatic {
+  bool valid = false;
+  // copies of the inputs the cache was built from
+  std::vector<uint8_t> isE, isBV, isRV;
+  std::vector<int32_t> rid;
+  int nb = 0;
+  // built
+  int n_rigid_elements = 0;
+  bool identity_list = false;
+  std::vector<int> color_count;  // per colour: number of elastic tets
+  std::vector<int> color_start;  // per colour: start in the elastic list
+  std::vector<int> packed;       // body_vert_off | body_verts | bnd_off | bnd_verts | list | vert_body
+  size_t o_bvo = 0, o_bv = 0, o_bo = 0, o_bnd = 0, o_list = 0, o_vb = 0;
+  int n_bnd = 0;
+  DevBuf dev;       // packed ints
+  DevBuf dev_rigid; // vert_rigid bytes
+};
+
+}  // namespace
+
+namespace mlx {
+
+// Per-call bookkeeping of the layer loop (the scalars layerSolve threads
+// through projectGS, xpbdLayer3D.m:94-232).
+struct RunState {
+  std::vector<double> residualArray;
+  double runUntil = -1;
+  double sumNonMon = 0;
+  int totalIterations = 0;
+  long long launches = 0;  // kernels launched by the loop
+};
+
+template <typename R>
+struct Solver final : SolverBase {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int N = 0, T = 0, C = 0, energy = 0, mat_kind = 0;
+  bool damp = false;
+  std::vector<int> s2e, color_off;
+  std::vector<int32_t> pinned;  // 0-based DOFs
+  std::vector<double> vmass_h, mass3;
+  DevBuf d_vid, d_dminv, d_vol, d_mat, d_lambda, d_pos, d_oldp, d_xprev, d_resv, d_vmass, d_ri,
+      d_bodies, d_lamB, d_pin_dofs, d_pinx, d_partials, d_scalar, d_stage, d_s2e, d_mass3,
+      d_contacts, d_cvid, d_clam, d_cgroups;
+  PinnedBuf h_stage, h_scalar, h_cstage;
+  std::vector<std::unique_ptr<LayerStatic>> cache;
+
+  ~Solver() override {
+    for (cudaEvent_t e : tev) cudaEventDestroy(e);
+    if (sim.graph) cudaGraphExecDestroy(sim.graph);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  int create(const mlx_mesh_desc* md);
+  int layer_solve(const mlx_layer_desc* ld, const mlx_solve_params* P, const mlx_contacts* K,
+                  const mlx_solve_inputs* in, mlx_solve_outputs* out) override;
+
+  TetData<R> tets() const {
+    TetData<R> td;
+    td.vid = d_vid.as<int4>();
+    td.dminv = d_dminv.as<R>();
+    td.vol = d_vol.as<R>();
+    td.mat = d_mat.as<R>();
+    td.lambda = d_lambda.as<R>();
+    td.T = T;
+    return td;
+  }
+  R4<R>* pos() const { return d_pos.as<R4<R>>(); }
+
+  int build_static(const mlx_layer_desc* ld, int col, LayerStatic& ls, bool capturing);
+  int launch_color(int c, const LayerStatic& ls, const int* dlist, R h);
+  int residual(const ContactData& cd, double contact_resistance, double h, double* out);
+  int norm_resv(double* out);
+  int validate_layers(const mlx_layer_desc* ld, const mlx_solve_params* P);
+  int upload_contacts(const mlx_contacts* K, ContactData& cd);
+  int run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, const mlx_contacts* K,
+                 const ContactData& cd, RunState& st, bool capturing);
+
+  // resident stepper (one per solver)
+  struct Sim {
+    bool ready = false;
+    mlx_layer_desc ld{};
+    mlx_solve_params P{};
+    double air_drag = 0;
+    std::vector<int32_t> layers_map, iterations, sets, rid, nr;
+    std::vector<uint8_t> isE, isR, isBV, isRV;
+    cudaGraphExec_t graph = nullptr;
+    long long launches_per_step = 0;
+  } sim;
+  DevBuf d_vel, d_pin_mask;
+  long long last_launches = 0;
+  // colour-sweep timing: an event pair around every iteration's sweep
+  bool sweep_timing = false;
+  std::vector<cudaEvent_t> tev;
+  size_t tev_used = 0;
+  std::vector<double> tev_bytes;    // algorithmic bytes of the sweep of each pair
+  std::vector<long long> tev_launches;
+  double sweep_ms = 0, sweep_bytes = 0;
+  long long sweep_launches = 0;
+  double bytes_per_tet() const;
+  int record_event(cudaEvent_t e, bool capturing);
+  int enable_sweep_timing(int on) override;
+  int sweep_stats(double* ms, double* bytes, long long* launches, int reset) override;
+  int collect_sweep_times();
+  int sim_setup(const mlx_layer_desc* ld, const mlx_solve_params* P, const double* p0, const double* v0);
+  int sim_issue_step(long long* launches);
+  int sim_step(int nsteps, int use_graph, double* device_ms) override;
+  int sim_add_velocity(const int32_t* dofs, const double* dv, int n) override;
+  int sim_get_state(double* p, double* v) override;
+  int sim_init(const mlx_layer_desc* ld, const mlx_solve_params* P, const double* p0, const double* v0,
+               double air_drag) override {
+    sim.air_drag = air_drag;
+    return sim_setup(ld, P, p0, v0);
+  }
+  long long sim_launches_per_step() const override { return sim.launches_per_step; }
+  long long launches_last_call() const override { return last_launches; }
+};
+
+template <typename R>
+int Solver<R>::create(const mlx_mesh_desc* md) {
+  N = md->num_vertices;
+  T = md->num_tets;
+  C = md->num_colors;
+  energy = md->energy_type;
+  device = md->device;
+  if (N <= 0 || T <= 0 || C <= 0) return set_error(MLX_ERR_ARGUMENT, "mesh needs N, T, num_colors > 0");
+  if (!md->t || !md->mass || !md->DmInv || !md->volume || !md->element_color)
+    return set_error(MLX_ERR_ARGUMENT, "mesh arrays t, mass, DmInv, volume, element_color are required");
+  if (md->num_pinned_dofs > 0 && !md->pinned_dofs) return set_error(MLX_ERR_ARGUMENT, "pinned_dofs is NULL");
+  // colour validity: every colour id in range and no two tets of one colour share a vertex
+  std::vector<int> cnt(C + 1, 0);
+  for (int e = 0; e < T; ++e) {
+    int c = md->element_color[e];
+    if (c < 1 || c > C) return set_error(MLX_ERR_ARGUMENT, "element_color out of [1, num_colors]");
+    ++cnt[c];
+    for (int k = 0; k < 4; ++k) {
+      int v = md->t[e + (size_t)T * k];
+      if (v < 1 || v > N) return set_error(MLX_ERR_ARGUMENT, "tet vertex index out of range");
+    }
+  }
+  {
+    std::vector<int> last(N, -1);  // last colour that touched a vertex, per colour pass
+    std::vector<std::vector<int>> byc(C + 1);
+    for (int e = 0; e < T; ++e) byc[md->element_color[e]].push_back(e);
+    for (int c = 1; c <= C; ++c)
+      for (int e : byc[c])
+        for (int k = 0; k < 4; ++k) {
+          int v = md->t[e + (size_t)T * k] - 1;
+          if (last[v] == c) return set_error(MLX_ERR_ARGUMENT, "element_color is not a valid colouring");
+          last[v] = c;
+        }
+  }
+  // colour-sorted order: stable by colour, ascending element id inside a colour
+  color_off.assign(C + 1, 0);
+  for (int c = 1; c <= C; ++c) color_off[c] = color_off[c - 1] + cnt[c];
+  s2e.assign(T, 0);
+  {
+    std::vector<int> fill(color_off.begin(), color_off.end() - 1);
+    for (int e = 0; e < T; ++e) s2e[fill[md->element_color[e] - 1]++] = e;
+  }
+  // material encoding
+  if (energy == MLX_ENERGY_NEOHOOKEAN) {
+    if (!md->mu || !md->lambda) return set_error(MLX_ERR_ARGUMENT, "Neo-Hookean mesh needs mu and lambda");
+    mat_kind = MAT_NH;
+    damp = false;
+  } else if (energy == MLX_ENERGY_STVK_VOIGT) {
+    if (md->alpha && md->beta) {
+      mat_kind = MAT_STVK_BLOCKS;
+      damp = false;
+      for (int e = 0; e < T; ++e) {
+        const double* a = md->alpha + 36 * (size_t)e;
+        const double* b = md->beta + 36 * (size_t)e;
+        for (int r = 0; r < 6; ++r)
+          for (int c = 0; c < 6; ++c) {
+            bool top = r < 3 && c < 3, diag = r >= 3 && r == c;
+            if (!top && !diag && (a[r + 6 * c] != 0.0 || b[r + 6 * c] != 0.0))
+              return set_error(MLX_ERR_UNSUPPORTED,
+                               "alpha/beta must be block diagonal (3x3 (+) diagonal 3x3) as Mesh3D.updateMaterials builds them");
+          }
+        for (int i = 0; i < 36; ++i)
+          if (b[i] != 0.0) damp = true;
+      }
+    } else if (md->mu && md->lambda) {
+      mat_kind = MAT_STVK_LAME;
+      damp = false;
+      if (md->alpha1)
+        for (int e = 0; e < T; ++e)
+          if (md->alpha1[e] != 0.0) damp = true;
+    } else {
+      return set_error(MLX_ERR_ARGUMENT, "StVK mesh needs alpha/beta or mu/lambda");
+    }
+  } else {
+    return set_error(MLX_ERR_ARGUMENT, "unknown energy_type");
+  }
+  for (int i = 0; i < md->num_pinned_dofs; ++i) {
+    int d = md->pinned_dofs[i] - 1;
+    if (d < 0 || d >= 3 * N) return set_error(MLX_ERR_ARGUMENT, "pinned DOF out of range");
+    pinned.push_back(d);
+  }
+  mass3.assign(md->mass, md->mass + 3 * (size_t)N);
+  vmass_h.resize(N);
+  for (int v = 0; v < N; ++v) {
+    double m = md->mass[3 * v];
+    if (!(m > 0)) return set_error(MLX_ERR_ARGUMENT, "vertex masses must be positive");
+    vmass_h[v] = m;
+  }
+
+  // ---- host-side packing of the rest data in sorted order ----
+  const int stride = mat_stride(mat_kind);
+  std::vector<int4> vid(T);
+  std::vector<R> dminv(9 * (size_t)T), vol(T), mat((size_t)stride * T);
+  for (int s = 0; s < T; ++s) {
+    int e = s2e[s];
+    vid[s] = make_int4(md->t[e] - 1, md->t[e + (size_t)T] - 1, md->t[e + 2 * (size_t)T] - 1,
+                       md->t[e + 3 * (size_t)T] - 1);
+    for (int j = 0; j < 9; ++j) dminv[(size_t)j * T + s] = (R)md->DmInv[9 * (size_t)e + j];
+    vol[s] = (R)md->volume[e];
+    if (mat_kind == MAT_STVK_BLOCKS) {
+      const double* a = md->alpha + 36 * (size_t)e;
+      const double* b = md->beta + 36 * (size_t)e;
+      double ab[36];
+      for (int c = 0; c < 6; ++c)
+        for (int r = 0; r < 6; ++r) {
+          double acc = 0;
+          for (int k = 0; k < 6; ++k) acc += a[r + 6 * k] * b[k + 6 * c];
+          ab[r + 6 * c] = acc;
+        }
+      for (int c = 0; c < 3; ++c)
+        for (int r = 0; r < 3; ++r) {
+          mat[(size_t)(r + 3 * c) * T + s] = (R)a[r + 6 * c];
+          mat[(size_t)(12 + r + 3 * c) * T + s] = (R)ab[r + 6 * c];
+        }
+      for (int q = 0; q < 3; ++q) {
+        mat[(size_t)(9 + q) * T + s] = (R)a[(3 + q) + 6 * (3 + q)];
+        mat[(size_t)(21 + q) * T + s] = (R)ab[(3 + q) + 6 * (3 + q)];
+      }
+    } else {
+      mat[s] = (R)md->mu[e];
+      mat[(size_t)T + s] = (R)md->lambda[e];
+      if (mat_kind == MAT_STVK_LAME) mat[2 * (size_t)T + s] = (R)(md->alpha1 ? md->alpha1[e] : 0.0);
+    }
+  }
+
+  DeviceGuard g(device);
+  CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  CHECK(d_vid.ensure(sizeof(int4) * T));
+  CHECK(d_dminv.ensure(sizeof(R) * 9 * (size_t)T));
+  CHECK(d_vol.ensure(sizeof(R) * T));
+  CHECK(d_mat.ensure(sizeof(R) * stride * (size_t)T));
+  CHECK(d_lambda.ensure(sizeof(R) * 6 * (size_t)T));
+  CHECK(d_pos.ensure(sizeof(R4<R>) * N));
+  CHECK(d_oldp.ensure(sizeof(R4<R>) * N));
+  CHECK(d_xprev.ensure(sizeof(R4<R>) * N));
+  CHECK(d_resv.ensure(sizeof(R4<R>) * N));
+  CHECK(d_vmass.ensure(sizeof(double) * N));
+  CHECK(d_mass3.ensure(sizeof(double) * 3 * (size_t)N));
+  CHECK(d_ri.ensure(sizeof(double4) * N));
+  CHECK(d_s2e.ensure(sizeof(int) * T));
+  CHECK(d_partials.ensure(sizeof(double) * 1024));
+  CHECK(d_scalar.ensure(sizeof(double) * 8));
+  CHECK(h_scalar.ensure(sizeof(double) * 8));
+  CHECK(d_pin_dofs.ensure(sizeof(int) * std::max<size_t>(pinned.size(), 1)));
+  CHECK(d_pinx.ensure(sizeof(R) * std::max<size_t>(pinned.size(), 1)));
+  CU(cudaMemcpyAsync(d_vid.p, vid.data(), sizeof(int4) * T, cudaMemcpyHostToDevice, stream));
+  CU(cudaMemcpyAsync(d_dminv.p, dminv.data(), sizeof(R) * 9 * (size_t)T, cudaMemcpyHostToDevice, stream));
+  CU(cudaMemcpyAsync(d_vol.p, vol.data(), sizeof(R) * T, cudaMemcpyHostToDevice, stream));
+  CU(cudaMemcpyAsync(d_mat.p, mat.data(), sizeof(R) * stride * (size_t)T, cudaMemcpyHostToDevice, stream));
+  CU(cudaMemcpyAsync(d_vmass.p, vmass_h.data(), sizeof(double) * N, cudaMemcpyHostToDevice, stream));
+  CU(cudaMemcpyAsync(d_mass3.p, mass3.data(), sizeof(double) * 3 * (size_t)N, cudaMemcpyHostToDevice, stream));
+  CU(cudaMemcpyAsync(d_s2e.p, s2e.data(), sizeof(int) * T, cudaMemcpyHostToDevice, stream));
+  if (!pinned.empty())
+    CU(cudaMemcpyAsync(d_pin_dofs.p, pinned.data(), sizeof(int) * pinned.size(), cudaMemcpyHostToDevice, stream));
+  CU(cudaStreamSynchronize(stream));
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::build_static(const mlx_layer_desc* ld, int col, LayerStatic& ls, bool capturing) {
+  const uint8_t* isE = ld->is_elastic_element + (size_t)T * col;
+  const uint8_t* isR = ld->is_rigid_element + (size_t)T * col;
+  const int32_t* rid = ld->vertex_rigid_body + (size_t)N * col;
+  const uint8_t* isBV = ld->is_boundary_vertex + (size_t)N * col;
+  const uint8_t* isRV = ld->is_rigid_vertex + (size_t)N * col;
+  int nb = ld->num_rigids[col];
+  if (ls.valid && ls.nb == nb && std::memcmp(ls.isE.data(), isE, T) == 0 &&
+      std::memcmp(ls.isBV.data(), isBV, N) == 0 && std::memcmp(ls.isRV.data(), isRV, N) == 0 &&
+      std::memcmp(ls.rid.data(), rid, sizeof(int32_t) * N) == 0) {
+    int nre = 0;
+    for (int e = 0; e < T; ++e) nre += isR[e] != 0;
+    ls.n_rigid_elements = nre;
+    return MLX_OK;
+  }
+  if (nb < 0) return set_error(MLX_ERR_ARGUMENT, "num_rigids < 0");
+  if (capturing) return set_error(MLX_ERR_ARGUMENT, "layer cache miss inside a captured step");
+  ls.valid = false;
+  ls.isE.assign(isE, isE + T);
+  ls.isBV.assign(isBV, isBV + N);
+  ls.isRV.assign(isRV, isRV + N);
+  ls.rid.assign(rid, rid + N);
+  ls.nb = nb;
+  int nre = 0;
+  for (int e = 0; e < T; ++e) nre += isR[e] != 0;
+  ls.n_rigid_elements = nre;
+  // elastic tets per colour in sorted order
+  std::vector<int> list;
+  list.reserve(T);
+  ls.color_count.assign(C, 0);
+  ls.color_start.assign(C, 0);
+  for (int c = 0; c < C; ++c) {
+    ls.color_start[c] = (int)list.size();
+    for (int s = color_off[c]; s < color_off[c + 1]; ++s)
+      if (isE[s2e[s]]) list.push_back(s);
+    ls.color_count[c] = (int)list.size() - ls.color_start[c];
+  }
+  ls.identity_list = (int)list.size() == T;
+  // bodies
+  std::vector<int> bvo(nb + 1, 0), bo(nb + 1, 0);
+  for (int v = 0; v < N; ++v) {
+    int b = rid[v];
+    if (b < 0 || b > nb) return set_error(MLX_ERR_ARGUMENT, "vertex_rigid_body id out of [0, num_rigids]");
+    if (b > 0) ++bvo[b];
+    if (isBV[v]) {
+      if (b == 0) return set_error(MLX_ERR_ARGUMENT, "a boundary vertex has no rigid body");
+      ++bo[b];
+    }
+  }
+  for (int b = 1; b <= nb; ++b) { bvo[b] += bvo[b - 1]; bo[b] += bo[b - 1]; }
+  std::vector<int> bverts(bvo[nb]), bnd(bo[nb]);
+  {
+    std::vector<int> f1(bvo.begin(), bvo.end() - 1), f2(bo.begin(), bo.end() - 1);
+    for (int v = 0; v < N; ++v) {
+      int b = rid[v];
+      if (b > 0) bverts[f1[b - 1]++] = v;
+      if (isBV[v]) bnd[f2[b - 1]++] = v;
+    }
+  }
+  ls.n_bnd = bo[nb];
+  // pack
+  ls.packed.clear();
+  auto put = [&](const std::vector<int>& a) {
+    size_t o = ls.packed.size();
+    ls.packed.insert(ls.packed.end(), a.begin(), a.end());
+    return o;
+  };
+  ls.o_bvo = put(bvo);
+  ls.o_bv = put(bverts);
+  ls.o_bo = put(bo);
+  ls.o_bnd = put(bnd);
+  ls.o_list = put(ls.identity_list ? std::vector<int>() : list);
+  ls.o_vb = ls.packed.size();
+  ls.packed.insert(ls.packed.end(), rid, rid + N);
+  CHECK(ls.dev.ensure(sizeof(int) * ls.packed.size()));
+  CHECK(ls.dev_rigid.ensure(N));
+  CU(cudaMemcpyAsync(ls.dev.p, ls.packed.data(), sizeof(int) * ls.packed.size(), cudaMemcpyHostToDevice, stream));
+  CU(cudaMemcpyAsync(ls.dev_rigid.p, isRV, N, cudaMemcpyHostToDevice, stream));
+  // the host copies above are pageable: make sure they finished before the
+  // cached vectors can change
+  CU(cudaStreamSynchronize(stream));
+  ls.valid = true;
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::launch_color(int c, const LayerStatic& ls, const int* dlist, R h) {
+  int count = ls.color_count[c];
+  if (count == 0) return MLX_OK;
+  const int bs = 64;
+  int grid = blocks_for(count, bs);
+  R inv_h2 = R(1) / (h * h), inv_h = R(1) / h;
+  TetData<R> td = tets();
+  const int* list = ls.identity_list ? nullptr : dlist;
+  int begin = ls.identity_list ? color_off[c] : ls.color_start[c];
+  const R4<R>* oldp = d_oldp.as<R4<R>>();
+  switch (mat_kind) {
+    case MAT_NH:
+      k_project_color<R, MAT_NH, false><<<grid, bs, 0, stream>>>(td, list, begin, count, pos(), oldp, inv_h2, inv_h);
+      break;
+    case MAT_STVK_BLOCKS:
+      if (damp)
+        k_project_color<R, MAT_STVK_BLOCKS, true><<<grid, bs, 0, stream>>>(td, list, begin, count, pos(), oldp, inv_h2, inv_h);
+      else
+        k_project_color<R, MAT_STVK_BLOCKS, false><<<grid, bs, 0, stream>>>(td, list, begin, count, pos(), oldp, inv_h2, inv_h);
+      break;
+    default:
+      if (damp)
+        k_project_color<R, MAT_STVK_LAME, true><<<grid, bs, 0, stream>>>(td, list, begin, count, pos(), oldp, inv_h2, inv_h);
+      else
+        k_project_color<R, MAT_STVK_LAME, false><<<grid, bs, 0, stream>>>(td, list, begin, count, pos(), oldp, inv_h2, inv_h);
+  }
+  CU(cudaGetLastError());
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::residual(const ContactData& cd, double contact_resistance, double h, double* out) {
+  const int bs = 256;
+  int tetBlocks = std::min(blocks_for(T, bs), 592);
+  int cBlocks = cd.K > 0 ? std::min(blocks_for(cd.K, bs), 64) : 0;
+  R inv_h2 = R(1) / ((R)h * (R)h), inv_h = R(1) / (R)h;
+  double inv_h2_d = 1.0 / (h * h);
+  TetData<R> td = tets();
+  double* partials = d_partials.as<double>();
+  switch (mat_kind) {
+    case MAT_NH:
+      k_residual_partials<R, MAT_NH><<<tetBlocks + cBlocks, bs, 0, stream>>>(td, pos(), cd, contact_resistance, inv_h2, inv_h, inv_h2_d, tetBlocks, partials);
+      break;
+    case MAT_STVK_BLOCKS:
+      k_residual_partials<R, MAT_STVK_BLOCKS><<<tetBlocks + cBlocks, bs, 0, stream>>>(td, pos(), cd, contact_resistance, inv_h2, inv_h, inv_h2_d, tetBlocks, partials);
+      break;
+    default:
+      k_residual_partials<R, MAT_STVK_LAME><<<tetBlocks + cBlocks, bs, 0, stream>>>(td, pos(), cd, contact_resistance, inv_h2, inv_h, inv_h2_d, tetBlocks, partials);
+  }
+  CU(cudaGetLastError());
+  k_finish_norm<<<1, 256, 0, stream>>>(partials, tetBlocks + cBlocks, d_scalar.as<double>());
+  CU(cudaGetLastError());
+  CU(cudaMemcpyAsync(h_scalar.p, d_scalar.p, sizeof(double), cudaMemcpyDeviceToHost, stream));
+  CU(cudaStreamSynchronize(stream));
+  *out = h_scalar.as<double>()[0];
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::norm_resv(double* out) {
+  const int bs = 256;
+  int grid = std::min(blocks_for(N, bs), 296);
+  k_norm3_partials<R><<<grid, bs, 0, stream>>>(d_resv.as<R4<R>>(), N, d_partials.as<double>());
+  CU(cudaGetLastError());
+  k_finish_norm<<<1, 256, 0, stream>>>(d_partials.as<double>(), grid, d_scalar.as<double>() + 1);
+  CU(cudaGetLastError());
+  CU(cudaMemcpyAsync(h_scalar.as<double>() + 1, d_scalar.as<double>() + 1, sizeof(double), cudaMemcpyDeviceToHost, stream));
+  CU(cudaStreamSynchronize(stream));
+  *out = h_scalar.as<double>()[1];
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::validate_layers(const mlx_layer_desc* ld, const mlx_solve_params* P) {
+  if (!ld || !P) return set_error(MLX_ERR_ARGUMENT, "null argument");
+  if (ld->num_layers < 0 || ld->num_columns < 1) return set_error(MLX_ERR_ARGUMENT, "bad layer counts");
+  if (ld->num_layers > 0 && (!ld->layers_map || !ld->iterations || !ld->is_elastic_element ||
+                             !ld->is_rigid_element || !ld->vertex_rigid_body || !ld->is_boundary_vertex ||
+                             !ld->is_rigid_vertex || !ld->num_rigids))
+    return set_error(MLX_ERR_ARGUMENT, "layer description has NULL arrays");
+  if (P->run_until >= 0 && !P->compute_residuals)
+    return set_error(MLX_ERR_ARGUMENT, "run_until >= 0 needs compute_residuals (the reference loop would never end)");
+  if (!(P->h > 0)) return set_error(MLX_ERR_ARGUMENT, "h must be > 0");
+  for (int l = 0; l < ld->num_layers; ++l) {
+    if (ld->layers_map[l] < 1 || ld->layers_map[l] > ld->num_columns)
+      return set_error(MLX_ERR_ARGUMENT, "layers_map entry out of range");
+    if (ld->iterations[l] < 0) return set_error(MLX_ERR_ARGUMENT, "iterations must be >= 0");
+  }
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::upload_contacts(const mlx_contacts* K, ContactData& cd) {
+  const int nK = (K && K->num_contacts > 0) ? K->num_contacts : 0;
+  cd = ContactData{};
+  cd.K = nK;
+  if (nK == 0) return MLX_OK;
+  if (!K->normals || !K->point_colliders || !K->vertex_ids || !K->compliance)
+    return set_error(MLX_ERR_ARGUMENT, "contact arrays are NULL");
+  for (int k = 0; k < nK; ++k)
+    if (K->vertex_ids[k] < 1 || K->vertex_ids[k] > N) return set_error(MLX_ERR_ARGUMENT, "contact vertex id out of range");
+  CHECK(h_cstage.ensure(sizeof(double) * 7 * nK + sizeof(int) * nK));
+  CHECK(d_contacts.ensure(sizeof(double) * 7 * nK));
+  CHECK(d_cvid.ensure(sizeof(int) * nK));
+  CHECK(d_clam.ensure(sizeof(double) * nK));
+  double* hc = h_cstage.as<double>();
+  std::memcpy(hc, K->normals, sizeof(double) * 3 * nK);
+  std::memcpy(hc + 3 * nK, K->point_colliders, sizeof(double) * 3 * nK);
+  std::memcpy(hc + 6 * nK, K->compliance, sizeof(double) * nK);
+  int* hv = reinterpret_cast<int*>(hc + 7 * nK);
+  for (int k = 0; k < nK; ++k) hv[k] = K->vertex_ids[k] - 1;
+  CU(cudaMemcpyAsync(d_contacts.p, hc, sizeof(double) * 7 * nK, cudaMemcpyHostToDevice, stream));
+  CU(cudaMemcpyAsync(d_cvid.p, hv, sizeof(int) * nK, cudaMemcpyHostToDevice, stream));
+  CU(cudaMemsetAsync(d_clam.p, 0, sizeof(double) * nK, stream));
+  cd.normal = d_contacts.as<double>();
+  cd.point = cd.normal + 3 * nK;
+  cd.compliance = cd.normal + 6 * nK;
+  cd.vid = d_cvid.as<int>();
+  cd.lambda = d_clam.as<double>();
+  return MLX_OK;
+}
+
+// The layer loop of layerSolve (xpbdLayer3D.m:109-226) on the device-resident
+// state (pos, resv, oldp, lambda, pinned values).  With `capturing` set the
+// loop issues only stream work (no host synchronisation), so it can be
+// recorded into a CUDA graph; residual monitoring needs the host and is
+// refused in that mode.
+template <typename R>
+int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, const mlx_contacts* K,
+                          const ContactData& cd, RunState& st, bool capturing) {
+  if (capturing && P->compute_residuals)
+    return set_error(MLX_ERR_UNSUPPORTED, "residual monitoring cannot run inside a captured step");
+  const double h = P->h;
+  const R hR = (R)h;
+  const int nK = cd.K;
+  const size_t np = pinned.size();
+  bool errorChangeDecreased = false;
+  while ((int)cache.size() < ld->num_columns) cache.emplace_back(new LayerStatic());
+  const long long kSafetyIterations = 100000000LL;
+
+  for (int layer = 0; layer < ld->num_layers; ++layer) {
+    double setPercentStop = layer == 0 ? P->stop_at_improvement_percent : 0;
+    bool isLast = layer == ld->num_layers - 1;
+    int col = ld->layers_map[layer] - 1;
+    LayerStatic& ls = *cache[col];
+    CHECK(build_static(ld, col, ls, capturing));
+    const int* dint = ls.dev.as<int>();
+    LayerDev L{};
+    L.nb = ls.nb;
+    L.body_vert_off = dint + ls.o_bvo;
+    L.body_verts = dint + ls.o_bv;
+    L.bnd_off = dint + ls.o_bo;
+    L.bnd_verts = dint + ls.o_bnd;
+    L.vert_body = dint + ls.o_vb;
+    L.vert_rigid = ls.dev_rigid.as<unsigned char>();
+    L.any_boundary = ls.n_bnd > 0;
+    // contact lists of this layer
+    std::vector<int> cpack;
+    if (nK > 0) {
+      const int32_t* rid = ls.rid.data();
+      std::vector<int> rc_off(ls.nb + 1, 0), rc_ids;
+      if (P->use_rigid_contacts) {
+        for (int k = 0; k < nK; ++k) {
+          int b = rid[K->vertex_ids[k] - 1];
+          if (b > 0) ++rc_off[b];
+        }
+        for (int b = 1; b <= ls.nb; ++b) rc_off[b] += rc_off[b - 1];
+        rc_ids.resize(rc_off[ls.nb]);
+        std::vector<int> f(rc_off.begin(), rc_off.end() - 1);
+        for (int k = 0; k < nK; ++k) {
+          int b = rid[K->vertex_ids[k] - 1];
+          if (b > 0) rc_ids[f[b - 1]++] = k;
+        }
+      }
+      // elastic contacts grouped by vertex (groups in first-occurrence order)
+      std::vector<int> first(N, -1), ec_cnt;
+      std::vector<int> group_of(nK, -1);
+      for (int k = 0; k < nK; ++k) {
+        int v = K->vertex_ids[k] - 1;
+        if (rid[v] != 0) continue;
+        if (first[v] < 0) { first[v] = (int)ec_cnt.size(); ec_cnt.push_back(0); }
+        group_of[k] = first[v];
+        ++ec_cnt[first[v]];
+      }
+      int ng = (int)ec_cnt.size();
+      std::vector<int> ec_off(ng + 1, 0), ec_ids;
+      for (int q = 0; q < ng; ++q) ec_off[q + 1] = ec_off[q] + ec_cnt[q];
+      ec_ids.resize(ec_off[ng]);
+      {
+        std::vector<int> f(ec_off.begin(), ec_off.end() - 1);
+        for (int k = 0; k < nK; ++k)
+          if (group_of[k] >= 0) ec_ids[f[group_of[k]]++] = k;
+      }
+      size_t o_rco = 0, o_rci = rc_off.size(), o_eco = o_rci + rc_ids.size(), o_eci = o_eco + ec_off.size();
+      cpack.reserve(o_eci + ec_ids.size());
+      cpack.insert(cpack.end(), rc_off.begin(), rc_off.end());
+      cpack.insert(cpack.end(), rc_ids.begin(), rc_ids.end());
+      cpack.insert(cpack.end(), ec_off.begin(), ec_off.end());
+      cpack.insert(cpack.end(), ec_ids.begin(), ec_ids.end());
+      CHECK(d_cgroups.ensure(sizeof(int) * cpack.size()));
+      CU(cudaMemcpyAsync(d_cgroups.p, cpack.data(), sizeof(int) * cpack.size(), cudaMemcpyHostToDevice, stream));
+      const int* dc = d_cgroups.as<int>();
+      L.rc_off = dc + o_rco;
+      L.rc_ids = dc + o_rci;
+      L.any_rigid_contact = rc_ids.size() > 0;
+      L.n_ec_groups = ng;
+      L.ec_off = dc + o_eco;
+      L.ec_ids = dc + o_eci;
+    }
+    const bool rigidLayer = ls.n_rigid_elements > 0;
+    R4<R>* p = pos();
+    R4<R>* resv = d_resv.as<R4<R>>();
+    R4<R>* xprev = d_xprev.as<R4<R>>();
+    double4* ri = d_ri.as<double4>();
+    if (rigidLayer && ls.nb > 0) CU(cudaMemcpyAsync(xprev, p, sizeof(R4<R>) * N, cudaMemcpyDeviceToDevice, stream));
+    if (ls.nb > 0) {
+      if (!capturing) CHECK(d_bodies.ensure(sizeof(Body) * ls.nb));
+      else if (d_bodies.bytes < sizeof(Body) * ls.nb) return set_error(MLX_ERR_ARGUMENT, "body buffer not reserved");
+      k_make_rigids<R><<<ls.nb, 256, 0, stream>>>(L, d_bodies.as<Body>(), p, resv, d_vmass.as<double>(), ri);
+      CU(cudaGetLastError());
+      ++st.launches;
+    }
+    k_release_elastic<R><<<blocks_for(N, 256), 256, 0, stream>>>(p, resv, L.vert_rigid, N, hR);
+    CU(cudaGetLastError());
+    ++st.launches;
+    if (rigidLayer && ls.nb > 0) {
+      k_rigid_step<R><<<ls.nb, 256, 0, stream>>>(L, d_bodies.as<Body>(), p, xprev, resv, ri, h);
+      CU(cudaGetLastError());
+      ++st.launches;
+    }
+    double normresv = 0;
+    if (P->compute_residuals) {
+      CU(cudaStreamSynchronize(stream));
+      auto t0 = std::chrono::steady_clock::now();
+      CHECK(norm_resv(&normresv));
+      st.sumNonMon += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    if (ls.n_bnd > 0) {
+      if (!capturing) CHECK(d_lamB.ensure(sizeof(double) * ls.n_bnd));
+      else if (d_lamB.bytes < sizeof(double) * ls.n_bnd) return set_error(MLX_ERR_ARGUMENT, "boundary buffer not reserved");
+      CU(cudaMemsetAsync(d_lamB.p, 0, sizeof(double) * ls.n_bnd, stream));
+    }
+    const int* dlist = dint + ls.o_list;
+    const bool bodyWork = (ls.nb > 0 && (L.any_boundary || (P->use_rigid_contacts && L.any_rigid_contact))) ||
+                          L.n_ec_groups > 0;
+    const int ecBlocks = blocks_for(L.n_ec_groups, 128);
+    bool stopSolve = false;
+    long long it = 1;
+    while (it <= ld->iterations[layer] || (!stopSolve && st.runUntil >= 0 && isLast)) {
+      ++it;
+      if (it > kSafetyIterations) return set_error(MLX_ERR_LIMIT, "iteration safety limit reached");
+      ++st.totalIterations;
+      const bool timed = sweep_timing && tev_used + 2 <= tev.size();
+      if (timed) CHECK(record_event(tev[tev_used], capturing));
+      long long sweep_l = 0;
+      double sweep_b = 0;
+      for (int c = 0; c < C; ++c) {
+        if (ls.color_count[c] == 0) continue;
+        CHECK(launch_color(c, ls, dlist, hR));
+        ++st.launches;
+        ++sweep_l;
+        sweep_b += ls.color_count[c] * (bytes_per_tet() + (ls.identity_list ? 0.0 : 4.0));
+      }
+      if (timed) {
+        CHECK(record_event(tev[tev_used + 1], capturing));
+        tev_bytes[tev_used / 2] = sweep_b;
+        tev_launches[tev_used / 2] = sweep_l;
+        tev_used += 2;
+      }
+      if (bodyWork) {
+        k_iterate_bodies<R><<<ls.nb + ecBlocks, 128, 0, stream>>>(
+            L, d_bodies.as<Body>(), p, ri, d_vmass.as<double>(), d_lamB.as<double>(), cd, h,
+            P->boundary_compliance, P->contact_resistance, P->use_rigid_contacts);
+        CU(cudaGetLastError());
+        ++st.launches;
+      }
+      if (np) {
+        k_pin<R><<<blocks_for((long long)np, 256), 256, 0, stream>>>(p, d_pin_dofs.as<int>(), d_pinx.as<R>(), (int)np);
+        CU(cudaGetLastError());
+        ++st.launches;
+      }
+      bool endLayer = false;
+      if (P->compute_residuals) {
+        CU(cudaStreamSynchronize(stream));
+        auto t0 = std::chrono::steady_clock::now();
+        double newRes = 0;
+        CHECK(residual(cd, P->contact_resistance, h, &newRes));
+        st.launches += 2;
+        std::vector<double>& ra = st.residualArray;
+        ra.push_back(newRes);
+        double lastResidual = std::fabs(ra[ra.size() - 2]);
+        double newResidual = std::fabs(newRes);
+        double errorChange = newResidual - lastResidual;
+        if (setPercentStop > 0) {
+          st.runUntil = std::max((1 - setPercentStop / 100.0) * newResidual, 1e-8);
+          setPercentStop = 0;
+        }
+        if (errorChange < 0) errorChangeDecreased = true;
+        if (P->give_up_enabled && errorChange > P->give_up_threshold && errorChangeDecreased &&
+            (!isLast || P->last_layer_give_up_enabled))
+          endLayer = true;
+        bool stopHanging = (long long)ra.size() > P->hanging_stop && P->hanging_stop >= 0;
+        if (stopHanging || (st.runUntil >= 0 && (st.runUntil >= newResidual && (isLast || normresv < st.runUntil))))
+          stopSolve = true;
+        st.sumNonMon += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      }
+      if (endLayer || stopSolve) break;
+    }
+    if (ls.nb > 0) {
+      k_finish_layer<R><<<ls.nb, 256, 0, stream>>>(L, d_bodies.as<Body>(), p, resv, ri, rigidLayer ? 1 : 0);
+      CU(cudaGetLastError());
+      ++st.launches;
+    }
+    if (nK > 0) CU(cudaStreamSynchronize(stream));  // cpack is a pageable host source
+    if (stopSolve) break;
+  }
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::layer_solve(const mlx_layer_desc* ld, const mlx_solve_params* P, const mlx_contacts* K,
+                           const mlx_solve_inputs* in, mlx_solve_outputs* out) {
+  if (!ld || !P || !in || !out) return set_error(MLX_ERR_ARGUMENT, "null argument");
+  if (!in->xi || !in->lambdai || !in->oldp || !in->residualv || !out->xi)
+    return set_error(MLX_ERR_ARGUMENT, "xi, lambdai, oldp, residualv and out->xi are required");
+  if (!pinned.empty() && !in->pinnedx) return set_error(MLX_ERR_ARGUMENT, "pinnedx is NULL");
+  CHECK(validate_layers(ld, P));
+  if (in->residual_in_len < 1 && P->compute_residuals)
+    return set_error(MLX_ERR_ARGUMENT, "residual_in must hold at least the initial entry");
+
+  DeviceGuard g(device);
+  const size_t n3 = 3 * (size_t)N, n6 = 6 * (size_t)T, np = pinned.size();
+  // ---- upload per-call vectors (one pinned staging copy) ----
+  size_t nst = n3 * 3 + n6 + np;
+  CHECK(h_stage.ensure(sizeof(double) * nst));
+  CHECK(d_stage.ensure(sizeof(double) * nst));
+  double* hs = h_stage.as<double>();
+  std::memcpy(hs, in->xi, sizeof(double) * n3);
+  std::memcpy(hs + n3, in->oldp, sizeof(double) * n3);
+  std::memcpy(hs + 2 * n3, in->residualv, sizeof(double) * n3);
+  std::memcpy(hs + 3 * n3, in->lambdai, sizeof(double) * n6);
+  if (np) std::memcpy(hs + 3 * n3 + n6, in->pinnedx, sizeof(double) * np);
+  CU(cudaMemcpyAsync(d_stage.p, hs, sizeof(double) * nst, cudaMemcpyHostToDevice, stream));
+  double* ds = d_stage.as<double>();
+  const int bs = 256;
+  k_load_pos<R><<<blocks_for(N, bs), bs, 0, stream>>>(ds, d_mass3.as<double>(), pos(), N);
+  if (damp) k_load_vec<R><<<blocks_for(N, bs), bs, 0, stream>>>(ds + n3, d_oldp.as<R4<R>>(), N);
+  k_load_vec<R><<<blocks_for(N, bs), bs, 0, stream>>>(ds + 2 * n3, d_resv.as<R4<R>>(), N);
+  k_load_lambda<R><<<blocks_for(T, bs), bs, 0, stream>>>(ds + 3 * n3, d_s2e.as<int>(), d_lambda.as<R>(), T);
+  if (np) k_cast<R><<<blocks_for((long long)np, bs), bs, 0, stream>>>(ds + 3 * n3 + n6, d_pinx.as<R>(), (int)np);
+  CU(cudaGetLastError());
+  ContactData cd;
+  CHECK(upload_contacts(K, cd));
+
+  RunState st;
+  st.residualArray.assign(in->residual_in, in->residual_in + std::max(in->residual_in_len, 0));
+  st.runUntil = P->run_until;
+  st.sumNonMon = in->sum_non_monitored_time;
+  CHECK(run_layers(ld, P, K, cd, st, false));
+  // ---- download ----
+  k_store_pos<R><<<blocks_for(N, bs), bs, 0, stream>>>(pos(), ds, N);
+  if (out->lambdai) k_store_lambda<R><<<blocks_for(T, bs), bs, 0, stream>>>(d_lambda.as<R>(), d_s2e.as<int>(), ds + n3, T);
+  CU(cudaGetLastError());
+  CU(cudaMemcpyAsync(hs, ds, sizeof(double) * (out->lambdai ? n3 + n6 : n3), cudaMemcpyDeviceToHost, stream));
+  CU(cudaStreamSynchronize(stream));
+  std::memcpy(out->xi, hs, sizeof(double) * n3);
+  if (out->lambdai) std::memcpy(out->lambdai, hs + n3, sizeof(double) * n6);
+  int n = (int)st.residualArray.size();
+  if (out->residual) {
+    if (n > out->residual_capacity) return set_error(MLX_ERR_ARGUMENT, "residual capacity too small");
+    std::memcpy(out->residual, st.residualArray.data(), sizeof(double) * n);
+  }
+  out->residual_len = n;
+  out->run_until = st.runUntil;
+  out->sum_non_monitored_time = st.sumNonMon;
+  out->total_iterations = st.totalIterations;
+  last_launches = st.launches;
+  return MLX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Device-resident stepping: xpbdLayer3D.integrate (xpbdLayer3D.m:621-745) with
+// a fixed layer description, no host round trip between steps.
+
+// Step start (xpbdLayer3D.m:638-666): f = m g on z, oldp = p, residual
+// velocity = v + h f/m on unpinned DOFs, times (1 - airDrag).
+template <typename R>
+__global__ void k_sim_begin(const R4<R>* __restrict__ pos, const R4<R>* __restrict__ vel,
+                            R4<R>* __restrict__ oldp, R4<R>* __restrict__ resv,
+                            const double* __restrict__ mass3, const unsigned char* __restrict__ pin_mask,
+                            int N, double h, double gravity, double air) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= N) return;
+  R4<R> p = pos[v], u = vel[v];
+  oldp[v] = make_r4<R>(p.x, p.y, p.z, 0);
+  unsigned char pm = pin_mask[v];
+  double r[3] = {(double)u.x, (double)u.y, (double)u.z};
+  double fz = 0.0 + mass3[3 * v + 2] * gravity;
+  if (!(pm & 4)) r[2] = r[2] + (h * fz) / mass3[3 * v + 2];
+  if (!(pm & 1)) r[0] = r[0] + (h * 0.0) / mass3[3 * v];
+  if (!(pm & 2)) r[1] = r[1] + (h * 0.0) / mass3[3 * v + 1];
+  double k = 1.0 - air;
+  resv[v] = make_r4<R>((R)(k * r[0]), (R)(k * r[1]), (R)(k * r[2]), 0);
+}
+
+// Step end (xpbdLayer3D.m:737-738): v = (xi - oldp)/h, p = xi.
+template <typename R>
+__global__ void k_sim_end(const R4<R>* __restrict__ pos, const R4<R>* __restrict__ oldp,
+                          R4<R>* __restrict__ vel, int N, double h) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= N) return;
+  R4<R> p = pos[v], o = oldp[v];
+  vel[v] = make_r4<R>((R)(((double)p.x - o.x) / h), (R)(((double)p.y - o.y) / h), (R)(((double)p.z - o.z) / h), 0);
+}
+
+template <typename R>
+__global__ void k_add_velocity(R4<R>* __restrict__ vel, const int* __restrict__ dofs,
+                               const double* __restrict__ dv, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int d = dofs[i];
+  R* u = reinterpret_cast<R*>(&vel[d / 3]);
+  u[d % 3] = (R)((double)u[d % 3] + dv[i]);
+}
+
+template <typename R>
+int Solver<R>::sim_setup(const mlx_layer_desc* ld, const mlx_solve_params* P, const double* p0, const double* v0) {
+  CHECK(validate_layers(ld, P));
+  if (P->compute_residuals)
+    return set_error(MLX_ERR_UNSUPPORTED, "the resident stepper runs fixed iteration counts (compute_residuals = 0)");
+  if (!p0) return set_error(MLX_ERR_ARGUMENT, "initial positions are required");
+  DeviceGuard g(device);
+  // copy the fixed layer description (the caller's arrays may go away)
+  const size_t TL = (size_t)T * ld->num_columns, NL = (size_t)N * ld->num_columns;
+  sim.layers_map.assign(ld->layers_map, ld->layers_map + ld->num_layers);
+  sim.iterations.assign(ld->iterations, ld->iterations + ld->num_layers);
+  sim.isE.assign(ld->is_elastic_element, ld->is_elastic_element + TL);
+  sim.isR.assign(ld->is_rigid_element, ld->is_rigid_element + TL);
+  sim.sets.assign(ld->rigid_body_sets, ld->rigid_body_sets + TL);
+  sim.rid.assign(ld->vertex_rigid_body, ld->vertex_rigid_body + NL);
+  sim.isBV.assign(ld->is_boundary_vertex, ld->is_boundary_vertex + NL);
+  sim.isRV.assign(ld->is_rigid_vertex, ld->is_rigid_vertex + NL);
+  sim.nr.assign(ld->num_rigids, ld->num_rigids + ld->num_columns);
+  sim.ld = *ld;
+  sim.ld.layers_map = sim.layers_map.data();
+  sim.ld.iterations = sim.iterations.data();
+  sim.ld.is_elastic_element = sim.isE.data();
+  sim.ld.is_rigid_element = sim.isR.data();
+  sim.ld.rigid_body_sets = sim.sets.data();
+  sim.ld.vertex_rigid_body = sim.rid.data();
+  sim.ld.is_boundary_vertex = sim.isBV.data();
+  sim.ld.is_rigid_vertex = sim.isRV.data();
+  sim.ld.num_rigids = sim.nr.data();
+  sim.P = *P;
+  // build every column once and reserve the body buffers for capture
+  while ((int)cache.size() < ld->num_columns) cache.emplace_back(new LayerStatic());
+  int maxb = 1, maxbnd = 1;
+  for (int c = 0; c < ld->num_columns; ++c) {
+    CHECK(build_static(&sim.ld, c, *cache[c], false));
+    maxb = std::max(maxb, cache[c]->nb);
+    maxbnd = std::max(maxbnd, cache[c]->n_bnd);
+  }
+  CHECK(d_bodies.ensure(sizeof(Body) * maxb));
+  CHECK(d_lamB.ensure(sizeof(double) * maxbnd));
+  CHECK(d_vel.ensure(sizeof(R4<R>) * N));
+  CHECK(d_pin_mask.ensure(N));
+  std::vector<unsigned char> pm(N, 0);
+  for (int d : pinned) pm[d / 3] |= (unsigned char)(1u << (d % 3));
+  // state: positions, velocities, pinned values = positions of frame 1
+  const size_t n3 = 3 * (size_t)N, np = pinned.size();
+  CHECK(h_stage.ensure(sizeof(double) * (2 * n3 + np)));
+  CHECK(d_stage.ensure(sizeof(double) * (2 * n3 + np)));
+  double* hs = h_stage.as<double>();
+  std::memcpy(hs, p0, sizeof(double) * n3);
+  if (v0) std::memcpy(hs + n3, v0, sizeof(double) * n3);
+  else std::memset(hs + n3, 0, sizeof(double) * n3);
+  for (size_t i = 0; i < np; ++i) hs[2 * n3 + i] = p0[pinned[i]];
+  CU(cudaMemcpyAsync(d_stage.p, hs, sizeof(double) * (2 * n3 + np), cudaMemcpyHostToDevice, stream));
+  CU(cudaMemcpyAsync(d_pin_mask.p, pm.data(), N, cudaMemcpyHostToDevice, stream));
+  double* ds = d_stage.as<double>();
+  k_load_pos<R><<<blocks_for(N, 256), 256, 0, stream>>>(ds, d_mass3.as<double>(), pos(), N);
+  k_load_vec<R><<<blocks_for(N, 256), 256, 0, stream>>>(ds + n3, d_vel.as<R4<R>>(), N);
+  if (np) k_cast<R><<<blocks_for((long long)np, 256), 256, 0, stream>>>(ds + 2 * n3, d_pinx.as<R>(), (int)np);
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(stream));
+  if (sim.graph) { cudaGraphExecDestroy(sim.graph); sim.graph = nullptr; }
+  sim.ready = true;
+  return MLX_OK;
+}
+
+template <typename R>
+double Solver<R>::bytes_per_tet() const {
+  // algorithmic bytes of one tet projection in this layout: vertex ids,
+  // DmInv, volume, material, lambda read+write, four vertex records read and
+  // written (+ four step-start records with Rayleigh damping)
+  const double r = sizeof(R);
+  const int nl = mat_kind == MAT_NH ? 2 : 6;
+  double b = 16 + 9 * r + r + mat_stride(mat_kind) * r + 2 * nl * r + 8 * 4 * r;
+  if (damp) b += 4 * 4 * r;
+  return b;
+}
+
+template <typename R>
+int Solver<R>::record_event(cudaEvent_t e, bool capturing) {
+  if (capturing) CU(cudaEventRecordWithFlags(e, stream, cudaEventRecordExternal));
+  else CU(cudaEventRecord(e, stream));
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::enable_sweep_timing(int on) {
+  DeviceGuard g(device);
+  sweep_timing = on != 0;
+  if (sim.graph) { cudaGraphExecDestroy(sim.graph); sim.graph = nullptr; }
+  if (sweep_timing && tev.empty()) {
+    long long pairs = 0;
+    for (size_t l = 0; l < sim.iterations.size(); ++l) pairs += sim.iterations[l];
+    pairs = std::max<long long>(pairs, 1);
+    tev.resize(2 * pairs);
+    for (cudaEvent_t& e : tev) CU(cudaEventCreate(&e));
+    tev_bytes.assign(pairs, 0);
+    tev_launches.assign(pairs, 0);
+  }
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::collect_sweep_times() {
+  for (size_t q = 0; q + 1 < tev_used; q += 2) {
+    float ms = 0;
+    CU(cudaEventElapsedTime(&ms, tev[q], tev[q + 1]));
+    sweep_ms += ms;
+    sweep_bytes += tev_bytes[q / 2];
+    sweep_launches += tev_launches[q / 2];
+  }
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::sweep_stats(double* ms, double* bytes, long long* launches, int reset) {
+  if (ms) *ms = sweep_ms;
+  if (bytes) *bytes = sweep_bytes;
+  if (launches) *launches = sweep_launches;
+  if (reset) { sweep_ms = 0; sweep_bytes = 0; sweep_launches = 0; }
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::sim_issue_step(long long* launches) {
+  const double h = sim.P.h;
+  tev_used = 0;
+  R4<R>* p = pos();
+  k_sim_begin<R><<<blocks_for(N, 256), 256, 0, stream>>>(p, d_vel.as<R4<R>>(), d_oldp.as<R4<R>>(),
+                                                          d_resv.as<R4<R>>(), d_mass3.as<double>(),
+                                                          d_pin_mask.as<unsigned char>(), N, h, sim.P.gravity,
+                                                          sim.air_drag);
+  CU(cudaGetLastError());
+  CU(cudaMemsetAsync(d_lambda.p, 0, sizeof(R) * 6 * (size_t)T, stream));
+  RunState st;
+  st.runUntil = sim.P.run_until;
+  ContactData cd{};
+  CHECK(run_layers(&sim.ld, &sim.P, nullptr, cd, st, true));
+  k_sim_end<R><<<blocks_for(N, 256), 256, 0, stream>>>(p, d_oldp.as<R4<R>>(), d_vel.as<R4<R>>(), N, h);
+  CU(cudaGetLastError());
+  if (launches) *launches = st.launches + 2;
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::sim_step(int nsteps, int use_graph, double* device_ms) {
+  if (!sim.ready) return set_error(MLX_ERR_ARGUMENT, "sim_setup has not been called");
+  if (nsteps < 0) return set_error(MLX_ERR_ARGUMENT, "nsteps < 0");
+  DeviceGuard g(device);
+  if (use_graph && !sim.graph) {
+    cudaGraph_t graph = nullptr;
+    CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    long long nl = 0;
+    int rc = sim_issue_step(&nl);
+    cudaError_t e = cudaStreamEndCapture(stream, &graph);
+    if (rc != MLX_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    if (e != cudaSuccess) return set_error(MLX_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&sim.graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return set_error(MLX_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    sim.launches_per_step = nl;
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (device_ms) {
+    CU(cudaEventCreate(&e0));
+    CU(cudaEventCreate(&e1));
+    CU(cudaEventRecord(e0, stream));
+  }
+  for (int s = 0; s < nsteps; ++s) {
+    if (use_graph) {
+      CU(cudaGraphLaunch(sim.graph, stream));
+    } else {
+      long long nl = 0;
+      CHECK(sim_issue_step(&nl));
+      sim.launches_per_step = nl;
+    }
+    if (sweep_timing) {  // the event pairs are reused by every step
+      CU(cudaStreamSynchronize(stream));
+      CHECK(collect_sweep_times());
+    }
+  }
+  if (device_ms) {
+    CU(cudaEventRecord(e1, stream));
+    CU(cudaEventSynchronize(e1));
+    float ms = 0;
+    CU(cudaEventElapsedTime(&ms, e0, e1));
+    *device_ms = ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  CU(cudaStreamSynchronize(stream));
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::sim_add_velocity(const int32_t* dofs, const double* dv, int n) {
+  if (!sim.ready) return set_error(MLX_ERR_ARGUMENT, "sim_setup has not been called");
+  if (n <= 0) return MLX_OK;
+  std::vector<int> d0(n);
+  for (int i = 0; i < n; ++i) {
+    if (dofs[i] < 1 || dofs[i] > 3 * N) return set_error(MLX_ERR_ARGUMENT, "velocity DOF out of range");
+    d0[i] = dofs[i] - 1;
+  }
+  DeviceGuard g(device);
+  DevBuf dd, dvv;
+  CHECK(dd.ensure(sizeof(int) * n));
+  CHECK(dvv.ensure(sizeof(double) * n));
+  CU(cudaMemcpyAsync(dd.p, d0.data(), sizeof(int) * n, cudaMemcpyHostToDevice, stream));
+  CU(cudaMemcpyAsync(dvv.p, dv, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+  k_add_velocity<R><<<blocks_for(n, 256), 256, 0, stream>>>(d_vel.as<R4<R>>(), dd.as<int>(), dvv.as<double>(), n);
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(stream));
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::sim_get_state(double* p, double* v) {
+  if (!sim.ready) return set_error(MLX_ERR_ARGUMENT, "sim_setup has not been called");
+  DeviceGuard g(device);
+  const size_t n3 = 3 * (size_t)N;
+  CHECK(h_stage.ensure(sizeof(double) * 2 * n3));
+  CHECK(d_stage.ensure(sizeof(double) * 2 * n3));
+  double* ds = d_stage.as<double>();
+  k_store_pos<R><<<blocks_for(N, 256), 256, 0, stream>>>(pos(), ds, N);
+  k_store_pos<R><<<blocks_for(N, 256), 256, 0, stream>>>(d_vel.as<R4<R>>(), ds + n3, N);
+  CU(cudaGetLastError());
+  CU(cudaMemcpyAsync(h_stage.p, ds, sizeof(double) * 2 * n3, cudaMemcpyDeviceToHost, stream));
+  CU(cudaStreamSynchronize(stream));
+  if (p) std::memcpy(p, h_stage.p, sizeof(double) * n3);
+  if (v) std::memcpy(v, h_stage.as<double>() + n3, sizeof(double) * n3);
+  return MLX_OK;
+}
+
+template struct Solver<float>;
+template struct Solver<double>;
+
+SolverBase* make_solver(const mlx_mesh_desc* md, int* rc) {
+  if (md->precision == MLX_FP64) {
+    auto* s = new Solver<double>();
+    *rc = s->create(md);
+    return s;
+  }
+  auto* s = new Solver<float>();
+  *rc = s->create(md);
+  return s;
+}
+
+}  // namespace mlx
+
+// ---------------------------------------------------------------------------
+// C ABI
+struct mlx_solver {
+  int device;
+  mlx::SolverBase* impl;
+};
+
+extern "C" {
+
+const char* mlx_last_error(void) { return mlx::g_err.c_str(); }
+int mlx_abi_version(void) { return MLX_ABI_VERSION; }
+
+int mlx_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  int good = 0;
+  for (int d = 0; d < n; ++d) {
+    cudaDeviceProp pr;
+    if (cudaGetDeviceProperties(&pr, d) == cudaSuccess && pr.major == 10) ++good;
+  }
+  return good;
+}
+
+int mlx_create(const mlx_mesh_desc* mesh, mlx_solver** out) {
+  if (!mesh || !out) return set_error(MLX_ERR_ARGUMENT, "null argument");
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return set_error(MLX_ERR_NO_DEVICE, "no CUDA device visible");
+  }
+  if (mesh->device < 0 || mesh->device >= n) return set_error(MLX_ERR_ARGUMENT, "device ordinal out of range");
+  cudaDeviceProp pr;
+  if (cudaGetDeviceProperties(&pr, mesh->device) != cudaSuccess || pr.major != 10)
+    return set_error(MLX_ERR_NO_DEVICE, "this library is built for sm_100a (B200)");
+  int rc = MLX_OK;
+  mlx::SolverBase* impl = mlx::make_solver(mesh, &rc);
+  if (rc != MLX_OK) {
+    delete impl;
+    return rc;
+  }
+  *out = new mlx_solver{mesh->device, impl};
+  return MLX_OK;
+}
+
+int mlx_destroy(mlx_solver* s) {
+  if (!s) return MLX_OK;
+  {
+    DeviceGuard g(s->device);
+    delete s->impl;
+  }
+  delete s;
+  return MLX_OK;
+}
+
+int mlx_layer_solve(mlx_solver* s, const mlx_layer_desc* layers, const mlx_solve_params* params,
+                    const mlx_contacts* contacts, const mlx_solve_inputs* in, mlx_solve_outputs* out) {
+  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+  return s->impl->layer_solve(layers, params, contacts, in, out);
+}
+
+int mlx_sim_init(mlx_solver* s, const mlx_layer_desc* layers, const mlx_solve_params* params, const double* p0,
+                 const double* v0, double air_drag) {
+  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+  return s->impl->sim_init(layers, params, p0, v0, air_drag);
+}
+
+int mlx_sim_add_velocity(mlx_solver* s, const int32_t* dofs, const double* dv, int32_t n) {
+  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+  if (n > 0 && (!dofs || !dv)) return set_error(MLX_ERR_ARGUMENT, "null arrays");
+  return s->impl->sim_add_velocity(dofs, dv, n);
+}
+
+int mlx_sim_step(mlx_solver* s, int32_t nsteps, int32_t use_graph, double* device_ms) {
+  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+  return s->impl->sim_step(nsteps, use_graph, device_ms);
+}
+
+int mlx_sim_get_state(mlx_solver* s, double* p, double* v) {
+  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+  return s->impl->sim_get_state(p, v);
+}
+
+int mlx_sim_sweep_timing(mlx_solver* s, int32_t on) {
+  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+  return s->impl->enable_sweep_timing(on);
+}
+
+int mlx_sim_sweep_stats(mlx_solver* s, double* ms, double* bytes, long long* launches, int32_t reset) {
+  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+  return s->impl->sweep_stats(ms, bytes, launches, reset);
+}
+
+long long mlx_sim_launches_per_step(const mlx_solver* s) { return s ? s->impl->sim_launches_per_step() : 0; }
+long long mlx_last_call_launches(const mlx_solver* s) { return s ? s->impl->launches_last_call() : 0; }
+
+}  // extern "C"

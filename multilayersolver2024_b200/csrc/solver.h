@@ -1,0 +1,30 @@
+// solver.h -- internal interface between the C ABI and the precision-typed
+// solver implementations.
+#pragma once
+
+#include <string>
+#include "../../include/mlxpbd.h"
+
+namespace mlx {
+
+extern thread_local std::string g_err;
+int set_error(int code, const std::string& msg);
+
+struct SolverBase {
+  virtual ~SolverBase() {}
+  virtual int layer_solve(const mlx_layer_desc* ld, const mlx_solve_params* P, const mlx_contacts* K,
+                          const mlx_solve_inputs* in, mlx_solve_outputs* out) = 0;
+  virtual int sim_init(const mlx_layer_desc* ld, const mlx_solve_params* P, const double* p0, const double* v0,
+                       double air_drag) = 0;
+  virtual int sim_step(int nsteps, int use_graph, double* device_ms) = 0;
+  virtual int sim_add_velocity(const int32_t* dofs, const double* dv, int n) = 0;
+  virtual int sim_get_state(double* p, double* v) = 0;
+  virtual long long sim_launches_per_step() const = 0;
+  virtual long long launches_last_call() const = 0;
+  virtual int enable_sweep_timing(int on) = 0;
+  virtual int sweep_stats(double* ms, double* bytes, long long* launches, int reset) = 0;
+};
+
+SolverBase* make_solver(const mlx_mesh_desc* md, int* rc);
+
+}  // namespace mlx

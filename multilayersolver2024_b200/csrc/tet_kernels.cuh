@@ -1,0 +1,501 @@
+// tet_kernels.cuh -- per-tet constraint projection and residual kernels.
+//
+// One thread projects one tet of the current colour (tets of one colour share
+// no vertex, xpbdLayer3D.m:374-377).  Tet rest data is stored structure-of-
+// arrays in colour-sorted order, so the threads of a warp read consecutive
+// words of every field; the four vertex records are gathered with one vector
+// load each (position + inverse mass).
+#pragma once
+
+#include "common.cuh"
+
+namespace mlx {
+
+// material encodings of the per-tet compliance block
+enum MatKind : int {
+  MAT_STVK_BLOCKS = 0,  // alpha and alpha*beta blocks, 24 values per tet
+  MAT_STVK_LAME = 1,    // mu, lambda, alpha1 -> blocks formed in registers
+  MAT_NH = 2            // mu, lambda (stable Neo-Hookean D/H pair)
+};
+__host__ __device__ constexpr int mat_stride(int kind) {
+  return kind == MAT_STVK_BLOCKS ? 24 : (kind == MAT_STVK_LAME ? 3 : 2);
+}
+
+template <typename R> struct V3 { R x, y, z; };
+template <typename R> __device__ __forceinline__ V3<R> v3r(R x, R y, R z) { return {x, y, z}; }
+template <typename R> __device__ __forceinline__ V3<R> vsub(V3<R> a, V3<R> b) {
+  return {a.x - b.x, a.y - b.y, a.z - b.z};
+}
+template <typename R> __device__ __forceinline__ R vdot(V3<R> a, V3<R> b) {
+  return a.x * b.x + a.y * b.y + a.z * b.z;
+}
+template <typename R> __device__ __forceinline__ V3<R> vcross(V3<R> a, V3<R> b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+template <typename R> __device__ __forceinline__ V3<R> vaxpy3(R a, V3<R> u, R b, V3<R> v, R c, V3<R> w) {
+  return {a * u.x + b * v.x + c * w.x, a * u.y + b * v.y + c * w.y, a * u.z + b * v.z + c * w.z};
+}
+
+// 3x3 solve A x = b by Gaussian elimination with partial pivoting (the
+// pagemldivide of matStvkVoigtConstraint3D.m:42).  A is row-major here.
+template <typename R> __device__ __forceinline__ void solve3x3(R A[3][3], R b[3], R x[3]) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    int p = k;
+    R best = fabs(A[k][k]);
+#pragma unroll
+    for (int r = k + 1; r < 3; ++r) {
+      R v = fabs(A[r][k]);
+      if (v > best) { best = v; p = r; }
+    }
+    // swap rows k and p with compile-time indices only (keeps A in registers)
+#pragma unroll
+    for (int r = k + 1; r < 3; ++r) {
+      if (p == r) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) { R t = A[k][c]; A[k][c] = A[r][c]; A[r][c] = t; }
+        R t = b[k]; b[k] = b[r]; b[r] = t;
+      }
+    }
+#pragma unroll
+    for (int r = k + 1; r < 3; ++r) {
+      R f = A[r][k] / A[k][k];
+#pragma unroll
+      for (int c = k; c < 3; ++c) A[r][c] -= f * A[k][c];
+      b[r] -= f * b[k];
+    }
+  }
+#pragma unroll
+  for (int k = 2; k >= 0; --k) {
+    R s = b[k];
+#pragma unroll
+    for (int c = k + 1; c < 3; ++c) s -= A[k][c] * x[c];
+    x[k] = s / A[k][k];
+  }
+}
+
+// Compliance of one tet in the form the projection needs:
+// alphaTilde top block (3x3, row-major), alphaTilde shear diagonal,
+// gamma = alphaTilde*betaTilde/h top block and shear diagonal.
+template <typename R> struct Compliance {
+  R aT[3][3];
+  R aS[3];
+  R gT[3][3];
+  R gS[3];
+};
+
+template <typename R, int MAT>
+__device__ __forceinline__ void load_compliance(const R* __restrict__ mat, int s, int T, R inv_h2,
+                                                R inv_h, Compliance<R>& c, bool need_gamma) {
+  if (MAT == MAT_STVK_BLOCKS) {
+#pragma unroll
+    for (int col = 0; col < 3; ++col)
+#pragma unroll
+      for (int row = 0; row < 3; ++row) c.aT[row][col] = mat[(size_t)(row + 3 * col) * T + s] * inv_h2;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) c.aS[q] = mat[(size_t)(9 + q) * T + s] * inv_h2;
+    if (need_gamma) {
+#pragma unroll
+      for (int col = 0; col < 3; ++col)
+#pragma unroll
+        for (int row = 0; row < 3; ++row) c.gT[row][col] = mat[(size_t)(12 + row + 3 * col) * T + s] * inv_h;
+#pragma unroll
+      for (int q = 0; q < 3; ++q) c.gS[q] = mat[(size_t)(21 + q) * T + s] * inv_h;
+    } else {
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        c.gS[i] = 0;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) c.gT[i][j] = 0;
+      }
+    }
+  } else {  // MAT_STVK_LAME: K = [lam+4mu lam lam; ...] (+) 2mu I (Mesh3D.m:449-456)
+    R mu = mat[s], lam = mat[(size_t)T + s], a1 = mat[(size_t)2 * T + s];
+    R inv4mu = R(1) / (R(4) * mu);
+    R den = R(1) / (R(4) * mu + R(3) * lam);
+    R dg = inv4mu * (R(4) * mu + R(2) * lam) * den;
+    R off = -inv4mu * lam * den;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) c.aT[i][j] = (i == j ? dg : off) * inv_h2;
+    R sh = R(1) / (R(2) * mu) * inv_h2;
+    c.aS[0] = c.aS[1] = c.aS[2] = sh;
+    // beta = alpha1*K and alpha = inv(K) give alpha*beta = alpha1*I
+    R g = a1 * inv_h;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      c.gS[i] = g;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) c.gT[i][j] = (i == j ? g : R(0));
+    }
+  }
+}
+
+// Green-strain kinematics shared by projection and residual
+// (StVKconstraintGrad3D.m:1-70 in analytic form): f_i = sum_k (x0-x_k)
+// DmInv(k,i), d[a][i] = coefficient of x_a in f_i.
+template <typename R> struct StrainKin {
+  V3<R> f[3];
+  R d[4][3];
+};
+template <typename R>
+__device__ __forceinline__ void strain_kin(const V3<R> X[4], const R G[9], StrainKin<R>& k) {
+  V3<R> e1 = vsub(X[0], X[1]), e2 = vsub(X[0], X[2]), e3 = vsub(X[0], X[3]);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    k.f[i] = vaxpy3(G[0 + 3 * i], e1, G[1 + 3 * i], e2, G[2 + 3 * i], e3);
+    k.d[0][i] = G[0 + 3 * i] + G[1 + 3 * i] + G[2 + 3 * i];
+    k.d[1][i] = -G[0 + 3 * i];
+    k.d[2][i] = -G[1 + 3 * i];
+    k.d[3][i] = -G[2 + 3 * i];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// StVK "Voigt" projection of one tet: matStvkVoigtConstraint3D.m:1-22 with the
+// block-decoupled solve of decomposeSolve (:31-45).  Returns dx (in X) and
+// dlambda.
+template <typename R, int MAT, bool DAMP>
+__device__ __forceinline__ void stvk_project(V3<R> X[4], const V3<R>* Xold, const R minv[4],
+                                             const R G[9], R vol, const Compliance<R>& cm,
+                                             const R lam[6], R dl[6]) {
+  StrainKin<R> k;
+  strain_kin<R>(X, G, k);
+  R FF[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = i; j < 3; ++j) { FF[i][j] = vdot(k.f[i], k.f[j]); FF[j][i] = FF[i][j]; }
+  R W[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = i; j < 3; ++j) {
+      R s = 0;
+#pragma unroll
+      for (int a = 0; a < 4; ++a) s += minv[a] * k.d[a][i] * k.d[a][j];
+      W[i][j] = s; W[j][i] = s;
+    }
+  const R half = R(0.5);
+  R C[6] = {vol * (half * FF[0][0] - half), vol * (half * FF[1][1] - half), vol * (half * FF[2][2] - half),
+            vol * (half * FF[0][1]), vol * (half * FF[0][2]), vol * (half * FF[1][2])};
+  R v2 = vol * vol;
+  // numGamma = gamma * (gradC * (x - xprev))
+  R ng[6] = {0, 0, 0, 0, 0, 0};
+  if (DAMP) {
+    V3<R> dX[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) dX[a] = vsub(X[a], Xold[a]);
+    V3<R> e1 = vsub(dX[0], dX[1]), e2 = vsub(dX[0], dX[2]), e3 = vsub(dX[0], dX[3]);
+    V3<R> D[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) D[i] = vaxpy3(G[0 + 3 * i], e1, G[1 + 3 * i], e2, G[2 + 3 * i], e3);
+    R gdx[6];
+    gdx[0] = vol * vdot(k.f[0], D[0]);
+    gdx[1] = vol * vdot(k.f[1], D[1]);
+    gdx[2] = vol * vdot(k.f[2], D[2]);
+    gdx[3] = vol * half * (vdot(k.f[0], D[1]) + vdot(k.f[1], D[0]));
+    gdx[4] = vol * half * (vdot(k.f[0], D[2]) + vdot(k.f[2], D[0]));
+    gdx[5] = vol * half * (vdot(k.f[1], D[2]) + vdot(k.f[2], D[1]));
+#pragma unroll
+    for (int r = 0; r < 3; ++r) ng[r] = cm.gT[r][0] * gdx[0] + cm.gT[r][1] * gdx[1] + cm.gT[r][2] * gdx[2];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) ng[3 + q] = cm.gS[q] * gdx[3 + q];
+  }
+  // top block: ((I + gammaTop) * (gradCM gradC')_top + alphaTop) dl = b
+  R GM[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) GM[i][j] = v2 * W[i][j] * FF[i][j];
+  R A[3][3], b[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      R s = GM[r][c];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) s += cm.gT[r][q] * GM[q][c];
+      A[r][c] = s + cm.aT[r][c];
+    }
+    b[r] = -C[r] - (cm.aT[r][0] * lam[0] + cm.aT[r][1] * lam[1] + cm.aT[r][2] * lam[2]) - ng[r];
+  }
+  solve3x3<R>(A, b, dl);
+  // shear rows: scalar solves with alphaTilde(4,4), DenomGamma(4,4)
+  const int si[3] = {0, 0, 1}, sj[3] = {1, 2, 2};
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    int i = si[q], j = sj[q];
+    R S = v2 * R(0.25) * (W[i][i] * FF[j][j] + R(2) * W[i][j] * FF[i][j] + W[j][j] * FF[i][i]);
+    dl[3 + q] = (-C[3 + q] - cm.aS[0] * lam[3 + q] - ng[3 + q]) / ((R(1) + cm.gS[0]) * S + cm.aS[0]);
+  }
+  // dx_a = minv_a vol sum_i c_i(a) f_i
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    R c0 = dl[0] * k.d[a][0] + half * (dl[3] * k.d[a][1] + dl[4] * k.d[a][2]);
+    R c1 = dl[1] * k.d[a][1] + half * (dl[3] * k.d[a][0] + dl[5] * k.d[a][2]);
+    R c2 = dl[2] * k.d[a][2] + half * (dl[4] * k.d[a][0] + dl[5] * k.d[a][1]);
+    R s = minv[a] * vol;
+    V3<R> dx = vaxpy3(c0, k.f[0], c1, k.f[1], c2, k.f[2]);
+    X[a].x += s * dx.x;
+    X[a].y += s * dx.y;
+    X[a].z += s * dx.z;
+  }
+}
+
+// StVK residual terms of one tet (simpleEvaluateAllConstraintResiduals,
+// xpbdLayer3D.m:555-568): sum over components of (|C| - min(|C|, |aT*lambda|))^2
+template <typename R>
+__device__ __forceinline__ double stvk_residual(const V3<R> X[4], const R G[9], R vol,
+                                                const Compliance<R>& cm, const R lam[6]) {
+  StrainKin<R> k;
+  strain_kin<R>(X, G, k);
+  const R half = R(0.5);
+  R C[6] = {vol * (half * vdot(k.f[0], k.f[0]) - half), vol * (half * vdot(k.f[1], k.f[1]) - half),
+            vol * (half * vdot(k.f[2], k.f[2]) - half), vol * (half * vdot(k.f[0], k.f[1])),
+            vol * (half * vdot(k.f[0], k.f[2])), vol * (half * vdot(k.f[1], k.f[2]))};
+  R corr[6];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) corr[r] = cm.aT[r][0] * lam[0] + cm.aT[r][1] * lam[1] + cm.aT[r][2] * lam[2];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) corr[3 + q] = cm.aS[q] * lam[3 + q];
+  double acc = 0;
+#pragma unroll
+  for (int r = 0; r < 6; ++r) {
+    double a = fabs((double)C[r]), c = fabs((double)corr[r]);
+    double v = a - fmin(a, c);
+    acc += v * v;
+  }
+  return acc;
+}
+
+// ---------------------------------------------------------------------------
+// Stable Neo-Hookean pair of one tet, the 3D form of
+// 2d/mex/mexNeoHookeanDConstraint.cpp and mexNeoHookeanHConstraint.cpp:
+// C_D = ||F||_F with alphaTilde 1/(vol mu h^2); C_H = det F - (1 + mu/lambda)
+// with alphaTilde 1/(vol lambda h^2); both at the same positions, corrections
+// summed (xpbdLayer2D.m:282-289).  F = Ds * DmInv, Ds = [x1-x0 x2-x0 x3-x0].
+template <typename R> struct NHEval {
+  R CD, CH, aD, aH;
+  V3<R> gD[4], gH[4];
+};
+template <typename R>
+__device__ __forceinline__ void nh_eval(const V3<R> X[4], const R G[9], R mu, R lm, R vol, R inv_h2,
+                                        NHEval<R>& e) {
+  V3<R> u1 = vsub(X[1], X[0]), u2 = vsub(X[2], X[0]), u3 = vsub(X[3], X[0]);
+  V3<R> f[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) f[c] = vaxpy3(G[0 + 3 * c], u1, G[1 + 3 * c], u2, G[2 + 3 * c], u3);
+  R n2 = vdot(f[0], f[0]) + vdot(f[1], f[1]) + vdot(f[2], f[2]);
+  e.CD = sqrt(n2);
+  V3<R> cf[3] = {vcross(f[1], f[2]), vcross(f[2], f[0]), vcross(f[0], f[1])};
+  e.CH = vdot(f[0], cf[0]) - (R(1) + mu / lm);
+  e.aD = inv_h2 / (vol * mu);
+  e.aH = inv_h2 / (vol * lm);
+  R invCD = R(1) / e.CD;
+  V3<R> sD = {0, 0, 0}, sH = {0, 0, 0};
+#pragma unroll
+  for (int kk = 1; kk <= 3; ++kk) {
+    R g0 = G[(kk - 1) + 0], g1 = G[(kk - 1) + 3], g2 = G[(kk - 1) + 6];
+    V3<R> d = vaxpy3(g0, f[0], g1, f[1], g2, f[2]);
+    e.gD[kk] = {d.x * invCD, d.y * invCD, d.z * invCD};
+    e.gH[kk] = vaxpy3(g0, cf[0], g1, cf[1], g2, cf[2]);
+    sD = {sD.x + e.gD[kk].x, sD.y + e.gD[kk].y, sD.z + e.gD[kk].z};
+    sH = {sH.x + e.gH[kk].x, sH.y + e.gH[kk].y, sH.z + e.gH[kk].z};
+  }
+  e.gD[0] = {-sD.x, -sD.y, -sD.z};
+  e.gH[0] = {-sH.x, -sH.y, -sH.z};
+}
+
+template <typename R>
+__device__ __forceinline__ void nh_project(V3<R> X[4], const R minv[4], const R G[9], R mu, R lm, R vol,
+                                           R inv_h2, const R lam[2], R dl[2]) {
+  NHEval<R> e;
+  nh_eval<R>(X, G, mu, lm, vol, inv_h2, e);
+  R wD = 0, wH = 0;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    wD += minv[a] * vdot(e.gD[a], e.gD[a]);
+    wH += minv[a] * vdot(e.gH[a], e.gH[a]);
+  }
+  dl[0] = (-e.CD - e.aD * lam[0]) / (wD + e.aD);
+  dl[1] = (-e.CH - e.aH * lam[1]) / (wH + e.aH);
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    X[a].x += minv[a] * (e.gD[a].x * dl[0] + e.gH[a].x * dl[1]);
+    X[a].y += minv[a] * (e.gD[a].y * dl[0] + e.gH[a].y * dl[1]);
+    X[a].z += minv[a] * (e.gD[a].z * dl[0] + e.gH[a].z * dl[1]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Rest data of the mesh in colour-sorted order.
+template <typename R> struct TetData {
+  const int4* vid;     // [T] 0-based vertex ids
+  const R* dminv;      // [9][T] DmInv, column-major entry j of tet s at dminv[j*T+s]
+  const R* vol;        // [T]
+  const R* mat;        // [stride][T]
+  R* lambda;           // [6][T]
+  int T;
+};
+
+template <typename R>
+__device__ __forceinline__ void load_tet(const TetData<R>& td, int s, const R4<R>* __restrict__ pos,
+                                         int4& v, R G[9], V3<R> X[4], R minv[4]) {
+  v = td.vid[s];
+#pragma unroll
+  for (int j = 0; j < 9; ++j) G[j] = td.dminv[(size_t)j * td.T + s];
+  R4<R> p0 = pos[v.x], p1 = pos[v.y], p2 = pos[v.z], p3 = pos[v.w];
+  X[0] = {p0.x, p0.y, p0.z}; X[1] = {p1.x, p1.y, p1.z};
+  X[2] = {p2.x, p2.y, p2.z}; X[3] = {p3.x, p3.y, p3.z};
+  minv[0] = p0.w; minv[1] = p1.w; minv[2] = p2.w; minv[3] = p3.w;
+}
+
+// One colour of the Gauss-Seidel sweep (xpbdLayer3D.m:357-378).  `list` holds
+// the colour-sorted ids of this layer's elastic tets of this colour; NULL
+// means the identity over [begin, begin+count).
+template <typename R, int MAT, bool DAMP>
+__global__ void __launch_bounds__(128) k_project_color(TetData<R> td, const int* __restrict__ list,
+                                                       int begin, int count, R4<R>* __restrict__ pos,
+                                                       const R4<R>* __restrict__ oldp, R inv_h2, R inv_h) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  int s = list ? list[begin + i] : begin + i;
+  int4 v;
+  R G[9], minv[4];
+  V3<R> X[4];
+  load_tet<R>(td, s, pos, v, G, X, minv);
+  R vol = td.vol[s];
+  const int T = td.T;
+  if (MAT == MAT_NH) {
+    R mu = td.mat[s], lm = td.mat[(size_t)T + s];
+    R lam[2] = {td.lambda[s], td.lambda[(size_t)T + s]}, dl[2];
+    nh_project<R>(X, minv, G, mu, lm, vol, inv_h2, lam, dl);
+    td.lambda[s] = lam[0] + dl[0];
+    td.lambda[(size_t)T + s] = lam[1] + dl[1];
+  } else {
+    Compliance<R> cm;
+    load_compliance<R, MAT>(td.mat, s, T, inv_h2, inv_h, cm, DAMP);
+    R lam[6], dl[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) lam[q] = td.lambda[(size_t)q * T + s];
+    V3<R> Xo[4];
+    if (DAMP) {
+      R4<R> o0 = oldp[v.x], o1 = oldp[v.y], o2 = oldp[v.z], o3 = oldp[v.w];
+      Xo[0] = {o0.x, o0.y, o0.z}; Xo[1] = {o1.x, o1.y, o1.z};
+      Xo[2] = {o2.x, o2.y, o2.z}; Xo[3] = {o3.x, o3.y, o3.z};
+    }
+    stvk_project<R, MAT, DAMP>(X, Xo, minv, G, vol, cm, lam, dl);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) td.lambda[(size_t)q * T + s] = lam[q] + dl[q];
+  }
+  pos[v.x] = make_r4<R>(X[0].x, X[0].y, X[0].z, minv[0]);
+  pos[v.y] = make_r4<R>(X[1].x, X[1].y, X[1].z, minv[1]);
+  pos[v.z] = make_r4<R>(X[2].x, X[2].y, X[2].z, minv[2]);
+  pos[v.w] = make_r4<R>(X[3].x, X[3].y, X[3].z, minv[3]);
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic block sum of NV doubles (fixed shuffle tree + fixed warp
+// order).  All threads get the result.  blockDim.x must be a multiple of 32.
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV]) {
+  __shared__ double sh[32][NV];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NV; ++q)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < NV; ++q) sh[warp][q] = v[q];
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+      double x = lane < nw ? sh[lane][q] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+      if (lane == 0) sh[0][q] = x;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < NV; ++q) v[q] = sh[0][q];
+  __syncthreads();
+}
+
+struct ContactData {
+  int K;
+  const double* normal;     // [3][K]
+  const double* point;      // [3][K]
+  const double* compliance; // [K]
+  const int* vid;           // [K] 0-based
+  double* lambda;           // [K]
+};
+
+// Residual partial sums over all tets (blocks [0, tetBlocks)) and all
+// contacts (the remaining blocks), one double per block
+// (simpleEvaluateAllConstraintResiduals, xpbdLayer3D.m:546-586).
+template <typename R, int MAT>
+__global__ void __launch_bounds__(256) k_residual_partials(TetData<R> td, const R4<R>* __restrict__ pos,
+                                                           ContactData cd, double contact_resistance,
+                                                           R inv_h2, R inv_h, double inv_h2_d,
+                                                           int tetBlocks, double* __restrict__ partials) {
+  double acc[1] = {0.0};
+  if ((int)blockIdx.x < tetBlocks) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < td.T; s += tetBlocks * blockDim.x) {
+      int4 v;
+      R G[9], minv[4];
+      V3<R> X[4];
+      load_tet<R>(td, s, pos, v, G, X, minv);
+      R vol = td.vol[s];
+      const int T = td.T;
+      if (MAT == MAT_NH) {
+        NHEval<R> e;
+        nh_eval<R>(X, G, td.mat[s], td.mat[(size_t)T + s], vol, inv_h2, e);
+        double l0 = td.lambda[s], l1 = td.lambda[(size_t)T + s];
+        double a = fabs((double)e.CD), c = fabs((double)e.aD * l0);
+        double r0 = a - fmin(a, c);
+        a = fabs((double)e.CH); c = fabs((double)e.aH * l1);
+        double r1 = a - fmin(a, c);
+        acc[0] += r0 * r0 + r1 * r1;
+      } else {
+        Compliance<R> cm;
+        load_compliance<R, MAT>(td.mat, s, T, inv_h2, inv_h, cm, false);
+        R lam[6];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) lam[q] = td.lambda[(size_t)q * T + s];
+        acc[0] += stvk_residual<R>(X, G, vol, cm, lam);
+      }
+    }
+  } else {
+    int cb = blockIdx.x - tetBlocks, ncb = gridDim.x - tetBlocks;
+    for (int k = cb * blockDim.x + threadIdx.x; k < cd.K; k += ncb * blockDim.x) {
+      R4<R> p = pos[cd.vid[k]];
+      double n0 = cd.normal[k], n1 = cd.normal[cd.K + k], n2 = cd.normal[2 * cd.K + k];
+      double phi = n0 * ((double)p.x - cd.point[k]) + n1 * ((double)p.y - cd.point[cd.K + k]) +
+                   n2 * ((double)p.z - cd.point[2 * cd.K + k]);
+      if (phi > 0) phi = 0;
+      double a = fabs(contact_resistance * phi);
+      double c = fabs((cd.compliance[k] * inv_h2_d) * cd.lambda[k]);
+      double r = a - fmin(a, c);
+      acc[0] += r * r;
+    }
+  }
+  block_sum<1>(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc[0];
+}
+
+// Sums `n` partials in index order (one block) and writes sqrt of the sum.
+__global__ void __launch_bounds__(256) k_finish_norm(const double* __restrict__ partials, int n,
+                                                     double* __restrict__ out) {
+  double acc[1] = {0.0};
+  for (int i = threadIdx.x; i < n; i += blockDim.x) acc[0] += partials[i];
+  block_sum<1>(acc);
+  if (threadIdx.x == 0) *out = sqrt(acc[0]);
+}
+
+}  // namespace mlx

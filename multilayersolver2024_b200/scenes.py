@@ -1,0 +1,122 @@
+"""Synthetic scenes of the benchmark configurations (seeded, no datasets).
+
+``generate_beam`` follows the reference's cube-grid generator
+(3d/tools/meshReaders/generateBeam.m:1-41): vertices on a unit grid, six tets
+per cube with the same corner pattern.  Two deliberate differences, both
+required by the solver: the long axis is x (so the x = 0 face can be pinned),
+and a tet whose corner order gives det(Dm) < 0 has its last two corners
+swapped, because the reference's pattern leaves half the tets inverted and its
+mass/volume precompute assumes positive volumes.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from .mesh3d import Mesh3D, to_lame
+
+
+def generate_beam(nx: int, ny: int, nz: int, edge: float = 1.0, origin=(0.0, 0.0, 0.0)):
+    """Cube grid of nx*ny*nz cubes, 6 tets per cube.  Returns V (N, 3) and
+    1-based T (6*nx*ny*nz, 4) plus the (ix, iy, iz) cube of every tet."""
+    ix, iy, iz = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), np.arange(nz + 1), indexing="ij")
+    # vertex id = iz*(ny+1)*(nx+1) + iy*(nx+1) + ix (x fastest)
+    V = np.zeros(((nx + 1) * (ny + 1) * (nz + 1), 3))
+    vid = lambda a, b, c: c * (ny + 1) * (nx + 1) + b * (nx + 1) + a
+    V[vid(ix, iy, iz).ravel()] = np.stack([ix.ravel(), iy.ravel(), iz.ravel()], 1) * edge
+    V += np.asarray(origin, dtype=np.float64)
+    cx, cy, cz = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    # cubes in generateBeam's loop order: z outer, then y, then x
+    order = np.lexsort((cx.ravel(), cy.ravel(), cz.ravel()))
+    cx, cy, cz = cx.ravel()[order], cy.ravel()[order], cz.ravel()[order]
+    v1 = vid(cx, cy, cz); v2 = vid(cx + 1, cy, cz); v3 = vid(cx, cy + 1, cz); v4 = vid(cx + 1, cy + 1, cz)
+    v5 = vid(cx, cy, cz + 1); v6 = vid(cx + 1, cy, cz + 1); v7 = vid(cx, cy + 1, cz + 1)
+    v8 = vid(cx + 1, cy + 1, cz + 1)
+    pattern = [(v1, v2, v3, v6), (v2, v3, v4, v6), (v3, v5, v6, v7), (v3, v6, v7, v8), (v1, v3, v5, v6),
+               (v3, v4, v6, v8)]
+    T = np.stack([np.stack(p, 1) for p in pattern], 1).reshape(-1, 4)
+    cube = np.repeat(np.stack([cx, cy, cz], 1), 6, axis=0)
+    D = np.stack([V[T[:, k]] - V[T[:, 0]] for k in (1, 2, 3)], axis=2)
+    neg = np.linalg.det(D) < 0
+    T[neg, 2], T[neg, 3] = T[neg, 3].copy(), T[neg, 2].copy()
+    return V, (T + 1).astype(np.int32), cube
+
+
+def cluster_rigid_sets(cube: np.ndarray, dims, cluster: int, forced_elastic: np.ndarray) -> np.ndarray:
+    """Fixed rigid clusters of cluster^3 cubes for a coarse layer.  A cube on
+    an internal cluster seam (index % cluster == cluster-1, not on the outer
+    face) stays elastic, so neighbouring clusters never share a vertex and
+    each cluster is exactly one body; forced-elastic (pinned) tets stay
+    elastic as buildLayers does (xpbdLayer3D.m:614-615).  Body ids are
+    numbered 1.. by their first tet, as mexUnionFindByVertice's copyLayer."""
+    dims = np.asarray(dims)
+    seam = np.zeros(cube.shape[0], dtype=bool)
+    for a in range(3):
+        seam |= (cube[:, a] % cluster == cluster - 1) & (cube[:, a] != dims[a] - 1)
+    key = (cube[:, 0] // cluster) + (dims[0] // cluster + 1) * (
+        (cube[:, 1] // cluster) + (dims[1] // cluster + 1) * (cube[:, 2] // cluster))
+    rigid = ~seam & ~forced_elastic
+    sets = np.zeros(cube.shape[0], dtype=np.int32)
+    label = {}
+    for e in np.nonzero(rigid)[0]:
+        k = int(key[e])
+        if k not in label:
+            label[k] = len(label) + 1
+        sets[e] = label[k]
+    return sets
+
+
+@dataclass
+class Scene:
+    name: str
+    mesh: Mesh3D
+    h: float
+    steps: int
+    layers: list
+    iterations: list
+    gravity: float = -9.81
+    custom_sets: np.ndarray = None       # (T, Lsorted) fixed rigid sets, or None
+    contact_finders: list = field(default_factory=list)
+    impulse: tuple = None                # (dofs 1-based, dv) applied before step 1
+    settings: dict = field(default_factory=dict)
+
+
+def config1(energy=_lib.MLX_ENERGY_STVK_VOIGT) -> Scene:
+    """Plain single-layer XPBD cantilever: 8x2x2 cubes of 0.1 m (81 vertices,
+    192 tets), E = 1e5, nu = 0.3, rho = 1000, x = 0 face pinned, dt = 0.01,
+    20 iterations, layers [0], 200 steps, undamped (alpha1 = 0)."""
+    V, T, cube = generate_beam(8, 2, 2, 0.1)
+    mu, lam = to_lame(0.3, 1e5)
+    m = Mesh3D.from_arrays(V, T, mu, lam, rho=1000.0, alpha1=0.0, energy_type=energy)
+    m.pin(np.nonzero(np.isclose(V[:, 0], 0.0))[0] + 1)
+    return Scene("config1_cantilever_8x2x2", m, 0.01, 200, [0], [20])
+
+
+def config2(seed: int = 2, nx=64, ny=16, nz=16, cluster=8) -> Scene:
+    """Plain multi-layer Neo-Hookean block: 64x16x16 cubes (18,785 vertices,
+    98,304 tets), per-tet E log-uniform in [1e4, 1e7], nu uniform in
+    [0.25, 0.45], coarse layer of fixed 8^3-cube rigid clusters then the fine
+    layer, 5 coarse + 10 fine iterations, dt = 1/60, base (z = 0) pinned,
+    seeded random surface impulse at t = 0, 300 steps."""
+    rng = np.random.default_rng(seed)
+    V, T, cube = generate_beam(nx, ny, nz, 0.1)
+    nt = T.shape[0]
+    E = np.exp(rng.uniform(np.log(1e4), np.log(1e7), nt))
+    nu = rng.uniform(0.25, 0.45, nt)
+    mu, lam = to_lame(nu, E)
+    m = Mesh3D.from_arrays(V, T, mu, lam, rho=1000.0, alpha1=0.0, energy_type=_lib.MLX_ENERGY_NEOHOOKEAN)
+    m.pin(np.nonzero(np.isclose(V[:, 2], 0.0))[0] + 1)
+    forced = np.zeros(nt, dtype=bool)
+    forced[m.pinnedTets - 1] = True
+    coarse = cluster_rigid_sets(cube, (nx, ny, nz), cluster, forced)
+    sets = np.asfortranarray(np.stack([np.zeros(nt, np.int32), coarse], 1))  # sorted columns: [fine, coarse]
+    # impulse: random velocity on a seeded patch of the top surface
+    top = np.nonzero(np.isclose(V[:, 2], nz * 0.1))[0]
+    c = V[top[rng.integers(len(top))]]
+    patch = top[np.linalg.norm(V[top, :2] - c[:2], axis=1) < 0.4]
+    dv = rng.normal(0.0, 1.0, (len(patch), 3)) * 0.5 + np.array([0.0, 0.0, -2.0])
+    dofs = np.stack([patch * 3 + 1, patch * 3 + 2, patch * 3 + 3], 1).ravel().astype(np.int32)
+    return Scene("config2_nh_block_64x16x16", m, 1.0 / 60.0, 300, [50, 0], [5, 10], custom_sets=sets,
+                 impulse=(dofs, dv.ravel()))

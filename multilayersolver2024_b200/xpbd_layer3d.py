@@ -1,0 +1,454 @@
+"""Host-side mirror of the reference integrator ``xpbdLayer3D``.
+
+Same property names and defaults (3d/integrator/xpbdLayer3D.m:5-40,
+2d/integrator/Integrator.m:17-27), same ``setLayers`` / ``buildLayers`` /
+``integrate`` flow (xpbdLayer3D.m:595-745), and a static ``layerSolve`` with
+the reference's argument order (xpbdLayer3D.m:44-93).  ``layerSolve`` runs on
+the GPU through the C ABI (include/mlxpbd.h); there is no CPU fallback: if the
+native library or the device is missing the call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import (Contacts, LayerDesc, MeshDesc, SolveInputs, SolveOutputs, SolveParams, check, f64, i32,
+                   load, u8)
+from .mesh3d import Mesh3D
+
+
+def _F(a, dtype):
+    return np.asfortranarray(np.asarray(a, dtype=dtype))
+
+
+@dataclass
+class LayerSet:
+    """buildLayers + findBoundaryVertices output (xpbdLayer3D.m:646-652)."""
+
+    rigidBodySetsPerLayer: np.ndarray   # (T, Ls) int32, Fortran order
+    numRigids: np.ndarray               # (Ls,) int32
+    isRigidElement: np.ndarray          # (T, Ls) uint8
+    isElasticElement: np.ndarray        # (T, Ls) uint8
+    isBoundaryVertex: np.ndarray        # (N, Ls) uint8
+    isRigidVertex: np.ndarray           # (N, Ls) uint8
+    vertexRigidBody: np.ndarray         # (N, Ls) int32
+
+
+def find_boundary_vertices(mesh: Mesh3D, sets: np.ndarray, num_rigids) -> LayerSet:
+    """xpbdLayer2D.findBoundaryVertices through the native helper."""
+    lib = load()
+    sets = _F(sets, np.int32)
+    T, L = sets.shape
+    N = mesh.N
+    bnd = np.zeros((N, L), np.uint8, order="F")
+    ela = np.zeros((T, L), np.uint8, order="F")
+    rig = np.zeros((N, L), np.uint8, order="F")
+    vb = np.zeros((N, L), np.int32, order="F")
+    check("mlx_find_boundary_vertices",
+          lib.mlx_find_boundary_vertices(i32(mesh.t), T, N, i32(sets), L, u8(bnd), u8(ela), u8(rig), i32(vb)))
+    return LayerSet(sets, np.asarray(num_rigids, np.int32), _F(sets != 0, np.uint8), ela, bnd, rig, vb)
+
+
+def strain_rate_norms(mesh: Mesh3D, p, oldp, h) -> np.ndarray:
+    lib = load()
+    out = np.zeros(mesh.T)
+    check("mlx_strain_rate_norms",
+          lib.mlx_strain_rate_norms(i32(mesh.t), mesh.T, f64(mesh.DmInv), f64(np.ascontiguousarray(p)),
+                                    f64(np.ascontiguousarray(oldp)), float(h), f64(out)))
+    return out
+
+
+def union_find_layers(mesh: Mesh3D, order, sorted_layers, forced_elastic):
+    lib = load()
+    order = np.ascontiguousarray(order, dtype=np.int32)
+    sl = np.ascontiguousarray(sorted_layers, dtype=np.float64)
+    fe = np.ascontiguousarray(forced_elastic, dtype=np.uint8)
+    sets = np.zeros((mesh.T, sl.size), np.int32, order="F")
+    nr = np.zeros(sl.size, np.int32)
+    check("mlx_union_find_layers",
+          lib.mlx_union_find_layers(i32(order), mesh.T, f64(sl), sl.size, u8(fe), i32(mesh.t), mesh.N,
+                                    i32(sets), i32(nr)))
+    return sets, nr
+
+
+def mesh_desc(mesh: Mesh3D, precision=_lib.MLX_FP32, device=0, material="blocks"):
+    """The mlx_mesh_desc of a mesh; returns (desc, arrays to keep alive)."""
+    keep = {}
+
+    def k(name, a):
+        keep[name] = a
+        return a
+
+    d = MeshDesc()
+    d.num_vertices = mesh.N
+    d.num_tets = mesh.T
+    d.t = i32(k("t", _F(mesh.t, np.int32)))
+    d.mass = f64(k("mass", np.ascontiguousarray(mesh.mass)))
+    d.DmInv = f64(k("DmInv", np.ascontiguousarray(mesh.DmInv)))
+    d.volume = f64(k("vol", np.ascontiguousarray(mesh.elV)))
+    d.element_color = i32(k("color", np.ascontiguousarray(mesh.elementColor, np.int32)))
+    d.num_colors = mesh.numColors
+    d.pinned_dofs = i32(k("pin", np.ascontiguousarray(mesh.pinnedDOFs, np.int32)))
+    d.num_pinned_dofs = int(mesh.pinnedDOFs.size)
+    d.energy_type = mesh.energy_type
+    if mesh.energy_type == _lib.MLX_ENERGY_STVK_VOIGT and material == "blocks":
+        d.alpha = f64(k("alpha", np.ascontiguousarray(mesh.perElementXPBDalphaMatrix)))
+        d.beta = f64(k("beta", np.ascontiguousarray(mesh.perElementXPBDbeta)))
+    else:
+        d.mu = f64(k("mu", np.ascontiguousarray(mesh.mu)))
+        d.lambda_ = f64(k("lam", np.ascontiguousarray(mesh.lam)))
+        d.alpha1 = f64(k("a1", np.ascontiguousarray(mesh.alpha1)))
+    d.precision = precision
+    d.device = device
+    return d, keep
+
+
+class Solver:
+    """A device-resident copy of one mesh (``mlx_create``)."""
+
+    def __init__(self, mesh: Mesh3D, precision=_lib.MLX_FP32, device=0, material="blocks"):
+        lib = load()
+        self._lib = lib
+        self.mesh = mesh
+        self.precision = precision
+        d, keep = mesh_desc(mesh, precision, device, material)
+        h = C.c_void_p()
+        check("mlx_create", lib.mlx_create(C.byref(d), C.byref(h)), lib)
+        self.handle = h
+
+    def close(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            self._lib.mlx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ResidentSim:
+    """Device-resident stepping of one mesh (``mlx_sim_*``): the integrate step
+    of xpbdLayer3D with a fixed layer description and the state kept on the GPU."""
+
+    def __init__(self, solver: Solver, integ: "XpbdLayer3D", ls: LayerSet, h: float, p0=None, v0=None):
+        self.solver = solver
+        self._lib = solver._lib
+        mesh = solver.mesh
+        self._ld, self._keep = pack_layer_desc(ls, integ.layersMap, integ.iterations)
+        P = make_params(integ, h)
+        p0 = np.ascontiguousarray(mesh.p if p0 is None else p0, np.float64)
+        v0 = np.ascontiguousarray(mesh.v if v0 is None else v0, np.float64)
+        check("mlx_sim_init", self._lib.mlx_sim_init(solver.handle, C.byref(self._ld), C.byref(P), f64(p0), f64(v0),
+                                                      float(integ.airDrag)), self._lib)
+
+    def add_velocity(self, dofs, dv):
+        d = np.ascontiguousarray(dofs, np.int32)
+        v = np.ascontiguousarray(dv, np.float64)
+        check("mlx_sim_add_velocity", self._lib.mlx_sim_add_velocity(self.solver.handle, i32(d), f64(v), d.size),
+              self._lib)
+
+    def step(self, n=1, graph=True, timed=False):
+        ms = C.c_double(0.0)
+        check("mlx_sim_step", self._lib.mlx_sim_step(self.solver.handle, int(n), int(bool(graph)),
+                                                      C.byref(ms) if timed else None), self._lib)
+        return ms.value if timed else None
+
+    def state(self):
+        N = self.solver.mesh.N
+        p, v = np.zeros(3 * N), np.zeros(3 * N)
+        check("mlx_sim_get_state", self._lib.mlx_sim_get_state(self.solver.handle, f64(p), f64(v)), self._lib)
+        return p, v
+
+    def sweep_timing(self, on=True):
+        check("mlx_sim_sweep_timing", self._lib.mlx_sim_sweep_timing(self.solver.handle, int(bool(on))), self._lib)
+
+    def sweep_stats(self, reset=True):
+        ms, b, n = C.c_double(), C.c_double(), C.c_longlong()
+        check("mlx_sim_sweep_stats", self._lib.mlx_sim_sweep_stats(self.solver.handle, C.byref(ms), C.byref(b),
+                                                                    C.byref(n), int(bool(reset))), self._lib)
+        return ms.value, b.value, n.value
+
+    @property
+    def launches_per_step(self):
+        return int(self._lib.mlx_sim_launches_per_step(self.solver.handle))
+
+
+def pack_layer_desc(ls: LayerSet, layersMap, iterations):
+    keep = [ls]
+    lm = np.ascontiguousarray(layersMap, np.int32)
+    it = np.ascontiguousarray(iterations, np.int32)
+    keep += [lm, it]
+    d = LayerDesc()
+    d.num_layers = lm.size
+    d.num_columns = ls.rigidBodySetsPerLayer.shape[1]
+    d.layers_map = i32(lm)
+    d.iterations = i32(it)
+    d.is_elastic_element = u8(ls.isElasticElement)
+    d.is_rigid_element = u8(ls.isRigidElement)
+    d.rigid_body_sets = i32(ls.rigidBodySetsPerLayer)
+    d.vertex_rigid_body = i32(ls.vertexRigidBody)
+    d.is_boundary_vertex = u8(ls.isBoundaryVertex)
+    d.is_rigid_vertex = u8(ls.isRigidVertex)
+    nr = np.ascontiguousarray(ls.numRigids, np.int32)
+    keep.append(nr)
+    d.num_rigids = i32(nr)
+    return d, keep
+
+
+def pack_contacts(normals, points, vertex_ids, compliance):
+    c = Contacts()
+    K = 0 if vertex_ids is None else int(np.asarray(vertex_ids).size)
+    keep = []
+    c.num_contacts = K
+    if K:
+        n = _F(np.asarray(normals).reshape(K, 3), np.float64)
+        p = _F(np.asarray(points).reshape(K, 3), np.float64)
+        v = np.ascontiguousarray(vertex_ids, np.int32).ravel()
+        a = np.ascontiguousarray(compliance, np.float64).ravel()
+        keep = [n, p, v, a]
+        c.normals, c.point_colliders, c.vertex_ids, c.compliance = f64(n), f64(p), i32(v), f64(a)
+    return c, keep
+
+
+def make_params(integ: "XpbdLayer3D", h: float) -> SolveParams:
+    P = SolveParams()
+    P.h = h
+    P.boundary_compliance = integ.boundaryCompliance
+    P.contact_resistance = integ.contactResistance
+    P.run_until = integ.runUntilResSmallerThan
+    P.give_up_threshold = integ.giveUpThreshold
+    P.gravity_compliance = integ.gravityCompliance
+    P.gravity = integ.Gravity
+    P.stop_at_improvement_percent = integ.StopAtImprovementPercent
+    P.compute_residuals = int(bool(integ.computeResiduals))
+    P.hanging_stop = int(integ.hangingStop)
+    P.give_up_enabled = int(bool(integ.giveUpEnabled))
+    P.last_layer_give_up_enabled = int(bool(integ.LastLayerGiveUpEnabled))
+    P.use_gravity_constraints = int(bool(integ.useGravityConstraints))
+    P.use_rigid_contacts = int(bool(integ.useRigidContacts))
+    return P
+
+
+def call_layer_solve(fn, solver_or_desc, layer_desc, params, contacts, xi, lambdai, oldp, oldOldp, f,
+                     residualv, pinnedx, residual_in, sum_non_monitored_time=0.0, want_lambda=False,
+                     residual_capacity=None):
+    """Marshal one layerSolve call for ``fn`` (mlx_layer_solve or the same
+    signature); returns (xi, sumNonMonitoredTime, residualArray, runUntil,
+    lambdai or None, total_iterations)."""
+    N3 = xi.size
+    keep = []
+    arr = lambda a, dt=np.float64: keep.append(np.ascontiguousarray(a, dt)) or keep[-1]
+    xi_ = arr(xi); lam_ = _F(lambdai, np.float64); keep.append(lam_)
+    oldp_ = arr(oldp); oo_ = arr(oldOldp); f_ = arr(f); rv_ = arr(residualv)
+    px_ = arr(pinnedx if pinnedx is not None else np.zeros(0)); rin = arr(residual_in)
+    inp = SolveInputs()
+    inp.xi, inp.lambdai, inp.oldp, inp.old_oldp, inp.f = f64(xi_), f64(lam_), f64(oldp_), f64(oo_), f64(f_)
+    inp.residualv, inp.pinnedx, inp.residual_in = f64(rv_), f64(px_), f64(rin)
+    inp.residual_in_len = rin.size
+    inp.sum_non_monitored_time = sum_non_monitored_time
+    cap = residual_capacity or (rin.size + 1 + max(0, params.hanging_stop if params.hanging_stop >= 0 else 0) +
+                                sum(int(layer_desc.iterations[i]) for i in range(layer_desc.num_layers)) + 100000)
+    out_xi = np.zeros(N3)
+    out_lam = np.zeros(lam_.shape, order="F") if want_lambda else None
+    out_res = np.zeros(cap)
+    out = SolveOutputs()
+    out.xi = f64(out_xi)
+    out.lambdai = f64(out_lam)
+    out.residual = f64(out_res)
+    out.residual_capacity = cap
+    rc = fn(solver_or_desc, C.byref(layer_desc), C.byref(params), C.byref(contacts), C.byref(inp), C.byref(out))
+    return rc, (out_xi, out.sum_non_monitored_time, out_res[:out.residual_len].copy(), out.run_until,
+                out_lam, out.total_iterations)
+
+
+@dataclass
+class StepCache:
+    """The per-mesh cache fields integrate touches (3d/tools/solve/setupCache.m:41-42)."""
+
+    oldp: np.ndarray = None
+    oldOldp: np.ndarray = None
+    residualArray: np.ndarray = None
+    layers: np.ndarray = None
+
+
+@dataclass
+class ContactSet:
+    normals: np.ndarray = field(default_factory=lambda: np.zeros((0, 3)))
+    points: np.ndarray = field(default_factory=lambda: np.zeros((0, 3)))
+    vertex_ids: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    compliance: np.ndarray = field(default_factory=lambda: np.zeros(0))
+
+    @staticmethod
+    def concat(sets):
+        sets = [s for s in sets if s is not None and s.vertex_ids.size]
+        if not sets:
+            return ContactSet()
+        return ContactSet(np.concatenate([s.normals for s in sets]), np.concatenate([s.points for s in sets]),
+                          np.concatenate([s.vertex_ids for s in sets]).astype(np.int32),
+                          np.concatenate([s.compliance for s in sets]))
+
+
+def contact_velocity_update(normals, vertex_ids, v, h, gravity, dim=3, restitution=1e-5):
+    """xpbdLayer2D.contactVelocityUpdate (2d/integrator/xpbdLayer2D.m:577-603)."""
+    K = normals.shape[0]
+    if K == 0:
+        return v
+    e = np.full(K, restitution)
+    dofs = (np.asarray(vertex_ids, np.int64)[:, None] * dim - np.arange(dim - 1, -1, -1)[None, :]) - 1
+    vn = v[dofs]
+    e[np.linalg.norm(vn, axis=1) <= 2 * gravity * h] = 0
+    vt = np.sum(normals * vn, axis=1)
+    dv = normals * (-vn + np.minimum(-e * vt, 0)[:, None])
+    v = v.copy()
+    v[dofs] = vn + dv
+    return v
+
+
+class XpbdLayer3D:
+    """xpbdLayer3D: the multi-layer XPBD integrator."""
+
+    def __init__(self):
+        # Integrator base (2d/integrator/Integrator.m:17-27)
+        self.Gravity = -9.8
+        self.CustomForce = 0.0
+        # xpbdLayer3D properties (xpbdLayer3D.m:5-40)
+        self.iterations = [10]
+        self.layers = [0]
+        self.sortedLayers = [0]
+        self.layersMap = [1]
+        self.boundaryCompliance = 1e-8
+        self.computeResiduals = False
+        self.energyType = 2
+        self.giveUpEnabled = False
+        self.LastLayerGiveUpEnabled = False
+        self.giveUpThreshold = 0.0
+        self.contactResistance = 0.5
+        self.gravityCompliance = 0.001
+        self.LayerOrderingType = 0
+        self.runUntilResSmallerThan = -1.0
+        self.hangingStop = 1000
+        self.useGravityConstraints = True
+        self.runOnGPU = True
+        self.airDrag = 0.0
+        self.useRigidContacts = True
+        self.StopAtImprovementPercent = 0.0
+        self.pinnedx = None
+        # fixed rigid sets per sorted layer column (LayerOrderingType 4, "custom")
+        self.customRigidSets = None
+        self.rng = np.random.default_rng(0)
+        self.precision = _lib.MLX_FP32
+        self.device = 0
+        self._solvers = {}
+        self.last_total_iterations = 0
+
+    def setLayers(self, layers):
+        """xpbdLayer3D.setLayers (:595-599): sortedLayers = unique(layers),
+        layersMap = its inverse index (1-based)."""
+        self.layers = list(layers)
+        s, ic = np.unique(np.asarray(layers, dtype=np.float64), return_inverse=True)
+        self.sortedLayers = s.tolist()
+        self.layersMap = (ic + 1).astype(np.int32).tolist()
+
+    def solver(self, mesh: Mesh3D) -> Solver:
+        key = id(mesh)
+        s = self._solvers.get(key)
+        if s is None or s.mesh is not mesh:
+            s = Solver(mesh, precision=self.precision, device=self.device)
+            self._solvers[key] = s
+        return s
+
+    def buildLayers(self, mesh: Mesh3D, cache: StepCache, h: float):
+        """xpbdLayer3D.buildLayers (:601-619)."""
+        if self.customRigidSets is not None:
+            sets = _F(self.customRigidSets, np.int32)
+            return sets, np.asarray([int(sets[:, c].max(initial=0)) for c in range(sets.shape[1])], np.int32)
+        if self.LayerOrderingType == 1:
+            order = self.rng.permutation(mesh.T) + 1
+        else:
+            norms = strain_rate_norms(mesh, mesh.p, cache.oldp, h)
+            order = np.argsort(norms, kind="stable") + 1
+        forced = np.zeros(mesh.T, np.uint8)
+        forced[mesh.pinnedTets - 1] = 1
+        return union_find_layers(mesh, order, self.sortedLayers, forced)
+
+    @staticmethod
+    def layerSolve(isElasticElement, isRigidElement, rigidBodySetsPerLayer, vertexRigidBody, isBoundaryVertex,
+                   isRigidVertex, xi, lambdai, sumNonMonitoredTime, h, numRigids, residualArray,
+                   boundaryCompliance, contactResistance, contactCompliance, iterations, layers,
+                   runUntilResSmallerThan, computeResiduals, hangingStop, giveUpEnabled, giveUpThreshold,
+                   LastLayerGiveUpEnabled, useGravityConstraints, oldp, oldOldp, contactNormals, pointColliders,
+                   contactVertexID, mass, T, unpinnedDOFs, pinnedDOFs, DmInv, perElementXPBDalphaMatrix,
+                   perElementXPBDalphaInvMatrix, elementColor, elementDOFs, numColors, f, layersMap,
+                   gravityCompliance, gravity, residualv, perElementXPBDBeta, volume, runOnGPU, useRigidContacts,
+                   StopAtImprovementPercent, pinnedx, *, solver: Solver):
+        """xpbdLayer3D.layerSolve (xpbdLayer3D.m:44-232) on the GPU.  Argument
+        order and meaning as the reference; the mesh arrays must be those the
+        ``solver`` was created from.  Returns (xi, sumNonMonitoredTime,
+        residualArray, runUntilResSmallerThan)."""
+        ls = LayerSet(_F(rigidBodySetsPerLayer, np.int32), np.asarray(numRigids, np.int32),
+                      _F(isRigidElement, np.uint8), _F(isElasticElement, np.uint8), _F(isBoundaryVertex, np.uint8),
+                      _F(isRigidVertex, np.uint8), _F(vertexRigidBody, np.int32))
+        ld, keep = pack_layer_desc(ls, layersMap, iterations)
+        P = SolveParams()
+        P.h, P.boundary_compliance, P.contact_resistance = h, boundaryCompliance, contactResistance
+        P.run_until, P.give_up_threshold = runUntilResSmallerThan, giveUpThreshold
+        P.gravity_compliance, P.gravity = gravityCompliance, gravity
+        P.stop_at_improvement_percent = StopAtImprovementPercent
+        P.compute_residuals, P.hanging_stop = int(bool(computeResiduals)), int(hangingStop)
+        P.give_up_enabled, P.last_layer_give_up_enabled = int(bool(giveUpEnabled)), int(bool(LastLayerGiveUpEnabled))
+        P.use_gravity_constraints, P.use_rigid_contacts = int(bool(useGravityConstraints)), int(bool(useRigidContacts))
+        cts, keep2 = pack_contacts(contactNormals, pointColliders, contactVertexID,
+                                   np.asarray(contactCompliance).ravel())
+        lib = load()
+        rc, res = call_layer_solve(lib.mlx_layer_solve, solver.handle, ld, P, cts, xi, lambdai, oldp, oldOldp, f,
+                                   residualv, pinnedx, residualArray, sumNonMonitoredTime)
+        check("mlx_layer_solve", rc, lib)
+        return res[0], res[1], res[2], res[3]
+
+    def integrate(self, mesh: Mesh3D, h: float, contacts: ContactSet, cache: StepCache, frame: int):
+        """xpbdLayer3D.integrate (xpbdLayer3D.m:621-745)."""
+        assert len(self.layers) and len(self.iterations)
+        assert self.boundaryCompliance < 1e-5
+        sumNonMonitoredTime = 0.0
+        if cache.oldp is None or np.any(np.isnan(cache.oldp)) or frame == 1:
+            cache.oldp = mesh.p.copy()
+            self.pinnedx = mesh.p[mesh.pinnedDOFs - 1].copy()
+        tic = time.perf_counter()
+        f = np.zeros(3 * mesh.N)
+        f[2::3] = f[2::3] + mesh.mass[2::3] * self.Gravity
+        f = f + self.CustomForce
+        mesh.f = f
+        sets, numRigids = self.buildLayers(mesh, cache, h)
+        ls = find_boundary_vertices(mesh, sets, numRigids)
+        cache.layers = ls.isRigidElement
+        cache.oldOldp = cache.oldp
+        cache.oldp = mesh.p.copy()
+        xi = mesh.p.copy()
+        resv = mesh.v.copy()
+        up = mesh.unpinnedDOFs - 1
+        resv[up] = resv[up] + h * f[up] / mesh.mass[up]
+        resv = (1 - self.airDrag) * resv
+        lambdai = np.zeros((mesh.T, 6), order="F")
+        residualArray = np.array([0.0])
+        ld, keep = pack_layer_desc(ls, self.layersMap, self.iterations)
+        cts, keep2 = pack_contacts(contacts.normals, contacts.points, contacts.vertex_ids, contacts.compliance)
+        lib = load()
+        rc, res = call_layer_solve(lib.mlx_layer_solve, self.solver(mesh).handle, ld, make_params(self, h), cts,
+                                   xi, lambdai, cache.oldp, cache.oldOldp, f, resv, self.pinnedx, residualArray,
+                                   sumNonMonitoredTime)
+        check("mlx_layer_solve", rc, lib)
+        xi, sumNonMonitoredTime, residualArray, self.runUntilResSmallerThan = res[0], res[1], res[2], res[3]
+        self.last_total_iterations = res[5]
+        cache.residualArray = residualArray[1:]
+        mesh.v = (xi - cache.oldp) / h
+        mesh.p = xi
+        mesh.v = contact_velocity_update(contacts.normals, contacts.vertex_ids, mesh.v, h, self.Gravity, 3, 1e-2)
+        integrate_forces = time.perf_counter() - tic - sumNonMonitoredTime
+        return {"integrateForces": integrate_forces, "residual": float(residualArray[-1]),
+                "residualPreSolve": float(residualArray[0]), "iterations": res[5]}

@@ -1,0 +1,125 @@
+"""Parity of the CUDA layerSolve (through the C ABI) with the CPU oracle.
+
+Every case feeds identical inputs to both sides.  Tolerances:
+  FP64 product vs FP64 oracle: max |dx| <= 1e-9 of the bounding-box diagonal
+    (same algorithm, different summation order in reductions);
+  FP32 product vs FP64 oracle, one layerSolve call: <= 2e-5 of the diagonal.
+"""
+import numpy as np
+import pytest
+
+from multilayersolver2024_b200 import _lib
+from multilayersolver2024_b200.xpbd_layer3d import ContactSet, Solver
+
+from helpers import Case, block_mesh, plane_contacts, rel_pos_err, sphere_contacts
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-9
+TOL32 = 2e-5
+
+
+def _contacts(case):
+    p = case.xi
+    return ContactSet.concat([plane_contacts(p, [0, 0, 1.0], [0, 0, 0.004]),
+                              sphere_contacts(p, 0.12, [0.45, 0.15, 0.3])])
+
+
+def _compare(case, prec=_lib.MLX_FP64, material="blocks", tol=TOL64):
+    got = case.product(prec, material)
+    ref = case.oracle(material)
+    err = rel_pos_err(got[0], ref[0], case.mesh)
+    assert err <= tol, f"position error {err:.3e} > {tol:.1e}"
+    return got, ref
+
+
+@pytest.mark.parametrize("energy", [_lib.MLX_ENERGY_STVK_VOIGT, _lib.MLX_ENERGY_NEOHOOKEAN])
+def test_single_layer_fp64(gpu, energy):
+    m = block_mesh(energy=energy, alpha1=0.01 if energy == _lib.MLX_ENERGY_STVK_VOIGT else 0.0)
+    case = Case(m, [0], [12], seed=1)
+    got, ref = _compare(case)
+    lam_err = np.abs(got[4] - ref[4]).max() / max(np.abs(ref[4]).max(), 1e-30)
+    assert lam_err <= 1e-8
+    assert got[5] == ref[5] == 12
+
+
+@pytest.mark.parametrize("energy", [_lib.MLX_ENERGY_STVK_VOIGT, _lib.MLX_ENERGY_NEOHOOKEAN])
+@pytest.mark.parametrize("rigid_contacts", [True, False])
+def test_multilayer_bodies_contacts_fp64(gpu, energy, rigid_contacts):
+    m = block_mesh(dims=(8, 3, 3), energy=energy, seed=2)
+    case = Case(m, [50, 25, 0], [2, 3, 6], seed=3)
+    case.integ.boundaryCompliance = 0.0
+    case.integ.useRigidContacts = rigid_contacts
+    case.integ.contactResistance = 0.9
+    case.contacts = _contacts(case)
+    assert case.contacts.vertex_ids.size > 0
+    assert case.ls.numRigids.max() > 0 and case.ls.isBoundaryVertex.any()
+    _compare(case)
+
+
+def test_residual_monitor_and_stop_rules_fp64(gpu):
+    """computeResiduals + StopAtImprovementPercent + runUntil + hangingStop +
+    give-up: identical residual arrays, iteration counts and runUntil."""
+    m = block_mesh(dims=(6, 3, 3), seed=4)
+    case = Case(m, [60, 30, 0], [3, 3, 4], seed=5)
+    integ = case.integ
+    integ.computeResiduals = True
+    integ.StopAtImprovementPercent = 60
+    integ.runUntilResSmallerThan = 0.0
+    integ.hangingStop = 40
+    integ.giveUpEnabled = True
+    case.contacts = _contacts(case)
+    got, ref = _compare(case)
+    assert got[5] == ref[5], (got[5], ref[5])
+    assert got[2].size == ref[2].size
+    np.testing.assert_allclose(got[2], ref[2], rtol=1e-9, atol=1e-14)
+    np.testing.assert_allclose(got[3], ref[3], rtol=1e-9)
+
+
+def test_lame_material_form_matches_blocks_fp64(gpu):
+    m = block_mesh(alpha1=0.02, seed=6)
+    case = Case(m, [40, 0], [3, 6], seed=7)
+    a = case.product(_lib.MLX_FP64, "lame")
+    b = case.oracle("blocks")
+    assert rel_pos_err(a[0], b[0], m) <= 1e-9
+
+
+@pytest.mark.parametrize("energy", [_lib.MLX_ENERGY_STVK_VOIGT, _lib.MLX_ENERGY_NEOHOOKEAN])
+def test_multilayer_fp32_within_tolerance(gpu, energy):
+    m = block_mesh(dims=(8, 3, 3), energy=energy, seed=8)
+    case = Case(m, [50, 0], [3, 8], seed=9)
+    case.integ.boundaryCompliance = 0.0
+    case.contacts = _contacts(case)
+    _compare(case, prec=_lib.MLX_FP32, material="lame", tol=TOL32)
+
+
+def test_solver_reuse_across_calls(gpu):
+    """Cached layer descriptions are refreshed when the layer masks change."""
+    m = block_mesh(seed=10)
+    s = Solver(m, precision=_lib.MLX_FP64)
+    c1 = Case(m, [50, 0], [2, 4], seed=11)
+    c2 = Case(m, [50, 0], [2, 4], seed=12)
+    for c in (c1, c2, c1):
+        got = c.product(solver=s)
+        ref = c.oracle()
+        assert rel_pos_err(got[0], ref[0], m) <= TOL64
+
+
+def test_errors_are_reported(gpu, lib):
+    import ctypes as C
+    from multilayersolver2024_b200.xpbd_layer3d import mesh_desc
+    m = block_mesh(seed=13)
+    bad = m.elementColor.copy()
+    bad[:] = 1
+    d, keep = mesh_desc(m, 1, 0)
+    keep["c"] = np.ascontiguousarray(bad, np.int32)
+    d.element_color = _lib.i32(keep["c"])
+    h = C.c_void_p()
+    rc = lib.mlx_create(C.byref(d), C.byref(h))
+    assert rc == _lib.MLX_ERR_ARGUMENT if hasattr(_lib, "MLX_ERR_ARGUMENT") else rc == 1
+    assert b"colouring" in lib.mlx_last_error()
+    case = Case(m, [0], [3], seed=14)
+    case.integ.runUntilResSmallerThan = 1e-3
+    case.integ.computeResiduals = False
+    rc, _ = case.run(lib.mlx_layer_solve, Solver(m, precision=_lib.MLX_FP64).handle)
+    assert rc == 1 and b"compute_residuals" in lib.mlx_last_error()
