@@ -173,6 +173,14 @@ struct LayerStatic {
 
 namespace mlx {
 
+// Layer caches and body buffers one caller of the layer loop owns: the
+// host-buffer layerSolve and the resident stepper each have their own, so a
+// captured step graph never points at memory the other path reallocates.
+struct LayerWork {
+  std::vector<std::unique_ptr<LayerStatic>> cache;
+  DevBuf bodies, lamB;
+};
+
 // Per-call bookkeeping of the layer loop (the scalars layerSolve threads
 // through projectGS, xpbdLayer3D.m:94-232).
 struct RunState {
@@ -193,10 +201,10 @@ struct Solver final : SolverBase {
   std::vector<int32_t> pinned;  // 0-based DOFs
   std::vector<double> vmass_h, mass3;
   DevBuf d_vid, d_dminv, d_vol, d_mat, d_lambda, d_pos, d_oldp, d_xprev, d_resv, d_vmass, d_ri,
-      d_bodies, d_lamB, d_pin_dofs, d_pinx, d_partials, d_scalar, d_stage, d_s2e, d_mass3,
+      d_pin_dofs, d_pinx, d_partials, d_scalar, d_stage, d_s2e, d_mass3,
       d_contacts, d_cvid, d_clam, d_cgroups;
   PinnedBuf h_stage, h_scalar, h_cstage;
-  std::vector<std::unique_ptr<LayerStatic>> cache;
+  LayerWork work, sim_work;
 
   ~Solver() override {
     for (cudaEvent_t e : tev) cudaEventDestroy(e);
@@ -227,7 +235,7 @@ struct Solver final : SolverBase {
   int validate_layers(const mlx_layer_desc* ld, const mlx_solve_params* P);
   int upload_contacts(const mlx_contacts* K, ContactData& cd);
   int run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, const mlx_contacts* K,
-                 const ContactData& cd, RunState& st, bool capturing);
+                 const ContactData& cd, RunState& st, bool capturing, LayerWork& w);
 
   // resident stepper (one per solver)
   struct Sim {
@@ -643,7 +651,7 @@ int Solver<R>::upload_contacts(const mlx_contacts* K, ContactData& cd) {
 // refused in that mode.
 template <typename R>
 int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, const mlx_contacts* K,
-                          const ContactData& cd, RunState& st, bool capturing) {
+                          const ContactData& cd, RunState& st, bool capturing, LayerWork& w) {
   if (capturing && P->compute_residuals)
     return set_error(MLX_ERR_UNSUPPORTED, "residual monitoring cannot run inside a captured step");
   const double h = P->h;
@@ -651,14 +659,14 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
   const int nK = cd.K;
   const size_t np = pinned.size();
   bool errorChangeDecreased = false;
-  while ((int)cache.size() < ld->num_columns) cache.emplace_back(new LayerStatic());
+  while ((int)w.cache.size() < ld->num_columns) w.cache.emplace_back(new LayerStatic());
   const long long kSafetyIterations = 100000000LL;
 
   for (int layer = 0; layer < ld->num_layers; ++layer) {
     double setPercentStop = layer == 0 ? P->stop_at_improvement_percent : 0;
     bool isLast = layer == ld->num_layers - 1;
     int col = ld->layers_map[layer] - 1;
-    LayerStatic& ls = *cache[col];
+    LayerStatic& ls = *w.cache[col];
     CHECK(build_static(ld, col, ls, capturing));
     const int* dint = ls.dev.as<int>();
     LayerDev L{};
@@ -730,9 +738,9 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
     double4* ri = d_ri.as<double4>();
     if (rigidLayer && ls.nb > 0) CU(cudaMemcpyAsync(xprev, p, sizeof(R4<R>) * N, cudaMemcpyDeviceToDevice, stream));
     if (ls.nb > 0) {
-      if (!capturing) CHECK(d_bodies.ensure(sizeof(Body) * ls.nb));
-      else if (d_bodies.bytes < sizeof(Body) * ls.nb) return set_error(MLX_ERR_ARGUMENT, "body buffer not reserved");
-      k_make_rigids<R><<<ls.nb, 256, 0, stream>>>(L, d_bodies.as<Body>(), p, resv, d_vmass.as<double>(), ri);
+      if (!capturing) CHECK(w.bodies.ensure(sizeof(Body) * ls.nb));
+      else if (w.bodies.bytes < sizeof(Body) * ls.nb) return set_error(MLX_ERR_ARGUMENT, "body buffer not reserved");
+      k_make_rigids<R><<<ls.nb, 256, 0, stream>>>(L, w.bodies.as<Body>(), p, resv, d_vmass.as<double>(), ri);
       CU(cudaGetLastError());
       ++st.launches;
     }
@@ -740,7 +748,7 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
     CU(cudaGetLastError());
     ++st.launches;
     if (rigidLayer && ls.nb > 0) {
-      k_rigid_step<R><<<ls.nb, 256, 0, stream>>>(L, d_bodies.as<Body>(), p, xprev, resv, ri, h);
+      k_rigid_step<R><<<ls.nb, 256, 0, stream>>>(L, w.bodies.as<Body>(), p, xprev, resv, ri, h);
       CU(cudaGetLastError());
       ++st.launches;
     }
@@ -752,9 +760,9 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
       st.sumNonMon += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     }
     if (ls.n_bnd > 0) {
-      if (!capturing) CHECK(d_lamB.ensure(sizeof(double) * ls.n_bnd));
-      else if (d_lamB.bytes < sizeof(double) * ls.n_bnd) return set_error(MLX_ERR_ARGUMENT, "boundary buffer not reserved");
-      CU(cudaMemsetAsync(d_lamB.p, 0, sizeof(double) * ls.n_bnd, stream));
+      if (!capturing) CHECK(w.lamB.ensure(sizeof(double) * ls.n_bnd));
+      else if (w.lamB.bytes < sizeof(double) * ls.n_bnd) return set_error(MLX_ERR_ARGUMENT, "boundary buffer not reserved");
+      CU(cudaMemsetAsync(w.lamB.p, 0, sizeof(double) * ls.n_bnd, stream));
     }
     const int* dlist = dint + ls.o_list;
     const bool bodyWork = (ls.nb > 0 && (L.any_boundary || (P->use_rigid_contacts && L.any_rigid_contact))) ||
@@ -785,7 +793,7 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
       }
       if (bodyWork) {
         k_iterate_bodies<R><<<ls.nb + ecBlocks, 128, 0, stream>>>(
-            L, d_bodies.as<Body>(), p, ri, d_vmass.as<double>(), d_lamB.as<double>(), cd, h,
+            L, w.bodies.as<Body>(), p, ri, d_vmass.as<double>(), w.lamB.as<double>(), cd, h,
             P->boundary_compliance, P->contact_resistance, P->use_rigid_contacts);
         CU(cudaGetLastError());
         ++st.launches;
@@ -823,7 +831,7 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
       if (endLayer || stopSolve) break;
     }
     if (ls.nb > 0) {
-      k_finish_layer<R><<<ls.nb, 256, 0, stream>>>(L, d_bodies.as<Body>(), p, resv, ri, rigidLayer ? 1 : 0);
+      k_finish_layer<R><<<ls.nb, 256, 0, stream>>>(L, w.bodies.as<Body>(), p, resv, ri, rigidLayer ? 1 : 0);
       CU(cudaGetLastError());
       ++st.launches;
     }
@@ -872,7 +880,7 @@ int Solver<R>::layer_solve(const mlx_layer_desc* ld, const mlx_solve_params* P, 
   st.residualArray.assign(in->residual_in, in->residual_in + std::max(in->residual_in_len, 0));
   st.runUntil = P->run_until;
   st.sumNonMon = in->sum_non_monitored_time;
-  CHECK(run_layers(ld, P, K, cd, st, false));
+  CHECK(run_layers(ld, P, K, cd, st, false, work));
   // ---- download ----
   k_store_pos<R><<<blocks_for(N, bs), bs, 0, stream>>>(pos(), ds, N);
   if (out->lambdai) k_store_lambda<R><<<blocks_for(T, bs), bs, 0, stream>>>(d_lambda.as<R>(), d_s2e.as<int>(), ds + n3, T);
@@ -969,15 +977,17 @@ int Solver<R>::sim_setup(const mlx_layer_desc* ld, const mlx_solve_params* P, co
   sim.ld.num_rigids = sim.nr.data();
   sim.P = *P;
   // build every column once and reserve the body buffers for capture
-  while ((int)cache.size() < ld->num_columns) cache.emplace_back(new LayerStatic());
+  if (sim.graph) { cudaGraphExecDestroy(sim.graph); sim.graph = nullptr; }
+  sim_work.cache.clear();
+  while ((int)sim_work.cache.size() < ld->num_columns) sim_work.cache.emplace_back(new LayerStatic());
   int maxb = 1, maxbnd = 1;
   for (int c = 0; c < ld->num_columns; ++c) {
-    CHECK(build_static(&sim.ld, c, *cache[c], false));
-    maxb = std::max(maxb, cache[c]->nb);
-    maxbnd = std::max(maxbnd, cache[c]->n_bnd);
+    CHECK(build_static(&sim.ld, c, *sim_work.cache[c], false));
+    maxb = std::max(maxb, sim_work.cache[c]->nb);
+    maxbnd = std::max(maxbnd, sim_work.cache[c]->n_bnd);
   }
-  CHECK(d_bodies.ensure(sizeof(Body) * maxb));
-  CHECK(d_lamB.ensure(sizeof(double) * maxbnd));
+  CHECK(sim_work.bodies.ensure(sizeof(Body) * maxb));
+  CHECK(sim_work.lamB.ensure(sizeof(double) * maxbnd));
   CHECK(d_vel.ensure(sizeof(R4<R>) * N));
   CHECK(d_pin_mask.ensure(N));
   std::vector<unsigned char> pm(N, 0);
@@ -1075,7 +1085,7 @@ int Solver<R>::sim_issue_step(long long* launches) {
   RunState st;
   st.runUntil = sim.P.run_until;
   ContactData cd{};
-  CHECK(run_layers(&sim.ld, &sim.P, nullptr, cd, st, true));
+  CHECK(run_layers(&sim.ld, &sim.P, nullptr, cd, st, true, sim_work));
   k_sim_end<R><<<blocks_for(N, 256), 256, 0, stream>>>(p, d_oldp.as<R4<R>>(), d_vel.as<R4<R>>(), N, h);
   CU(cudaGetLastError());
   if (launches) *launches = st.launches + 2;
