@@ -271,61 +271,88 @@ __device__ __forceinline__ double stvk_residual(const V3<R> X[4], const R G[9], 
 }
 
 // ---------------------------------------------------------------------------
-// Stable Neo-Hookean pair of one tet, the 3D form of
-// 2d/mex/mexNeoHookeanDConstraint.cpp and mexNeoHookeanHConstraint.cpp:
-// C_D = ||F||_F with alphaTilde 1/(vol mu h^2); C_H = det F - (1 + mu/lambda)
-// with alphaTilde 1/(vol lambda h^2); both at the same positions, corrections
-// summed (xpbdLayer2D.m:282-289).  F = Ds * DmInv, Ds = [x1-x0 x2-x0 x3-x0].
-template <typename R> struct NHEval {
-  R CD, CH, aD, aH;
-  V3<R> gD[4], gH[4];
+// Stable Neo-Hookean tet, psi = mu/2 (I_C - 3) + lambda/2 (J - 1 - mu/lambda)^2
+// (the energy of the 2D pair 2d/mex/mexNeoHookeanDConstraint.cpp /
+// mexNeoHookeanHConstraint.cpp), written as two constraints that vanish at
+// rest: psi = mu/2 B + (lambda - mu)/2 (J - 1)^2 + const with
+// B = ||F||^2 + J^2 - 4J >= 0, so C_D = sqrt(B) (compliance 1/(vol mu)) and
+// C_H = J - 1 (compliance 1/(vol (lambda - mu)), absent when lambda <= mu),
+// solved as one 2x2 block.  sqrt(B) loses half its digits to the cancellation
+// in B, so this math runs in FP64 registers on every storage precision.
+struct NHEval {
+  double CD, CH, aD, aH;
+  bool hasH;
+  D3 gD[4], gH[4];
 };
 template <typename R>
-__device__ __forceinline__ void nh_eval(const V3<R> X[4], const R G[9], R mu, R lm, R vol, R inv_h2,
-                                        NHEval<R>& e) {
-  V3<R> u1 = vsub(X[1], X[0]), u2 = vsub(X[2], X[0]), u3 = vsub(X[3], X[0]);
-  V3<R> f[3];
+__device__ __forceinline__ void nh_eval(const V3<R> X[4], const R Gr[9], double mu, double lm, double vol,
+                                        double inv_h2, NHEval& e) {
+  double G[9];
 #pragma unroll
-  for (int c = 0; c < 3; ++c) f[c] = vaxpy3(G[0 + 3 * c], u1, G[1 + 3 * c], u2, G[2 + 3 * c], u3);
-  R n2 = vdot(f[0], f[0]) + vdot(f[1], f[1]) + vdot(f[2], f[2]);
-  e.CD = sqrt(n2);
-  V3<R> cf[3] = {vcross(f[1], f[2]), vcross(f[2], f[0]), vcross(f[0], f[1])};
-  e.CH = vdot(f[0], cf[0]) - (R(1) + mu / lm);
+  for (int j = 0; j < 9; ++j) G[j] = (double)Gr[j];
+  D3 x0 = d3(X[0].x, X[0].y, X[0].z);
+  D3 u1 = d3(X[1].x, X[1].y, X[1].z) - x0, u2 = d3(X[2].x, X[2].y, X[2].z) - x0,
+     u3 = d3(X[3].x, X[3].y, X[3].z) - x0;
+  D3 f[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) f[c] = G[0 + 3 * c] * u1 + G[1 + 3 * c] * u2 + G[2 + 3 * c] * u3;
+  D3 cf[3] = {cross(f[1], f[2]), cross(f[2], f[0]), cross(f[0], f[1])};
+  double J = dot(f[0], cf[0]);
+  double IC = dot(f[0], f[0]) + dot(f[1], f[1]) + dot(f[2], f[2]);
+  double B = IC + J * J - 4.0 * J;
+  e.CD = sqrt(fmax(B, 0.0));
+  e.hasH = lm > mu;
+  e.CH = e.hasH ? J - 1.0 : 0.0;
   e.aD = inv_h2 / (vol * mu);
-  e.aH = inv_h2 / (vol * lm);
-  R invCD = R(1) / e.CD;
-  V3<R> sD = {0, 0, 0}, sH = {0, 0, 0};
+  e.aH = e.hasH ? inv_h2 / (vol * (lm - mu)) : 0.0;
+  const double invCD = e.CD > 1e-12 ? 1.0 / e.CD : 0.0;
+  D3 pd[3];
 #pragma unroll
-  for (int kk = 1; kk <= 3; ++kk) {
-    R g0 = G[(kk - 1) + 0], g1 = G[(kk - 1) + 3], g2 = G[(kk - 1) + 6];
-    V3<R> d = vaxpy3(g0, f[0], g1, f[1], g2, f[2]);
-    e.gD[kk] = {d.x * invCD, d.y * invCD, d.z * invCD};
-    e.gH[kk] = vaxpy3(g0, cf[0], g1, cf[1], g2, cf[2]);
-    sD = {sD.x + e.gD[kk].x, sD.y + e.gD[kk].y, sD.z + e.gD[kk].z};
-    sH = {sH.x + e.gH[kk].x, sH.y + e.gH[kk].y, sH.z + e.gH[kk].z};
+  for (int c = 0; c < 3; ++c) pd[c] = invCD * (f[c] + (J - 2.0) * cf[c]);
+  D3 sD = d3(0, 0, 0), sH = d3(0, 0, 0);
+#pragma unroll
+  for (int k = 1; k <= 3; ++k) {
+    double g0 = G[(k - 1) + 0], g1 = G[(k - 1) + 3], g2 = G[(k - 1) + 6];
+    e.gD[k] = g0 * pd[0] + g1 * pd[1] + g2 * pd[2];
+    e.gH[k] = g0 * cf[0] + g1 * cf[1] + g2 * cf[2];
+    sD = sD + e.gD[k];
+    sH = sH + e.gH[k];
   }
-  e.gD[0] = {-sD.x, -sD.y, -sD.z};
-  e.gH[0] = {-sH.x, -sH.y, -sH.z};
+  e.gD[0] = -1.0 * sD;
+  e.gH[0] = -1.0 * sH;
 }
 
 template <typename R>
-__device__ __forceinline__ void nh_project(V3<R> X[4], const R minv[4], const R G[9], R mu, R lm, R vol,
-                                           R inv_h2, const R lam[2], R dl[2]) {
-  NHEval<R> e;
+__device__ __forceinline__ void nh_project(V3<R> X[4], const R minv[4], const R G[9], double mu, double lm,
+                                           double vol, double inv_h2, const double lam[2], double dl[2]) {
+  NHEval e;
   nh_eval<R>(X, G, mu, lm, vol, inv_h2, e);
-  R wD = 0, wH = 0;
+  double wD = 0, wH = 0, wDH = 0;
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
-    wD += minv[a] * vdot(e.gD[a], e.gD[a]);
-    wH += minv[a] * vdot(e.gH[a], e.gH[a]);
+    double m = minv[a];
+    wD += m * dot(e.gD[a], e.gD[a]);
+    wH += m * dot(e.gH[a], e.gH[a]);
+    wDH += m * dot(e.gD[a], e.gH[a]);
   }
-  dl[0] = (-e.CD - e.aD * lam[0]) / (wD + e.aD);
-  dl[1] = (-e.CH - e.aH * lam[1]) / (wH + e.aH);
+  double b1 = -e.CD - e.aD * lam[0];
+  if (e.hasH) {
+    double a11 = wD + e.aD, a22 = wH + e.aH, a12 = wDH;
+    double b2 = -e.CH - e.aH * lam[1];
+    double det = a11 * a22 - a12 * a12;
+    dl[0] = (b1 * a22 - a12 * b2) / det;
+    dl[1] = (a11 * b2 - a12 * b1) / det;
+  } else {
+    dl[0] = b1 / (wD + e.aD);
+    dl[1] = 0.0;
+  }
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
-    X[a].x += minv[a] * (e.gD[a].x * dl[0] + e.gH[a].x * dl[1]);
-    X[a].y += minv[a] * (e.gD[a].y * dl[0] + e.gH[a].y * dl[1]);
-    X[a].z += minv[a] * (e.gD[a].z * dl[0] + e.gH[a].z * dl[1]);
+    double m = minv[a];
+    D3 d = dl[0] * e.gD[a] + dl[1] * e.gH[a];
+    X[a].x = (R)((double)X[a].x + m * d.x);
+    X[a].y = (R)((double)X[a].y + m * d.y);
+    X[a].z = (R)((double)X[a].z + m * d.z);
   }
 }
 
@@ -369,11 +396,11 @@ __global__ void __launch_bounds__(128) k_project_color(TetData<R> td, const int*
   R vol = td.vol[s];
   const int T = td.T;
   if (MAT == MAT_NH) {
-    R mu = td.mat[s], lm = td.mat[(size_t)T + s];
-    R lam[2] = {td.lambda[s], td.lambda[(size_t)T + s]}, dl[2];
-    nh_project<R>(X, minv, G, mu, lm, vol, inv_h2, lam, dl);
-    td.lambda[s] = lam[0] + dl[0];
-    td.lambda[(size_t)T + s] = lam[1] + dl[1];
+    double mu = td.mat[s], lm = td.mat[(size_t)T + s];
+    double lam[2] = {(double)td.lambda[s], (double)td.lambda[(size_t)T + s]}, dl[2];
+    nh_project<R>(X, minv, G, mu, lm, (double)vol, (double)inv_h2, lam, dl);
+    td.lambda[s] = (R)(lam[0] + dl[0]);
+    td.lambda[(size_t)T + s] = (R)(lam[1] + dl[1]);
   } else {
     Compliance<R> cm;
     load_compliance<R, MAT>(td.mat, s, T, inv_h2, inv_h, cm, DAMP);
@@ -454,12 +481,12 @@ __global__ void __launch_bounds__(256) k_residual_partials(TetData<R> td, const 
       R vol = td.vol[s];
       const int T = td.T;
       if (MAT == MAT_NH) {
-        NHEval<R> e;
-        nh_eval<R>(X, G, td.mat[s], td.mat[(size_t)T + s], vol, inv_h2, e);
+        NHEval e;
+        nh_eval<R>(X, G, (double)td.mat[s], (double)td.mat[(size_t)T + s], (double)vol, inv_h2_d, e);
         double l0 = td.lambda[s], l1 = td.lambda[(size_t)T + s];
-        double a = fabs((double)e.CD), c = fabs((double)e.aD * l0);
+        double a = fabs(e.CD), c = fabs(e.aD * l0);
         double r0 = a - fmin(a, c);
-        a = fabs((double)e.CH); c = fabs((double)e.aH * l1);
+        a = fabs(e.CH); c = fabs(e.aH * l1);
         double r1 = a - fmin(a, c);
         acc[0] += r0 * r0 + r1 * r1;
       } else {

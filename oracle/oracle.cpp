@@ -12,8 +12,9 @@
 // values evaluated from the reference's own symbolic expressions
 // (3d/constraints/StVKconstraintGrad3D.m), and the layer builder against the
 // reference's mexUnionFindByVertice.cpp / mexEdiffNorm3D.cpp compiled unchanged
-// (oracle/_ref).  The 3D Neo-Hookean constraint has no 3D reference; it extends
-// the 2D pair 2d/mex/mexNeoHookean{D,H}Constraint.cpp and is parity unpinned.
+// (oracle/_ref).  The 3D Neo-Hookean constraint has no 3D reference (the 2D
+// pair 2d/mex/mexNeoHookean{D,H}Constraint.cpp defines its energy); it is
+// parity unpinned.
 //
 // Optional OpenMP: the per-colour tet loop and the residual loop run in
 // parallel when compiled with -fopenmp and orc_set_threads(n>1) is called;
@@ -243,12 +244,20 @@ void stvk_voigt_project(const double* x, const double* xprev, const double* DmIn
   }
 }
 
-// 3D stable Neo-Hookean pair, the 3D form of 2d/mex/mexNeoHookeanDConstraint.cpp
-// (C_D = ||F||_F, alphaTilde = 1/(vol mu h^2)) and mexNeoHookeanHConstraint.cpp
-// (C_H = det F - gamma, gamma = 1 + mu/lambda (2d/@Mesh/Mesh.m:244),
-// alphaTilde = 1/(vol lambda h^2)).  As in xpbdLayer2D.m:282-289 both
-// constraints are evaluated at the same positions and their corrections
-// summed.  F = Ds * DmInv with Ds = [x1-x0, x2-x0, x3-x0].
+// 3D stable Neo-Hookean constraint pair.  The 2D reference
+// (2d/mex/mexNeoHookeanDConstraint.cpp, mexNeoHookeanHConstraint.cpp, gamma =
+// 1 + mu/lambda at 2d/@Mesh/Mesh.m:244) projects C_D = ||F|| (compliance
+// 1/mu) and C_H = det F - gamma (1/lambda), whose energy is the stable
+// Neo-Hookean psi = mu/2 (I_C - 3) + lambda/2 (J - gamma)^2 + const.  In 3D the
+// pair needs large multipliers at rest (C_D = sqrt 3 there) that XPBD rebuilds
+// from zero every step, which drifts from rest for stiff tets.  The same
+// energy is written here as two constraints that both vanish at rest:
+//   psi = mu/2 B + (lambda - mu)/2 (J - 1)^2 + const,  B = ||F||^2 + J^2 - 4J,
+// B >= 0 with B = 0 exactly for rotations, so
+//   C_D = sqrt(B),  compliance 1/(vol mu);   C_H = J - 1, compliance
+//   1/(vol (lambda - mu)) (dropped when lambda <= mu, i.e. nu <= 0.25);
+// the pair is solved as one 2x2 block per tet (the block-solve style of
+// matStvkVoigtConstraint3D.m:31-45).  F = Ds * DmInv, Ds = [x1-x0 x2-x0 x3-x0].
 void nh_project(const double* x, const double* DmInv, double mu, double lam, double vol,
                 double h, const double* lambda, const double* minv, double* dx,
                 double* dlambda, double* Cout, double* alphaTildeOut) {
@@ -262,23 +271,27 @@ void nh_project(const double* x, const double* DmInv, double mu, double lam, dou
   double F[9];
   matmul3(Ds, DmInv, F);
   V3 f1 = v3(F[0], F[1], F[2]), f2 = v3(F[3], F[4], F[5]), f3 = v3(F[6], F[7], F[8]);
-  double h2 = h * h;
-  double CD = 0;
-  for (int i = 0; i < 9; ++i) CD += F[i] * F[i];
-  CD = std::sqrt(CD);
-  double gammaH = 1.0 + mu / lam;
-  double detF = dot(f1, cross(f2, f3));
-  double CH = detF - gammaH;
-  double aD = 1.0 / (vol * mu * h2), aH = 1.0 / (vol * lam * h2);
-  if (Cout) { Cout[0] = CD; Cout[1] = CH; }
-  if (alphaTildeOut) { alphaTildeOut[0] = aD; alphaTildeOut[1] = aH; }
-  // P = dC/dF; gradient wrt x_k (k=1..3) is column k of P * DmInv'
-  double PD[9], PH[9];
-  for (int i = 0; i < 9; ++i) PD[i] = F[i] / CD;
   V3 c1 = cross(f2, f3), c2 = cross(f3, f1), c3 = cross(f1, f2);
+  double J = dot(f1, c1);
+  double IC = 0;
+  for (int i = 0; i < 9; ++i) IC += F[i] * F[i];
+  double B = IC + J * J - 4 * J;
+  double CD = std::sqrt(std::max(B, 0.0));
+  double CH = J - 1;
+  const bool hasH = lam > mu;
+  double h2 = h * h;
+  double aD = 1.0 / (vol * mu * h2);
+  double aH = hasH ? 1.0 / (vol * (lam - mu) * h2) : 0.0;
+  if (Cout) { Cout[0] = CD; Cout[1] = hasH ? CH : 0.0; }
+  if (alphaTildeOut) { alphaTildeOut[0] = aD; alphaTildeOut[1] = aH; }
+  // dC/dF: D -> (F + (J - 2) cof F) / C_D (zero at C_D = 0), H -> cof F
+  double PD[9] = {0}, PH[9];
   PH[0] = c1.x; PH[1] = c1.y; PH[2] = c1.z;
   PH[3] = c2.x; PH[4] = c2.y; PH[5] = c2.z;
   PH[6] = c3.x; PH[7] = c3.y; PH[8] = c3.z;
+  if (CD > 1e-12)
+    for (int i = 0; i < 9; ++i) PD[i] = (F[i] + (J - 2) * PH[i]) / CD;
+  // gradient wrt x_k (k=1..3) = column k of P * DmInv'; x0 gets minus the sum
   double GD[9], GH[9];
   matmul3_bt(PD, DmInv, GD);
   matmul3_bt(PH, DmInv, GH);
@@ -292,10 +305,24 @@ void nh_project(const double* x, const double* DmInv, double mu, double lam, dou
     gD[a] = -(gD[3 + a] + gD[6 + a] + gD[9 + a]);
     gH[a] = -(gH[3 + a] + gH[6 + a] + gH[9 + a]);
   }
-  double wD = 0, wH = 0;
-  for (int c = 0; c < 12; ++c) { wD += minv[c] * gD[c] * gD[c]; wH += minv[c] * gH[c] * gH[c]; }
-  double dlD = (-CD - aD * lambda[0]) / (wD + aD);
-  double dlH = (-CH - aH * lambda[1]) / (wH + aH);
+  double wD = 0, wH = 0, wDH = 0;
+  for (int c = 0; c < 12; ++c) {
+    wD += minv[c] * gD[c] * gD[c];
+    wH += minv[c] * gH[c] * gH[c];
+    wDH += minv[c] * gD[c] * gH[c];
+  }
+  double b1 = -CD - aD * lambda[0];
+  double dlD, dlH;
+  if (hasH) {
+    double a11 = wD + aD, a22 = wH + aH, a12 = wDH;
+    double b2 = -CH - aH * lambda[1];
+    double det = a11 * a22 - a12 * a12;
+    dlD = (b1 * a22 - a12 * b2) / det;
+    dlH = (a11 * b2 - a12 * b1) / det;
+  } else {
+    dlD = b1 / (wD + aD);
+    dlH = 0;
+  }
   dlambda[0] = dlD;
   dlambda[1] = dlH;
   for (int c = 0; c < 12; ++c) dx[c] = minv[c] * (gD[c] * dlD + gH[c] * dlH);

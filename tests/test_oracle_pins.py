@@ -103,27 +103,33 @@ def test_stvk_one_tet_stretch_known_answer(oracle):
 
 
 def test_nh_gradients_match_finite_differences(oracle):
-    """The 3D Neo-Hookean pair's update direction equals the finite-difference
-    gradient of C_D = ||F|| and C_H = det F - gamma (no 3D reference exists)."""
+    """The 3D Neo-Hookean pair (no 3D reference exists): C_D = sqrt(||F||^2 +
+    J^2 - 4J), C_H = J - 1; the update uses their finite-difference gradients
+    and solves the coupled 2x2 block; at rest both vanish and nothing moves."""
     lib = oracle.load()
     rng = np.random.default_rng(1)
     x0, G = _rest_tet()
     Gc = np.ascontiguousarray(G.T.reshape(-1))
-    x = x0 + rng.normal(0, 0.01, 12)
     mu, lm, vol, h = 3e4, 5e4, 1e-3 / 6, 0.01
+    minv = rng.uniform(0.5, 2.0, 4).repeat(3)
 
     def CC(xx):
         dx, dl, C, aT = np.zeros(12), np.zeros(2), np.zeros(2), np.zeros(2)
         lib.orc_nh_project(oracle.f64(np.ascontiguousarray(xx)), oracle.f64(Gc), mu, lm, vol, h,
-                           oracle.f64(np.zeros(2)), oracle.f64(np.ones(12)), oracle.f64(dx), oracle.f64(dl),
-                           oracle.f64(C), oracle.f64(aT))
+                           oracle.f64(np.zeros(2)), oracle.f64(np.ascontiguousarray(minv)), oracle.f64(dx),
+                           oracle.f64(dl), oracle.f64(C), oracle.f64(aT))
         return C, dx, dl, aT
 
+    C, dx, dl, aT = CC(x0)
+    assert np.abs(C).max() < 1e-7 and np.abs(dx).max() < 1e-15
+    x = x0 + rng.normal(0, 0.01, 12)
     C, dx, dl, aT = CC(x)
     Ds = np.stack([x[3:6] - x[:3], x[6:9] - x[:3], x[9:12] - x[:3]], 1)
     F = Ds @ G
-    assert abs(C[0] - np.linalg.norm(F)) < 1e-14
-    assert abs(C[1] - (np.linalg.det(F) - (1 + mu / lm))) < 1e-14
+    J = np.linalg.det(F)
+    assert abs(C[0] - np.sqrt((F * F).sum() + J * J - 4 * J)) < 1e-12
+    assert abs(C[1] - (J - 1)) < 1e-14
+    np.testing.assert_allclose(aT, [1 / (vol * mu * h * h), 1 / (vol * (lm - mu) * h * h)], rtol=1e-14)
     eps = 1e-7
     gD = np.zeros(12)
     gH = np.zeros(12)
@@ -132,7 +138,21 @@ def test_nh_gradients_match_finite_differences(oracle):
         e[i] = eps
         gD[i] = (CC(x + e)[0][0] - CC(x - e)[0][0]) / (2 * eps)
         gH[i] = (CC(x + e)[0][1] - CC(x - e)[0][1]) / (2 * eps)
-    # with unit inverse masses dx = gD dlD + gH dlH and dl = (-C - aT*0)/(|g|^2 + aT)
-    np.testing.assert_allclose(dl[0], -C[0] / (gD @ gD + aT[0]), rtol=1e-6)
-    np.testing.assert_allclose(dl[1], -C[1] / (gH @ gH + aT[1]), rtol=1e-6)
-    np.testing.assert_allclose(dx, gD * dl[0] + gH * dl[1], rtol=1e-5, atol=1e-12)
+    A = np.array([[gD @ (minv * gD) + aT[0], gD @ (minv * gH)], [gD @ (minv * gH), gH @ (minv * gH) + aT[1]]])
+    np.testing.assert_allclose(dl, np.linalg.solve(A, -C), rtol=1e-6)
+    np.testing.assert_allclose(dx, minv * (gD * dl[0] + gH * dl[1]), rtol=1e-5, atol=1e-13)
+
+
+def test_nh_energy_is_stable_neo_hookean():
+    """mu/2 B + (lambda-mu)/2 (J-1)^2 equals the stable Neo-Hookean energy
+    mu/2 (I_C - 3) + lambda/2 (J - 1 - mu/lambda)^2 up to a constant."""
+    rng = np.random.default_rng(4)
+    mu, lm = 2.0, 7.0
+    for _ in range(20):
+        F = np.eye(3) + rng.normal(0, 0.4, (3, 3))
+        J = np.linalg.det(F)
+        Ic = (F * F).sum()
+        split = mu / 2 * (Ic + J * J - 4 * J) + (lm - mu) / 2 * (J - 1) ** 2
+        snh = mu / 2 * (Ic - 3) + lm / 2 * (J - 1 - mu / lm) ** 2
+        assert abs(split - snh + mu * mu / (2 * lm)) < 1e-12
+        assert Ic + J * J - 4 * J >= -1e-12
