@@ -93,6 +93,15 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def profiled_dram_bytes_per_tet():
+    """DRAM bytes per projected tet of the colour kernel from the committed ncu
+    summary (profiles/k_project_color_config2.json), or None."""
+    f = ROOT / "profiles" / "k_project_color_config2.json"
+    if f.exists():
+        return float(json.loads(f.read_text())["dram_bytes_per_tet"])
+    return None
+
+
 def measured_peak_hbm():
     f = ROOT / "MEASURED_PEAKS.json"
     if f.exists():
@@ -261,7 +270,11 @@ def run_ours(args, rank, world, local):
                        "graph": "one CUDA graph per step"},
             "roofline": {"bound": "hbm", "kernel": "k_project_color (all colours of a sweep)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "frac": (achieved / peak) if achieved else None,
+                         "traffic": (profiled_dram_bytes_per_tet() * sweep_bytes / solver_bytes_per_tet(m, MLX_FP32)
+                                     / max(sweep_launches, 1)) if profiled_dram_bytes_per_tet() else None,
+                         "traffic_note": "DRAM bytes per launch from one ncu capture (cold cache) scaled by the "
+                                         "tets per launch; achieved uses algorithmic bytes",
                          "peak_kind": peak_kind, "bytes_per_tet": solver_bytes_per_tet(m, MLX_FP32),
                          "sweep_ms_per_step": sweep_ms / args.steps,
                          "colour_launches_per_step": sweep_launches / args.steps,
