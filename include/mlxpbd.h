@@ -212,6 +212,25 @@ int mlx_sim_sweep_stats(mlx_solver* solver, double* ms, double* bytes, long long
 long long mlx_sim_launches_per_step(const mlx_solver* solver);
 long long mlx_last_call_launches(const mlx_solver* solver);
 
+/* ---- allocation-free residual ------------------------------------------
+ * No counterpart in the reference.  The elastic constraint residual of
+ * simpleEvaluateAllConstraintResiduals (StVK Voigt tets, no contacts) on
+ * device arrays the caller owns, for callers that cannot allocate device
+ * memory (a MATLAB mexcuda function working on gpuArray memory, a fixed-rate
+ * loop where cudaMalloc would stall).  Inputs are device pointers in the
+ * MATLAB layout of mlx_mesh_desc / mlx_solve_inputs; d_residual receives one
+ * double.  The call only enqueues work on `stream` (a cudaStream_t, NULL =
+ * default stream) and allocates nothing: its scratch is a fixed device array
+ * of MLX_NOALLOC_MAX_TETS/256 doubles inside the library, shared by all calls
+ * (calls that overlap on the GPU race; serialise them).  The first call on a
+ * device looks that array up and should come before any stream capture.
+ * More than MLX_NOALLOC_MAX_TETS tets is rejected with MLX_ERR_ARGUMENT. */
+#define MLX_NOALLOC_MAX_TETS 524288
+int mlx_stvk_residual_noalloc(int32_t num_vertices, int32_t num_tets, const double* d_x,
+                              const int32_t* d_t, const double* d_DmInv, const double* d_alpha,
+                              const double* d_lambda, const double* d_volume, double h,
+                              double* d_residual, void* stream);
+
 /* ---- host-side helpers of the step (run on the CPU in the reference too) */
 
 /* naiveGraphColoring (2d/tools/functionalities/naiveGraphColoring.m:1-19):

@@ -17,6 +17,7 @@ MLX_OK = 0
 MLX_ERR_ARGUMENT = 1
 MLX_ERR_UNSUPPORTED = 2
 MLX_ERR_NO_DEVICE = 4
+MLX_NOALLOC_MAX_TETS = 524288
 MLX_ENERGY_NEOHOOKEAN = 1
 MLX_ENERGY_STVK_VOIGT = 2
 MLX_FP32 = 0
@@ -122,6 +123,8 @@ SIGNATURES = {
     "mlx_sim_sweep_stats": ([C.c_void_p, _f64p, _f64p, C.POINTER(C.c_longlong), C.c_int32], C.c_int),
     "mlx_sim_launches_per_step": ([C.c_void_p], C.c_longlong),
     "mlx_last_call_launches": ([C.c_void_p], C.c_longlong),
+    "mlx_stvk_residual_noalloc": ([C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p], C.c_int),
     "mlx_greedy_coloring": ([_i32p, C.c_int32, C.c_int32, _i32p, _i32p], C.c_int),
     "mlx_strain_rate_norms": ([_i32p, C.c_int32, _f64p, _f64p, _f64p, C.c_double, _f64p], C.c_int),
     "mlx_union_find_layers": ([_i32p, C.c_int32, _f64p, C.c_int32, _u8p, _i32p, C.c_int32, _i32p, _i32p],

@@ -572,7 +572,7 @@ int Solver<R>::residual(const ContactData& cd, double contact_resistance, double
       k_residual_partials<R, MAT_STVK_LAME><<<tetBlocks + cBlocks, bs, 0, stream>>>(td, pos(), cd, contact_resistance, inv_h2, inv_h, inv_h2_d, tetBlocks, partials);
   }
   CU(cudaGetLastError());
-  k_finish_norm<<<1, 256, 0, stream>>>(partials, tetBlocks + cBlocks, d_scalar.as<double>());
+  k_finish_norm<256><<<1, 256, 0, stream>>>(partials, tetBlocks + cBlocks, d_scalar.as<double>());
   CU(cudaGetLastError());
   CU(cudaMemcpyAsync(h_scalar.p, d_scalar.p, sizeof(double), cudaMemcpyDeviceToHost, stream));
   CU(cudaStreamSynchronize(stream));
@@ -586,7 +586,7 @@ int Solver<R>::norm_resv(double* out) {
   int grid = std::min(blocks_for(N, bs), 296);
   k_norm3_partials<R><<<grid, bs, 0, stream>>>(d_resv.as<R4<R>>(), N, d_partials.as<double>());
   CU(cudaGetLastError());
-  k_finish_norm<<<1, 256, 0, stream>>>(d_partials.as<double>(), grid, d_scalar.as<double>() + 1);
+  k_finish_norm<256><<<1, 256, 0, stream>>>(d_partials.as<double>(), grid, d_scalar.as<double>() + 1);
   CU(cudaGetLastError());
   CU(cudaMemcpyAsync(h_scalar.as<double>() + 1, d_scalar.as<double>() + 1, sizeof(double), cudaMemcpyDeviceToHost, stream));
   CU(cudaStreamSynchronize(stream));

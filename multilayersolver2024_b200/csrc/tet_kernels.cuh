@@ -517,7 +517,9 @@ __global__ void __launch_bounds__(256) k_residual_partials(TetData<R> td, const 
 }
 
 // Sums `n` partials in index order (one block) and writes sqrt of the sum.
-__global__ void __launch_bounds__(256) k_finish_norm(const double* __restrict__ partials, int n,
+// (A template so that every translation unit can instantiate it.)
+template <int kBlock = 256>
+__global__ void __launch_bounds__(kBlock) k_finish_norm(const double* __restrict__ partials, int n,
                                                      double* __restrict__ out) {
   double acc[1] = {0.0};
   for (int i = threadIdx.x; i < n; i += blockDim.x) acc[0] += partials[i];
