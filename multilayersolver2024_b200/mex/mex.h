@@ -65,6 +65,7 @@ bool mxIsComplex(const mxArray* a);
 bool mxIsEmpty(const mxArray* a);
 
 void mexErrMsgIdAndTxt(const char* id, const char* fmt, ...);
+int mexAtExit(void (*exit_fcn)(void));
 int mexPrintf(const char* fmt, ...);
 
 /* the gateway every mex file defines */

@@ -117,6 +117,21 @@ void mexErrMsgIdAndTxt(const char* id, const char* fmt, ...) {
   throw MexError(id, buf);
 }
 
+// MATLAB calls the registered function when the mex file is cleared; the
+// headless runtime calls it at process exit.
+int mexAtExit(void (*exit_fcn)(void)) {
+  static void (*registered)(void) = nullptr;
+  static bool hooked = false;
+  registered = exit_fcn;
+  if (!hooked) {
+    hooked = true;
+    std::atexit([] {
+      if (registered) registered();
+    });
+  }
+  return 0;
+}
+
 int mexPrintf(const char* fmt, ...) {
   va_list ap;
   va_start(ap, fmt);

@@ -230,11 +230,13 @@ def integrate(integ, mesh, h, contacts, cache, frame, material="blocks"):
 
 
 # ---- the reference's own mex files (compiled unchanged, oracle/_ref) --------
-class RefMex:
-    """Calls a reference mexFunction compiled against the headless runtime."""
+class MexLib:
+    """Calls the mexFunction of a library built against the headless mx
+    runtime (multilayersolver2024_b200/mex), passing numpy arrays as mxArrays
+    (bool -> logical, int32 -> int32, anything else -> double)."""
 
-    def __init__(self, name):
-        path = REF / f"{name}.so"
+    def __init__(self, path):
+        path = Path(path)
         if not path.exists():
             raise FileNotFoundError(path)
         lib = C.CDLL(str(path))
@@ -295,6 +297,13 @@ class RefMex:
             self.lib.mxDestroyArray(h)
             outs.append(out)
         return outs
+
+
+class RefMex(MexLib):
+    """A reference mex file compiled unchanged into oracle/_ref."""
+
+    def __init__(self, name):
+        super().__init__(REF / f"{name}.so")
 
 
 def ref_available(name="mexUnionFindByVertice"):
