@@ -759,6 +759,9 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
       CHECK(norm_resv(&normresv));
       st.sumNonMon += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     }
+    // contact multipliers restart at zero in every layer: projectGS does not
+    // return them (xpbdLayer3D.m:163), so each layer sees layerSolve's zeros
+    if (nK > 0) CU(cudaMemsetAsync(cd.lambda, 0, sizeof(double) * nK, stream));
     if (ls.n_bnd > 0) {
       if (!capturing) CHECK(w.lamB.ensure(sizeof(double) * ls.n_bnd));
       else if (w.lamB.bytes < sizeof(double) * ls.n_bnd) return set_error(MLX_ERR_ARGUMENT, "boundary buffer not reserved");

@@ -499,6 +499,9 @@ __global__ void __launch_bounds__(256) k_residual_partials(TetData<R> td, const 
       }
     }
   } else {
+    // contacts: the reference's correction term is the K x 1 x K implicit
+    // expansion of (compliance/h^2) (1x1xK) times lambda (Kx1)
+    // (xpbdLayer3D.m:581-583), so contact k meets every compliance j
     int cb = blockIdx.x - tetBlocks, ncb = gridDim.x - tetBlocks;
     for (int k = cb * blockDim.x + threadIdx.x; k < cd.K; k += ncb * blockDim.x) {
       R4<R> p = pos[cd.vid[k]];
@@ -507,9 +510,12 @@ __global__ void __launch_bounds__(256) k_residual_partials(TetData<R> td, const 
                    n2 * ((double)p.z - cd.point[2 * cd.K + k]);
       if (phi > 0) phi = 0;
       double a = fabs(contact_resistance * phi);
-      double c = fabs((cd.compliance[k] * inv_h2_d) * cd.lambda[k]);
-      double r = a - fmin(a, c);
-      acc[0] += r * r;
+      double lk = cd.lambda[k];
+      for (int j = 0; j < cd.K; ++j) {
+        double c = fabs((cd.compliance[j] * inv_h2_d) * lk);
+        double r = a - fmin(a, c);
+        acc[0] += r * r;
+      }
     }
   }
   block_sum<1>(acc);

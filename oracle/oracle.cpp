@@ -665,6 +665,11 @@ struct Solve {
         }
       }
     }
+    // contacts: (contactCompliance/h2) is 1x1xK and contactLambdas(:) is Kx1,
+    // so implicit expansion makes the correction term K x 1 x K
+    // (xpbdLayer3D.m:581-583): every |C_k| is compared with every
+    // |compliance_j / h^2 * lambda_k|, K^2 terms in all
+    std::vector<double> absC(K);
     for (int k = 0; k < K; ++k) {
       int v = cv[k] - 1;
       V3 x = v3(xi[3 * v], xi[3 * v + 1], xi[3 * v + 2]);
@@ -672,11 +677,14 @@ struct Solve {
       V3 c = v3(cp[k], cp[k + K], cp[k + 2 * K]);
       double phi = dot(n, sub(x, c));
       if (phi > 0) phi = 0;
-      double a = std::fabs(P.contact_resistance * phi);
-      double cr = std::fabs((ccomp[k] / h2) * contactLambdas[k]);
-      double vv = a - std::min(a, cr);
-      acc += vv * vv;
+      absC[k] = std::fabs(P.contact_resistance * phi);
     }
+    for (int j = 0; j < K; ++j)
+      for (int k = 0; k < K; ++k) {
+        double cr = std::fabs((ccomp[j] / h2) * contactLambdas[k]);
+        double vv = absC[k] - std::min(absC[k], cr);
+        acc += vv * vv;
+      }
     return std::sqrt(acc);
   }
 };
@@ -988,6 +996,9 @@ int orc_layer_solve(const mlx_mesh_desc* md, const mlx_layer_desc* ld, const mlx
     normresv = std::sqrt(normresv);
 
     // ---- projectGS ----
+    // projectGS does not return contactLambdas (xpbdLayer3D.m:163): every
+    // layer starts from the zeros layerSolve created (xpbdLayer3D.m:99-102)
+    std::fill(S.contactLambdas.begin(), S.contactLambdas.end(), 0.0);
     std::vector<int> bverts;
     for (int v = 0; v < N; ++v) if (isBV[v]) bverts.push_back(v);
     std::vector<double> lamB(bverts.size(), 0.0);

@@ -13,7 +13,12 @@ Writes
   layers.npz      per-tet strain-rate norms and rigid-body IDs per layer from the
                   reference's 3d/mex/mexEdiffNorm3D.cpp and
                   2d/mex/mexUnionFindByVertice.cpp, compiled unchanged against
-                  the headless mx runtime (oracle/_ref).
+                  the headless mx runtime (oracle/_ref);
+  layer_solve.npz inputs and results of xpbdLayer3D.layerSolve
+                  (3d/integrator/xpbdLayer3D.m:44-232) on small scenes,
+                  produced by executing the reference's own MATLAB functions
+                  with the MATLAB-subset interpreter tests/golden/mlite.py
+                  (MATLAB itself is not installed).
 The reference sources are read, never copied; only computed numbers are kept.
 """
 from __future__ import annotations
@@ -137,6 +142,82 @@ def make_layers(out: Path, seed=5):
     np.savez_compressed(out / "layers.npz", **data)
 
 
+LAYER_SOLVE_CASES = {
+    # name: (dims, energy seed, alpha1, layers, iterations, case seed, contacts, settings)
+    "single_damped": ((4, 2, 2), 31, 0.01, [0], [3], 32, False, {}),
+    "three_layers_contacts_monitor": ((4, 3, 3), 2, 0.0, [50, 25, 0], [2, 3, 4], 3, True,
+                                      dict(boundaryCompliance=0.0, contactResistance=0.9, computeResiduals=True,
+                                           StopAtImprovementPercent=60, runUntilResSmallerThan=0.0,
+                                           hangingStop=40, giveUpEnabled=True)),
+    "two_layers_elastic_contacts": ((4, 3, 3), 5, 0.02, [60, 0], [3, 5], 6, True,
+                                    dict(boundaryCompliance=1e-8, useRigidContacts=False)),
+    "run_until_hanging_stop": ((5, 2, 2), 7, 0.0, [40, 0], [2, 3], 8, False,
+                               dict(computeResiduals=True, runUntilResSmallerThan=1e-9, hangingStop=12,
+                                    boundaryCompliance=0.0)),
+}
+
+
+def build_case(name):
+    """The layerSolve inputs of one named case (deterministic)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from helpers import Case, block_mesh, plane_contacts, sphere_contacts
+    from multilayersolver2024_b200.xpbd_layer3d import ContactSet
+    dims, eseed, a1, layers, iters, cseed, contacts, settings = LAYER_SOLVE_CASES[name]
+    m = block_mesh(dims=dims, seed=eseed, alpha1=a1)
+    case = Case(m, layers, iters, seed=cseed)
+    for k, v in settings.items():
+        setattr(case.integ, k, v)
+    if contacts:
+        case.contacts = ContactSet.concat([plane_contacts(case.xi, [0, 0, 1.0], [0, 0, 0.004]),
+                                           sphere_contacts(case.xi, 0.12, [0.25, 0.15, 0.0])])
+    return case
+
+
+def reference_layer_solve_args(case):
+    """layerSolve's 50 arguments with the MATLAB classes and page shapes of
+    xpbdLayer3D.integrate (xpbdLayer3D.m:684-733)."""
+    import mlite
+    m, ls, it, c = case.mesh, case.ls, case.integ, case.contacts
+    K = c.vertex_ids.size
+    col = lambda a: mlite.M(np.asarray(a, dtype=float).reshape(-1, 1))
+    sc = lambda v: mlite.M(float(v))
+    pages = lambda a, n: np.ascontiguousarray(np.asarray(a).reshape(-1, n, n).transpose(2, 1, 0))
+    return [
+        ls.isElasticElement.astype(bool), ls.isRigidElement.astype(bool), ls.rigidBodySetsPerLayer,
+        ls.vertexRigidBody, ls.isBoundaryVertex.astype(bool), ls.isRigidVertex.astype(bool),
+        col(case.xi), np.asfortranarray(case.lam), sc(0.0), sc(case.h), col(ls.numRigids), sc(0.0),
+        sc(it.boundaryCompliance), sc(it.contactResistance),
+        np.asarray(c.compliance, float).reshape(1, 1, K) if K else np.zeros((1, 1, 0)),
+        mlite.M(np.array(it.iterations, float)), mlite.M(np.array(it.layers, float)),
+        sc(it.runUntilResSmallerThan), mlite.M(bool(it.computeResiduals)), sc(it.hangingStop),
+        mlite.M(bool(it.giveUpEnabled)), sc(it.giveUpThreshold), mlite.M(bool(it.LastLayerGiveUpEnabled)),
+        mlite.M(bool(it.useGravityConstraints)), col(case.oldp), col(case.oldOldp),
+        mlite.M(np.asarray(c.normals, float).reshape(K, 3)) if K else np.zeros((0, 3)),
+        mlite.M(np.asarray(c.points, float).reshape(K, 3)) if K else np.zeros((0, 3)),
+        col(c.vertex_ids) if K else np.zeros((0, 1)), col(m.mass), np.asfortranarray(m.t),
+        mlite.M(m.unpinnedDOFs.astype(float)), col(m.pinnedDOFs), pages(m.DmInv, 3),
+        pages(m.perElementXPBDalphaMatrix, 6), pages(m.perElementXPBDalphaInvMatrix, 6), col(m.elementColor),
+        m.elementDOFs, sc(m.numColors), col(case.f), col(it.layersMap), sc(it.gravityCompliance),
+        sc(it.Gravity), col(case.resv), pages(m.perElementXPBDbeta, 6), col(m.elV), mlite.M(False),
+        mlite.M(bool(it.useRigidContacts)), sc(it.StopAtImprovementPercent), col(case.pinnedx),
+    ]
+
+
+def make_layer_solve(ref: Path, out: Path):
+    sys.path.insert(0, str(Path(__file__).resolve().parent))
+    import mlite
+    interp = mlite.Interpreter(ref, mlite.LAYER_SOLVE_TABLE)
+    data = {}
+    for name in LAYER_SOLVE_CASES:
+        case = build_case(name)
+        xi, _snm, res, run_until = interp.call("xpbdLayer3D.layerSolve", reference_layer_solve_args(case), nargout=4)
+        data[f"{name}_xi"] = np.asarray(xi, float).ravel()
+        data[f"{name}_residual"] = np.asarray(res, float).ravel()
+        data[f"{name}_run_until"] = float(np.asarray(run_until).ravel()[0])
+        data[f"{name}_input_xi"] = case.xi  # lets a test confirm it rebuilt the same inputs
+    np.savez_compressed(out / "layer_solve.npz", **data)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -144,6 +225,7 @@ def main():
     out = Path(__file__).resolve().parent
     make_stvk(Path(a.ref), out)
     make_layers(out)
+    make_layer_solve(Path(a.ref), out)
     print("wrote", sorted(p.name for p in out.glob("*.npz")))
 
 

@@ -127,3 +127,16 @@ def test_errors_are_reported(gpu, lib):
     rc, _ = case.run(lib.mlx_layer_solve, solver.handle)
     assert rc == _lib.MLX_ERR_ARGUMENT and b"compute_residuals" in lib.mlx_last_error()
     solver.close()
+
+
+@pytest.mark.parametrize("name", ["single_damped", "three_layers_contacts_monitor", "two_layers_elastic_contacts",
+                                  "run_until_hanging_stop"])
+def test_fp64_matches_reference_execution(gpu, name):
+    """The CUDA layerSolve (FP64) against results of the reference's own
+    MATLAB source executed by tests/golden/mlite.py."""
+    from test_oracle_pins import reference_case
+    case, gold = reference_case(name)
+    xi, _, res, run_until, _, _ = case.product(_lib.MLX_FP64)
+    assert rel_pos_err(xi, gold[f"{name}_xi"], case.mesh) <= TOL64
+    np.testing.assert_allclose(res, gold[f"{name}_residual"], rtol=1e-9, atol=1e-14)
+    assert run_until == pytest.approx(float(gold[f"{name}_run_until"]), rel=1e-9)

@@ -156,3 +156,30 @@ def test_nh_energy_is_stable_neo_hookean():
         snh = mu / 2 * (Ic - 3) + lm / 2 * (J - 1 - mu / lm) ** 2
         assert abs(split - snh + mu * mu / (2 * lm)) < 1e-12
         assert Ic + J * J - 4 * J >= -1e-12
+
+
+LAYER_SOLVE_CASES = ["single_damped", "three_layers_contacts_monitor", "two_layers_elastic_contacts",
+                     "run_until_hanging_stop"]
+
+
+def reference_case(name):
+    import sys
+    sys.path.insert(0, str(GOLD))
+    from make_golden import build_case
+    case = build_case(name)
+    gold = np.load(GOLD / "layer_solve.npz")
+    np.testing.assert_array_equal(case.xi, gold[f"{name}_input_xi"])  # same inputs as when generated
+    return case, gold
+
+
+@pytest.mark.parametrize("name", LAYER_SOLVE_CASES)
+def test_oracle_layer_solve_matches_reference_execution(oracle, name):
+    """xpbdLayer3D.layerSolve executed from the reference's MATLAB source
+    (tests/golden/mlite.py) vs the oracle restatement: positions, residual
+    array (incl. the K x K contact term) and runUntil."""
+    case, gold = reference_case(name)
+    xi, _, res, run_until, _, _ = case.oracle()
+    d = case.mesh.bbox_diagonal()
+    assert np.abs(xi - gold[f"{name}_xi"]).max() / d <= 1e-12
+    np.testing.assert_allclose(res, gold[f"{name}_residual"], rtol=1e-10, atol=1e-15)
+    assert run_until == pytest.approx(float(gold[f"{name}_run_until"]), rel=1e-10)
