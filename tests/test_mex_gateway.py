@@ -69,7 +69,7 @@ def test_gateway_matches_oracle(gpu, monkeypatch):
     ref = case.oracle()
     assert rel_pos_err(xi.ravel(), ref[0], m) <= 1e-9
     np.testing.assert_allclose(res.ravel(), ref[2], rtol=1e-9, atol=1e-14)
-    assert float(run_until) == pytest.approx(ref[3])
+    assert float(run_until.ravel()[0]) == pytest.approx(ref[3])
     # a second call reuses the cached solver
     xi2, _, _, _ = g(4, *args)
     assert rel_pos_err(xi2.ravel(), ref[0], m) <= 1e-9
