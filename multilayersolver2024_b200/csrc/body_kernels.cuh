@@ -81,8 +81,8 @@ __device__ __forceinline__ D3 body_point(const Body& b, const double4& r) {
 
 template <typename R>
 __device__ __forceinline__ void store_xyz(R4<R>* pos, int v, D3 x) {
-  R4<R> p = pos[v];
-  pos[v] = make_r4<R>((R)x.x, (R)x.y, (R)x.z, p.w);
+  R4<R> p = ldcg_r4(pos + v);
+  stcg_r4(pos + v, make_r4<R>((R)x.x, (R)x.y, (R)x.z, p.w));
 }
 
 // AdaptiveMesh3D.makeRigidsFromConnectivity (AdaptiveMesh3D.m:32-43) ->
@@ -215,48 +215,48 @@ __device__ __forceinline__ void apply_increments(Body& B, const double* s, doubl
   mm3(B.R, tmp, B.I);
 }
 
-// One iteration's rigid-elastic glue (rigidElasticBoundaryAccumulationConstraints,
-// xpbdLayer3D.m:381-420 + rigidBoundaryConstraint.m:4-35), rigid contacts
-// (contactConstraints rigid branch, xpbdLayer3D.m:440-484 +
-// penaltyConstraint.projectRigid :30-63) and elastic contacts
-// (projectElastic :4-28), Jacobi style as in the reference.
+// Elastic contacts of one vertex (contactConstraints elastic branch,
+// xpbdLayer3D.m:426-438 + penaltyConstraint.projectElastic :4-28): every
+// contact of the group reads the same step-start position, each updates its
+// multiplier, and the last one's position is kept (MATLAB's scatter).
 template <typename R>
-__global__ void __launch_bounds__(256) k_iterate_bodies(LayerDev L, Body* __restrict__ bodies,
-                                                        R4<R>* __restrict__ pos,
-                                                        const double4* __restrict__ ri,
-                                                        const double* __restrict__ vmass,
-                                                        double* __restrict__ lamB, ContactData cd,
-                                                        double h, double boundary_compliance,
-                                                        double contact_resistance, int use_rigid_contacts) {
-  __shared__ Body sb;
-  int b = blockIdx.x;
-  if (b >= L.nb) {
-    // elastic contacts: one thread per vertex group, all contacts of the group
-    // read the same step-start position and the last one's result is kept
-    int g = (b - L.nb) * blockDim.x + threadIdx.x;
-    if (g >= L.n_ec_groups) return;
-    double h2 = h * h;
-    int k0 = L.ec_off[g], k1 = L.ec_off[g + 1];
-    int v = cd.vid[L.ec_ids[k0]];
-    R4<R> p = pos[v];
-    D3 x = d3((double)p.x, (double)p.y, (double)p.z);
-    double minv = (double)p.w;
-    D3 xn = x;
-    for (int q = k0; q < k1; ++q) {
-      int k = L.ec_ids[q];
-      D3 n = d3(cd.normal[k], cd.normal[cd.K + k], cd.normal[2 * cd.K + k]);
-      D3 c = d3(cd.point[k], cd.point[cd.K + k], cd.point[2 * cd.K + k]);
-      double phi = dot(n, x - c);
-      if (phi > 0) phi = 0;
-      double C = contact_resistance * phi;
-      double aT = cd.compliance[k] / h2;
-      double dl = (-C - aT * cd.lambda[k]) / (2 * minv + aT);
-      cd.lambda[k] += dl;
-      xn = d3(x.x + minv * (dl * n.x), x.y + minv * (dl * n.y), x.z + minv * (dl * n.z));
-    }
-    pos[v] = make_r4<R>((R)xn.x, (R)xn.y, (R)xn.z, p.w);
-    return;
+__device__ __forceinline__ void elastic_contact_group(const LayerDev& L, int g, R4<R>* __restrict__ pos,
+                                                      const ContactData& cd, double h, double contact_resistance) {
+  double h2 = h * h;
+  int k0 = L.ec_off[g], k1 = L.ec_off[g + 1];
+  int v = cd.vid[L.ec_ids[k0]];
+  R4<R> p = ldcg_r4(pos + v);
+  D3 x = d3((double)p.x, (double)p.y, (double)p.z);
+  double minv = (double)p.w;
+  D3 xn = x;
+  for (int q = k0; q < k1; ++q) {
+    int k = L.ec_ids[q];
+    D3 n = d3(cd.normal[k], cd.normal[cd.K + k], cd.normal[2 * cd.K + k]);
+    D3 c = d3(cd.point[k], cd.point[cd.K + k], cd.point[2 * cd.K + k]);
+    double phi = dot(n, x - c);
+    if (phi > 0) phi = 0;
+    double C = contact_resistance * phi;
+    double aT = cd.compliance[k] / h2;
+    double dl = (-C - aT * cd.lambda[k]) / (2 * minv + aT);
+    cd.lambda[k] += dl;
+    xn = d3(x.x + minv * (dl * n.x), x.y + minv * (dl * n.y), x.z + minv * (dl * n.z));
   }
+  stcg_r4(pos + v, make_r4<R>((R)xn.x, (R)xn.y, (R)xn.z, p.w));
+}
+
+// One iteration of one rigid body, run by a whole CTA: the rigid-elastic glue
+// of its boundary vertices (rigidElasticBoundaryAccumulationConstraints,
+// xpbdLayer3D.m:381-420 + rigidBoundaryConstraint.m:4-35) and then its rigid
+// contacts (contactConstraints rigid branch, xpbdLayer3D.m:440-484 +
+// penaltyConstraint.projectRigid :30-63), Jacobi style as in the reference.
+// All bodies are updated whenever the layer has any boundary vertex / rigid
+// contact, as the reference's vectorised update does.
+template <typename R>
+__device__ __forceinline__ void body_iteration(const LayerDev& L, int b, Body* __restrict__ bodies,
+                                               R4<R>* __restrict__ pos, const double4* __restrict__ ri,
+                                               const double* __restrict__ vmass, double* __restrict__ lamB,
+                                               const ContactData& cd, double h, double boundary_compliance,
+                                               double contact_resistance, int use_rigid_contacts, Body& sb) {
   if (threadIdx.x == 0) sb = bodies[b];
   __syncthreads();
   bool dirty = false;
@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(256) k_iterate_bodies(LayerDev L, Body* __rest
     D3 com = d3(sb.com[0], sb.com[1], sb.com[2]);
     for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
       int v = L.bnd_verts[i];
-      R4<R> p = pos[v];
+      R4<R> p = ldcg_r4(pos + v);
       D3 pE = d3((double)p.x, (double)p.y, (double)p.z);
       double minvE = 1.0 / vmass[v];
       D3 pR = body_point(sb, ri[v]);
@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(256) k_iterate_bodies(LayerDev L, Body* __rest
     for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
       int k = L.rc_ids[i];
       int v = cd.vid[k];
-      R4<R> p = pos[v];
+      R4<R> p = ldcg_r4(pos + v);
       D3 x = d3((double)p.x, (double)p.y, (double)p.z);
       D3 pR = body_point(sb, ri[v]);
       D3 r = pR - com;
@@ -332,6 +332,28 @@ __global__ void __launch_bounds__(256) k_iterate_bodies(LayerDev L, Body* __rest
     dirty = true;
   }
   if (dirty && threadIdx.x == 0) bodies[b] = sb;
+  __syncthreads();
+}
+
+// One iteration's body phase as its own launch: CTAs [0, nb) run one body
+// each, the remaining CTAs the elastic contact groups.
+template <typename R>
+__global__ void __launch_bounds__(256) k_iterate_bodies(LayerDev L, Body* __restrict__ bodies,
+                                                        R4<R>* __restrict__ pos,
+                                                        const double4* __restrict__ ri,
+                                                        const double* __restrict__ vmass,
+                                                        double* __restrict__ lamB, ContactData cd,
+                                                        double h, double boundary_compliance,
+                                                        double contact_resistance, int use_rigid_contacts) {
+  __shared__ Body sb;
+  int b = blockIdx.x;
+  if (b >= L.nb) {
+    int g = (b - L.nb) * blockDim.x + threadIdx.x;
+    if (g < L.n_ec_groups) elastic_contact_group<R>(L, g, pos, cd, h, contact_resistance);
+    return;
+  }
+  body_iteration<R>(L, b, bodies, pos, ri, vmass, lamB, cd, h, boundary_compliance, contact_resistance,
+                    use_rigid_contacts, sb);
 }
 
 // xi(pinnedDOFs) = pinnedx (xpbdLayer3D.m:333)
@@ -341,7 +363,7 @@ __global__ void k_pin(R4<R>* __restrict__ pos, const int* __restrict__ dofs,
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int d = dofs[i];
-  reinterpret_cast<R*>(&pos[d / 3])[d % 3] = vals[i];
+  __stcg(reinterpret_cast<R*>(&pos[d / 3]) + d % 3, vals[i]);
 }
 
 // End of projectGS / layer: rotateAllVerts (xpbdLayer3D.m:344, 508-513) and,

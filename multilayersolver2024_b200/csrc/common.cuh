@@ -21,9 +21,22 @@ template <> __host__ __device__ inline double4 make_r4<double>(double x, double 
   return make_double4(x, y, z, w);
 }
 
-// 32-byte aligned double4 loads are split by the compiler into two 16-byte
-// transactions on sm_100; float4 is one 16-byte transaction.
-template <typename R> __device__ __forceinline__ R4<R> ld_r4(const R4<R>* p) { return *p; }
+// Vertex records are read and written through L2 (.cg): inside one
+// persistent launch another SM may have written the record since this SM
+// last cached it, and a tet's corners are never reused by the same SM within
+// a colour, so L1 would only hold stale lines.
+__device__ __forceinline__ float4 ldcg_r4(const float4* p) { return __ldcg(p); }
+__device__ __forceinline__ double4 ldcg_r4(const double4* p) {
+  const double2* q = reinterpret_cast<const double2*>(p);
+  double2 a = __ldcg(q), b = __ldcg(q + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ void stcg_r4(float4* p, float4 v) { __stcg(p, v); }
+__device__ __forceinline__ void stcg_r4(double4* p, double4 v) {
+  double2* q = reinterpret_cast<double2*>(p);
+  __stcg(q, make_double2(v.x, v.y));
+  __stcg(q + 1, make_double2(v.z, v.w));
+}
 
 struct D3 { double x, y, z; };
 __host__ __device__ inline D3 d3(double x, double y, double z) { return {x, y, z}; }

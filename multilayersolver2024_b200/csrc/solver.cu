@@ -14,10 +14,12 @@
 #include "common.cuh"
 #include "tet_kernels.cuh"
 #include "body_kernels.cuh"
+#include "persistent.cuh"
 #include "solver.h"
 
 #include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -163,7 +165,7 @@ struct LayerStatic {
   std::vector<int> color_count;  // per colour: number of elastic tets
   std::vector<int> color_start;  // per colour: start in the elastic list
   std::vector<int> packed;       // body_vert_off | body_verts | bnd_off | bnd_verts | list | vert_body
-  size_t o_bvo = 0, o_bv = 0, o_bo = 0, o_bnd = 0, o_list = 0, o_vb = 0;
+  size_t o_bvo = 0, o_bv = 0, o_bo = 0, o_bnd = 0, o_list = 0, o_vb = 0, o_cstart = 0, o_ccount = 0;
   int n_bnd = 0;
   DevBuf dev;       // packed ints
   DevBuf dev_rigid; // vert_rigid bytes
@@ -248,8 +250,21 @@ struct Solver final : SolverBase {
     cudaGraphExec_t graph = nullptr;
     long long launches_per_step = 0;
   } sim;
-  DevBuf d_vel, d_pin_mask;
+  DevBuf d_vel, d_pin_mask, d_gsync;
+  PinnedBuf h_gsync;
   long long last_launches = 0;
+  // Fixed-iteration layers run as one launch per colour, each launched as a
+  // programmatic dependent of the previous (off with MLXPBD_PDL=0).  The
+  // persistent one-launch-per-layer kernel (MLXPBD_PERSISTENT=1; one CTA of
+  // 128 threads per SM unless MLXPBD_PERSIST_CTAS says otherwise) is kept as
+  // an option: on B200 its grid barrier costs more than a dependent launch.
+  bool persistent = false;
+  bool pdl = true;
+  int persist_ctas = 0;
+  int launch_persistent(const LayerStatic& ls, const int* dint, const LayerDev& L, const ContactData& cd,
+                        const mlx_solve_params* P, int iterations, bool body_work, LayerWork& w);
+  int reset_gsync();
+  int check_gsync();
   // colour-sweep timing: an event pair around every iteration's sweep
   bool sweep_timing = false;
   std::vector<cudaEvent_t> tev;
@@ -420,6 +435,19 @@ int Solver<R>::create(const mlx_mesh_desc* md) {
   CHECK(d_partials.ensure(sizeof(double) * 1024));
   CHECK(d_scalar.ensure(sizeof(double) * 8));
   CHECK(h_scalar.ensure(sizeof(double) * 8));
+  CHECK(d_gsync.ensure(sizeof(unsigned int) * 4));
+  CHECK(h_gsync.ensure(sizeof(int) * 4));
+  CU(cudaMemsetAsync(d_gsync.p, 0, sizeof(unsigned int) * 4, stream));
+  {
+    const char* e = std::getenv("MLXPBD_PERSISTENT");
+    persistent = e && std::string(e) == "1";
+    const char* q = std::getenv("MLXPBD_PDL");
+    pdl = !(q && std::string(q) == "0");
+    const char* n = std::getenv("MLXPBD_PERSIST_CTAS");
+    int sms = 0;
+    CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    persist_ctas = n ? std::max(1, std::min(std::atoi(n), sms)) : sms;
+  }
   CHECK(d_pin_dofs.ensure(sizeof(int) * std::max<size_t>(pinned.size(), 1)));
   CHECK(d_pinx.ensure(sizeof(R) * std::max<size_t>(pinned.size(), 1)));
   CU(cudaMemcpyAsync(d_vid.p, vid.data(), sizeof(int4) * T, cudaMemcpyHostToDevice, stream));
@@ -510,6 +538,12 @@ int Solver<R>::build_static(const mlx_layer_desc* ld, int col, LayerStatic& ls, 
   ls.o_list = put(ls.identity_list ? std::vector<int>() : list);
   ls.o_vb = ls.packed.size();
   ls.packed.insert(ls.packed.end(), rid, rid + N);
+  // colour ranges for the persistent kernel (starts index the list, or the
+  // sorted order when the list is the identity)
+  std::vector<int> cstart(C);
+  for (int c = 0; c < C; ++c) cstart[c] = ls.identity_list ? color_off[c] : ls.color_start[c];
+  ls.o_cstart = put(cstart);
+  ls.o_ccount = put(ls.color_count);
   CHECK(ls.dev.ensure(sizeof(int) * ls.packed.size()));
   CHECK(ls.dev_rigid.ensure(N));
   CU(cudaMemcpyAsync(ls.dev.p, ls.packed.data(), sizeof(int) * ls.packed.size(), cudaMemcpyHostToDevice, stream));
@@ -526,29 +560,39 @@ int Solver<R>::launch_color(int c, const LayerStatic& ls, const int* dlist, R h)
   int count = ls.color_count[c];
   if (count == 0) return MLX_OK;
   const int bs = 64;
-  int grid = blocks_for(count, bs);
   R inv_h2 = R(1) / (h * h), inv_h = R(1) / h;
   TetData<R> td = tets();
   const int* list = ls.identity_list ? nullptr : dlist;
   int begin = ls.identity_list ? color_off[c] : ls.color_start[c];
   const R4<R>* oldp = d_oldp.as<R4<R>>();
+  R4<R>* p = pos();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks_for(count, bs));
+  cfg.blockDim = dim3(bs);
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  cudaError_t e;
   switch (mat_kind) {
     case MAT_NH:
-      k_project_color<R, MAT_NH, false><<<grid, bs, 0, stream>>>(td, list, begin, count, pos(), oldp, inv_h2, inv_h);
+      e = cudaLaunchKernelEx(&cfg, k_project_color<R, MAT_NH, false>, td, list, begin, count, p, oldp, inv_h2, inv_h);
       break;
     case MAT_STVK_BLOCKS:
-      if (damp)
-        k_project_color<R, MAT_STVK_BLOCKS, true><<<grid, bs, 0, stream>>>(td, list, begin, count, pos(), oldp, inv_h2, inv_h);
-      else
-        k_project_color<R, MAT_STVK_BLOCKS, false><<<grid, bs, 0, stream>>>(td, list, begin, count, pos(), oldp, inv_h2, inv_h);
+      e = damp ? cudaLaunchKernelEx(&cfg, k_project_color<R, MAT_STVK_BLOCKS, true>, td, list, begin, count, p, oldp,
+                                    inv_h2, inv_h)
+               : cudaLaunchKernelEx(&cfg, k_project_color<R, MAT_STVK_BLOCKS, false>, td, list, begin, count, p, oldp,
+                                    inv_h2, inv_h);
       break;
     default:
-      if (damp)
-        k_project_color<R, MAT_STVK_LAME, true><<<grid, bs, 0, stream>>>(td, list, begin, count, pos(), oldp, inv_h2, inv_h);
-      else
-        k_project_color<R, MAT_STVK_LAME, false><<<grid, bs, 0, stream>>>(td, list, begin, count, pos(), oldp, inv_h2, inv_h);
+      e = damp ? cudaLaunchKernelEx(&cfg, k_project_color<R, MAT_STVK_LAME, true>, td, list, begin, count, p, oldp,
+                                    inv_h2, inv_h)
+               : cudaLaunchKernelEx(&cfg, k_project_color<R, MAT_STVK_LAME, false>, td, list, begin, count, p, oldp,
+                                    inv_h2, inv_h);
   }
-  CU(cudaGetLastError());
+  if (e != cudaSuccess) return set_error(MLX_ERR_CUDA, std::string("colour launch: ") + cudaGetErrorString(e));
   return MLX_OK;
 }
 
@@ -772,6 +816,32 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
                           L.n_ec_groups > 0;
     const int ecBlocks = blocks_for(L.n_ec_groups, 128);
     bool stopSolve = false;
+    if (persistent && !P->compute_residuals) {
+      // fixed iteration count: the whole projectGS loop of the layer in one launch
+      const int iters = std::max(ld->iterations[layer], 0);
+      if (iters > 0) {
+        const bool timed = sweep_timing && tev_used + 2 <= tev.size();
+        if (timed) CHECK(record_event(tev[tev_used], capturing));
+        CHECK(launch_persistent(ls, dint, L, cd, P, iters, bodyWork, w));
+        if (timed) {
+          double b = 0;
+          for (int c = 0; c < C; ++c) b += ls.color_count[c] * (bytes_per_tet() + (ls.identity_list ? 0.0 : 4.0));
+          CHECK(record_event(tev[tev_used + 1], capturing));
+          tev_bytes[tev_used / 2] = b * iters;
+          tev_launches[tev_used / 2] = 1;
+          tev_used += 2;
+        }
+        ++st.launches;
+        st.totalIterations += iters;
+      }
+      if (ls.nb > 0) {
+        k_finish_layer<R><<<ls.nb, 256, 0, stream>>>(L, w.bodies.as<Body>(), p, resv, ri, rigidLayer ? 1 : 0);
+        CU(cudaGetLastError());
+        ++st.launches;
+      }
+      if (nK > 0) CU(cudaStreamSynchronize(stream));  // cpack is a pageable host source
+      continue;
+    }
     long long it = 1;
     while (it <= ld->iterations[layer] || (!stopSolve && st.runUntil >= 0 && isLast)) {
       ++it;
@@ -845,6 +915,89 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
 }
 
 template <typename R>
+int Solver<R>::reset_gsync() {
+  CU(cudaMemsetAsync(d_gsync.p, 0, sizeof(unsigned int) * 4, stream));
+  return MLX_OK;
+}
+
+// Copies the barrier error flag to the host (stream-ordered); check_gsync
+// reads it after the stream has been synchronised.
+template <typename R>
+int Solver<R>::check_gsync() {
+  if (h_gsync.as<int>()[2] != 0)
+    return set_error(MLX_ERR_LIMIT, "a grid barrier of the persistent layer kernel waited more than 1 s");
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::launch_persistent(const LayerStatic& ls, const int* dint, const LayerDev& L, const ContactData& cd,
+                                 const mlx_solve_params* P, int iterations, bool body_work, LayerWork& w) {
+  PersistArgs pa;
+  pa.list = ls.identity_list ? nullptr : dint + ls.o_list;
+  pa.cstart = dint + ls.o_cstart;
+  pa.ccount = dint + ls.o_ccount;
+  pa.C = C;
+  pa.iterations = iterations;
+  pa.body_work = body_work ? 1 : 0;
+  pa.pin_dofs = d_pin_dofs.as<int>();
+  pa.npin = (int)pinned.size();
+  int maxc = 0;
+  for (int c = 0; c < C; ++c) maxc = std::max(maxc, ls.color_count[c]);
+  pa.one_per_thread = maxc <= persist_ctas * 128 ? 1 : 0;
+  GridSync gs;
+  gs.count = d_gsync.as<unsigned int>();
+  gs.error = reinterpret_cast<int*>(d_gsync.as<unsigned int>() + 2);
+  const R hR = (R)P->h;
+  const R inv_h2 = R(1) / (hR * hR), inv_h = R(1) / hR;
+  TetData<R> td = tets();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(persist_ctas);
+  cfg.blockDim = dim3(128);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  // the arrival counter restarts at zero for every launch (barrier k of a
+  // launch waits for k * grid arrivals); the error flag is kept for the step
+  CU(cudaMemsetAsync(d_gsync.p, 0, sizeof(unsigned int), stream));
+  Body* bodies = w.bodies.as<Body>();
+  double* lamB = w.lamB.as<double>();
+  const double4* ri = d_ri.as<double4>();
+  const R4<R>* oldp = d_oldp.as<R4<R>>();
+  const double* vm = d_vmass.as<double>();
+  const R* pv = d_pinx.as<R>();
+  const double h = P->h;
+  cudaError_t e;
+  switch (mat_kind) {
+    case MAT_NH:
+      e = cudaLaunchKernelEx(&cfg, k_layer_persistent<R, MAT_NH, false>, td, pa, pos(), oldp, inv_h2, inv_h, L,
+                             bodies, ri, vm, lamB, cd, h, P->boundary_compliance, P->contact_resistance,
+                             P->use_rigid_contacts, pv, gs);
+      break;
+    case MAT_STVK_BLOCKS:
+      e = damp ? cudaLaunchKernelEx(&cfg, k_layer_persistent<R, MAT_STVK_BLOCKS, true>, td, pa, pos(), oldp, inv_h2,
+                                    inv_h, L, bodies, ri, vm, lamB, cd, h, P->boundary_compliance,
+                                    P->contact_resistance, P->use_rigid_contacts, pv, gs)
+               : cudaLaunchKernelEx(&cfg, k_layer_persistent<R, MAT_STVK_BLOCKS, false>, td, pa, pos(), oldp,
+                                    inv_h2, inv_h, L, bodies, ri, vm, lamB, cd, h, P->boundary_compliance,
+                                    P->contact_resistance, P->use_rigid_contacts, pv, gs);
+      break;
+    default:
+      e = damp ? cudaLaunchKernelEx(&cfg, k_layer_persistent<R, MAT_STVK_LAME, true>, td, pa, pos(), oldp, inv_h2,
+                                    inv_h, L, bodies, ri, vm, lamB, cd, h, P->boundary_compliance,
+                                    P->contact_resistance, P->use_rigid_contacts, pv, gs)
+               : cudaLaunchKernelEx(&cfg, k_layer_persistent<R, MAT_STVK_LAME, false>, td, pa, pos(), oldp,
+                                    inv_h2, inv_h, L, bodies, ri, vm, lamB, cd, h, P->boundary_compliance,
+                                    P->contact_resistance, P->use_rigid_contacts, pv, gs);
+  }
+  if (e != cudaSuccess) return set_error(MLX_ERR_CUDA, std::string("persistent layer launch: ") + cudaGetErrorString(e));
+  return MLX_OK;
+}
+
+template <typename R>
 int Solver<R>::layer_solve(const mlx_layer_desc* ld, const mlx_solve_params* P, const mlx_contacts* K,
                            const mlx_solve_inputs* in, mlx_solve_outputs* out) {
   if (!ld || !P || !in || !out) return set_error(MLX_ERR_ARGUMENT, "null argument");
@@ -883,13 +1036,16 @@ int Solver<R>::layer_solve(const mlx_layer_desc* ld, const mlx_solve_params* P, 
   st.residualArray.assign(in->residual_in, in->residual_in + std::max(in->residual_in_len, 0));
   st.runUntil = P->run_until;
   st.sumNonMon = in->sum_non_monitored_time;
+  CHECK(reset_gsync());
   CHECK(run_layers(ld, P, K, cd, st, false, work));
+  CU(cudaMemcpyAsync(h_gsync.p, d_gsync.p, sizeof(unsigned int) * 4, cudaMemcpyDeviceToHost, stream));
   // ---- download ----
   k_store_pos<R><<<blocks_for(N, bs), bs, 0, stream>>>(pos(), ds, N);
   if (out->lambdai) k_store_lambda<R><<<blocks_for(T, bs), bs, 0, stream>>>(d_lambda.as<R>(), d_s2e.as<int>(), ds + n3, T);
   CU(cudaGetLastError());
   CU(cudaMemcpyAsync(hs, ds, sizeof(double) * (out->lambdai ? n3 + n6 : n3), cudaMemcpyDeviceToHost, stream));
   CU(cudaStreamSynchronize(stream));
+  CHECK(check_gsync());
   std::memcpy(out->xi, hs, sizeof(double) * n3);
   if (out->lambdai) std::memcpy(out->lambdai, hs + n3, sizeof(double) * n6);
   int n = (int)st.residualArray.size();
@@ -1085,12 +1241,14 @@ int Solver<R>::sim_issue_step(long long* launches) {
                                                           sim.air_drag);
   CU(cudaGetLastError());
   CU(cudaMemsetAsync(d_lambda.p, 0, sizeof(R) * 6 * (size_t)T, stream));
+  CHECK(reset_gsync());
   RunState st;
   st.runUntil = sim.P.run_until;
   ContactData cd{};
   CHECK(run_layers(&sim.ld, &sim.P, nullptr, cd, st, true, sim_work));
   k_sim_end<R><<<blocks_for(N, 256), 256, 0, stream>>>(p, d_oldp.as<R4<R>>(), d_vel.as<R4<R>>(), N, h);
   CU(cudaGetLastError());
+  CU(cudaMemcpyAsync(h_gsync.p, d_gsync.p, sizeof(unsigned int) * 4, cudaMemcpyDeviceToHost, stream));
   if (launches) *launches = st.launches + 2;
   return MLX_OK;
 }
@@ -1133,6 +1291,7 @@ int Solver<R>::sim_step(int nsteps, int use_graph, double* device_ms) {
     if (sweep_timing) {  // the event pairs are reused by every step
       CU(cudaStreamSynchronize(stream));
       CHECK(collect_sweep_times());
+      CHECK(check_gsync());
     }
   }
   if (device_ms) {
@@ -1145,6 +1304,7 @@ int Solver<R>::sim_step(int nsteps, int use_graph, double* device_ms) {
     cudaEventDestroy(e1);
   }
   CU(cudaStreamSynchronize(stream));
+  CHECK(check_gsync());
   return MLX_OK;
 }
 

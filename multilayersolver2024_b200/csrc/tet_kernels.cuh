@@ -373,22 +373,17 @@ __device__ __forceinline__ void load_tet(const TetData<R>& td, int s, const R4<R
   v = td.vid[s];
 #pragma unroll
   for (int j = 0; j < 9; ++j) G[j] = td.dminv[(size_t)j * td.T + s];
-  R4<R> p0 = pos[v.x], p1 = pos[v.y], p2 = pos[v.z], p3 = pos[v.w];
+  R4<R> p0 = ldcg_r4(pos + v.x), p1 = ldcg_r4(pos + v.y), p2 = ldcg_r4(pos + v.z), p3 = ldcg_r4(pos + v.w);
   X[0] = {p0.x, p0.y, p0.z}; X[1] = {p1.x, p1.y, p1.z};
   X[2] = {p2.x, p2.y, p2.z}; X[3] = {p3.x, p3.y, p3.z};
   minv[0] = p0.w; minv[1] = p1.w; minv[2] = p2.w; minv[3] = p3.w;
 }
 
-// One colour of the Gauss-Seidel sweep (xpbdLayer3D.m:357-378).  `list` holds
-// the colour-sorted ids of this layer's elastic tets of this colour; NULL
-// means the identity over [begin, begin+count).
+// Projection of one tet (colour-sorted id s) in place: gather, project,
+// scatter, lambda += dlambda (xpbdLayer3D.m:358-377 for one element).
 template <typename R, int MAT, bool DAMP>
-__global__ void __launch_bounds__(128) k_project_color(TetData<R> td, const int* __restrict__ list,
-                                                       int begin, int count, R4<R>* __restrict__ pos,
-                                                       const R4<R>* __restrict__ oldp, R inv_h2, R inv_h) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= count) return;
-  int s = list ? list[begin + i] : begin + i;
+__device__ __forceinline__ void project_tet(const TetData<R>& td, int s, R4<R>* __restrict__ pos,
+                                            const R4<R>* __restrict__ oldp, R inv_h2, R inv_h) {
   int4 v;
   R G[9], minv[4];
   V3<R> X[4];
@@ -417,10 +412,75 @@ __global__ void __launch_bounds__(128) k_project_color(TetData<R> td, const int*
 #pragma unroll
     for (int q = 0; q < 6; ++q) td.lambda[(size_t)q * T + s] = lam[q] + dl[q];
   }
-  pos[v.x] = make_r4<R>(X[0].x, X[0].y, X[0].z, minv[0]);
-  pos[v.y] = make_r4<R>(X[1].x, X[1].y, X[1].z, minv[1]);
-  pos[v.z] = make_r4<R>(X[2].x, X[2].y, X[2].z, minv[2]);
-  pos[v.w] = make_r4<R>(X[3].x, X[3].y, X[3].z, minv[3]);
+  stcg_r4(pos + v.x, make_r4<R>(X[0].x, X[0].y, X[0].z, minv[0]));
+  stcg_r4(pos + v.y, make_r4<R>(X[1].x, X[1].y, X[1].z, minv[1]));
+  stcg_r4(pos + v.z, make_r4<R>(X[2].x, X[2].y, X[2].z, minv[2]));
+  stcg_r4(pos + v.w, make_r4<R>(X[3].x, X[3].y, X[3].z, minv[3]));
+}
+
+// Programmatic dependent launch: a colour kernel launched with
+// cudaLaunchAttributeProgrammaticStreamSerialization starts while the previous
+// kernel of the stream still runs; griddepcontrol.wait blocks until that
+// kernel has completed and its writes are visible (a no-op without the
+// attribute).  launch_dependents lets the next colour start early in turn.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;"); }
+
+// One colour of the Gauss-Seidel sweep (xpbdLayer3D.m:357-378).  `list` holds
+// the colour-sorted ids of this layer's elastic tets of this colour; NULL
+// means the identity over [begin, begin+count).  The tet's read-only data
+// (ids, DmInv, volume, material) is loaded before waiting on the previous
+// colour; positions and multipliers after.
+template <typename R, int MAT, bool DAMP>
+__global__ void __launch_bounds__(128) k_project_color(TetData<R> td, const int* __restrict__ list,
+                                                       int begin, int count, R4<R>* __restrict__ pos,
+                                                       const R4<R>* __restrict__ oldp, R inv_h2, R inv_h) {
+  pdl_launch_dependents();
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = i < count;
+  const int T = td.T;
+  int s = 0;
+  int4 v = make_int4(0, 0, 0, 0);
+  R G[9], vol = 0, mat[mat_stride(MAT)];
+  if (active) {
+    s = list ? list[begin + i] : begin + i;
+    v = td.vid[s];
+#pragma unroll
+    for (int j = 0; j < 9; ++j) G[j] = td.dminv[(size_t)j * T + s];
+    vol = td.vol[s];
+#pragma unroll
+    for (int q = 0; q < mat_stride(MAT); ++q) mat[q] = td.mat[(size_t)q * T + s];
+  }
+  pdl_wait();
+  if (!active) return;
+  R4<R> p0 = ldcg_r4(pos + v.x), p1 = ldcg_r4(pos + v.y), p2 = ldcg_r4(pos + v.z), p3 = ldcg_r4(pos + v.w);
+  V3<R> X[4] = {{p0.x, p0.y, p0.z}, {p1.x, p1.y, p1.z}, {p2.x, p2.y, p2.z}, {p3.x, p3.y, p3.z}};
+  R minv[4] = {p0.w, p1.w, p2.w, p3.w};
+  if (MAT == MAT_NH) {
+    double lam[2] = {(double)td.lambda[s], (double)td.lambda[(size_t)T + s]}, dl[2];
+    nh_project<R>(X, minv, G, (double)mat[0], (double)mat[1], (double)vol, (double)inv_h2, lam, dl);
+    td.lambda[s] = (R)(lam[0] + dl[0]);
+    td.lambda[(size_t)T + s] = (R)(lam[1] + dl[1]);
+  } else {
+    Compliance<R> cm;
+    load_compliance<R, MAT>(mat, 0, 1, inv_h2, inv_h, cm, DAMP);
+    R lam[6], dl[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) lam[q] = td.lambda[(size_t)q * T + s];
+    V3<R> Xo[4];
+    if (DAMP) {
+      R4<R> o0 = oldp[v.x], o1 = oldp[v.y], o2 = oldp[v.z], o3 = oldp[v.w];
+      Xo[0] = {o0.x, o0.y, o0.z}; Xo[1] = {o1.x, o1.y, o1.z};
+      Xo[2] = {o2.x, o2.y, o2.z}; Xo[3] = {o3.x, o3.y, o3.z};
+    }
+    stvk_project<R, MAT, DAMP>(X, Xo, minv, G, vol, cm, lam, dl);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) td.lambda[(size_t)q * T + s] = lam[q] + dl[q];
+  }
+  stcg_r4(pos + v.x, make_r4<R>(X[0].x, X[0].y, X[0].z, minv[0]));
+  stcg_r4(pos + v.y, make_r4<R>(X[1].x, X[1].y, X[1].z, minv[1]));
+  stcg_r4(pos + v.z, make_r4<R>(X[2].x, X[2].y, X[2].z, minv[2]));
+  stcg_r4(pos + v.w, make_r4<R>(X[3].x, X[3].y, X[3].z, minv[3]));
 }
 
 // ---------------------------------------------------------------------------
@@ -504,7 +564,7 @@ __global__ void __launch_bounds__(256) k_residual_partials(TetData<R> td, const 
     // (xpbdLayer3D.m:581-583), so contact k meets every compliance j
     int cb = blockIdx.x - tetBlocks, ncb = gridDim.x - tetBlocks;
     for (int k = cb * blockDim.x + threadIdx.x; k < cd.K; k += ncb * blockDim.x) {
-      R4<R> p = pos[cd.vid[k]];
+      R4<R> p = ldcg_r4(pos + cd.vid[k]);
       double n0 = cd.normal[k], n1 = cd.normal[cd.K + k], n2 = cd.normal[2 * cd.K + k];
       double phi = n0 * ((double)p.x - cd.point[k]) + n1 * ((double)p.y - cd.point[cd.K + k]) +
                    n2 * ((double)p.z - cd.point[2 * cd.K + k]);

@@ -140,3 +140,18 @@ def test_fp64_matches_reference_execution(gpu, name):
     assert rel_pos_err(xi, gold[f"{name}_xi"], case.mesh) <= TOL64
     np.testing.assert_allclose(res, gold[f"{name}_residual"], rtol=1e-9, atol=1e-14)
     assert run_until == pytest.approx(float(gold[f"{name}_run_until"]), rel=1e-9)
+
+
+@pytest.mark.parametrize("persistent,pdl", [("0", "1"), ("0", "0"), ("1", "1")])
+def test_launch_paths_agree(gpu, monkeypatch, persistent, pdl):
+    """Fixed iteration counts run as one launch per colour with programmatic
+    dependent launches (default), without them (MLXPBD_PDL=0), or as one
+    cooperative launch per layer (MLXPBD_PERSISTENT=1); all match the oracle,
+    bodies, glue and contacts included."""
+    monkeypatch.setenv("MLXPBD_PERSISTENT", persistent)
+    monkeypatch.setenv("MLXPBD_PDL", pdl)
+    m = block_mesh(dims=(8, 3, 3), energy=_lib.MLX_ENERGY_NEOHOOKEAN, seed=41)
+    case = Case(m, [50, 25, 0], [2, 3, 5], seed=42)
+    case.integ.boundaryCompliance = 0.0
+    case.contacts = _contacts(case)
+    _compare(case)
