@@ -197,11 +197,21 @@ __global__ void __launch_bounds__(256) k_rigid_step(LayerDev L, Body* __restrict
   }
 }
 
-// rigidGeneralizedInverseMass (3d/constraints/rigidGeneralizedInverseMass.m)
-__device__ __forceinline__ double gen_inv_mass(double invM, D3 r, const double* I, D3 n) {
+// rigidGeneralizedInverseMass (3d/constraints/rigidGeneralizedInverseMass.m):
+// w = 1/M + (r x n)' I^-1 (r x n), with I^-1 formed once per body update
+// (the reference solves I \ axis per vertex; the results agree to rounding).
+__device__ __forceinline__ double gen_inv_mass(double invM, D3 r, const double* invI, D3 n) {
   D3 axis = cross(r, n);
-  D3 ic = solve3_piv(I, axis);
-  return invM + dot(axis, ic);
+  return invM + dot(axis, mv3(invI, axis));
+}
+
+// inverse of a 3x3 column-major matrix by columns of a pivoted solve
+__device__ __forceinline__ void inverse3(const double* A, double* inv) {
+  for (int c = 0; c < 3; ++c) {
+    D3 e = d3(c == 0, c == 1, c == 2);
+    D3 col = solve3_piv(A, e);
+    inv[3 * c] = col.x; inv[3 * c + 1] = col.y; inv[3 * c + 2] = col.z;
+  }
 }
 
 // Per-body update after an accumulation (xpbdLayer3D.m:401-414, 466-479).
@@ -256,8 +266,12 @@ __device__ __forceinline__ void body_iteration(const LayerDev& L, int b, Body* _
                                                R4<R>* __restrict__ pos, const double4* __restrict__ ri,
                                                const double* __restrict__ vmass, double* __restrict__ lamB,
                                                const ContactData& cd, double h, double boundary_compliance,
-                                               double contact_resistance, int use_rigid_contacts, Body& sb) {
-  if (threadIdx.x == 0) sb = bodies[b];
+                                               double contact_resistance, int use_rigid_contacts, Body& sb,
+                                               double* invI) {
+  if (threadIdx.x == 0) {
+    sb = bodies[b];
+    inverse3(sb.I, invI);
+  }
   __syncthreads();
   bool dirty = false;
   if (L.any_boundary) {
@@ -278,7 +292,7 @@ __device__ __forceinline__ void body_iteration(const LayerDev& L, int b, Body* _
       if (isnan(n.x)) n.x = 0;
       if (isnan(n.y)) n.y = 0;
       if (isnan(n.z)) n.z = 0;
-      double w = gen_inv_mass(invM, r, sb.I, n);
+      double w = gen_inv_mass(invM, r, invI, n);
       double dl = (-C - boundary_compliance * lamB[i]) / ((minvE + w) + boundary_compliance);
       lamB[i] += dl;
       D3 pp = dl * n;
@@ -287,7 +301,10 @@ __device__ __forceinline__ void body_iteration(const LayerDev& L, int b, Body* _
       s[3] += dw.x; s[4] += dw.y; s[5] += dw.z;
     }
     block_sum<6>(s);
-    if (threadIdx.x == 0) apply_increments(sb, s, h);
+    if (threadIdx.x == 0) {
+      apply_increments(sb, s, h);
+      inverse3(sb.I, invI);
+    }
     __syncthreads();
     for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
       int v = L.bnd_verts[i];
@@ -313,7 +330,7 @@ __device__ __forceinline__ void body_iteration(const LayerDev& L, int b, Body* _
       double phi = dot(n, x - c);
       if (phi > 0) phi = 0;
       double C = contact_resistance * phi;
-      double w = gen_inv_mass(invM, r, sb.I, n);
+      double w = gen_inv_mass(invM, r, invI, n);
       double aT = (2 * cd.compliance[k]) / h2;
       double dl = (-C - aT * cd.lambda[k]) / (2 * w + aT);
       cd.lambda[k] += dl;
@@ -346,6 +363,9 @@ __global__ void __launch_bounds__(256) k_iterate_bodies(LayerDev L, Body* __rest
                                                         double h, double boundary_compliance,
                                                         double contact_resistance, int use_rigid_contacts) {
   __shared__ Body sb;
+  __shared__ double invI[9];
+  pdl_launch_dependents();
+  pdl_wait();
   int b = blockIdx.x;
   if (b >= L.nb) {
     int g = (b - L.nb) * blockDim.x + threadIdx.x;
@@ -353,13 +373,15 @@ __global__ void __launch_bounds__(256) k_iterate_bodies(LayerDev L, Body* __rest
     return;
   }
   body_iteration<R>(L, b, bodies, pos, ri, vmass, lamB, cd, h, boundary_compliance, contact_resistance,
-                    use_rigid_contacts, sb);
+                    use_rigid_contacts, sb, invI);
 }
 
 // xi(pinnedDOFs) = pinnedx (xpbdLayer3D.m:333)
 template <typename R>
 __global__ void k_pin(R4<R>* __restrict__ pos, const int* __restrict__ dofs,
                       const R* __restrict__ vals, int n) {
+  pdl_launch_dependents();
+  pdl_wait();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int d = dofs[i];

@@ -154,6 +154,7 @@ __global__ void __launch_bounds__(128) k_layer_persistent(TetData<R> td, Persist
                                                           int use_rigid_contacts, const R* __restrict__ pin_vals,
                                                           GridSync gs) {
   __shared__ Body sb;
+  __shared__ double invI[9];
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int nthreads = gridDim.x * blockDim.x;
   unsigned k = 0;  // barriers passed
@@ -191,7 +192,7 @@ __global__ void __launch_bounds__(128) k_layer_persistent(TetData<R> td, Persist
     if (pa.body_work) {
       for (int b = blockIdx.x; b < L.nb; b += gridDim.x)
         body_iteration<R>(L, b, bodies, pos, ri, vmass, lamB, cd, h, boundary_compliance, contact_resistance,
-                          use_rigid_contacts, sb);
+                          use_rigid_contacts, sb, invI);
       for (int g = tid; g < L.n_ec_groups; g += nthreads) elastic_contact_group<R>(L, g, pos, cd, h, contact_resistance);
       if (!grid_sync(gs, k)) return;
     }

@@ -265,6 +265,19 @@ struct Solver final : SolverBase {
                         const mlx_solve_params* P, int iterations, bool body_work, LayerWork& w);
   int reset_gsync();
   int check_gsync();
+  cudaLaunchConfig_t pdl_config(int grid, int block) const {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.stream = stream;
+    return cfg;
+  }
+  static cudaLaunchAttribute pdl_attr() {
+    cudaLaunchAttribute a;
+    a.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    a.val.programmaticStreamSerializationAllowed = 1;
+    return a;
+  }
   // colour-sweep timing: an event pair around every iteration's sweep
   bool sweep_timing = false;
   std::vector<cudaEvent_t> tev;
@@ -865,15 +878,21 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
         tev_used += 2;
       }
       if (bodyWork) {
-        k_iterate_bodies<R><<<ls.nb + ecBlocks, 128, 0, stream>>>(
-            L, w.bodies.as<Body>(), p, ri, d_vmass.as<double>(), w.lamB.as<double>(), cd, h,
-            P->boundary_compliance, P->contact_resistance, P->use_rigid_contacts);
-        CU(cudaGetLastError());
+        cudaLaunchConfig_t cfg = pdl_config(ls.nb + ecBlocks, 128);
+        cudaLaunchAttribute attr = pdl_attr();
+        cfg.attrs = &attr;
+        cfg.numAttrs = pdl ? 1 : 0;
+        CU(cudaLaunchKernelEx(&cfg, k_iterate_bodies<R>, L, w.bodies.as<Body>(), p, (const double4*)ri,
+                              (const double*)d_vmass.as<double>(), w.lamB.as<double>(), cd, h,
+                              P->boundary_compliance, P->contact_resistance, (int)P->use_rigid_contacts));
         ++st.launches;
       }
       if (np) {
-        k_pin<R><<<blocks_for((long long)np, 256), 256, 0, stream>>>(p, d_pin_dofs.as<int>(), d_pinx.as<R>(), (int)np);
-        CU(cudaGetLastError());
+        cudaLaunchConfig_t cfg = pdl_config(blocks_for((long long)np, 256), 256);
+        cudaLaunchAttribute attr = pdl_attr();
+        cfg.attrs = &attr;
+        cfg.numAttrs = pdl ? 1 : 0;
+        CU(cudaLaunchKernelEx(&cfg, k_pin<R>, p, (const int*)d_pin_dofs.as<int>(), (const R*)d_pinx.as<R>(), (int)np));
         ++st.launches;
       }
       bool endLayer = false;
