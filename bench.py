@@ -252,6 +252,8 @@ def run_ours(args, rank, world, local):
     line = None
     if rank == 0:
         peak, peak_kind = measured_peak_hbm()
+        sweep_kernel = ("k_layer_cluster (whole projectGS loop of a layer)" if solver.launch_path.startswith("cluster")
+                        else "k_project_color (all colours of a sweep)")
         achieved = (sweep_bytes / (sweep_ms / 1000.0)) / 1e9 if sweep_ms > 0 else None
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
@@ -268,7 +270,8 @@ def run_ours(args, rank, world, local):
                        "iterations_per_step": int(sum(sc.iterations)), "precision": "FP32 bulk, FP64 rigid bodies",
                        "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}",
                        "graph": "one CUDA graph per step"},
-            "roofline": {"bound": "hbm", "kernel": "k_project_color (all colours of a sweep)",
+            "roofline": {"bound": "hbm", "kernel": sweep_kernel,
+                         "launch_path": solver.launch_path,
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None,
                          "traffic": (profiled_dram_bytes_per_tet() * sweep_bytes / solver_bytes_per_tet(m, MLX_FP32)
@@ -295,13 +298,14 @@ def run_ours(args, rank, world, local):
 
 def solver_bytes_per_tet(mesh, precision):
     """Algorithmic bytes of one tet projection in the device layout: vertex
-    ids (16), DmInv (9 r), volume (r), material (2 r for Neo-Hookean, 3 r for
-    StVK from Lame parameters), lambda read + write (2 x 2 r or 2 x 6 r), four
-    vertex records read and written (8 x 4 r); r = 4 (FP32) or 8 (FP64)."""
+    ids (16), DmInv (9 r), volume (r, StVK only), material (2 r for the
+    Neo-Hookean compliances, which include the volume, 3 r for StVK from Lame
+    parameters), lambda read + write (2 x 2 r or 2 x 6 r), four vertex records
+    read and written (8 x 4 r); r = 4 (FP32) or 8 (FP64)."""
     from multilayersolver2024_b200 import MLX_ENERGY_NEOHOOKEAN
     r = 4 if precision == 0 else 8
     nh = mesh.energy_type == MLX_ENERGY_NEOHOOKEAN
-    return 16 + 9 * r + r + (2 if nh else 3) * r + 2 * (2 if nh else 6) * r + 8 * 4 * r
+    return 16 + 9 * r + (0 if nh else r) + (2 if nh else 3) * r + 2 * (2 if nh else 6) * r + 8 * 4 * r
 
 
 def main():

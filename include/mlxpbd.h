@@ -211,6 +211,11 @@ int mlx_sim_sweep_stats(mlx_solver* solver, double* ms, double* bytes, long long
  * kernel launches of the last mlx_layer_solve call. */
 long long mlx_sim_launches_per_step(const mlx_solver* solver);
 long long mlx_last_call_launches(const mlx_solver* solver);
+/* No counterpart in the reference.  Writes a one-line description of how
+ * fixed-iteration layers are launched on this solver's device (thread-block
+ * cluster size and threads, or per-colour launches) into buf (NUL-terminated,
+ * at most n bytes).  Returns the length of the full description. */
+int mlx_launch_path(const mlx_solver* solver, char* buf, int32_t n);
 
 /* ---- allocation-free residual ------------------------------------------
  * No counterpart in the reference.  The elastic constraint residual of

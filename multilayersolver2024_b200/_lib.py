@@ -123,6 +123,7 @@ SIGNATURES = {
     "mlx_sim_sweep_stats": ([C.c_void_p, _f64p, _f64p, C.POINTER(C.c_longlong), C.c_int32], C.c_int),
     "mlx_sim_launches_per_step": ([C.c_void_p], C.c_longlong),
     "mlx_last_call_launches": ([C.c_void_p], C.c_longlong),
+    "mlx_launch_path": ([C.c_void_p, C.c_char_p, C.c_int32], C.c_int),
     "mlx_stvk_residual_noalloc": ([C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p], C.c_int),
     "mlx_greedy_coloring": ([_i32p, C.c_int32, C.c_int32, _i32p, _i32p], C.c_int),

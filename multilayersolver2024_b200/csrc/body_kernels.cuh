@@ -79,10 +79,14 @@ __device__ __forceinline__ D3 body_point(const Body& b, const double4& r) {
   return mv3(b.R, d3(r.x, r.y, r.z)) + d3(b.com[0], b.com[1], b.com[2]);
 }
 
+template <typename R, typename P>
+__device__ __forceinline__ void store_xyz(const P& pos, int v, D3 x) {
+  R4<R> p = pos.ld(v);
+  pos.st(v, make_r4<R>((R)x.x, (R)x.y, (R)x.z, p.w));
+}
 template <typename R>
 __device__ __forceinline__ void store_xyz(R4<R>* pos, int v, D3 x) {
-  R4<R> p = ldcg_r4(pos + v);
-  stcg_r4(pos + v, make_r4<R>((R)x.x, (R)x.y, (R)x.z, p.w));
+  store_xyz<R>(GlobalPos<R>{pos}, v, x);
 }
 
 // AdaptiveMesh3D.makeRigidsFromConnectivity (AdaptiveMesh3D.m:32-43) ->
@@ -229,13 +233,13 @@ __device__ __forceinline__ void apply_increments(Body& B, const double* s, doubl
 // xpbdLayer3D.m:426-438 + penaltyConstraint.projectElastic :4-28): every
 // contact of the group reads the same step-start position, each updates its
 // multiplier, and the last one's position is kept (MATLAB's scatter).
-template <typename R>
-__device__ __forceinline__ void elastic_contact_group(const LayerDev& L, int g, R4<R>* __restrict__ pos,
+template <typename R, typename P>
+__device__ __forceinline__ void elastic_contact_group(const LayerDev& L, int g, const P& pos,
                                                       const ContactData& cd, double h, double contact_resistance) {
   double h2 = h * h;
   int k0 = L.ec_off[g], k1 = L.ec_off[g + 1];
   int v = cd.vid[L.ec_ids[k0]];
-  R4<R> p = ldcg_r4(pos + v);
+  R4<R> p = pos.ld(v);
   D3 x = d3((double)p.x, (double)p.y, (double)p.z);
   double minv = (double)p.w;
   D3 xn = x;
@@ -251,7 +255,7 @@ __device__ __forceinline__ void elastic_contact_group(const LayerDev& L, int g, 
     cd.lambda[k] += dl;
     xn = d3(x.x + minv * (dl * n.x), x.y + minv * (dl * n.y), x.z + minv * (dl * n.z));
   }
-  stcg_r4(pos + v, make_r4<R>((R)xn.x, (R)xn.y, (R)xn.z, p.w));
+  pos.st(v, make_r4<R>((R)xn.x, (R)xn.y, (R)xn.z, p.w));
 }
 
 // One iteration of one rigid body, run by a whole CTA: the rigid-elastic glue
@@ -261,9 +265,9 @@ __device__ __forceinline__ void elastic_contact_group(const LayerDev& L, int g, 
 // penaltyConstraint.projectRigid :30-63), Jacobi style as in the reference.
 // All bodies are updated whenever the layer has any boundary vertex / rigid
 // contact, as the reference's vectorised update does.
-template <typename R>
+template <typename R, typename P>
 __device__ __forceinline__ void body_iteration(const LayerDev& L, int b, Body* __restrict__ bodies,
-                                               R4<R>* __restrict__ pos, const double4* __restrict__ ri,
+                                               const P& pos, const double4* __restrict__ ri,
                                                const double* __restrict__ vmass, double* __restrict__ lamB,
                                                const ContactData& cd, double h, double boundary_compliance,
                                                double contact_resistance, int use_rigid_contacts, Body& sb,
@@ -281,7 +285,7 @@ __device__ __forceinline__ void body_iteration(const LayerDev& L, int b, Body* _
     D3 com = d3(sb.com[0], sb.com[1], sb.com[2]);
     for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
       int v = L.bnd_verts[i];
-      R4<R> p = ldcg_r4(pos + v);
+      R4<R> p = pos.ld(v);
       D3 pE = d3((double)p.x, (double)p.y, (double)p.z);
       double minvE = 1.0 / vmass[v];
       D3 pR = body_point(sb, ri[v]);
@@ -313,6 +317,7 @@ __device__ __forceinline__ void body_iteration(const LayerDev& L, int b, Body* _
     dirty = true;
   }
   if (use_rigid_contacts && L.any_rigid_contact) {
+    pos.fence();
     __syncthreads();
     double s[6] = {0, 0, 0, 0, 0, 0};
     int beg = L.rc_off[b], end = L.rc_off[b + 1];
@@ -321,7 +326,7 @@ __device__ __forceinline__ void body_iteration(const LayerDev& L, int b, Body* _
     for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
       int k = L.rc_ids[i];
       int v = cd.vid[k];
-      R4<R> p = ldcg_r4(pos + v);
+      R4<R> p = pos.ld(v);
       D3 x = d3((double)p.x, (double)p.y, (double)p.z);
       D3 pR = body_point(sb, ri[v]);
       D3 r = pR - com;
@@ -349,6 +354,7 @@ __device__ __forceinline__ void body_iteration(const LayerDev& L, int b, Body* _
     dirty = true;
   }
   if (dirty && threadIdx.x == 0) bodies[b] = sb;
+  pos.fence();
   __syncthreads();
 }
 
@@ -369,10 +375,10 @@ __global__ void __launch_bounds__(256) k_iterate_bodies(LayerDev L, Body* __rest
   int b = blockIdx.x;
   if (b >= L.nb) {
     int g = (b - L.nb) * blockDim.x + threadIdx.x;
-    if (g < L.n_ec_groups) elastic_contact_group<R>(L, g, pos, cd, h, contact_resistance);
+    if (g < L.n_ec_groups) elastic_contact_group<R>(L, g, GlobalPos<R>{pos}, cd, h, contact_resistance);
     return;
   }
-  body_iteration<R>(L, b, bodies, pos, ri, vmass, lamB, cd, h, boundary_compliance, contact_resistance,
+  body_iteration<R>(L, b, bodies, GlobalPos<R>{pos}, ri, vmass, lamB, cd, h, boundary_compliance, contact_resistance,
                     use_rigid_contacts, sb, invI);
 }
 
@@ -385,7 +391,7 @@ __global__ void k_pin(R4<R>* __restrict__ pos, const int* __restrict__ dofs,
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int d = dofs[i];
-  __stcg(reinterpret_cast<R*>(&pos[d / 3]) + d % 3, vals[i]);
+  GlobalPos<R>{pos}.st_comp(d / 3, d % 3, vals[i]);
 }
 
 // End of projectGS / layer: rotateAllVerts (xpbdLayer3D.m:344, 508-513) and,

@@ -38,6 +38,21 @@ __device__ __forceinline__ void stcg_r4(double4* p, double4 v) {
   __stcg(q + 1, make_double2(v.z, v.w));
 }
 
+// Vertex records addressed by vertex id in global memory.  The body, contact
+// and pinning phases are written against this interface so the cluster
+// kernel can run them on records held in distributed shared memory.
+template <typename R> struct GlobalPos {
+  R4<R>* p;
+  __device__ __forceinline__ R4<R> ld(int v) const { return ldcg_r4(p + v); }
+  __device__ __forceinline__ void st(int v, R4<R> x) const { stcg_r4(p + v, x); }
+  __device__ __forceinline__ void st_comp(int v, int c, R val) const {
+    __stcg(reinterpret_cast<R*>(p + v) + c, val);
+  }
+  // orders this thread's record stores before a following CTA barrier
+  // (__syncthreads already does so for global memory)
+  __device__ __forceinline__ void fence() const {}
+};
+
 struct D3 { double x, y, z; };
 __host__ __device__ inline D3 d3(double x, double y, double z) { return {x, y, z}; }
 __host__ __device__ inline D3 operator+(D3 a, D3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }

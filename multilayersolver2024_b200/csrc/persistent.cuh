@@ -80,6 +80,7 @@ template <typename R, int MAT> struct TetRest {
   R vol;
   R mat[mat_stride(MAT)];
   R lam[MAT == MAT_NH ? 2 : 6];
+  int j;  // slot of the multipliers in shared memory (cluster kernel)
 };
 
 template <typename R, int MAT>
@@ -89,11 +90,42 @@ __device__ __forceinline__ void load_rest(const TetData<R>& td, int s, TetRest<R
   r.v = td.vid[s];
 #pragma unroll
   for (int j = 0; j < 9; ++j) r.G[j] = td.dminv[(size_t)j * T + s];
-  r.vol = td.vol[s];
+  if (MAT != MAT_NH) r.vol = td.vol[s];
 #pragma unroll
   for (int q = 0; q < mat_stride(MAT); ++q) r.mat[q] = td.mat[(size_t)q * T + s];
 #pragma unroll
   for (int q = 0; q < (MAT == MAT_NH ? 2 : 6); ++q) r.lam[q] = td.lambda[(size_t)q * T + s];
+}
+
+template <int MAT> __host__ __device__ constexpr int num_lambda() { return MAT == MAT_NH ? 2 : 6; }
+
+// The projection of one tet whose rest data is in registers and whose four
+// corner records have been gathered into X / minv: X is updated in place and
+// lnew receives lambda + dlambda (xpbdLayer3D.m:358-377 for one element).
+template <typename R, int MAT, bool DAMP>
+__device__ __forceinline__ void tet_update(const TetRest<R, MAT>& r, V3<R> X[4], const R minv[4],
+                                           const R4<R>* __restrict__ oldp, R inv_h2, R inv_h,
+                                           R (&lnew)[num_lambda<MAT>()]) {
+  if constexpr (MAT == MAT_NH) {
+    double lam[2] = {(double)r.lam[0], (double)r.lam[1]}, dl[2];
+    nh_project<R>(X, minv, r.G, (double)r.mat[0], (double)r.mat[1], (double)inv_h2, lam, dl);
+    lnew[0] = (R)(lam[0] + dl[0]);
+    lnew[1] = (R)(lam[1] + dl[1]);
+  } else {
+    Compliance<R> cm;
+    load_compliance<R, MAT>(r.mat, 0, 1, inv_h2, inv_h, cm, DAMP);
+    R dl[6];
+    V3<R> Xo[4];
+    if (DAMP) {
+      const int4 v = r.v;
+      R4<R> o0 = oldp[v.x], o1 = oldp[v.y], o2 = oldp[v.z], o3 = oldp[v.w];
+      Xo[0] = {o0.x, o0.y, o0.z}; Xo[1] = {o1.x, o1.y, o1.z};
+      Xo[2] = {o2.x, o2.y, o2.z}; Xo[3] = {o3.x, o3.y, o3.z};
+    }
+    stvk_project<R, MAT, DAMP>(X, Xo, minv, r.G, r.vol, cm, r.lam, dl);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) lnew[q] = r.lam[q] + dl[q];
+  }
 }
 
 // project_tet with the rest data already in registers.
@@ -105,26 +137,10 @@ __device__ __forceinline__ void project_loaded(const TetData<R>& td, const TetRe
   R4<R> p0 = ldcg_r4(pos + v.x), p1 = ldcg_r4(pos + v.y), p2 = ldcg_r4(pos + v.z), p3 = ldcg_r4(pos + v.w);
   V3<R> X[4] = {{p0.x, p0.y, p0.z}, {p1.x, p1.y, p1.z}, {p2.x, p2.y, p2.z}, {p3.x, p3.y, p3.z}};
   R minv[4] = {p0.w, p1.w, p2.w, p3.w};
-  const int T = td.T, s = r.s;
-  if (MAT == MAT_NH) {
-    double lam[2] = {(double)r.lam[0], (double)r.lam[1]}, dl[2];
-    nh_project<R>(X, minv, r.G, (double)r.mat[0], (double)r.mat[1], (double)r.vol, (double)inv_h2, lam, dl);
-    td.lambda[s] = (R)(lam[0] + dl[0]);
-    td.lambda[(size_t)T + s] = (R)(lam[1] + dl[1]);
-  } else {
-    Compliance<R> cm;
-    load_compliance<R, MAT>(r.mat, 0, 1, inv_h2, inv_h, cm, DAMP);
-    R dl[6];
-    V3<R> Xo[4];
-    if (DAMP) {
-      R4<R> o0 = oldp[v.x], o1 = oldp[v.y], o2 = oldp[v.z], o3 = oldp[v.w];
-      Xo[0] = {o0.x, o0.y, o0.z}; Xo[1] = {o1.x, o1.y, o1.z};
-      Xo[2] = {o2.x, o2.y, o2.z}; Xo[3] = {o3.x, o3.y, o3.z};
-    }
-    stvk_project<R, MAT, DAMP>(X, Xo, minv, r.G, r.vol, cm, r.lam, dl);
+  R lnew[num_lambda<MAT>()];
+  tet_update<R, MAT, DAMP>(r, X, minv, oldp, inv_h2, inv_h, lnew);
 #pragma unroll
-    for (int q = 0; q < 6; ++q) td.lambda[(size_t)q * T + s] = r.lam[q] + dl[q];
-  }
+  for (int q = 0; q < num_lambda<MAT>(); ++q) td.lambda[(size_t)q * td.T + r.s] = lnew[q];
   stcg_r4(pos + v.x, make_r4<R>(X[0].x, X[0].y, X[0].z, minv[0]));
   stcg_r4(pos + v.y, make_r4<R>(X[1].x, X[1].y, X[1].z, minv[1]));
   stcg_r4(pos + v.z, make_r4<R>(X[2].x, X[2].y, X[2].z, minv[2]));
@@ -191,15 +207,15 @@ __global__ void __launch_bounds__(128) k_layer_persistent(TetData<R> td, Persist
     }
     if (pa.body_work) {
       for (int b = blockIdx.x; b < L.nb; b += gridDim.x)
-        body_iteration<R>(L, b, bodies, pos, ri, vmass, lamB, cd, h, boundary_compliance, contact_resistance,
+        body_iteration<R>(L, b, bodies, GlobalPos<R>{pos}, ri, vmass, lamB, cd, h, boundary_compliance, contact_resistance,
                           use_rigid_contacts, sb, invI);
-      for (int g = tid; g < L.n_ec_groups; g += nthreads) elastic_contact_group<R>(L, g, pos, cd, h, contact_resistance);
+      for (int g = tid; g < L.n_ec_groups; g += nthreads) elastic_contact_group<R>(L, g, GlobalPos<R>{pos}, cd, h, contact_resistance);
       if (!grid_sync(gs, k)) return;
     }
     if (pa.npin) {
       for (int i = tid; i < pa.npin; i += nthreads) {
         int d = pa.pin_dofs[i];
-        __stcg(reinterpret_cast<R*>(&pos[d / 3]) + d % 3, pin_vals[i]);
+        GlobalPos<R>{pos}.st_comp(d / 3, d % 3, pin_vals[i]);
       }
       if (!grid_sync(gs, k)) return;
     }

@@ -15,6 +15,8 @@
 #include "tet_kernels.cuh"
 #include "body_kernels.cuh"
 #include "persistent.cuh"
+#include "cluster.cuh"
+#include "partition.h"
 #include "solver.h"
 
 #include <algorithm>
@@ -167,6 +169,15 @@ struct LayerStatic {
   std::vector<int> packed;       // body_vert_off | body_verts | bnd_off | bnd_verts | list | vert_body
   size_t o_bvo = 0, o_bv = 0, o_bo = 0, o_bnd = 0, o_list = 0, o_vb = 0, o_cstart = 0, o_ccount = 0;
   int n_bnd = 0;
+  // cluster kernel: (colour, part) ranges of the elastic tets, colours with work
+  size_t o_cloff = 0, o_clcol = 0, o_cllb = 0;
+  int cl_nC = 0, cl_max_range = 0;
+  // vertex slots of the cluster kernel for this layer (see cluster.cuh)
+  bool cl_ok = false;
+  int cl_slots = 0, cl_lam = 0;
+  size_t cl_smem = 0;
+  DevBuf cl_dev;  // tsrc int4[nE] | tdst int2[nE] | vhome int[N] | home_v int[N] | home_s int[N] | home_off int[P+1]
+  size_t o_tsrc = 0, o_tdst = 0, o_vhome = 0, o_hv = 0, o_hs = 0, o_hoff = 0;
   DevBuf dev;       // packed ints
   DevBuf dev_rigid; // vert_rigid bytes
 };
@@ -263,6 +274,22 @@ struct Solver final : SolverBase {
   int persist_ctas = 0;
   int launch_persistent(const LayerStatic& ls, const int* dint, const LayerDev& L, const ContactData& cd,
                         const mlx_solve_params* P, int iterations, bool body_work, LayerWork& w);
+  // Thread-block-cluster path (cluster.cuh): with MLXPBD_CLUSTER=1,
+  // fixed-iteration layers run as one cluster launch each when the vertex
+  // records of the mesh fit in the shared memory of a cluster
+  // (MLXPBD_CLUSTER_SIZE forces the number of CTAs, a power of two up to 16).
+  // Off by default: on a 98k-tet mesh one launch per colour is faster.
+  bool cluster_ok = false;
+  int cl_size = 0, cl_threads = 0, cl_rec_slots = 0, cl_lam_slots = 0;
+  size_t cl_smem = 0;
+  std::vector<int> tpart_sorted;  // part of each tet, sorted order
+  std::vector<int4> vid_sorted;   // 0-based corners, sorted order
+  std::vector<int> vowner;        // part owning each vertex
+  long long cl_budget = 0;        // dynamic shared memory a CTA may use
+  int plan_cluster(const mlx_mesh_desc* md, MeshPartition& mp);
+  int build_cluster_slots(LayerStatic& ls, const std::vector<int>& list);
+  int launch_cluster(const LayerStatic& ls, const int* dint, const LayerDev& L, const ContactData& cd,
+                     const mlx_solve_params* P, int iterations, bool body_work, LayerWork& w);
   int reset_gsync();
   int check_gsync();
   cudaLaunchConfig_t pdl_config(int grid, int block) const {
@@ -302,6 +329,13 @@ struct Solver final : SolverBase {
     return sim_setup(ld, P, p0, v0);
   }
   long long sim_launches_per_step() const override { return sim.launches_per_step; }
+  std::string launch_path() const override {
+    if (persistent) return "persistent cooperative kernel per layer (" + std::to_string(persist_ctas) + " CTAs)";
+    if (cluster_ok)
+      return "cluster kernel per layer: " + std::to_string(cl_size) + " CTAs x " + std::to_string(cl_threads) +
+             " threads, vertex slots" + (cl_lam_slots ? " and multipliers" : "") + " in shared memory";
+    return std::string("one launch per colour") + (pdl ? " (programmatic dependent launches)" : "");
+  }
   long long launches_last_call() const override { return last_launches; }
 };
 
@@ -339,17 +373,12 @@ int Solver<R>::create(const mlx_mesh_desc* md) {
           last[v] = c;
         }
   }
-  // colour-sorted order: stable by colour, ascending element id inside a colour
-  color_off.assign(C + 1, 0);
-  for (int c = 1; c <= C; ++c) color_off[c] = color_off[c - 1] + cnt[c];
-  s2e.assign(T, 0);
-  {
-    std::vector<int> fill(color_off.begin(), color_off.end() - 1);
-    for (int e = 0; e < T; ++e) s2e[fill[md->element_color[e] - 1]++] = e;
-  }
   // material encoding
   if (energy == MLX_ENERGY_NEOHOOKEAN) {
     if (!md->mu || !md->lambda) return set_error(MLX_ERR_ARGUMENT, "Neo-Hookean mesh needs mu and lambda");
+    for (int e = 0; e < T; ++e)
+      if (!(md->mu[e] > 0) || !(md->volume[e] > 0))
+        return set_error(MLX_ERR_ARGUMENT, "Neo-Hookean mesh needs mu > 0 and volume > 0 for every tet");
     mat_kind = MAT_NH;
     damp = false;
   } else if (energy == MLX_ENERGY_STVK_VOIGT) {
@@ -394,6 +423,29 @@ int Solver<R>::create(const mlx_mesh_desc* md) {
     vmass_h[v] = m;
   }
 
+  DeviceGuard g(device);
+  color_off.assign(C + 1, 0);
+  for (int c = 1; c <= C; ++c) color_off[c] = color_off[c - 1] + cnt[c];
+  MeshPartition mp;
+  CHECK(plan_cluster(md, mp));
+  // sorted order: by colour, then (cluster path) by part, then element id.
+  // Tets of one colour share no vertex, so their order changes no result.
+  s2e.assign(T, 0);
+  {
+    std::vector<int> fill(color_off.begin(), color_off.end() - 1);
+    if (cluster_ok) {
+      const int P = cl_size;
+      std::vector<int> cp((size_t)C * P + 1, 0);
+      for (int e = 0; e < T; ++e) ++cp[(size_t)(md->element_color[e] - 1) * P + mp.tpart[e] + 1];
+      for (size_t q = 1; q < cp.size(); ++q) cp[q] += cp[q - 1];
+      for (int e = 0; e < T; ++e) s2e[cp[(size_t)(md->element_color[e] - 1) * P + mp.tpart[e]]++] = e;
+      tpart_sorted.assign(T, 0);
+      for (int s = 0; s < T; ++s) tpart_sorted[s] = mp.tpart[s2e[s]];
+    } else {
+      for (int e = 0; e < T; ++e) s2e[fill[md->element_color[e] - 1]++] = e;
+    }
+  }
+
   // ---- host-side packing of the rest data in sorted order ----
   const int stride = mat_stride(mat_kind);
   std::vector<int4> vid(T);
@@ -423,14 +475,17 @@ int Solver<R>::create(const mlx_mesh_desc* md) {
         mat[(size_t)(9 + q) * T + s] = (R)a[(3 + q) + 6 * (3 + q)];
         mat[(size_t)(21 + q) * T + s] = (R)ab[(3 + q) + 6 * (3 + q)];
       }
+    } else if (mat_kind == MAT_NH) {
+      const double v = md->volume[e], mu = md->mu[e], lm = md->lambda[e];
+      mat[s] = (R)(1.0 / (v * mu));
+      mat[(size_t)T + s] = (R)(lm > mu ? 1.0 / (v * (lm - mu)) : 0.0);
     } else {
       mat[s] = (R)md->mu[e];
       mat[(size_t)T + s] = (R)md->lambda[e];
-      if (mat_kind == MAT_STVK_LAME) mat[2 * (size_t)T + s] = (R)(md->alpha1 ? md->alpha1[e] : 0.0);
+      mat[2 * (size_t)T + s] = (R)(md->alpha1 ? md->alpha1[e] : 0.0);
     }
   }
 
-  DeviceGuard g(device);
   CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   CHECK(d_vid.ensure(sizeof(int4) * T));
   CHECK(d_dminv.ensure(sizeof(R) * 9 * (size_t)T));
@@ -472,7 +527,98 @@ int Solver<R>::create(const mlx_mesh_desc* md) {
   CU(cudaMemcpyAsync(d_s2e.p, s2e.data(), sizeof(int) * T, cudaMemcpyHostToDevice, stream));
   if (!pinned.empty())
     CU(cudaMemcpyAsync(d_pin_dofs.p, pinned.data(), sizeof(int) * pinned.size(), cudaMemcpyHostToDevice, stream));
+  if (cluster_ok) {
+    vid_sorted = vid;
+    vowner = mp.vowner;
+  }
   CU(cudaStreamSynchronize(stream));
+  return MLX_OK;
+}
+
+template <typename R>
+static const void* cluster_kernel(int mat_kind, bool damp) {
+  switch (mat_kind) {
+    case MAT_NH: return (const void*)k_layer_cluster<R, MAT_NH, false>;
+    case MAT_STVK_BLOCKS:
+      return damp ? (const void*)k_layer_cluster<R, MAT_STVK_BLOCKS, true>
+                  : (const void*)k_layer_cluster<R, MAT_STVK_BLOCKS, false>;
+    default:
+      return damp ? (const void*)k_layer_cluster<R, MAT_STVK_LAME, true>
+                  : (const void*)k_layer_cluster<R, MAT_STVK_LAME, false>;
+  }
+}
+
+// Chooses the cluster size: enough CTAs for ~64 tets of the largest colour
+// each (at most 16), fewer if the device cannot co-schedule that cluster.
+// The cluster path is left off when the vertex records of a part do not fit
+// in a CTA's shared memory.
+template <typename R>
+int Solver<R>::plan_cluster(const mlx_mesh_desc* md, MeshPartition& mp) {
+  cluster_ok = false;
+  const char* env = std::getenv("MLXPBD_CLUSTER");
+  if (!(env && std::string(env) == "1")) return MLX_OK;
+  int maxc = 0;
+  for (int c = 0; c < C; ++c) maxc = std::max(maxc, color_off[c + 1] - color_off[c]);
+  int want = 1;
+  while (want < 16 && want * 64 < maxc) want *= 2;
+  if (const char* f = std::getenv("MLXPBD_CLUSTER_SIZE")) {
+    int v = std::atoi(f);
+    want = 1;
+    while (want * 2 <= std::min(std::max(v, 1), 16)) want *= 2;
+  }
+  int optin = 0;
+  CU(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+  const void* fn = cluster_kernel<R>(mat_kind, damp);
+  cudaFuncAttributes fa;
+  CU(cudaFuncGetAttributes(&fa, fn));
+  const long long budget = (long long)optin - (long long)fa.sharedSizeBytes - 1024;
+  if (budget <= 0) return MLX_OK;
+  CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)budget));
+  cl_budget = budget;
+  CU(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  const int nl = mat_kind == MAT_NH ? 2 : 6;
+  for (int cs = want; cs >= 1; cs /= 2) {
+    partition_mesh(N, T, md->t, cs, mp);
+    const long long rec_bytes = (long long)mp.max_owned * (long long)sizeof(R4<R>);
+    if (rec_bytes > budget) break;  // fewer CTAs would need even more shared memory
+    std::vector<int> pc((size_t)C * cs, 0), tp(cs, 0);
+    for (int e = 0; e < T; ++e) {
+      ++pc[(size_t)(md->element_color[e] - 1) * cs + mp.tpart[e]];
+      ++tp[mp.tpart[e]];
+    }
+    int maxr = 0, tmax = 0;
+    for (int x : pc) maxr = std::max(maxr, x);
+    for (int x : tp) tmax = std::max(tmax, x);
+    // the multipliers of a CTA's tets join the records when they fit
+    const long long lam_bytes = (long long)tmax * nl * (long long)sizeof(R);
+    const bool lam_in_smem = rec_bytes + lam_bytes <= budget;
+    const long long smem = rec_bytes + (lam_in_smem ? lam_bytes : 0);
+    const int threads = std::min(std::max((maxr + 31) / 32 * 32, 64), kClusterMaxThreads);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = (size_t)smem;
+    cudaLaunchAttribute a;
+    a.id = cudaLaunchAttributeClusterDimension;
+    a.val.clusterDim.x = cs;
+    a.val.clusterDim.y = 1;
+    a.val.clusterDim.z = 1;
+    cfg.attrs = &a;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, fn, &cfg) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    if (nclusters < 1) continue;
+    cluster_ok = true;
+    cl_size = cs;
+    cl_threads = threads;
+    cl_rec_slots = mp.max_owned;
+    cl_lam_slots = lam_in_smem ? tmax : 0;
+    cl_smem = (size_t)smem;
+    return MLX_OK;
+  }
   return MLX_OK;
 }
 
@@ -557,6 +703,36 @@ int Solver<R>::build_static(const mlx_layer_desc* ld, int col, LayerStatic& ls, 
   for (int c = 0; c < C; ++c) cstart[c] = ls.identity_list ? color_off[c] : ls.color_start[c];
   ls.o_cstart = put(cstart);
   ls.o_ccount = put(ls.color_count);
+  if (cluster_ok) {
+    // the elastic list (or the identity) is in sorted order, which is
+    // (colour, part) order on the cluster path
+    const int P = cl_size;
+    std::vector<int> off((size_t)C * P + 1, 0), cols;
+    for (int c = 0; c < C; ++c)
+      for (int s = color_off[c]; s < color_off[c + 1]; ++s)
+        if (isE[s2e[s]]) ++off[(size_t)c * P + tpart_sorted[s] + 1];
+    for (size_t q = 1; q < off.size(); ++q) off[q] += off[q - 1];
+    int maxr = 0;
+    for (int c = 0; c < C; ++c) {
+      if (off[(size_t)(c + 1) * P] > off[(size_t)c * P]) cols.push_back(c);
+      for (int r = 0; r < P; ++r) maxr = std::max(maxr, off[(size_t)c * P + r + 1] - off[(size_t)c * P + r]);
+    }
+    // shared-memory multiplier slots: a rank's tets in colour order
+    std::vector<int> lb((size_t)C * P, 0);
+    for (int r = 0; r < P; ++r) {
+      int acc = 0;
+      for (int c = 0; c < C; ++c) {
+        lb[(size_t)c * P + r] = acc;
+        acc += off[(size_t)c * P + r + 1] - off[(size_t)c * P + r];
+      }
+    }
+    ls.cl_nC = (int)cols.size();
+    ls.cl_max_range = maxr;
+    ls.o_cloff = put(off);
+    ls.o_clcol = put(cols);
+    ls.o_cllb = put(lb);
+    CHECK(build_cluster_slots(ls, list));
+  }
   CHECK(ls.dev.ensure(sizeof(int) * ls.packed.size()));
   CHECK(ls.dev_rigid.ensure(N));
   CU(cudaMemcpyAsync(ls.dev.p, ls.packed.data(), sizeof(int) * ls.packed.size(), cudaMemcpyHostToDevice, stream));
@@ -829,13 +1005,14 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
                           L.n_ec_groups > 0;
     const int ecBlocks = blocks_for(L.n_ec_groups, 128);
     bool stopSolve = false;
-    if (persistent && !P->compute_residuals) {
+    if ((persistent || (cluster_ok && ls.cl_ok)) && !P->compute_residuals) {
       // fixed iteration count: the whole projectGS loop of the layer in one launch
       const int iters = std::max(ld->iterations[layer], 0);
       if (iters > 0) {
         const bool timed = sweep_timing && tev_used + 2 <= tev.size();
         if (timed) CHECK(record_event(tev[tev_used], capturing));
-        CHECK(launch_persistent(ls, dint, L, cd, P, iters, bodyWork, w));
+        if (persistent) CHECK(launch_persistent(ls, dint, L, cd, P, iters, bodyWork, w));
+        else CHECK(launch_cluster(ls, dint, L, cd, P, iters, bodyWork, w));
         if (timed) {
           double b = 0;
           for (int c = 0; c < C; ++c) b += ls.color_count[c] * (bytes_per_tet() + (ls.identity_list ? 0.0 : 4.0));
@@ -1013,6 +1190,180 @@ int Solver<R>::launch_persistent(const LayerStatic& ls, const int* dint, const L
                                     P->contact_resistance, P->use_rigid_contacts, pv, gs);
   }
   if (e != cudaSuccess) return set_error(MLX_ERR_CUDA, std::string("persistent layer launch: ") + cudaGetErrorString(e));
+  return MLX_OK;
+}
+
+// Vertex slots of the cluster kernel for one layer.  Every CTA keeps a slot
+// for each vertex its tets touch; a tet writes its four corners into its own
+// CTA's slots and reads each corner from the slot of that vertex's previous
+// writer in colour order (the schedule is static, so that slot is known
+// here).  Between two writers of a vertex no other tet touches it, so the
+// slot still holds the value when the next writer reads it, and no tet ever
+// stores into another CTA's shared memory.  A vertex's home slot is the one
+// of its last writer in a sweep (the owning part's slot if no elastic tet
+// touches it): the body, contact and pinning phases work there, the first
+// writer of the next sweep reads from there, and the launch fills and
+// drains it.
+template <typename R>
+int Solver<R>::build_cluster_slots(LayerStatic& ls, const std::vector<int>& list) {
+  const int P = cl_size;
+  const int nE = ls.identity_list ? T : (int)list.size();
+  auto sid = [&](int i) { return ls.identity_list ? i : list[i]; };
+  std::vector<int> slot((size_t)P * N, -1), cnt(P, 0), last(N, -1);
+  for (int i = 0; i < nE; ++i) {
+    const int s = sid(i), r = tpart_sorted[s];
+    const int4 q = vid_sorted[s];
+    for (int v : {q.x, q.y, q.z, q.w}) {
+      int& sl = slot[(size_t)r * N + v];
+      if (sl < 0) sl = cnt[r]++;
+      last[v] = r;
+    }
+  }
+  std::vector<int> home(N), vhome(N);
+  for (int v = 0; v < N; ++v) {
+    const int r = last[v] >= 0 ? last[v] : vowner[v];
+    int& sl = slot[(size_t)r * N + v];
+    if (sl < 0) sl = cnt[r]++;
+    home[v] = r;
+    vhome[v] = (r << 24) | sl;
+  }
+  int maxs = 0;
+  for (int r = 0; r < P; ++r) maxs = std::max(maxs, cnt[r]);
+  if (maxs >= 65536) {
+    ls.cl_ok = false;
+    return MLX_OK;
+  }
+  std::vector<int4> tsrc(nE);
+  std::vector<int2> tdst(nE);
+  std::vector<int> prev(home);
+  for (int i = 0; i < nE; ++i) {
+    const int s = sid(i), r = tpart_sorted[s];
+    const int4 q = vid_sorted[s];
+    int src[4], dst[4];
+    const int vv[4] = {q.x, q.y, q.z, q.w};
+    for (int k = 0; k < 4; ++k) {
+      const int v = vv[k];
+      src[k] = (prev[v] << 24) | slot[(size_t)prev[v] * N + v];
+      dst[k] = slot[(size_t)r * N + v];
+      prev[v] = r;
+    }
+    tsrc[i] = make_int4(src[0], src[1], src[2], src[3]);
+    tdst[i] = make_int2(dst[0] | (dst[1] << 16), dst[2] | (dst[3] << 16));
+  }
+  std::vector<int> hoff(P + 1, 0), hv(N), hs(N);
+  for (int v = 0; v < N; ++v) ++hoff[home[v] + 1];
+  for (int r = 0; r < P; ++r) hoff[r + 1] += hoff[r];
+  {
+    std::vector<int> fill(hoff.begin(), hoff.end() - 1);
+    for (int v = 0; v < N; ++v) {
+      const int q = fill[home[v]]++;
+      hv[q] = v;
+      hs[q] = vhome[v] & 0xffffff;
+    }
+  }
+  // shared memory: slots, then the multipliers when they fit
+  const long long rec = (long long)maxs * (long long)sizeof(R4<R>);
+  const int nl = mat_kind == MAT_NH ? 2 : 6;
+  int lam = cl_lam_slots;
+  long long smem = rec + (long long)lam * nl * (long long)sizeof(R);
+  if (smem > cl_budget) {
+    lam = 0;
+    smem = rec;
+  }
+  if (smem > cl_budget) {
+    ls.cl_ok = false;
+    return MLX_OK;
+  }
+  size_t ints = 0;
+  ls.o_tsrc = ints; ints += 4 * (size_t)nE;
+  ls.o_tdst = ints; ints += 2 * (size_t)nE;
+  ls.o_vhome = ints; ints += N;
+  ls.o_hv = ints; ints += N;
+  ls.o_hs = ints; ints += N;
+  ls.o_hoff = ints; ints += P + 1;
+  std::vector<int> pack(ints);
+  std::memcpy(pack.data() + ls.o_tsrc, tsrc.data(), sizeof(int4) * nE);
+  std::memcpy(pack.data() + ls.o_tdst, tdst.data(), sizeof(int2) * nE);
+  std::memcpy(pack.data() + ls.o_vhome, vhome.data(), sizeof(int) * N);
+  std::memcpy(pack.data() + ls.o_hv, hv.data(), sizeof(int) * N);
+  std::memcpy(pack.data() + ls.o_hs, hs.data(), sizeof(int) * N);
+  std::memcpy(pack.data() + ls.o_hoff, hoff.data(), sizeof(int) * (P + 1));
+  CHECK(ls.cl_dev.ensure(sizeof(int) * ints));
+  CU(cudaMemcpyAsync(ls.cl_dev.p, pack.data(), sizeof(int) * ints, cudaMemcpyHostToDevice, stream));
+  CU(cudaStreamSynchronize(stream));
+  ls.cl_slots = maxs;
+  ls.cl_lam = lam;
+  ls.cl_smem = (size_t)smem;
+  ls.cl_ok = true;
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::launch_cluster(const LayerStatic& ls, const int* dint, const LayerDev& L, const ContactData& cd,
+                              const mlx_solve_params* P, int iterations, bool body_work, LayerWork& w) {
+  ClusterArgs ca;
+  ca.list = ls.identity_list ? nullptr : dint + ls.o_list;
+  ca.off = dint + ls.o_cloff;
+  ca.lbase = dint + ls.o_cllb;
+  ca.colours = dint + ls.o_clcol;
+  ca.rec_slots = ls.cl_slots;
+  ca.lam_slots = ls.cl_lam;
+  ca.nC = ls.cl_nC;
+  const int* cl = ls.cl_dev.as<int>();
+  ca.tsrc = reinterpret_cast<const int4*>(cl + ls.o_tsrc);
+  ca.tdst = reinterpret_cast<const int2*>(cl + ls.o_tdst);
+  ca.vhome = cl + ls.o_vhome;
+  ca.home_v = cl + ls.o_hv;
+  ca.home_s = cl + ls.o_hs;
+  ca.home_off = cl + ls.o_hoff;
+  ca.iterations = iterations;
+  ca.body_work = body_work ? 1 : 0;
+  ca.pin_dofs = d_pin_dofs.as<int>();
+  ca.npin = (int)pinned.size();
+  ca.one_per_thread = ls.cl_max_range <= cl_threads ? 1 : 0;
+  const R hR = (R)P->h;
+  const R inv_h2 = R(1) / (hR * hR), inv_h = R(1) / hR;
+  TetData<R> td = tets();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cl_size);
+  cfg.blockDim = dim3(cl_threads);
+  cfg.dynamicSmemBytes = ls.cl_smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cl_size;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  Body* bodies = w.bodies.as<Body>();
+  double* lamB = w.lamB.as<double>();
+  const double4* ri = d_ri.as<double4>();
+  const R4<R>* oldp = d_oldp.as<R4<R>>();
+  const double* vm = d_vmass.as<double>();
+  const R* pv = d_pinx.as<R>();
+  const double h = P->h;
+  const double bc = P->boundary_compliance, cr = P->contact_resistance;
+  const int urc = P->use_rigid_contacts;
+  cudaError_t e;
+  switch (mat_kind) {
+    case MAT_NH:
+      e = cudaLaunchKernelEx(&cfg, k_layer_cluster<R, MAT_NH, false>, td, ca, pos(), oldp, inv_h2, inv_h, L, bodies,
+                             ri, vm, lamB, cd, h, bc, cr, urc, pv);
+      break;
+    case MAT_STVK_BLOCKS:
+      e = damp ? cudaLaunchKernelEx(&cfg, k_layer_cluster<R, MAT_STVK_BLOCKS, true>, td, ca, pos(), oldp, inv_h2,
+                                    inv_h, L, bodies, ri, vm, lamB, cd, h, bc, cr, urc, pv)
+               : cudaLaunchKernelEx(&cfg, k_layer_cluster<R, MAT_STVK_BLOCKS, false>, td, ca, pos(), oldp, inv_h2,
+                                    inv_h, L, bodies, ri, vm, lamB, cd, h, bc, cr, urc, pv);
+      break;
+    default:
+      e = damp ? cudaLaunchKernelEx(&cfg, k_layer_cluster<R, MAT_STVK_LAME, true>, td, ca, pos(), oldp, inv_h2,
+                                    inv_h, L, bodies, ri, vm, lamB, cd, h, bc, cr, urc, pv)
+               : cudaLaunchKernelEx(&cfg, k_layer_cluster<R, MAT_STVK_LAME, false>, td, ca, pos(), oldp, inv_h2,
+                                    inv_h, L, bodies, ri, vm, lamB, cd, h, bc, cr, urc, pv);
+  }
+  if (e != cudaSuccess) return set_error(MLX_ERR_CUDA, std::string("cluster layer launch: ") + cudaGetErrorString(e));
   return MLX_OK;
 }
 
@@ -1199,7 +1550,8 @@ double Solver<R>::bytes_per_tet() const {
   // written (+ four step-start records with Rayleigh damping)
   const double r = sizeof(R);
   const int nl = mat_kind == MAT_NH ? 2 : 6;
-  double b = 16 + 9 * r + r + mat_stride(mat_kind) * r + 2 * nl * r + 8 * 4 * r;
+  const double vol = mat_kind == MAT_NH ? 0 : r;  // Neo-Hookean compliances include the volume
+  double b = 16 + 9 * r + vol + mat_stride(mat_kind) * r + 2 * nl * r + 8 * 4 * r;
   if (damp) b += 4 * 4 * r;
   return b;
 }
@@ -1480,5 +1832,15 @@ int mlx_sim_sweep_stats(mlx_solver* s, double* ms, double* bytes, long long* lau
 
 long long mlx_sim_launches_per_step(const mlx_solver* s) { return s ? s->impl->sim_launches_per_step() : 0; }
 long long mlx_last_call_launches(const mlx_solver* s) { return s ? s->impl->launches_last_call() : 0; }
+int mlx_launch_path(const mlx_solver* s, char* buf, int32_t n) {
+  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver"), -1;
+  std::string d = s->impl->launch_path();
+  if (buf && n > 0) {
+    size_t k = std::min<size_t>(d.size(), (size_t)n - 1);
+    std::memcpy(buf, d.data(), k);
+    buf[k] = 0;
+  }
+  return (int)d.size();
+}
 
 }  // extern "C"

@@ -15,7 +15,7 @@ namespace mlx {
 enum MatKind : int {
   MAT_STVK_BLOCKS = 0,  // alpha and alpha*beta blocks, 24 values per tet
   MAT_STVK_LAME = 1,    // mu, lambda, alpha1 -> blocks formed in registers
-  MAT_NH = 2            // mu, lambda (stable Neo-Hookean D/H pair)
+  MAT_NH = 2            // 1/(vol mu), 1/(vol (lambda - mu)) or 0 (stable Neo-Hookean D/H pair)
 };
 __host__ __device__ constexpr int mat_stride(int kind) {
   return kind == MAT_STVK_BLOCKS ? 24 : (kind == MAT_STVK_LAME ? 3 : 2);
@@ -277,82 +277,90 @@ __device__ __forceinline__ double stvk_residual(const V3<R> X[4], const R G[9], 
 // rest: psi = mu/2 B + (lambda - mu)/2 (J - 1)^2 + const with
 // B = ||F||^2 + J^2 - 4J >= 0, so C_D = sqrt(B) (compliance 1/(vol mu)) and
 // C_H = J - 1 (compliance 1/(vol (lambda - mu)), absent when lambda <= mu),
-// solved as one 2x2 block.  sqrt(B) loses half its digits to the cancellation
-// in B, so this math runs in FP64 registers on every storage precision.
-struct NHEval {
+// solved as one 2x2 block.  The per-tet compliances cD = 1/(vol mu) and
+// cH = 1/(vol (lambda - mu)) (0 = no C_H) are precomputed; alpha~ = c / h^2.
+//
+// Precision: F = Ds DmInv, the gradients G' [dC/dF] and the position update
+// run in the storage precision R.  B, sqrt(B), J and the numerator
+// F + (J - 2) cof(F) of dC_D/dF cancel to O(strain) near rest, so they are
+// formed in FP64 from F; since B is stationary at rotations, rounding F to R
+// moves B only by O(strain * eps_R).  The 2x2 solve is FP64.
+template <typename R> struct NHEval {
   double CD, CH, aD, aH;
   bool hasH;
-  D3 gD[4], gH[4];
+  V3<R> gD[4], gH[4];
 };
 template <typename R>
-__device__ __forceinline__ void nh_eval(const V3<R> X[4], const R Gr[9], double mu, double lm, double vol,
-                                        double inv_h2, NHEval& e) {
-  double G[9];
-#pragma unroll
-  for (int j = 0; j < 9; ++j) G[j] = (double)Gr[j];
-  D3 x0 = d3(X[0].x, X[0].y, X[0].z);
-  D3 u1 = d3(X[1].x, X[1].y, X[1].z) - x0, u2 = d3(X[2].x, X[2].y, X[2].z) - x0,
-     u3 = d3(X[3].x, X[3].y, X[3].z) - x0;
+__device__ __forceinline__ void nh_eval(const V3<R> X[4], const R G[9], double cD, double cH, double inv_h2,
+                                        NHEval<R>& e) {
+  const V3<R> u1 = vsub(X[1], X[0]), u2 = vsub(X[2], X[0]), u3 = vsub(X[3], X[0]);
   D3 f[3];
 #pragma unroll
-  for (int c = 0; c < 3; ++c) f[c] = G[0 + 3 * c] * u1 + G[1 + 3 * c] * u2 + G[2 + 3 * c] * u3;
+  for (int c = 0; c < 3; ++c) {
+    V3<R> fc = vaxpy3(G[0 + 3 * c], u1, G[1 + 3 * c], u2, G[2 + 3 * c], u3);
+    f[c] = d3(fc.x, fc.y, fc.z);
+  }
   D3 cf[3] = {cross(f[1], f[2]), cross(f[2], f[0]), cross(f[0], f[1])};
   double J = dot(f[0], cf[0]);
   double IC = dot(f[0], f[0]) + dot(f[1], f[1]) + dot(f[2], f[2]);
   double B = IC + J * J - 4.0 * J;
   e.CD = sqrt(fmax(B, 0.0));
-  e.hasH = lm > mu;
+  e.hasH = cH > 0.0;
   e.CH = e.hasH ? J - 1.0 : 0.0;
-  e.aD = inv_h2 / (vol * mu);
-  e.aH = e.hasH ? inv_h2 / (vol * (lm - mu)) : 0.0;
+  e.aD = inv_h2 * cD;
+  e.aH = e.hasH ? inv_h2 * cH : 0.0;
   const double invCD = e.CD > 1e-12 ? 1.0 / e.CD : 0.0;
-  D3 pd[3];
+  V3<R> pd[3], cr[3];
 #pragma unroll
-  for (int c = 0; c < 3; ++c) pd[c] = invCD * (f[c] + (J - 2.0) * cf[c]);
-  D3 sD = d3(0, 0, 0), sH = d3(0, 0, 0);
+  for (int c = 0; c < 3; ++c) {
+    D3 n = invCD * (f[c] + (J - 2.0) * cf[c]);
+    pd[c] = {(R)n.x, (R)n.y, (R)n.z};
+    cr[c] = {(R)cf[c].x, (R)cf[c].y, (R)cf[c].z};
+  }
+  V3<R> sD = {0, 0, 0}, sH = {0, 0, 0};
 #pragma unroll
   for (int k = 1; k <= 3; ++k) {
-    double g0 = G[(k - 1) + 0], g1 = G[(k - 1) + 3], g2 = G[(k - 1) + 6];
-    e.gD[k] = g0 * pd[0] + g1 * pd[1] + g2 * pd[2];
-    e.gH[k] = g0 * cf[0] + g1 * cf[1] + g2 * cf[2];
-    sD = sD + e.gD[k];
-    sH = sH + e.gH[k];
+    const R g0 = G[(k - 1) + 0], g1 = G[(k - 1) + 3], g2 = G[(k - 1) + 6];
+    e.gD[k] = vaxpy3(g0, pd[0], g1, pd[1], g2, pd[2]);
+    e.gH[k] = vaxpy3(g0, cr[0], g1, cr[1], g2, cr[2]);
+    sD = {sD.x + e.gD[k].x, sD.y + e.gD[k].y, sD.z + e.gD[k].z};
+    sH = {sH.x + e.gH[k].x, sH.y + e.gH[k].y, sH.z + e.gH[k].z};
   }
-  e.gD[0] = -1.0 * sD;
-  e.gH[0] = -1.0 * sH;
+  e.gD[0] = {-sD.x, -sD.y, -sD.z};
+  e.gH[0] = {-sH.x, -sH.y, -sH.z};
 }
 
 template <typename R>
-__device__ __forceinline__ void nh_project(V3<R> X[4], const R minv[4], const R G[9], double mu, double lm,
-                                           double vol, double inv_h2, const double lam[2], double dl[2]) {
-  NHEval e;
-  nh_eval<R>(X, G, mu, lm, vol, inv_h2, e);
-  double wD = 0, wH = 0, wDH = 0;
+__device__ __forceinline__ void nh_project(V3<R> X[4], const R minv[4], const R G[9], double cD, double cH,
+                                           double inv_h2, const double lam[2], double dl[2]) {
+  NHEval<R> e;
+  nh_eval<R>(X, G, cD, cH, inv_h2, e);
+  R wD = 0, wH = 0, wDH = 0;
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
-    double m = minv[a];
-    wD += m * dot(e.gD[a], e.gD[a]);
-    wH += m * dot(e.gH[a], e.gH[a]);
-    wDH += m * dot(e.gD[a], e.gH[a]);
+    const R m = minv[a];
+    wD += m * vdot(e.gD[a], e.gD[a]);
+    wH += m * vdot(e.gH[a], e.gH[a]);
+    wDH += m * vdot(e.gD[a], e.gH[a]);
   }
-  double b1 = -e.CD - e.aD * lam[0];
+  const double b1 = -e.CD - e.aD * lam[0];
   if (e.hasH) {
-    double a11 = wD + e.aD, a22 = wH + e.aH, a12 = wDH;
-    double b2 = -e.CH - e.aH * lam[1];
-    double det = a11 * a22 - a12 * a12;
-    dl[0] = (b1 * a22 - a12 * b2) / det;
-    dl[1] = (a11 * b2 - a12 * b1) / det;
+    const double a11 = (double)wD + e.aD, a22 = (double)wH + e.aH, a12 = (double)wDH;
+    const double b2 = -e.CH - e.aH * lam[1];
+    const double rdet = 1.0 / (a11 * a22 - a12 * a12);
+    dl[0] = (b1 * a22 - a12 * b2) * rdet;
+    dl[1] = (a11 * b2 - a12 * b1) * rdet;
   } else {
-    dl[0] = b1 / (wD + e.aD);
+    dl[0] = b1 / ((double)wD + e.aD);
     dl[1] = 0.0;
   }
+  const R d0 = (R)dl[0], d1 = (R)dl[1];
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
-    double m = minv[a];
-    D3 d = dl[0] * e.gD[a] + dl[1] * e.gH[a];
-    X[a].x = (R)((double)X[a].x + m * d.x);
-    X[a].y = (R)((double)X[a].y + m * d.y);
-    X[a].z = (R)((double)X[a].z + m * d.z);
+    const R m = minv[a];
+    X[a].x += m * (d0 * e.gD[a].x + d1 * e.gH[a].x);
+    X[a].y += m * (d0 * e.gD[a].y + d1 * e.gH[a].y);
+    X[a].z += m * (d0 * e.gD[a].z + d1 * e.gH[a].z);
   }
 }
 
@@ -391,9 +399,9 @@ __device__ __forceinline__ void project_tet(const TetData<R>& td, int s, R4<R>* 
   R vol = td.vol[s];
   const int T = td.T;
   if (MAT == MAT_NH) {
-    double mu = td.mat[s], lm = td.mat[(size_t)T + s];
+    double cD = td.mat[s], cH = td.mat[(size_t)T + s];
     double lam[2] = {(double)td.lambda[s], (double)td.lambda[(size_t)T + s]}, dl[2];
-    nh_project<R>(X, minv, G, mu, lm, (double)vol, (double)inv_h2, lam, dl);
+    nh_project<R>(X, minv, G, cD, cH, (double)inv_h2, lam, dl);
     td.lambda[s] = (R)(lam[0] + dl[0]);
     td.lambda[(size_t)T + s] = (R)(lam[1] + dl[1]);
   } else {
@@ -458,7 +466,7 @@ __global__ void __launch_bounds__(128) k_project_color(TetData<R> td, const int*
   R minv[4] = {p0.w, p1.w, p2.w, p3.w};
   if (MAT == MAT_NH) {
     double lam[2] = {(double)td.lambda[s], (double)td.lambda[(size_t)T + s]}, dl[2];
-    nh_project<R>(X, minv, G, (double)mat[0], (double)mat[1], (double)vol, (double)inv_h2, lam, dl);
+    nh_project<R>(X, minv, G, (double)mat[0], (double)mat[1], (double)inv_h2, lam, dl);
     td.lambda[s] = (R)(lam[0] + dl[0]);
     td.lambda[(size_t)T + s] = (R)(lam[1] + dl[1]);
   } else {
@@ -541,8 +549,8 @@ __global__ void __launch_bounds__(256) k_residual_partials(TetData<R> td, const 
       R vol = td.vol[s];
       const int T = td.T;
       if (MAT == MAT_NH) {
-        NHEval e;
-        nh_eval<R>(X, G, (double)td.mat[s], (double)td.mat[(size_t)T + s], (double)vol, inv_h2_d, e);
+        NHEval<R> e;
+        nh_eval<R>(X, G, (double)td.mat[s], (double)td.mat[(size_t)T + s], inv_h2_d, e);
         double l0 = td.lambda[s], l1 = td.lambda[(size_t)T + s];
         double a = fabs(e.CD), c = fabs(e.aD * l0);
         double r0 = a - fmin(a, c);

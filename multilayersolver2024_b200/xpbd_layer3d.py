@@ -120,6 +120,13 @@ class Solver:
         check("mlx_create", lib.mlx_create(C.byref(d), C.byref(h)), lib)
         self.handle = h
 
+    @property
+    def launch_path(self) -> str:
+        """How fixed-iteration layers are launched (``mlx_launch_path``)."""
+        buf = C.create_string_buffer(256)
+        self._lib.mlx_launch_path(self.handle, buf, 256)
+        return buf.value.decode()
+
     def close(self):
         if getattr(self, "handle", None) is not None and self.handle.value:
             self._lib.mlx_destroy(self.handle)

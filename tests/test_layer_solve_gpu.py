@@ -142,16 +142,55 @@ def test_fp64_matches_reference_execution(gpu, name):
     assert run_until == pytest.approx(float(gold[f"{name}_run_until"]), rel=1e-9)
 
 
-@pytest.mark.parametrize("persistent,pdl", [("0", "1"), ("0", "0"), ("1", "1")])
-def test_launch_paths_agree(gpu, monkeypatch, persistent, pdl):
-    """Fixed iteration counts run as one launch per colour with programmatic
-    dependent launches (default), without them (MLXPBD_PDL=0), or as one
-    cooperative launch per layer (MLXPBD_PERSISTENT=1); all match the oracle,
-    bodies, glue and contacts included."""
-    monkeypatch.setenv("MLXPBD_PERSISTENT", persistent)
-    monkeypatch.setenv("MLXPBD_PDL", pdl)
+LAUNCH_PATHS = {
+    # name: (MLXPBD_CLUSTER, MLXPBD_CLUSTER_SIZE, MLXPBD_PERSISTENT, MLXPBD_PDL)
+    "default": ("", "", "", ""),
+    "cluster_auto": ("1", "", "0", "1"),
+    "cluster_16": ("1", "16", "0", "1"),
+    "cluster_4": ("1", "4", "0", "1"),
+    "colour_launches_pdl": ("0", "", "0", "1"),
+    "colour_launches": ("0", "", "0", "0"),
+    "persistent_grid": ("0", "", "1", "1"),
+}
+
+
+def _set_path(monkeypatch, name):
+    for var, val in zip(("MLXPBD_CLUSTER", "MLXPBD_CLUSTER_SIZE", "MLXPBD_PERSISTENT", "MLXPBD_PDL"),
+                        LAUNCH_PATHS[name]):
+        if val:
+            monkeypatch.setenv(var, val)
+        else:
+            monkeypatch.delenv(var, raising=False)
+
+
+@pytest.mark.parametrize("path", list(LAUNCH_PATHS))
+def test_launch_paths_agree(gpu, monkeypatch, path):
+    """Fixed iteration counts run as one thread-block cluster per layer with
+    the vertex records in distributed shared memory (MLXPBD_CLUSTER=1; forced
+    to 16 and 4 CTAs so that small meshes exercise remote records), as one launch per
+    colour with or without programmatic dependent launches, or as one
+    cooperative launch per layer; all match the oracle, bodies, glue and
+    contacts included."""
+    _set_path(monkeypatch, path)
     m = block_mesh(dims=(8, 3, 3), energy=_lib.MLX_ENERGY_NEOHOOKEAN, seed=41)
     case = Case(m, [50, 25, 0], [2, 3, 5], seed=42)
     case.integ.boundaryCompliance = 0.0
     case.contacts = _contacts(case)
     _compare(case)
+
+
+@pytest.mark.parametrize("path", ["cluster_16", "cluster_4"])
+@pytest.mark.parametrize("prec,tol", [(_lib.MLX_FP64, TOL64), (_lib.MLX_FP32, TOL32)])
+@pytest.mark.parametrize("rigid_contacts", [True, False])
+def test_cluster_path_stvk_damped(gpu, monkeypatch, path, prec, tol, rigid_contacts):
+    """The cluster kernel on the damped StVK constraint (old positions read
+    from global memory), rigid and elastic contacts and pinning, both storage
+    precisions."""
+    _set_path(monkeypatch, path)
+    m = block_mesh(dims=(8, 3, 3), energy=_lib.MLX_ENERGY_STVK_VOIGT, alpha1=0.01, seed=43)
+    case = Case(m, [50, 25, 0], [2, 3, 5], seed=44)
+    case.integ.boundaryCompliance = 1e-7
+    case.integ.useRigidContacts = rigid_contacts
+    case.integ.contactResistance = 0.9
+    case.contacts = _contacts(case)
+    _compare(case, prec=prec, tol=tol)

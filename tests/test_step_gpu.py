@@ -98,10 +98,25 @@ def test_host_integrate_mirror_matches_oracle(gpu, oracle):
         assert np.abs(m.p - ref[frame - 1]).max() / m.bbox_diagonal() <= 1e-9
 
 
-def test_config2_fp32_resident_matches_oracle(gpu, oracle):
+_CONFIG2_REF = {}
+
+
+@pytest.mark.parametrize("cluster", ["1", "0"])
+def test_config2_fp32_resident_matches_oracle(gpu, oracle, monkeypatch, cluster):
+    """Config 2 (98,304 Neo-Hookean tets, rigid clusters) through the cluster
+    kernel (16 CTAs, vertex records and multipliers in distributed shared
+    memory) and through per-colour launches (the default)."""
+    monkeypatch.setenv("MLXPBD_CLUSTER", cluster)
+    monkeypatch.delenv("MLXPBD_CLUSTER_SIZE", raising=False)
+    monkeypatch.delenv("MLXPBD_PERSISTENT", raising=False)
+    if "ref" not in _CONFIG2_REF:
+        _CONFIG2_REF["ref"] = _oracle_run(scenes.config2(), 3, oracle, threads=16)
+    ref = _CONFIG2_REF["ref"]
     sc = scenes.config2()
-    ref = _oracle_run(scenes.config2(), 3, oracle, threads=16)
     got, sim = _resident_run(sc, 3, _lib.MLX_FP32)
+    path = sim.solver.launch_path
+    print(path)
+    assert path.startswith("cluster") == (cluster == "1")
     d = sc.mesh.bbox_diagonal()
     err = max(np.abs(a - b).max() / d for a, b in zip(got, ref))
     print(f"config2 FP32 max position error / bbox diagonal over 3 steps: {err:.3e}")
