@@ -33,9 +33,16 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "sim steps/sec & iters to residual 1e-4: learned warm-start vs plain, 1 B200"
-WORKLOAD = ("config2: plain multi-layer Neo-Hookean block 64x16x16 cubes (18785 vertices, 98304 tets), "
-            "coarse 8^3-cube rigid clusters (5 it) + fine layer (10 it), dt=1/60, base pinned, "
-            "seeded surface impulse at t=0")
+WORKLOADS = {
+    2: ("config2: plain multi-layer Neo-Hookean block 64x16x16 cubes (18785 vertices, 98304 tets), "
+        "coarse 8^3-cube rigid clusters (5 it) + fine layer (10 it), dt=1/60, base pinned, "
+        "seeded surface impulse at t=0"),
+    3: ("config3: 256 independent Neo-Hookean blocks of 2k-40k tets (log-uniform, seeded; 696279 vertices, "
+        "3352014 tets) merged into one mesh (colours overlaid as Mesh3D.mergeMesh), E log-uniform [1e4,1e6], "
+        "nu=0.35, coarse 4^3-cube rigid clusters (5 it) + fine layer (10 it), dt=1/60, bases pinned, "
+        "seeded surface impulses, per-colour tiles autotuned"),
+}
+WORKLOAD = WORKLOADS[2]
 
 
 def dist_env():
@@ -95,8 +102,8 @@ class ClockSampler:
 
 def profiled_dram_bytes_per_tet():
     """DRAM bytes per projected tet of the colour kernel from the committed ncu
-    summary (profiles/k_project_color_config2.json), or None."""
-    f = ROOT / "profiles" / "k_project_color_config2.json"
+    summary of this workload (profiles/k_project_color_config<N>.json), or None."""
+    f = ROOT / "profiles" / f"k_project_color_config{CONFIG}.json"
     if f.exists():
         return float(json.loads(f.read_text())["dram_bytes_per_tet"])
     return None
@@ -111,9 +118,12 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
+CONFIG = 2
+
+
 def make_scene():
     from multilayersolver2024_b200 import scenes
-    return scenes.config2()
+    return scenes.config3() if CONFIG == 3 else scenes.config2()
 
 
 def make_integrator(scene, precision):
@@ -200,6 +210,10 @@ def run_ours(args, rank, world, local):
     solver = Solver(m, precision=MLX_FP32, device=local, material="lame")
     sim = ResidentSim(solver, integ, ls, sc.h, p0=m.p, v0=np.zeros_like(m.p))
     sim.add_velocity(sc.impulse[0], sc.impulse[1])
+    tuned = None
+    if args.autotune:
+        before, after = sim.autotune(reps=5)
+        tuned = {"step_ms_default_tiles": before, "step_ms_tuned_tiles": after}
     sim.sweep_timing(True)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
     for _ in range(args.warmup):
@@ -232,7 +246,7 @@ def run_ours(args, rank, world, local):
     integ2 = make_integrator(sc2, MLX_FP32)
     cache = StepCache()
     m2.v[sc2.impulse[0] - 1] += sc2.impulse[1]
-    e2e_steps = 0 if args.no_e2e else max(3, min(args.steps, 20))
+    e2e_steps = 0 if args.no_e2e else max(3, min(args.steps, 20 if CONFIG == 2 else 3))
     for frame in range(1, 3 if e2e_steps else 1):  # warm-up: solver creation and layer caches
         integ2.integrate(m2, sc2.h, ContactSet(), cache, frame)
     barrier()
@@ -269,7 +283,7 @@ def run_ours(args, rank, world, local):
             "config": {"workload": WORKLOAD, "solver": "plain multi-layer (no warm-start)",
                        "iterations_per_step": int(sum(sc.iterations)), "precision": "FP32 bulk, FP64 rigid bodies",
                        "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}",
-                       "graph": "one CUDA graph per step"},
+                       "graph": "one CUDA graph per step", "autotune": tuned},
             "roofline": {"bound": "hbm", "kernel": sweep_kernel,
                          "launch_path": solver.launch_path,
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -317,7 +331,20 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-API leg (profiling runs)")
+    ap.add_argument("--config", type=int, choices=[2, 3], default=2,
+                    help="2: the plain multi-layer block (default); 3: the 256-scene batch")
+    ap.add_argument("--autotune", action="store_true", help="run the per-colour tile autotuner before timing "
+                    "(on by default for config 3)")
+    ap.add_argument("--no-autotune", action="store_true", help="never run the autotuner (profiling runs)")
     args = ap.parse_args()
+    global CONFIG, WORKLOAD
+    CONFIG = args.config
+    WORKLOAD = WORKLOADS[CONFIG]
+    if CONFIG == 3:
+        args.autotune = True
+        args.cpu_steps = min(args.cpu_steps, 1)
+    if args.no_autotune:
+        args.autotune = False
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     rank, world, local = dist_env()

@@ -211,6 +211,13 @@ int mlx_sim_sweep_stats(mlx_solver* solver, double* ms, double* bytes, long long
  * kernel launches of the last mlx_layer_solve call. */
 long long mlx_sim_launches_per_step(const mlx_solver* solver);
 long long mlx_last_call_launches(const mlx_solver* solver);
+/* No counterpart in the reference.  Per-colour tile autotuner of the
+ * resident stepper: for every layer and colour, times `reps` launches of the
+ * colour kernel at block sizes 32..256 on the current state, keeps the
+ * fastest (positions and multipliers are restored) and recaptures the step.
+ * before_ms / after_ms (optional) receive one step's device time with the
+ * default and the tuned tiles. */
+int mlx_sim_autotune(mlx_solver* solver, int32_t reps, double* before_ms, double* after_ms);
 /* No counterpart in the reference.  Writes a one-line description of how
  * fixed-iteration layers are launched on this solver's device (thread-block
  * cluster size and threads, or per-colour launches) into buf (NUL-terminated,

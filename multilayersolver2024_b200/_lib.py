@@ -124,6 +124,7 @@ SIGNATURES = {
     "mlx_sim_launches_per_step": ([C.c_void_p], C.c_longlong),
     "mlx_last_call_launches": ([C.c_void_p], C.c_longlong),
     "mlx_launch_path": ([C.c_void_p, C.c_char_p, C.c_int32], C.c_int),
+    "mlx_sim_autotune": ([C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
     "mlx_stvk_residual_noalloc": ([C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p], C.c_int),
     "mlx_greedy_coloring": ([_i32p, C.c_int32, C.c_int32, _i32p, _i32p], C.c_int),

@@ -169,6 +169,7 @@ struct LayerStatic {
   std::vector<int> packed;       // body_vert_off | body_verts | bnd_off | bnd_verts | list | vert_body
   size_t o_bvo = 0, o_bv = 0, o_bo = 0, o_bnd = 0, o_list = 0, o_vb = 0, o_cstart = 0, o_ccount = 0;
   int n_bnd = 0;
+  std::vector<int> tile;  // block size of each colour kernel (0 = default), set by the autotuner
   // cluster kernel: (colour, part) ranges of the elastic tets, colours with work
   size_t o_cloff = 0, o_clcol = 0, o_cllb = 0;
   int cl_nC = 0, cl_max_range = 0;
@@ -242,7 +243,12 @@ struct Solver final : SolverBase {
   R4<R>* pos() const { return d_pos.as<R4<R>>(); }
 
   int build_static(const mlx_layer_desc* ld, int col, LayerStatic& ls, bool capturing);
-  int launch_color(int c, const LayerStatic& ls, const int* dlist, R h);
+  int launch_color(int c, const LayerStatic& ls, const int* dlist, R h, int bs_override = 0);
+  // per-colour tile autotuner of the resident stepper (block size of each
+  // colour kernel, chosen by timing; kept per layer column)
+  static constexpr int kDefaultTile = 64;
+  std::vector<std::vector<int>> tiles;  // [column][colour], 0 = default
+  int sim_autotune(int reps, double* before_ms, double* after_ms) override;
   int residual(const ContactData& cd, double contact_resistance, double h, double* out);
   int norm_resv(double* out);
   int validate_layers(const mlx_layer_desc* ld, const mlx_solve_params* P);
@@ -334,7 +340,15 @@ struct Solver final : SolverBase {
     if (cluster_ok)
       return "cluster kernel per layer: " + std::to_string(cl_size) + " CTAs x " + std::to_string(cl_threads) +
              " threads, vertex slots" + (cl_lam_slots ? " and multipliers" : "") + " in shared memory";
-    return std::string("one launch per colour") + (pdl ? " (programmatic dependent launches)" : "");
+    std::string t;
+    if (!tiles.empty()) {
+      int lo = 1 << 30, hi = 0;
+      for (const auto& v : tiles)
+        for (int b : v)
+          if (b > 0) { lo = std::min(lo, b); hi = std::max(hi, b); }
+      if (hi > 0) t = ", autotuned tiles " + std::to_string(lo) + "-" + std::to_string(hi) + " threads";
+    }
+    return std::string("one launch per colour") + (pdl ? " (programmatic dependent launches)" : "") + t;
   }
   long long launches_last_call() const override { return last_launches; }
 };
@@ -636,11 +650,13 @@ int Solver<R>::build_static(const mlx_layer_desc* ld, int col, LayerStatic& ls, 
     int nre = 0;
     for (int e = 0; e < T; ++e) nre += isR[e] != 0;
     ls.n_rigid_elements = nre;
+    ls.tile = col < (int)tiles.size() ? tiles[col] : std::vector<int>();
     return MLX_OK;
   }
   if (nb < 0) return set_error(MLX_ERR_ARGUMENT, "num_rigids < 0");
   if (capturing) return set_error(MLX_ERR_ARGUMENT, "layer cache miss inside a captured step");
   ls.valid = false;
+  ls.tile = col < (int)tiles.size() ? tiles[col] : std::vector<int>();
   ls.isE.assign(isE, isE + T);
   ls.isBV.assign(isBV, isBV + N);
   ls.isRV.assign(isRV, isRV + N);
@@ -745,10 +761,10 @@ int Solver<R>::build_static(const mlx_layer_desc* ld, int col, LayerStatic& ls, 
 }
 
 template <typename R>
-int Solver<R>::launch_color(int c, const LayerStatic& ls, const int* dlist, R h) {
+int Solver<R>::launch_color(int c, const LayerStatic& ls, const int* dlist, R h, int bs_override) {
   int count = ls.color_count[c];
   if (count == 0) return MLX_OK;
-  const int bs = 64;
+  const int bs = bs_override > 0 ? bs_override : (ls.tile.empty() || ls.tile[c] <= 0 ? kDefaultTile : ls.tile[c]);
   R inv_h2 = R(1) / (h * h), inv_h = R(1) / h;
   TetData<R> td = tets();
   const int* list = ls.identity_list ? nullptr : dlist;
@@ -1543,6 +1559,107 @@ int Solver<R>::sim_setup(const mlx_layer_desc* ld, const mlx_solve_params* P, co
   return MLX_OK;
 }
 
+// Per-colour tile autotuner.  For every layer column of the resident
+// stepper and every colour with elastic tets, times `reps` back-to-back
+// launches of the colour kernel at each candidate block size on the current
+// state and keeps the fastest; positions and multipliers are restored
+// afterwards, so the simulation is unchanged.  The tuned tiles are kept only
+// if a captured step with them is faster than with the default tiles.  The
+// step graph is recaptured at the next step.  before_ms / after_ms
+// (optional) receive one captured step's device time with the default tiles
+// and with the tiles kept.
+template <typename R>
+int Solver<R>::sim_autotune(int reps, double* before_ms, double* after_ms) {
+  if (!sim.ready) return set_error(MLX_ERR_ARGUMENT, "mlx_sim_init first");
+  if (reps < 1) return set_error(MLX_ERR_ARGUMENT, "reps must be >= 1");
+  DeviceGuard g(device);
+  auto step_ms = [&](double* out) -> int {
+    if (!out) return MLX_OK;
+    DevBuf sp, sl, sv;
+    CHECK(sp.ensure(sizeof(R4<R>) * N));
+    CHECK(sv.ensure(sizeof(R4<R>) * N));
+    CHECK(sl.ensure(sizeof(R) * 6 * (size_t)T));
+    CU(cudaMemcpyAsync(sp.p, d_pos.p, sizeof(R4<R>) * N, cudaMemcpyDeviceToDevice, stream));
+    CU(cudaMemcpyAsync(sv.p, d_vel.p, sizeof(R4<R>) * N, cudaMemcpyDeviceToDevice, stream));
+    CU(cudaMemcpyAsync(sl.p, d_lambda.p, sizeof(R) * 6 * (size_t)T, cudaMemcpyDeviceToDevice, stream));
+    if (sim.graph) { cudaGraphExecDestroy(sim.graph); sim.graph = nullptr; }
+    double ms = 0;
+    CHECK(sim_step(1, 1, nullptr));   // capture
+    CHECK(sim_step(3, 1, &ms));
+    *out = ms / 3;
+    CU(cudaMemcpyAsync(d_pos.p, sp.p, sizeof(R4<R>) * N, cudaMemcpyDeviceToDevice, stream));
+    CU(cudaMemcpyAsync(d_vel.p, sv.p, sizeof(R4<R>) * N, cudaMemcpyDeviceToDevice, stream));
+    CU(cudaMemcpyAsync(d_lambda.p, sl.p, sizeof(R) * 6 * (size_t)T, cudaMemcpyDeviceToDevice, stream));
+    CU(cudaStreamSynchronize(stream));
+    return MLX_OK;
+  };
+  tiles.clear();
+  for (auto& c : sim_work.cache) c->tile.clear();
+  CHECK(step_ms(before_ms));
+  DevBuf save_p, save_l;
+  CHECK(save_p.ensure(sizeof(R4<R>) * N));
+  CHECK(save_l.ensure(sizeof(R) * 6 * (size_t)T));
+  CU(cudaMemcpyAsync(save_p.p, d_pos.p, sizeof(R4<R>) * N, cudaMemcpyDeviceToDevice, stream));
+  CU(cudaMemcpyAsync(save_l.p, d_lambda.p, sizeof(R) * 6 * (size_t)T, cudaMemcpyDeviceToDevice, stream));
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  const int cand[] = {32, 64, 128, 256};
+  static_assert(256 <= kMaxColorTile, "autotuner candidates exceed the colour kernel's launch bound");
+  const bool saved_pdl = pdl;
+  pdl = false;  // isolated launches
+  int rc = MLX_OK;
+  tiles.assign(sim.ld.num_columns, std::vector<int>());
+  const R hR = (R)sim.P.h;
+  for (int col = 0; col < sim.ld.num_columns && rc == MLX_OK; ++col) {
+    LayerStatic& ls = *sim_work.cache[col];
+    const int* dlist = ls.dev.as<int>() + ls.o_list;
+    std::vector<int> best(C, 0);
+    for (int c = 0; c < C && rc == MLX_OK; ++c) {
+      if (ls.color_count[c] == 0) continue;
+      float best_ms = 1e30f;
+      for (int bs : cand) {
+        rc = launch_color(c, ls, dlist, hR, bs);  // warm-up
+        if (rc != MLX_OK) break;
+        cudaEventRecord(e0, stream);
+        for (int r = 0; r < reps && rc == MLX_OK; ++r) rc = launch_color(c, ls, dlist, hR, bs);
+        cudaEventRecord(e1, stream);
+        if (rc != MLX_OK) break;
+        if (cudaEventSynchronize(e1) != cudaSuccess) { rc = set_error(MLX_ERR_CUDA, "autotune timing failed"); break; }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) { best_ms = ms; best[c] = bs; }
+      }
+    }
+    tiles[col] = best;
+    ls.tile = best;
+  }
+  pdl = saved_pdl;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CU(cudaMemcpyAsync(d_pos.p, save_p.p, sizeof(R4<R>) * N, cudaMemcpyDeviceToDevice, stream));
+  CU(cudaMemcpyAsync(d_lambda.p, save_l.p, sizeof(R) * 6 * (size_t)T, cudaMemcpyDeviceToDevice, stream));
+  CU(cudaStreamSynchronize(stream));
+  if (sim.graph) { cudaGraphExecDestroy(sim.graph); sim.graph = nullptr; }
+  if (rc != MLX_OK) return rc;
+  // keep the tiles only if the captured step (with programmatic dependent
+  // launches, unlike the isolated timings above) got faster
+  double before = 0, after = 0;
+  CHECK(step_ms(&before));  // tuned
+  const std::vector<std::vector<int>> tuned = tiles;
+  tiles.clear();
+  for (auto& c : sim_work.cache) c->tile.clear();
+  CHECK(step_ms(&after));   // default
+  if (before < after) {
+    tiles = tuned;
+    for (int col = 0; col < sim.ld.num_columns; ++col) sim_work.cache[col]->tile = tiles[col];
+  }
+  if (sim.graph) { cudaGraphExecDestroy(sim.graph); sim.graph = nullptr; }
+  if (after_ms) *after_ms = std::min(before, after);
+  for (auto& c : work.cache) c->valid = false;  // the host-buffer path picks the tiles up on its next build
+  return MLX_OK;
+}
+
 template <typename R>
 double Solver<R>::bytes_per_tet() const {
   // algorithmic bytes of one tet projection in this layout: vertex ids,
@@ -1832,6 +1949,10 @@ int mlx_sim_sweep_stats(mlx_solver* s, double* ms, double* bytes, long long* lau
 
 long long mlx_sim_launches_per_step(const mlx_solver* s) { return s ? s->impl->sim_launches_per_step() : 0; }
 long long mlx_last_call_launches(const mlx_solver* s) { return s ? s->impl->launches_last_call() : 0; }
+int mlx_sim_autotune(mlx_solver* s, int32_t reps, double* before_ms, double* after_ms) {
+  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+  return s->impl->sim_autotune(reps, before_ms, after_ms);
+}
 int mlx_launch_path(const mlx_solver* s, char* buf, int32_t n) {
   if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver"), -1;
   std::string d = s->impl->launch_path();

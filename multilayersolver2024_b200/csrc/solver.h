@@ -24,6 +24,7 @@ struct SolverBase {
   virtual int enable_sweep_timing(int on) = 0;
   virtual int sweep_stats(double* ms, double* bytes, long long* launches, int reset) = 0;
   virtual std::string launch_path() const = 0;
+  virtual int sim_autotune(int reps, double* before_ms, double* after_ms) = 0;
 };
 
 SolverBase* make_solver(const mlx_mesh_desc* md, int* rc);

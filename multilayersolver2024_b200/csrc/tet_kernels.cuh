@@ -426,6 +426,10 @@ __device__ __forceinline__ void project_tet(const TetData<R>& td, int s, R4<R>* 
   stcg_r4(pos + v.w, make_r4<R>(X[3].x, X[3].y, X[3].z, minv[3]));
 }
 
+// Largest block of a colour kernel (the tile autotuner's candidates stay
+// within it; FP64 variants need up to ~220 registers per thread).
+constexpr int kMaxColorTile = 256;
+
 // Programmatic dependent launch: a colour kernel launched with
 // cudaLaunchAttributeProgrammaticStreamSerialization starts while the previous
 // kernel of the stream still runs; griddepcontrol.wait blocks until that
@@ -440,7 +444,7 @@ __device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepc
 // (ids, DmInv, volume, material) is loaded before waiting on the previous
 // colour; positions and multipliers after.
 template <typename R, int MAT, bool DAMP>
-__global__ void __launch_bounds__(128) k_project_color(TetData<R> td, const int* __restrict__ list,
+__global__ void __launch_bounds__(kMaxColorTile) k_project_color(TetData<R> td, const int* __restrict__ list,
                                                        int begin, int count, R4<R>* __restrict__ pos,
                                                        const R4<R>* __restrict__ oldp, R inv_h2, R inv_h) {
   pdl_launch_dependents();

@@ -90,9 +90,6 @@ class Mesh3D:
     DmInv: np.ndarray = None
     elV: np.ndarray = None
     mass: np.ndarray = None
-    perElementXPBDalphaMatrix: np.ndarray = None
-    perElementXPBDalphaInvMatrix: np.ndarray = None
-    perElementXPBDbeta: np.ndarray = None
     pinnedInds: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
     pinnedDOFs: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
     unpinnedDOFs: np.ndarray = None
@@ -125,11 +122,28 @@ class Mesh3D:
         np.add.at(m, (np.asarray(self.t, np.int64) - 1).reshape(-1, order="C"),
                   np.repeat(self.elV * self.rho / 4.0, 4))
         self.mass = np.repeat(m, 3)
-        a, ainv, b = material_blocks(self.mu, self.lam, self.alpha1)
-        self.perElementXPBDalphaMatrix = a
-        self.perElementXPBDalphaInvMatrix = ainv
-        self.perElementXPBDbeta = b
+        self._blocks = None
         self.unpinnedDOFs = np.arange(1, 3 * self.N + 1, dtype=np.int32)
+
+    # The 6x6 compliance pages (Mesh3D.updateMaterials) are formed on first
+    # use: a Neo-Hookean mesh never needs them, and for a few million tets
+    # they take gigabytes.
+    def _material_blocks(self):
+        if self._blocks is None:
+            self._blocks = material_blocks(self.mu, self.lam, self.alpha1)
+        return self._blocks
+
+    @property
+    def perElementXPBDalphaMatrix(self):
+        return self._material_blocks()[0]
+
+    @property
+    def perElementXPBDalphaInvMatrix(self):
+        return self._material_blocks()[1]
+
+    @property
+    def perElementXPBDbeta(self):
+        return self._material_blocks()[2]
 
     def pin(self, pinned_inds):
         """Mesh3D.pin (pin.m:1-39): pinned DOFs sorted, pinned tets = tets with
@@ -151,3 +165,31 @@ class Mesh3D:
     def bbox_diagonal(self) -> float:
         V = self.p.reshape(-1, 3)
         return float(np.linalg.norm(V.max(0) - V.min(0)))
+
+
+def merge_meshes(meshes) -> "Mesh3D":
+    """Mesh3D.mergeMesh (3d/@Mesh3D/Mesh3D.m:300-338) applied in order: the
+    vertices, tets (offset by the vertices before them), materials and pins
+    are concatenated and the colours of the parts are overlaid (colour c of
+    every part is one colour of the result, numColors = max).  First-fit
+    colouring of the merged mesh gives exactly that overlay, because parts
+    share no vertex; it is checked here."""
+    meshes = list(meshes)
+    first = meshes[0]
+    offs = np.cumsum([0] + [m.N for m in meshes])
+    V = np.concatenate([m.p.reshape(-1, 3) for m in meshes])
+    T = np.concatenate([np.asarray(m.t, np.int64) + o for m, o in zip(meshes, offs[:-1])]).astype(np.int32)
+    cat = lambda name: np.concatenate([getattr(m, name) for m in meshes])
+    out = Mesh3D.from_arrays(V, T, cat("mu"), cat("lam"), rho=cat("rho"), alpha1=cat("alpha1"),
+                             energy_type=first.energy_type)
+    overlay = cat("elementColor")
+    if not np.array_equal(out.elementColor, overlay):
+        raise AssertionError("merged colouring differs from the overlay of the parts' colourings")
+    pins = [m.pinnedInds.astype(np.int64) + o for m, o in zip(meshes, offs[:-1]) if m.pinnedInds.size]
+    if pins:
+        out.pin(np.concatenate(pins).astype(np.int32))
+    out.v = cat("v")
+    out.f = cat("f")
+    out.part_vertex_offsets = offs
+    out.part_tet_offsets = np.cumsum([0] + [m.T for m in meshes])
+    return out

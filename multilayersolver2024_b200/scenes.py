@@ -15,7 +15,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib
-from .mesh3d import Mesh3D, to_lame
+from .mesh3d import Mesh3D, merge_meshes, to_lame
 
 
 def generate_beam(nx: int, ny: int, nz: int, edge: float = 1.0, origin=(0.0, 0.0, 0.0)):
@@ -120,3 +120,62 @@ def config2(seed: int = 2, nx=64, ny=16, nz=16, cluster=8) -> Scene:
     dofs = np.stack([patch * 3 + 1, patch * 3 + 2, patch * 3 + 3], 1).ravel().astype(np.int32)
     return Scene("config2_nh_block_64x16x16", m, 1.0 / 60.0, 300, [50, 0], [5, 10], custom_sets=sets,
                  impulse=(dofs, dv.ravel()))
+
+
+def _surface_impulse(rng, V, top_z, radius=0.4):
+    """A seeded velocity on a patch of the top surface (0-based vertex ids)."""
+    top = np.nonzero(np.isclose(V[:, 2], top_z))[0]
+    c = V[top[rng.integers(len(top))]]
+    patch = top[np.linalg.norm(V[top, :2] - c[:2], axis=1) < radius]
+    dv = rng.normal(0.0, 1.0, (len(patch), 3)) * 0.5 + np.array([0.0, 0.0, -2.0])
+    return patch, dv
+
+
+def batch_block_dims(rng, tmin=2000, tmax=40000):
+    """Cube-grid dimensions (nx, ny, nz) with 6*nx*ny*nz close to a tet count
+    drawn log-uniformly from [tmin, tmax], random aspect ratios in [1, 3]."""
+    target = np.exp(rng.uniform(np.log(tmin), np.log(tmax)))
+    rx, ry = rng.uniform(1.0, 3.0, 2)
+    n = (target / (6.0 * rx * ry)) ** (1.0 / 3.0)
+    return max(int(round(rx * n)), 2), max(int(round(ry * n)), 2), max(int(round(n)), 2)
+
+
+def config3(seed: int = 3, n_scenes: int = 256, tmin=2000, tmax=40000, cluster=4) -> Scene:
+    """Batched Neo-Hookean blocks: `n_scenes` independent cube-grid blocks
+    (0.1 m cubes) whose dimensions give 2k-40k tets (log-uniform, seeded),
+    per-tet E log-uniform in [1e4, 1e6] Pa, nu = 0.35, base pinned, a seeded
+    surface impulse each, merged into one mesh as Mesh3D.mergeMesh does
+    (colours overlaid).  Two layers: fixed cluster^3-cube rigid clusters (5
+    iterations), then the fine layer (10 iterations); dt = 1/60, 200 steps.
+    Blocks are laid out side by side along x, 1 m apart."""
+    rng = np.random.default_rng(seed)
+    meshes, sets, imp_dofs, imp_dv = [], [], [], []
+    x0, nbodies, voff = 0.0, 0, 0
+    for _ in range(n_scenes):
+        nx, ny, nz = batch_block_dims(rng, tmin, tmax)
+        V, T, cube = generate_beam(nx, ny, nz, 0.1, origin=(x0, 0.0, 0.0))
+        x0 += nx * 0.1 + 1.0
+        nt = T.shape[0]
+        E = np.exp(rng.uniform(np.log(1e4), np.log(1e6), nt))
+        mu, lam = to_lame(0.35, E)
+        m = Mesh3D.from_arrays(V, T, mu, lam, rho=1000.0, alpha1=0.0, energy_type=_lib.MLX_ENERGY_NEOHOOKEAN)
+        m.pin(np.nonzero(np.isclose(V[:, 2], 0.0))[0] + 1)
+        forced = np.zeros(nt, dtype=bool)
+        forced[m.pinnedTets - 1] = True
+        coarse = cluster_rigid_sets(cube, (nx, ny, nz), cluster, forced)
+        coarse[coarse > 0] += nbodies
+        nbodies = int(max(nbodies, coarse.max(initial=0)))
+        sets.append(coarse)
+        patch, dv = _surface_impulse(rng, V, nz * 0.1)
+        g = patch + voff
+        imp_dofs.append(np.stack([g * 3 + 1, g * 3 + 2, g * 3 + 3], 1).ravel())
+        imp_dv.append(dv.ravel())
+        voff += m.N
+        meshes.append(m)
+    mesh = merge_meshes(meshes)
+    coarse = np.concatenate(sets).astype(np.int32)
+    custom = np.asfortranarray(np.stack([np.zeros(mesh.T, np.int32), coarse], 1))
+    sc = Scene(f"config3_batch_{n_scenes}_nh_blocks", mesh, 1.0 / 60.0, 200, [50, 0], [5, 10], custom_sets=custom,
+               impulse=(np.concatenate(imp_dofs).astype(np.int32), np.concatenate(imp_dv)))
+    sc.settings["parts"] = meshes
+    return sc

@@ -185,6 +185,14 @@ class ResidentSim:
     def launches_per_step(self):
         return int(self._lib.mlx_sim_launches_per_step(self.solver.handle))
 
+    def autotune(self, reps=10):
+        """Per-colour tile autotuner (``mlx_sim_autotune``); returns one
+        step's device time in ms before and after tuning."""
+        b, a = C.c_double(), C.c_double()
+        check("mlx_sim_autotune", self._lib.mlx_sim_autotune(self.solver.handle, int(reps), C.byref(b), C.byref(a)),
+              self._lib)
+        return b.value, a.value
+
 
 def pack_layer_desc(ls: LayerSet, layersMap, iterations):
     keep = [ls]
