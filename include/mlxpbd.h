@@ -224,6 +224,57 @@ int mlx_sim_autotune(mlx_solver* solver, int32_t reps, double* before_ms, double
  * at most n bytes).  Returns the length of the full description. */
 int mlx_launch_path(const mlx_solver* solver, char* buf, int32_t n);
 
+/* ---- analytic obstacles (contact finders) ------------------------------
+ * One obstacle per contact finder of simulate3D (3d/simulate3D.m:156-171),
+ * in finder order:
+ *   MLX_OBSTACLE_PLANE  PlaneContactFinder3D(normal, position)
+ *                       (3d/contact/PlaneContactFinder3D.m:16-32): `normal`
+ *                       as given (the test uses it normalised, the offset
+ *                       D = dot(normal, position) as given), `center` = position;
+ *   MLX_OBSTACLE_SPHERE SphereContactFinder(radius, position)
+ *                       (3d/contact/SphereContactFinder.m:13-21): `radius`,
+ *                       `center`; its contacts keep contactInfo3D's default
+ *                       compliance 1e-4 (the `compliance` field is ignored);
+ *   MLX_OBSTACLE_BOX    PlatformContactDetector(degrees, scale, position)
+ *                       (3d/contact/PlatformContactDetector.m:22-63):
+ *                       `rotation` = RotationMatrixDegrees(degrees), row-major,
+ *                       `scale` = [width depth height], `center` = position.
+ * `compliance` is the finder's xpbdContactCompliance (1e-4 by default). */
+#define MLX_OBSTACLE_PLANE 1
+#define MLX_OBSTACLE_SPHERE 2
+#define MLX_OBSTACLE_BOX 3
+#define MLX_MAX_OBSTACLES 32
+typedef struct mlx_obstacle {
+  int32_t type;
+  double normal[3];
+  double center[3];
+  double radius;
+  double rotation[9];
+  double scale[3];
+  double compliance;
+} mlx_obstacle;
+
+/* Contact detection on the device for positions p (3N, host): the
+ * concatenated contact lists of the finders, each finder's contacts in
+ * ascending vertex order, as simulate3D builds them.  Writes, when
+ * *num_contacts <= max_contacts, 1-based vertex ids (K), normals and collider
+ * points (K x 3, column-major) and compliances (K); *num_contacts is always
+ * set.  Returns MLX_ERR_LIMIT when the contacts do not fit. */
+int mlx_find_contacts(mlx_solver* solver, const mlx_obstacle* obstacles, int32_t num_obstacles, const double* p,
+                      int32_t max_contacts, int32_t* vertex_ids, double* normals, double* point_colliders,
+                      double* compliance, int32_t* num_contacts);
+
+/* Resident stepper with obstacles: every step detects the contacts of the
+ * step-start positions on the device, projects them in every layer
+ * (contactConstraints, xpbdLayer3D.m:422-485) and applies
+ * contactVelocityUpdate with restitution e (xpbdLayer3D.m:740 uses 1e-2)
+ * after the step, without a host round trip.  num_obstacles = 0 removes them.
+ * Call after mlx_sim_init. */
+int mlx_sim_set_obstacles(mlx_solver* solver, const mlx_obstacle* obstacles, int32_t num_obstacles,
+                          double restitution);
+/* Number of contacts of the last resident step (reads one int from the device). */
+int mlx_sim_contact_count(mlx_solver* solver, int32_t* num_contact_vertices);
+
 /* ---- allocation-free residual ------------------------------------------
  * No counterpart in the reference.  The elastic constraint residual of
  * simpleEvaluateAllConstraintResiduals (StVK Voigt tets, no contacts) on

@@ -22,6 +22,11 @@ MLX_ENERGY_NEOHOOKEAN = 1
 MLX_ENERGY_STVK_VOIGT = 2
 MLX_FP32 = 0
 MLX_FP64 = 1
+MLX_OBSTACLE_PLANE = 1
+MLX_OBSTACLE_SPHERE = 2
+MLX_OBSTACLE_BOX = 3
+MLX_MAX_OBSTACLES = 32
+MLX_ERR_LIMIT = 6
 
 _i32p = C.POINTER(C.c_int32)
 _u8p = C.POINTER(C.c_uint8)
@@ -106,6 +111,18 @@ def u8(a):
     return ptr(a, C.c_uint8)
 
 
+class mlx_obstacle(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("normal", C.c_double * 3),
+        ("center", C.c_double * 3),
+        ("radius", C.c_double),
+        ("rotation", C.c_double * 9),
+        ("scale", C.c_double * 3),
+        ("compliance", C.c_double),
+    ]
+
+
 SIGNATURES = {
     "mlx_last_error": ([], C.c_char_p),
     "mlx_abi_version": ([], C.c_int),
@@ -125,6 +142,10 @@ SIGNATURES = {
     "mlx_last_call_launches": ([C.c_void_p], C.c_longlong),
     "mlx_launch_path": ([C.c_void_p, C.c_char_p, C.c_int32], C.c_int),
     "mlx_sim_autotune": ([C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
+    "mlx_find_contacts": ([C.c_void_p, C.c_void_p, C.c_int32, _f64p, C.c_int32, _i32p, _f64p, _f64p, _f64p, _i32p],
+                          C.c_int),
+    "mlx_sim_set_obstacles": ([C.c_void_p, C.c_void_p, C.c_int32, C.c_double], C.c_int),
+    "mlx_sim_contact_count": ([C.c_void_p, _i32p], C.c_int),
     "mlx_stvk_residual_noalloc": ([C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p], C.c_int),
     "mlx_greedy_coloring": ([_i32p, C.c_int32, C.c_int32, _i32p, _i32p], C.c_int),

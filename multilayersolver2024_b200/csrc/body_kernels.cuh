@@ -9,6 +9,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "contacts.cuh"
 #include "tet_kernels.cuh"
 
 namespace mlx {
@@ -271,7 +272,8 @@ __device__ __forceinline__ void body_iteration(const LayerDev& L, int b, Body* _
                                                const double* __restrict__ vmass, double* __restrict__ lamB,
                                                const ContactData& cd, double h, double boundary_compliance,
                                                double contact_resistance, int use_rigid_contacts, Body& sb,
-                                               double* invI) {
+                                               double* invI, const DevContacts& dc = DevContacts{},
+                                               const R4<R>* __restrict__ x0 = nullptr) {
   if (threadIdx.x == 0) {
     sb = bodies[b];
     inverse3(sb.I, invI);
@@ -353,6 +355,51 @@ __device__ __forceinline__ void body_iteration(const LayerDev& L, int b, Body* _
     }
     dirty = true;
   }
+  if (use_rigid_contacts && dc.nobs) {
+    // contacts detected on the device: the body's vertices carry finder masks
+    pos.fence();
+    __syncthreads();
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    const int beg = L.body_vert_off[b], end = L.body_vert_off[b + 1];
+    const double invM = 1.0 / sb.mass, h2 = h * h;
+    const D3 com = d3(sb.com[0], sb.com[1], sb.com[2]);
+    for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+      const int v = L.body_verts[i];
+      const unsigned m = dc.mask[v];
+      if (!m) continue;
+      const R4<R> p = pos.ld(v);
+      const R4<R> s0 = x0[v];
+      const D3 x = d3((double)p.x, (double)p.y, (double)p.z);
+      const D3 r = body_point(sb, ri[v]) - com;
+      const int ci = dc.cidx[v];
+      for (int f = 0; f < dc.nobs; ++f) {
+        if (!((m >> f) & 1u)) continue;
+        D3 n, c;
+        double comp;
+        obstacle_contact(dc.obs[f], (double)s0.x, (double)s0.y, (double)s0.z, n, c, comp);
+        double phi = dot(n, x - c);
+        if (phi > 0) phi = 0;
+        const double C = contact_resistance * phi;
+        const double w = gen_inv_mass(invM, r, invI, n);
+        const double aT = (2 * comp) / h2;
+        double& lam = dc.lambda[(size_t)ci * dc.nobs + f];
+        const double dl = (-C - aT * lam) / (2 * w + aT);
+        lam += dl;
+        const D3 pp = dl * n;
+        s[0] += pp.x * invM; s[1] += pp.y * invM; s[2] += pp.z * invM;
+        const D3 cr = cross(r, pp);
+        s[3] += (1 / h) * cr.x; s[4] += (1 / h) * cr.y; s[5] += (1 / h) * cr.z;
+      }
+    }
+    block_sum<6>(s);
+    if (threadIdx.x == 0) apply_increments(sb, s, h);
+    __syncthreads();
+    for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+      const int v = L.body_verts[i];
+      if (dc.mask[v]) store_xyz<R>(pos, v, body_point(sb, ri[v]));
+    }
+    dirty = true;
+  }
   if (dirty && threadIdx.x == 0) bodies[b] = sb;
   pos.fence();
   __syncthreads();
@@ -367,19 +414,28 @@ __global__ void __launch_bounds__(256) k_iterate_bodies(LayerDev L, Body* __rest
                                                         const double* __restrict__ vmass,
                                                         double* __restrict__ lamB, ContactData cd,
                                                         double h, double boundary_compliance,
-                                                        double contact_resistance, int use_rigid_contacts) {
+                                                        double contact_resistance, int use_rigid_contacts,
+                                                        DevContacts dc, const R4<R>* __restrict__ x0) {
   __shared__ Body sb;
   __shared__ double invI[9];
   pdl_launch_dependents();
   pdl_wait();
   int b = blockIdx.x;
   if (b >= L.nb) {
+    const GlobalPos<R> gp{pos};
+    if (dc.nobs) {
+      // device-detected contacts: elastic ones are those of non-rigid vertices
+      const int n = *dc.count, stride = (gridDim.x - L.nb) * blockDim.x;
+      for (int i = (b - L.nb) * blockDim.x + threadIdx.x; i < n; i += stride)
+        if (L.vert_body[dc.verts[i]] == 0) elastic_contacts_of_vertex<R>(dc, i, gp, x0, h, contact_resistance);
+      return;
+    }
     int g = (b - L.nb) * blockDim.x + threadIdx.x;
-    if (g < L.n_ec_groups) elastic_contact_group<R>(L, g, GlobalPos<R>{pos}, cd, h, contact_resistance);
+    if (g < L.n_ec_groups) elastic_contact_group<R>(L, g, gp, cd, h, contact_resistance);
     return;
   }
   body_iteration<R>(L, b, bodies, GlobalPos<R>{pos}, ri, vmass, lamB, cd, h, boundary_compliance, contact_resistance,
-                    use_rigid_contacts, sb, invI);
+                    use_rigid_contacts, sb, invI, dc, x0);
 }
 
 // xi(pinnedDOFs) = pinnedx (xpbdLayer3D.m:333)

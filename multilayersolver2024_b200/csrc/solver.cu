@@ -16,6 +16,7 @@
 #include "body_kernels.cuh"
 #include "persistent.cuh"
 #include "cluster.cuh"
+#include "contacts.cuh"
 #include "partition.h"
 #include "solver.h"
 
@@ -254,7 +255,8 @@ struct Solver final : SolverBase {
   int validate_layers(const mlx_layer_desc* ld, const mlx_solve_params* P);
   int upload_contacts(const mlx_contacts* K, ContactData& cd);
   int run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, const mlx_contacts* K,
-                 const ContactData& cd, RunState& st, bool capturing, LayerWork& w);
+                 const ContactData& cd, RunState& st, bool capturing, LayerWork& w,
+                 const DevContacts& dc = DevContacts{});
 
   // resident stepper (one per solver)
   struct Sim {
@@ -268,6 +270,27 @@ struct Solver final : SolverBase {
     long long launches_per_step = 0;
   } sim;
   DevBuf d_vel, d_pin_mask, d_gsync;
+  // obstacles of the resident stepper (contacts detected on the device)
+  std::vector<Obstacle> sim_obs;
+  double sim_restitution = 1e-2;
+  DevBuf d_obs, d_cmask, d_cverts, d_cidx, d_cscan, d_clam_dev;
+  DevContacts dev_contacts() const {
+    DevContacts dc{};
+    dc.nobs = (int)sim_obs.size();
+    if (!dc.nobs) return dc;
+    dc.obs = d_obs.as<Obstacle>();
+    dc.mask = d_cmask.as<unsigned>();
+    dc.verts = d_cverts.as<int>();
+    dc.cidx = d_cidx.as<int>();
+    dc.count = d_cscan.as<int>() + blocks_for(N, 256);
+    dc.lambda = d_clam_dev.as<double>();
+    return dc;
+  }
+  int detect_contacts(const R4<R>* x0);  // stream work only (captured in the step)
+  int find_contacts(const mlx_obstacle* obs, int nobs, const double* p, int max_contacts, int32_t* vids,
+                    double* normals, double* points, double* comp, int32_t* K) override;
+  int sim_set_obstacles(const mlx_obstacle* obs, int nobs, double restitution) override;
+  int sim_contact_count(int32_t* n) override;
   PinnedBuf h_gsync;
   long long last_launches = 0;
   // Fixed-iteration layers run as one launch per colour, each launched as a
@@ -900,7 +923,8 @@ int Solver<R>::upload_contacts(const mlx_contacts* K, ContactData& cd) {
 // refused in that mode.
 template <typename R>
 int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, const mlx_contacts* K,
-                          const ContactData& cd, RunState& st, bool capturing, LayerWork& w) {
+                          const ContactData& cd, RunState& st, bool capturing, LayerWork& w,
+                          const DevContacts& dc) {
   if (capturing && P->compute_residuals)
     return set_error(MLX_ERR_UNSUPPORTED, "residual monitoring cannot run inside a captured step");
   const double h = P->h;
@@ -1011,6 +1035,7 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
     // contact multipliers restart at zero in every layer: projectGS does not
     // return them (xpbdLayer3D.m:163), so each layer sees layerSolve's zeros
     if (nK > 0) CU(cudaMemsetAsync(cd.lambda, 0, sizeof(double) * nK, stream));
+    if (dc.nobs) CU(cudaMemsetAsync(dc.lambda, 0, sizeof(double) * (size_t)N * dc.nobs, stream));
     if (ls.n_bnd > 0) {
       if (!capturing) CHECK(w.lamB.ensure(sizeof(double) * ls.n_bnd));
       else if (w.lamB.bytes < sizeof(double) * ls.n_bnd) return set_error(MLX_ERR_ARGUMENT, "boundary buffer not reserved");
@@ -1018,10 +1043,12 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
     }
     const int* dlist = dint + ls.o_list;
     const bool bodyWork = (ls.nb > 0 && (L.any_boundary || (P->use_rigid_contacts && L.any_rigid_contact))) ||
-                          L.n_ec_groups > 0;
-    const int ecBlocks = blocks_for(L.n_ec_groups, 128);
+                          L.n_ec_groups > 0 || dc.nobs > 0;
+    // device-detected contacts: their number is only known on the device, so
+    // the extra CTAs stride over it
+    const int ecBlocks = dc.nobs ? std::max(1, std::min(blocks_for(N, 128), 592)) : blocks_for(L.n_ec_groups, 128);
     bool stopSolve = false;
-    if ((persistent || (cluster_ok && ls.cl_ok)) && !P->compute_residuals) {
+    if ((persistent || (cluster_ok && ls.cl_ok)) && !P->compute_residuals && !dc.nobs) {
       // fixed iteration count: the whole projectGS loop of the layer in one launch
       const int iters = std::max(ld->iterations[layer], 0);
       if (iters > 0) {
@@ -1077,7 +1104,8 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
         cfg.numAttrs = pdl ? 1 : 0;
         CU(cudaLaunchKernelEx(&cfg, k_iterate_bodies<R>, L, w.bodies.as<Body>(), p, (const double4*)ri,
                               (const double*)d_vmass.as<double>(), w.lamB.as<double>(), cd, h,
-                              P->boundary_compliance, P->contact_resistance, (int)P->use_rigid_contacts));
+                              P->boundary_compliance, P->contact_resistance, (int)P->use_rigid_contacts, dc,
+                              (const R4<R>*)d_oldp.as<R4<R>>()));
         ++st.launches;
       }
       if (np) {
@@ -1660,6 +1688,151 @@ int Solver<R>::sim_autotune(int reps, double* before_ms, double* after_ms) {
   return MLX_OK;
 }
 
+// Host preparation of the finders (their constructors): the plane's unit
+// normal and offset, the box's normalised directions and half extents.
+static int prepare_obstacles(const mlx_obstacle* in, int n, std::vector<Obstacle>& out) {
+  if (n < 0 || n > MLX_MAX_OBSTACLES) return set_error(MLX_ERR_ARGUMENT, "num_obstacles out of [0, 32]");
+  if (n > 0 && !in) return set_error(MLX_ERR_ARGUMENT, "obstacles is NULL");
+  out.clear();
+  for (int i = 0; i < n; ++i) {
+    const mlx_obstacle& a = in[i];
+    Obstacle o{};
+    o.type = a.type;
+    o.compliance = a.compliance;
+    for (int d = 0; d < 3; ++d) o.c[d] = a.center[d];
+    if (a.type == MLX_OBSTACLE_PLANE) {
+      const double nn = std::sqrt(a.normal[0] * a.normal[0] + a.normal[1] * a.normal[1] + a.normal[2] * a.normal[2]);
+      if (!(nn > 0)) return set_error(MLX_ERR_ARGUMENT, "plane normal is zero");
+      for (int d = 0; d < 3; ++d) o.n[d] = a.normal[d] / nn;
+      o.D = a.normal[0] * a.center[0] + a.normal[1] * a.center[1] + a.normal[2] * a.center[2];
+    } else if (a.type == MLX_OBSTACLE_SPHERE) {
+      if (!(a.radius >= 0)) return set_error(MLX_ERR_ARGUMENT, "sphere radius < 0");
+      o.radius = a.radius;
+    } else if (a.type == MLX_OBSTACLE_BOX) {
+      for (int r = 0; r < 3; ++r) {
+        const double* row = a.rotation + 3 * r;
+        const double nr = std::sqrt(row[0] * row[0] + row[1] * row[1] + row[2] * row[2]);
+        if (!(nr > 0)) return set_error(MLX_ERR_ARGUMENT, "box rotation has a zero row");
+        for (int d = 0; d < 3; ++d) o.dir[3 * r + d] = row[d] / nr;
+        o.half[r] = a.scale[r] / 2;
+      }
+    } else {
+      return set_error(MLX_ERR_ARGUMENT, "unknown obstacle type");
+    }
+    out.push_back(o);
+  }
+  return MLX_OK;
+}
+
+// Masks and the ordered list of contact vertices of positions x0 (stream
+// work only).  Uses d_obs / sim_obs.
+template <typename R>
+int Solver<R>::detect_contacts(const R4<R>* x0) {
+  const int nb = blocks_for(N, 256);
+  const int nobs = (int)sim_obs.size();
+  k_contact_mask<R><<<nb, 256, 0, stream>>>(x0, N, d_obs.as<Obstacle>(), nobs, d_cmask.as<unsigned>());
+  int* scan = d_cscan.as<int>();
+  k_compact_count<<<nb, 256, 0, stream>>>(d_cmask.as<unsigned>(), N, -1, scan);
+  k_compact_scan<<<1, 1024, 0, stream>>>(scan, nb, nullptr, scan + nb);
+  k_compact_scatter<<<nb, 256, 0, stream>>>(d_cmask.as<unsigned>(), N, -1, scan, d_cverts.as<int>(),
+                                            d_cidx.as<int>());
+  CU(cudaGetLastError());
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::sim_set_obstacles(const mlx_obstacle* obs, int nobs, double restitution) {
+  if (!sim.ready) return set_error(MLX_ERR_ARGUMENT, "mlx_sim_init first");
+  std::vector<Obstacle> o;
+  CHECK(prepare_obstacles(obs, nobs, o));
+  DeviceGuard g(device);
+  sim_obs = o;
+  sim_restitution = restitution;
+  if (!o.empty()) {
+    CHECK(d_obs.ensure(sizeof(Obstacle) * o.size()));
+    CHECK(d_cmask.ensure(sizeof(unsigned) * N));
+    CHECK(d_cverts.ensure(sizeof(int) * N));
+    CHECK(d_cidx.ensure(sizeof(int) * N));
+    CHECK(d_cscan.ensure(sizeof(int) * (blocks_for(N, 256) + 2)));
+    CHECK(d_clam_dev.ensure(sizeof(double) * (size_t)N * o.size()));
+    CU(cudaMemcpyAsync(d_obs.p, o.data(), sizeof(Obstacle) * o.size(), cudaMemcpyHostToDevice, stream));
+    CU(cudaMemsetAsync(d_cscan.p, 0, sizeof(int) * (blocks_for(N, 256) + 2), stream));
+    CU(cudaStreamSynchronize(stream));
+  }
+  if (sim.graph) { cudaGraphExecDestroy(sim.graph); sim.graph = nullptr; }
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::sim_contact_count(int32_t* n) {
+  if (!n) return set_error(MLX_ERR_ARGUMENT, "null argument");
+  *n = 0;
+  if (sim_obs.empty()) return MLX_OK;
+  DeviceGuard g(device);
+  CU(cudaMemcpyAsync(h_scalar.p, d_cscan.as<int>() + blocks_for(N, 256), sizeof(int), cudaMemcpyDeviceToHost, stream));
+  CU(cudaStreamSynchronize(stream));
+  *n = h_scalar.as<int>()[0];
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::find_contacts(const mlx_obstacle* obs, int nobs, const double* p, int max_contacts, int32_t* vids,
+                             double* normals, double* points, double* comp, int32_t* K) {
+  if (!p || !K) return set_error(MLX_ERR_ARGUMENT, "null argument");
+  std::vector<Obstacle> o;
+  CHECK(prepare_obstacles(obs, nobs, o));
+  *K = 0;
+  if (o.empty()) return MLX_OK;
+  DeviceGuard g(device);
+  const int nb = blocks_for(N, 256);
+  const size_t cap = (size_t)N * o.size();
+  DevBuf dob, dmask, dverts, dscan, dx, dvid, dout, dpos;
+  CHECK(dob.ensure(sizeof(Obstacle) * o.size()));
+  CHECK(dmask.ensure(sizeof(unsigned) * N));
+  CHECK(dverts.ensure(sizeof(int) * cap));
+  CHECK(dscan.ensure(sizeof(int) * (nb + o.size() + 1)));
+  CHECK(dx.ensure(sizeof(double) * 3 * (size_t)N));
+  CHECK(dpos.ensure(sizeof(double4) * N));
+  CHECK(dvid.ensure(sizeof(int) * cap));
+  CHECK(dout.ensure(sizeof(double) * 7 * cap));
+  CU(cudaMemcpyAsync(dob.p, o.data(), sizeof(Obstacle) * o.size(), cudaMemcpyHostToDevice, stream));
+  CU(cudaMemcpyAsync(dx.p, p, sizeof(double) * 3 * (size_t)N, cudaMemcpyHostToDevice, stream));
+  CU(cudaMemsetAsync(dscan.p, 0, sizeof(int) * (nb + o.size() + 1), stream));
+  // positions in FP64 whatever the solver's precision: detection on the caller's values
+  k_load_pos<double><<<nb, 256, 0, stream>>>(dx.as<double>(), d_mass3.as<double>(), dpos.as<double4>(), N);
+  const int no = (int)o.size();
+  k_contact_mask<double><<<nb, 256, 0, stream>>>(dpos.as<double4>(), N, dob.as<Obstacle>(), no, dmask.as<unsigned>());
+  int* blk = dscan.as<int>();
+  int* tot = blk + nb;  // tot[f] = contacts before finder f
+  double* out = dout.as<double>();
+  for (int f = 0; f < no; ++f) {
+    k_compact_count<<<nb, 256, 0, stream>>>(dmask.as<unsigned>(), N, f, blk);
+    k_compact_scan<<<1, 1024, 0, stream>>>(blk, nb, tot + f, tot + f + 1);
+    k_compact_scatter<<<nb, 256, 0, stream>>>(dmask.as<unsigned>(), N, f, blk, dverts.as<int>(), nullptr);
+    k_contact_list<double><<<nb, 256, 0, stream>>>(dpos.as<double4>(), dob.as<Obstacle>(), f, dverts.as<int>(),
+                                                   tot + f, tot + f + 1, (int)cap, dvid.as<int>(), out,
+                                                   out + 3 * cap, out + 6 * cap);
+  }
+  CU(cudaGetLastError());
+  int total = 0;
+  CU(cudaMemcpyAsync(&total, tot + no, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  CU(cudaStreamSynchronize(stream));
+  *K = total;
+  if (total > max_contacts) return set_error(MLX_ERR_LIMIT, "more contacts than max_contacts");
+  if (total == 0) return MLX_OK;
+  if (!vids || !normals || !points || !comp) return set_error(MLX_ERR_ARGUMENT, "null output array");
+  std::vector<double> h(7 * cap);
+  CU(cudaMemcpyAsync(vids, dvid.p, sizeof(int) * total, cudaMemcpyDeviceToHost, stream));
+  CU(cudaMemcpyAsync(h.data(), dout.p, sizeof(double) * 7 * cap, cudaMemcpyDeviceToHost, stream));
+  CU(cudaStreamSynchronize(stream));
+  for (int d = 0; d < 3; ++d) {
+    std::memcpy(normals + (size_t)d * total, h.data() + (size_t)d * cap, sizeof(double) * total);
+    std::memcpy(points + (size_t)d * total, h.data() + 3 * cap + (size_t)d * cap, sizeof(double) * total);
+  }
+  std::memcpy(comp, h.data() + 6 * cap, sizeof(double) * total);
+  return MLX_OK;
+}
+
 template <typename R>
 double Solver<R>::bytes_per_tet() const {
   // algorithmic bytes of one tet projection in this layout: vertex ids,
@@ -1733,9 +1906,22 @@ int Solver<R>::sim_issue_step(long long* launches) {
   RunState st;
   st.runUntil = sim.P.run_until;
   ContactData cd{};
-  CHECK(run_layers(&sim.ld, &sim.P, nullptr, cd, st, true, sim_work));
+  const DevContacts dc = dev_contacts();
+  if (dc.nobs) {
+    // contacts of the step-start positions (simulate3D detects on mesh3D.p
+    // before integrate; oldp holds those positions now)
+    CHECK(detect_contacts(d_oldp.as<R4<R>>()));
+    st.launches += 4;
+  }
+  CHECK(run_layers(&sim.ld, &sim.P, nullptr, cd, st, true, sim_work, dc));
   k_sim_end<R><<<blocks_for(N, 256), 256, 0, stream>>>(p, d_oldp.as<R4<R>>(), d_vel.as<R4<R>>(), N, h);
   CU(cudaGetLastError());
+  if (dc.nobs) {
+    k_contact_velocity<R><<<blocks_for(N, 256), 256, 0, stream>>>(dc, d_oldp.as<R4<R>>(), d_vel.as<R4<R>>(), h,
+                                                                  sim.P.gravity, sim_restitution);
+    CU(cudaGetLastError());
+    ++st.launches;
+  }
   CU(cudaMemcpyAsync(h_gsync.p, d_gsync.p, sizeof(unsigned int) * 4, cudaMemcpyDeviceToHost, stream));
   if (launches) *launches = st.launches + 2;
   return MLX_OK;
@@ -1952,6 +2138,21 @@ long long mlx_last_call_launches(const mlx_solver* s) { return s ? s->impl->laun
 int mlx_sim_autotune(mlx_solver* s, int32_t reps, double* before_ms, double* after_ms) {
   if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
   return s->impl->sim_autotune(reps, before_ms, after_ms);
+}
+int mlx_find_contacts(mlx_solver* s, const mlx_obstacle* obstacles, int32_t num_obstacles, const double* p,
+                      int32_t max_contacts, int32_t* vertex_ids, double* normals, double* point_colliders,
+                      double* compliance, int32_t* num_contacts) {
+  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+  return s->impl->find_contacts(obstacles, num_obstacles, p, max_contacts, vertex_ids, normals, point_colliders,
+                                compliance, num_contacts);
+}
+int mlx_sim_set_obstacles(mlx_solver* s, const mlx_obstacle* obstacles, int32_t num_obstacles, double restitution) {
+  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+  return s->impl->sim_set_obstacles(obstacles, num_obstacles, restitution);
+}
+int mlx_sim_contact_count(mlx_solver* s, int32_t* n) {
+  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+  return s->impl->sim_contact_count(n);
 }
 int mlx_launch_path(const mlx_solver* s, char* buf, int32_t n) {
   if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver"), -1;

@@ -25,6 +25,10 @@ struct SolverBase {
   virtual int sweep_stats(double* ms, double* bytes, long long* launches, int reset) = 0;
   virtual std::string launch_path() const = 0;
   virtual int sim_autotune(int reps, double* before_ms, double* after_ms) = 0;
+  virtual int find_contacts(const mlx_obstacle* obs, int nobs, const double* p, int max_contacts, int32_t* vids,
+                            double* normals, double* points, double* comp, int32_t* K) = 0;
+  virtual int sim_set_obstacles(const mlx_obstacle* obs, int nobs, double restitution) = 0;
+  virtual int sim_contact_count(int32_t* n) = 0;
 };
 
 SolverBase* make_solver(const mlx_mesh_desc* md, int* rc);

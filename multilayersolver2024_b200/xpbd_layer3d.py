@@ -185,6 +185,21 @@ class ResidentSim:
     def launches_per_step(self):
         return int(self._lib.mlx_sim_launches_per_step(self.solver.handle))
 
+    def set_obstacles(self, finders, restitution=1e-2):
+        """Contacts with analytic obstacles detected on the device every step
+        (``mlx_sim_set_obstacles``); restitution as contactVelocityUpdate's e."""
+        from .contacts import pack_finders
+        arr, n = pack_finders(finders)
+        self._obstacles = arr
+        check("mlx_sim_set_obstacles", self._lib.mlx_sim_set_obstacles(self.solver.handle, C.cast(arr, C.c_void_p), n,
+                                                                        float(restitution)), self._lib)
+
+    def contact_count(self):
+        """Contact vertices of the last step."""
+        n = C.c_int32(0)
+        check("mlx_sim_contact_count", self._lib.mlx_sim_contact_count(self.solver.handle, C.byref(n)), self._lib)
+        return n.value
+
     def autotune(self, reps=10):
         """Per-colour tile autotuner (``mlx_sim_autotune``); returns one
         step's device time in ms before and after tuning."""

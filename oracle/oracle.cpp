@@ -1140,4 +1140,54 @@ int orc_find_contacts_sphere(const double* p, int32_t N, double radius, const do
   return K;
 }
 
+// PlatformContactDetector.findContacts (3d/contact/PlatformContactDetector.m:65-119)
+// for a box with rotation R (row-major, RotationMatrixDegrees), full extents
+// scale = [width depth height] and centre: contacts of the vertices inside
+// the box, pushed out through the nearest face (first axis on ties),
+// normal = sign(dot) * direction of that axis, phi = -(half - |dot|).
+int orc_find_contacts_platform(const double* p, int32_t N, const double* R, const double* scale,
+                               const double* center, double compliance, int32_t* vids, double* normals,
+                               double* points, double* comp) {
+  double dir[9], half[3];
+  for (int r = 0; r < 3; ++r) {
+    const double* row = R + 3 * r;
+    double nr = std::sqrt(row[0] * row[0] + row[1] * row[1] + row[2] * row[2]);
+    for (int d = 0; d < 3; ++d) dir[3 * r + d] = row[d] / nr;
+    half[r] = scale[r] / 2;
+  }
+  std::vector<int> idx;
+  std::vector<V3> nrm;
+  std::vector<double> phis;
+  for (int i = 0; i < N; ++i) {
+    double e[3] = {p[3 * i] - center[0], p[3 * i + 1] - center[1], p[3 * i + 2] - center[2]};
+    double dots[3], ad[3];
+    bool inside = true;
+    for (int a = 0; a < 3; ++a) {
+      dots[a] = e[0] * dir[3 * a] + e[1] * dir[3 * a + 1] + e[2] * dir[3 * a + 2];
+      inside = inside && std::fabs(dots[a]) <= half[a];
+      ad[a] = half[a] - std::fabs(dots[a]);
+    }
+    if (!inside) continue;
+    int k = 0;
+    if (ad[1] < ad[k]) k = 1;
+    if (ad[2] < ad[k]) k = 2;
+    double sgn = dots[k] > 0 ? 1.0 : (dots[k] < 0 ? -1.0 : 0.0);
+    idx.push_back(i);
+    nrm.push_back(v3(sgn * dir[3 * k], sgn * dir[3 * k + 1], sgn * dir[3 * k + 2]));
+    phis.push_back(-ad[k]);
+  }
+  int K = (int)idx.size();
+  for (int k = 0; k < K; ++k) {
+    int i = idx[k];
+    V3 n = nrm[k];
+    vids[k] = i + 1;
+    normals[k] = n.x; normals[k + K] = n.y; normals[k + 2 * K] = n.z;
+    points[k] = p[3 * i] - n.x * phis[k];
+    points[k + K] = p[3 * i + 1] - n.y * phis[k];
+    points[k + 2 * K] = p[3 * i + 2] - n.z * phis[k];
+    comp[k] = compliance;
+  }
+  return K;
+}
+
 }  // extern "C"

@@ -66,6 +66,8 @@ def load():
         "orc_find_contacts_plane": ([_f64p, C.c_int32, _f64p, _f64p, C.c_double, _i32p, _f64p, _f64p, _f64p],
                                     C.c_int),
         "orc_find_contacts_sphere": ([_f64p, C.c_int32, C.c_double, _f64p, _i32p, _f64p, _f64p, _f64p], C.c_int),
+        "orc_find_contacts_platform": ([_f64p, C.c_int32, _f64p, _f64p, _f64p, C.c_double, _i32p, _f64p, _f64p,
+                                        _f64p], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -159,6 +161,34 @@ def find_contacts_sphere(p, radius, center):
     K = lib.orc_find_contacts_sphere(f64(np.ascontiguousarray(p)), N, radius, f64(np.asarray(center, float)),
                                      i32(ids), f64(n), f64(q), f64(a))
     return (n[:3 * K].reshape(3, K).T.copy(), q[:3 * K].reshape(3, K).T.copy(), ids[:K].copy(), a[:K].copy())
+
+
+def find_contacts_platform(p, rotation, scale, center, compliance=1e-4):
+    lib = load()
+    N = p.size // 3
+    ids = np.zeros(N, np.int32); n = np.zeros(3 * N); q = np.zeros(3 * N); a = np.zeros(N)
+    K = lib.orc_find_contacts_platform(f64(np.ascontiguousarray(p)), N,
+                                       f64(np.ascontiguousarray(np.asarray(rotation, float).reshape(9))),
+                                       f64(np.asarray(scale, float)), f64(np.asarray(center, float)), compliance,
+                                       i32(ids), f64(n), f64(q), f64(a))
+    return (n[:3 * K].reshape(3, K).T.copy(), q[:3 * K].reshape(3, K).T.copy(), ids[:K].copy(), a[:K].copy())
+
+
+def find_contacts(finders, p):
+    """simulate3D's finder loop (3d/simulate3D.m:156-171) on the oracle's
+    finders: the lists concatenated in finder order."""
+    from multilayersolver2024_b200 import _lib
+    from multilayersolver2024_b200.xpbd_layer3d import ContactSet
+    sets = []
+    for f in finders:
+        if f.kind == _lib.MLX_OBSTACLE_PLANE:
+            r = find_contacts_plane(p, f.normal, f.center, f.compliance)
+        elif f.kind == _lib.MLX_OBSTACLE_SPHERE:
+            r = find_contacts_sphere(p, f.radius, f.center)
+        else:
+            r = find_contacts_platform(p, f.rotation, f.scale, f.center, f.compliance)
+        sets.append(ContactSet(*r))
+    return ContactSet.concat(sets)
 
 
 def layer_solve(mesh, ls, layersMap, iterations, params, contacts, xi, lambdai, oldp, oldOldp, f, resv, pinnedx,
