@@ -196,6 +196,8 @@ int mlx_sim_init(mlx_solver* solver, const mlx_layer_desc* layers,
  * (3d/animations/VelocityImpulseAnimationScripter.m:16-30). */
 int mlx_sim_add_velocity(mlx_solver* solver, const int32_t* dofs, const double* dv, int32_t n);
 /* Runs `nsteps` steps; use_graph replays one captured CUDA graph per step.
+ * With compute_residuals in the parameters the layers iterate until the
+ * stop rules of simpleMonitorError end them (see mlx_sim_monitor).
  * device_ms (optional) receives the CUDA-event time of the steps. */
 int mlx_sim_step(mlx_solver* solver, int32_t nsteps, int32_t use_graph, double* device_ms);
 /* Copies positions and velocities (3N each, either may be NULL) to the host. */
@@ -272,6 +274,16 @@ int mlx_find_contacts(mlx_solver* solver, const mlx_obstacle* obstacles, int32_t
  * Call after mlx_sim_init. */
 int mlx_sim_set_obstacles(mlx_solver* solver, const mlx_obstacle* obstacles, int32_t num_obstacles,
                           double restitution);
+/* Residual monitor of the last resident step run with compute_residuals:
+ * its residualArray (the leading initial residual 0 included; at most
+ * `capacity` entries copied, *len = full length), the projectGS iterations of
+ * all layers, runUntilResSmallerThan after the step (it carries over to the
+ * next step as in xpbdLayer3D.integrate) and a status (0 ok, 1 a layer hit
+ * the iteration cap of 1e6, 2 the residual array overflowed).  In a graph
+ * step (use_graph) the stop rules of simpleMonitorError run on the device
+ * (conditional graph nodes); without a graph they run on the host. */
+int mlx_sim_monitor(mlx_solver* solver, double* residuals, int32_t capacity, int32_t* len,
+                    int32_t* total_iterations, double* run_until, int32_t* status);
 /* Number of contacts of the last resident step (reads one int from the device). */
 int mlx_sim_contact_count(mlx_solver* solver, int32_t* num_contact_vertices);
 

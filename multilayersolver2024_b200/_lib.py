@@ -146,6 +146,7 @@ SIGNATURES = {
                           C.c_int),
     "mlx_sim_set_obstacles": ([C.c_void_p, C.c_void_p, C.c_int32, C.c_double], C.c_int),
     "mlx_sim_contact_count": ([C.c_void_p, _i32p], C.c_int),
+    "mlx_sim_monitor": ([C.c_void_p, _f64p, C.c_int32, _i32p, _i32p, _f64p, _i32p], C.c_int),
     "mlx_stvk_residual_noalloc": ([C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p], C.c_int),
     "mlx_greedy_coloring": ([_i32p, C.c_int32, C.c_int32, _i32p, _i32p], C.c_int),

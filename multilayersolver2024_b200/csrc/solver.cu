@@ -17,10 +17,12 @@
 #include "persistent.cuh"
 #include "cluster.cuh"
 #include "contacts.cuh"
+#include "monitor.cuh"
 #include "partition.h"
 #include "solver.h"
 
 #include <algorithm>
+#include <cstddef>
 #include <chrono>
 #include <cstdlib>
 #include <cstdio>
@@ -224,6 +226,8 @@ struct Solver final : SolverBase {
   ~Solver() override {
     for (cudaEvent_t e : tev) cudaEventDestroy(e);
     if (sim.graph) cudaGraphExecDestroy(sim.graph);
+    if (cs_if) cudaStreamDestroy(cs_if);
+    if (cs_while) cudaStreamDestroy(cs_while);
     if (stream) cudaStreamDestroy(stream);
   }
 
@@ -287,6 +291,21 @@ struct Solver final : SolverBase {
     return dc;
   }
   int detect_contacts(const R4<R>* x0);  // stream work only (captured in the step)
+  // device residual monitor (monitor.cuh): conditional graph nodes
+  DevBuf d_mon;
+  cudaStream_t cs_if = nullptr, cs_while = nullptr;
+  MonState* mon() const { return d_mon.as<MonState>(); }
+  int cond_handle(cudaGraphConditionalHandle* h);
+  int cond_begin(cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type, cudaStream_t body);
+  int cond_end(cudaStream_t parent);
+  int residual_dev(double* out);
+  int norm_resv_dev(double* out);
+  int sim_monitor(double* ra, int cap, int32_t* len, int32_t* total_it, double* run_until, int32_t* status) override;
+  struct {
+    bool valid = false, device = false;
+    std::vector<double> ra;
+    int total_it = 0;
+  } sim_last;
   int find_contacts(const mlx_obstacle* obs, int nobs, const double* p, int max_contacts, int32_t* vids,
                     double* normals, double* points, double* comp, int32_t* K) override;
   int sim_set_obstacles(const mlx_obstacle* obs, int nobs, double restitution) override;
@@ -348,7 +367,7 @@ struct Solver final : SolverBase {
   int sweep_stats(double* ms, double* bytes, long long* launches, int reset) override;
   int collect_sweep_times();
   int sim_setup(const mlx_layer_desc* ld, const mlx_solve_params* P, const double* p0, const double* v0);
-  int sim_issue_step(long long* launches);
+  int sim_issue_step(long long* launches, bool capturing);
   int sim_step(int nsteps, int use_graph, double* device_ms) override;
   int sim_add_velocity(const int32_t* dofs, const double* dv, int n) override;
   int sim_get_state(double* p, double* v) override;
@@ -925,8 +944,36 @@ template <typename R>
 int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, const mlx_contacts* K,
                           const ContactData& cd, RunState& st, bool capturing, LayerWork& w,
                           const DevContacts& dc) {
-  if (capturing && P->compute_residuals)
-    return set_error(MLX_ERR_UNSUPPORTED, "residual monitoring cannot run inside a captured step");
+  // In a captured step the residual monitor runs on the device: every layer
+  // is a conditional IF node and its projectGS loop a conditional WHILE node
+  // (monitor.cuh).  Kernels keep plain stream order there.
+  const bool devmon = capturing && P->compute_residuals;
+  if (devmon && (cd.K > 0 || dc.nobs))
+    return set_error(MLX_ERR_UNSUPPORTED, "device residual monitoring does not cover contacts");
+  struct Guard {
+    Solver* s;
+    cudaStream_t outer;
+    bool pdl;
+    ~Guard() {
+      for (cudaStream_t b : {s->cs_while, s->cs_if}) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (b && cudaStreamIsCapturing(b, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+          cudaGraph_t g = nullptr;
+          cudaStreamEndCapture(b, &g);
+        }
+      }
+      s->stream = outer;
+      s->pdl = pdl;
+    }
+  } guard{this, stream, pdl};
+  if (devmon) {
+    pdl = false;
+    if (!cs_if) CU(cudaStreamCreateWithFlags(&cs_if, cudaStreamNonBlocking));
+    if (!cs_while) CU(cudaStreamCreateWithFlags(&cs_while, cudaStreamNonBlocking));
+  }
+  MonParams mp{P->stop_at_improvement_percent, P->give_up_threshold, P->give_up_enabled,
+               P->last_layer_give_up_enabled, (long long)P->hanging_stop};
+  const cudaStream_t outer = stream;
   const double h = P->h;
   const R hR = (R)h;
   const int nK = cd.K;
@@ -1009,6 +1056,15 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
     R4<R>* resv = d_resv.as<R4<R>>();
     R4<R>* xprev = d_xprev.as<R4<R>>();
     double4* ri = d_ri.as<double4>();
+    if (devmon) {
+      // the layer runs only while stopSolve is unset
+      cudaGraphConditionalHandle h_if;
+      CHECK(cond_handle(&h_if));
+      k_mon_layer_begin<<<1, 1, 0, stream>>>(mon(), h_if, layer, mp);
+      CU(cudaGetLastError());
+      ++st.launches;
+      CHECK(cond_begin(h_if, cudaGraphCondTypeIf, cs_if));
+    }
     if (rigidLayer && ls.nb > 0) CU(cudaMemcpyAsync(xprev, p, sizeof(R4<R>) * N, cudaMemcpyDeviceToDevice, stream));
     if (ls.nb > 0) {
       if (!capturing) CHECK(w.bodies.ensure(sizeof(Body) * ls.nb));
@@ -1026,7 +1082,10 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
       ++st.launches;
     }
     double normresv = 0;
-    if (P->compute_residuals) {
+    if (devmon) {
+      CHECK(norm_resv_dev(&mon()->normresv));
+      st.launches += 2;
+    } else if (P->compute_residuals) {
       CU(cudaStreamSynchronize(stream));
       auto t0 = std::chrono::steady_clock::now();
       CHECK(norm_resv(&normresv));
@@ -1075,12 +1134,21 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
       if (nK > 0) CU(cudaStreamSynchronize(stream));  // cpack is a pageable host source
       continue;
     }
+    cudaGraphConditionalHandle h_while_cur = 0;
+    if (devmon) {
+      // the projectGS loop as a WHILE node whose body is one iteration
+      CHECK(cond_handle(&h_while_cur));
+      k_mon_loop_begin<<<1, 1, 0, stream>>>(mon(), h_while_cur, ld->iterations[layer], isLast ? 1 : 0);
+      CU(cudaGetLastError());
+      ++st.launches;
+      CHECK(cond_begin(h_while_cur, cudaGraphCondTypeWhile, cs_while));
+    }
     long long it = 1;
-    while (it <= ld->iterations[layer] || (!stopSolve && st.runUntil >= 0 && isLast)) {
+    while (devmon || it <= ld->iterations[layer] || (!stopSolve && st.runUntil >= 0 && isLast)) {
       ++it;
       if (it > kSafetyIterations) return set_error(MLX_ERR_LIMIT, "iteration safety limit reached");
       ++st.totalIterations;
-      const bool timed = sweep_timing && tev_used + 2 <= tev.size();
+      const bool timed = !devmon && sweep_timing && tev_used + 2 <= tev.size();
       if (timed) CHECK(record_event(tev[tev_used], capturing));
       long long sweep_l = 0;
       double sweep_b = 0;
@@ -1117,6 +1185,14 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
         ++st.launches;
       }
       bool endLayer = false;
+      if (devmon) {
+        CHECK(residual_dev(&mon()->res));
+        k_mon_iter_end<<<1, 1, 0, stream>>>(mon(), h_while_cur, ld->iterations[layer], isLast ? 1 : 0, mp);
+        CU(cudaGetLastError());
+        st.launches += 3;
+        CHECK(cond_end(cs_if));  // end of the WHILE body
+        break;
+      }
       if (P->compute_residuals) {
         CU(cudaStreamSynchronize(stream));
         auto t0 = std::chrono::steady_clock::now();
@@ -1148,9 +1224,88 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
       CU(cudaGetLastError());
       ++st.launches;
     }
+    if (devmon) CHECK(cond_end(outer));  // end of the layer's IF body
     if (nK > 0) CU(cudaStreamSynchronize(stream));  // cpack is a pageable host source
     if (stopSolve) break;
   }
+  return MLX_OK;
+}
+
+// A conditional handle of the graph the solver's stream is capturing into.
+template <typename R>
+int Solver<R>::cond_handle(cudaGraphConditionalHandle* h) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaGraph_t g = nullptr;
+  CU(cudaStreamGetCaptureInfo(stream, &cs, nullptr, &g, nullptr, nullptr));
+  if (cs != cudaStreamCaptureStatusActive) return set_error(MLX_ERR_ARGUMENT, "conditional node outside a capture");
+  CU(cudaGraphConditionalHandleCreate(h, g, 0, 0));
+  return MLX_OK;
+}
+
+// Appends a conditional node after the captured work so far and continues
+// the capture inside its body on `body` (the solver's stream becomes `body`).
+template <typename R>
+int Solver<R>::cond_begin(cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type, cudaStream_t body) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  CU(cudaStreamGetCaptureInfo(stream, &cs, nullptr, &g, &deps, &nd));
+  cudaGraphNodeParams np = {};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = type;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  CU(cudaGraphAddNode(&node, g, deps, nd, &np));
+  CU(cudaStreamUpdateCaptureDependencies(stream, &node, 1, cudaStreamSetCaptureDependencies));
+  CU(cudaStreamBeginCaptureToGraph(body, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                   cudaStreamCaptureModeThreadLocal));
+  stream = body;
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::cond_end(cudaStream_t parent) {
+  cudaGraph_t g = nullptr;
+  CU(cudaStreamEndCapture(stream, &g));
+  stream = parent;
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::residual_dev(double* out) {
+  const int bs = 256;
+  const int tetBlocks = std::min(blocks_for(T, bs), 592);
+  ContactData cd{};
+  const R inv_h2 = R(1) / ((R)sim.P.h * (R)sim.P.h), inv_h = R(1) / (R)sim.P.h;
+  const double inv_h2_d = 1.0 / (sim.P.h * sim.P.h);
+  TetData<R> td = tets();
+  double* partials = d_partials.as<double>();
+  switch (mat_kind) {
+    case MAT_NH:
+      k_residual_partials<R, MAT_NH><<<tetBlocks, bs, 0, stream>>>(td, pos(), cd, 0.0, inv_h2, inv_h, inv_h2_d, tetBlocks, partials);
+      break;
+    case MAT_STVK_BLOCKS:
+      k_residual_partials<R, MAT_STVK_BLOCKS><<<tetBlocks, bs, 0, stream>>>(td, pos(), cd, 0.0, inv_h2, inv_h, inv_h2_d, tetBlocks, partials);
+      break;
+    default:
+      k_residual_partials<R, MAT_STVK_LAME><<<tetBlocks, bs, 0, stream>>>(td, pos(), cd, 0.0, inv_h2, inv_h, inv_h2_d, tetBlocks, partials);
+  }
+  CU(cudaGetLastError());
+  k_finish_norm<256><<<1, 256, 0, stream>>>(partials, tetBlocks, out);
+  CU(cudaGetLastError());
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::norm_resv_dev(double* out) {
+  const int bs = 256;
+  const int grid = std::min(blocks_for(N, bs), 296);
+  k_norm3_partials<R><<<grid, bs, 0, stream>>>(d_resv.as<R4<R>>(), N, d_partials.as<double>());
+  CU(cudaGetLastError());
+  k_finish_norm<256><<<1, 256, 0, stream>>>(d_partials.as<double>(), grid, out);
+  CU(cudaGetLastError());
   return MLX_OK;
 }
 
@@ -1523,10 +1678,15 @@ __global__ void k_add_velocity(R4<R>* __restrict__ vel, const int* __restrict__ 
 template <typename R>
 int Solver<R>::sim_setup(const mlx_layer_desc* ld, const mlx_solve_params* P, const double* p0, const double* v0) {
   CHECK(validate_layers(ld, P));
-  if (P->compute_residuals)
-    return set_error(MLX_ERR_UNSUPPORTED, "the resident stepper runs fixed iteration counts (compute_residuals = 0)");
   if (!p0) return set_error(MLX_ERR_ARGUMENT, "initial positions are required");
   DeviceGuard g(device);
+  if (P->compute_residuals) {
+    CHECK(d_mon.ensure(sizeof(MonState)));
+    CU(cudaMemsetAsync(d_mon.p, 0, sizeof(MonState), stream));
+    CU(cudaMemcpyAsync(&mon()->run_until, &P->run_until, sizeof(double), cudaMemcpyHostToDevice, stream));
+    CU(cudaStreamSynchronize(stream));
+  }
+  sim_last.valid = false;
   // copy the fixed layer description (the caller's arrays may go away)
   const size_t TL = (size_t)T * ld->num_columns, NL = (size_t)N * ld->num_columns;
   sim.layers_map.assign(ld->layers_map, ld->layers_map + ld->num_layers);
@@ -1764,6 +1924,38 @@ int Solver<R>::sim_set_obstacles(const mlx_obstacle* obs, int nobs, double resti
 }
 
 template <typename R>
+int Solver<R>::sim_monitor(double* ra, int cap, int32_t* len, int32_t* total_it, double* run_until, int32_t* status) {
+  if (!sim_last.valid) return set_error(MLX_ERR_ARGUMENT, "no monitored step has run (compute_residuals = 0?)");
+  int n = 0, tot = 0, err = 0;
+  double ru = sim.P.run_until;
+  std::vector<double> r;
+  if (sim_last.device) {
+    DeviceGuard g(device);
+    MonState hdr;
+    const size_t head = offsetof(MonState, ra);
+    CU(cudaMemcpyAsync(&hdr, d_mon.p, head, cudaMemcpyDeviceToHost, stream));
+    CU(cudaStreamSynchronize(stream));
+    n = hdr.ra_len;
+    tot = hdr.total_iterations;
+    err = hdr.error;
+    ru = hdr.run_until;
+    r.resize(n);
+    if (n) CU(cudaMemcpyAsync(r.data(), mon()->ra, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
+    CU(cudaStreamSynchronize(stream));
+  } else {
+    r = sim_last.ra;
+    n = (int)r.size();
+    tot = sim_last.total_it;
+  }
+  if (len) *len = n;
+  if (total_it) *total_it = tot;
+  if (run_until) *run_until = ru;
+  if (status) *status = err;
+  if (ra && cap > 0) std::memcpy(ra, r.data(), sizeof(double) * std::min(cap, n));
+  return MLX_OK;
+}
+
+template <typename R>
 int Solver<R>::sim_contact_count(int32_t* n) {
   if (!n) return set_error(MLX_ERR_ARGUMENT, "null argument");
   *n = 0;
@@ -1892,10 +2084,15 @@ int Solver<R>::sweep_stats(double* ms, double* bytes, long long* launches, int r
 }
 
 template <typename R>
-int Solver<R>::sim_issue_step(long long* launches) {
+int Solver<R>::sim_issue_step(long long* launches, bool capturing) {
   const double h = sim.P.h;
   tev_used = 0;
   R4<R>* p = pos();
+  const bool devmon = capturing && sim.P.compute_residuals;
+  if (devmon) {
+    k_mon_step_begin<<<1, 1, 0, stream>>>(mon());
+    CU(cudaGetLastError());
+  }
   k_sim_begin<R><<<blocks_for(N, 256), 256, 0, stream>>>(p, d_vel.as<R4<R>>(), d_oldp.as<R4<R>>(),
                                                           d_resv.as<R4<R>>(), d_mass3.as<double>(),
                                                           d_pin_mask.as<unsigned char>(), N, h, sim.P.gravity,
@@ -1905,6 +2102,7 @@ int Solver<R>::sim_issue_step(long long* launches) {
   CHECK(reset_gsync());
   RunState st;
   st.runUntil = sim.P.run_until;
+  st.residualArray.assign(1, 0.0);  // integrate's initialResidual (xpbdLayer3D.m:670-674)
   ContactData cd{};
   const DevContacts dc = dev_contacts();
   if (dc.nobs) {
@@ -1913,7 +2111,16 @@ int Solver<R>::sim_issue_step(long long* launches) {
     CHECK(detect_contacts(d_oldp.as<R4<R>>()));
     st.launches += 4;
   }
-  CHECK(run_layers(&sim.ld, &sim.P, nullptr, cd, st, true, sim_work, dc));
+  CHECK(run_layers(&sim.ld, &sim.P, nullptr, cd, st, capturing, sim_work, dc));
+  if (sim.P.compute_residuals) {
+    sim_last.valid = true;
+    sim_last.device = devmon;
+    if (!devmon) {
+      sim_last.ra = st.residualArray;
+      sim_last.total_it = st.totalIterations;
+      sim.P.run_until = st.runUntil;  // obj.runUntilResSmallerThan carries over to the next step
+    }
+  }
   k_sim_end<R><<<blocks_for(N, 256), 256, 0, stream>>>(p, d_oldp.as<R4<R>>(), d_vel.as<R4<R>>(), N, h);
   CU(cudaGetLastError());
   if (dc.nobs) {
@@ -1936,7 +2143,7 @@ int Solver<R>::sim_step(int nsteps, int use_graph, double* device_ms) {
     cudaGraph_t graph = nullptr;
     CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     long long nl = 0;
-    int rc = sim_issue_step(&nl);
+    int rc = sim_issue_step(&nl, true);
     cudaError_t e = cudaStreamEndCapture(stream, &graph);
     if (rc != MLX_OK) {
       if (graph) cudaGraphDestroy(graph);
@@ -1957,9 +2164,14 @@ int Solver<R>::sim_step(int nsteps, int use_graph, double* device_ms) {
   for (int s = 0; s < nsteps; ++s) {
     if (use_graph) {
       CU(cudaGraphLaunch(sim.graph, stream));
+      if (sim.P.compute_residuals) {
+        sim_last.valid = true;
+        sim_last.device = true;
+      }
     } else {
       long long nl = 0;
-      CHECK(sim_issue_step(&nl));
+      // without a graph the residual monitor runs on the host
+      CHECK(sim_issue_step(&nl, !sim.P.compute_residuals));
       sim.launches_per_step = nl;
     }
     if (sweep_timing) {  // the event pairs are reused by every step
@@ -2149,6 +2361,11 @@ int mlx_find_contacts(mlx_solver* s, const mlx_obstacle* obstacles, int32_t num_
 int mlx_sim_set_obstacles(mlx_solver* s, const mlx_obstacle* obstacles, int32_t num_obstacles, double restitution) {
   if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
   return s->impl->sim_set_obstacles(obstacles, num_obstacles, restitution);
+}
+int mlx_sim_monitor(mlx_solver* s, double* residuals, int32_t capacity, int32_t* len, int32_t* total_iterations,
+                    double* run_until, int32_t* status) {
+  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+  return s->impl->sim_monitor(residuals, capacity, len, total_iterations, run_until, status);
 }
 int mlx_sim_contact_count(mlx_solver* s, int32_t* n) {
   if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");

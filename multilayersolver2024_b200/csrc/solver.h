@@ -29,6 +29,8 @@ struct SolverBase {
                             double* normals, double* points, double* comp, int32_t* K) = 0;
   virtual int sim_set_obstacles(const mlx_obstacle* obs, int nobs, double restitution) = 0;
   virtual int sim_contact_count(int32_t* n) = 0;
+  virtual int sim_monitor(double* ra, int cap, int32_t* len, int32_t* total_it, double* run_until,
+                          int32_t* status) = 0;
 };
 
 SolverBase* make_solver(const mlx_mesh_desc* md, int* rc);

@@ -194,6 +194,17 @@ class ResidentSim:
         check("mlx_sim_set_obstacles", self._lib.mlx_sim_set_obstacles(self.solver.handle, C.cast(arr, C.c_void_p), n,
                                                                         float(restitution)), self._lib)
 
+    def monitor(self, capacity=16384):
+        """Residual monitor of the last step (``mlx_sim_monitor``): the
+        residual array, total projectGS iterations, runUntilResSmallerThan
+        and a status (0 ok)."""
+        ra = np.zeros(capacity)
+        n, it, st = C.c_int32(0), C.c_int32(0), C.c_int32(0)
+        ru = C.c_double(0)
+        check("mlx_sim_monitor", self._lib.mlx_sim_monitor(self.solver.handle, f64(ra), capacity, C.byref(n),
+                                                            C.byref(it), C.byref(ru), C.byref(st)), self._lib)
+        return ra[:min(n.value, capacity)].copy(), it.value, ru.value, st.value
+
     def contact_count(self):
         """Contact vertices of the last step."""
         n = C.c_int32(0)
