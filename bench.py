@@ -263,6 +263,33 @@ def run_ours(args, rank, world, local):
     h2d = 8 * (3 * 3 * N + 6 * T + m2.pinnedDOFs.size)
     d2h = 8 * 3 * N
 
+    # ---- iterations to residual 1e-4: the same workload with the residual
+    # monitor and stop rules on the device (conditional graph nodes) ----
+    to_res = None
+    if not args.no_residual_leg:
+        sc3 = make_scene()
+        m3 = sc3.mesh
+        integ3 = make_integrator(sc3, MLX_FP32)
+        integ3.computeResiduals = True
+        integ3.runUntilResSmallerThan = 1e-4
+        integ3.hangingStop = args.residual_cap
+        solver3 = Solver(m3, precision=MLX_FP32, device=local, material="lame")
+        sim3 = ResidentSim(solver3, integ3, ls, sc3.h, p0=m3.p, v0=np.zeros_like(m3.p))
+        sim3.add_velocity(sc3.impulse[0], sc3.impulse[1])
+        iters, ms_steps, finals, reached = [], [], [], []
+        for _ in range(args.residual_steps):
+            ms_steps.append(sim3.step(1, graph=True, timed=True))
+            ra, it_total, _, status = sim3.monitor()
+            iters.append(int(it_total))
+            finals.append(float(ra[-1]))
+            reached.append(bool(abs(ra[-1]) <= 1e-4))
+        solver3.close()
+        to_res = {"run_until": 1e-4, "hanging_stop": args.residual_cap, "steps": args.residual_steps,
+                  "iterations_per_step": iters, "ms_per_step": ms_steps,
+                  "steps_per_s": len(ms_steps) / (sum(ms_steps) / 1000.0), "final_residual": finals,
+                  "reached": reached,
+                  "monitor": "device (layers as conditional IF nodes, projectGS as conditional WHILE nodes)"}
+
     line = None
     if rank == 0:
         peak, peak_kind = measured_peak_hbm()
@@ -299,6 +326,7 @@ def run_ours(args, rank, world, local):
             "cpu_baseline": cpu,
             "e2e": None if not e2e_steps else {"value": e2e_steps * world / e2e_s, "unit": "steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "api": "XpbdLayer3D.integrate -> mlx_layer_solve"},
+            "to_residual": to_res,
             "gpu_launches": int(launches_per_step * args.steps),
             "clocks": clocks.summary(),
             "state_finite": finite,
@@ -336,6 +364,10 @@ def main():
     ap.add_argument("--autotune", action="store_true", help="run the per-colour tile autotuner before timing "
                     "(on by default for config 3)")
     ap.add_argument("--no-autotune", action="store_true", help="never run the autotuner (profiling runs)")
+    ap.add_argument("--no-residual-leg", action="store_true", help="skip the iterations-to-residual-1e-4 leg")
+    ap.add_argument("--residual-steps", type=int, default=2)
+    ap.add_argument("--residual-cap", type=int, default=15000,
+                    help="hangingStop of the residual leg (bounds the iterations of a step)")
     args = ap.parse_args()
     global CONFIG, WORKLOAD
     CONFIG = args.config
