@@ -287,6 +287,29 @@ int mlx_sim_monitor(mlx_solver* solver, double* residuals, int32_t capacity, int
 /* Number of contacts of the last resident step (reads one int from the device). */
 int mlx_sim_contact_count(mlx_solver* solver, int32_t* num_contact_vertices);
 
+/* ---- learned warm start: the perceptron ----------------------------------
+ * No counterpart in the reference.  n_in -> n_hidden (GELU) x
+ * n_hidden_layers -> n_out, BF16 weights and activations with FP32
+ * accumulation on the tensor cores (tcgen05), FP32 master parameters and
+ * Adam.  Parameters are flat FP32: per layer W (n_out x n_in, row-major) then
+ * b.  n_hidden is 64 or 128; batches hold at most max_batch rows.  Inputs,
+ * outputs and targets are row-major FP32 host arrays.  The loss is the mean
+ * squared error over the n_out outputs of the batch. */
+typedef struct mlx_mlp mlx_mlp;
+int mlx_mlp_create(int32_t n_in, int32_t n_hidden, int32_t n_hidden_layers, int32_t n_out, int32_t max_batch,
+                   uint64_t seed, int32_t device, mlx_mlp** out);
+int mlx_mlp_destroy(mlx_mlp* mlp);
+long long mlx_mlp_num_params(const mlx_mlp* mlp);
+int mlx_mlp_set_params(mlx_mlp* mlp, const float* params, long long n);
+int mlx_mlp_get_params(mlx_mlp* mlp, float* params, long long n);
+int mlx_mlp_forward(mlx_mlp* mlp, const float* x, int32_t batch, float* y);
+/* Loss and (optional) flat gradient of one batch, without an update. */
+int mlx_mlp_loss_grad(mlx_mlp* mlp, const float* x, const float* target, int32_t batch, float* loss, float* grad);
+/* Adam over `epochs` shuffled passes of n_samples rows in batches of `batch`
+ * (learning rate lr); losses (optional) receives each epoch's mean loss. */
+int mlx_mlp_train(mlx_mlp* mlp, const float* x, const float* target, int32_t n_samples, int32_t batch, int32_t epochs,
+                  float lr, uint64_t seed, float* losses);
+
 /* ---- allocation-free residual ------------------------------------------
  * No counterpart in the reference.  The elastic constraint residual of
  * simpleEvaluateAllConstraintResiduals (StVK Voigt tets, no contacts) on

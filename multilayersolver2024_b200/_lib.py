@@ -31,6 +31,7 @@ MLX_ERR_LIMIT = 6
 _i32p = C.POINTER(C.c_int32)
 _u8p = C.POINTER(C.c_uint8)
 _f64p = C.POINTER(C.c_double)
+_f32p = C.POINTER(C.c_float)
 
 
 class MeshDesc(C.Structure):
@@ -99,6 +100,10 @@ def ptr(a, ctype):
     return a.ctypes.data_as(C.POINTER(ctype))
 
 
+def f32(a):
+    return ptr(a, C.c_float)
+
+
 def f64(a):
     return ptr(a, C.c_double)
 
@@ -147,6 +152,16 @@ SIGNATURES = {
     "mlx_sim_set_obstacles": ([C.c_void_p, C.c_void_p, C.c_int32, C.c_double], C.c_int),
     "mlx_sim_contact_count": ([C.c_void_p, _i32p], C.c_int),
     "mlx_sim_monitor": ([C.c_void_p, _f64p, C.c_int32, _i32p, _i32p, _f64p, _i32p], C.c_int),
+    "mlx_mlp_create": ([C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.c_int32,
+                        C.POINTER(C.c_void_p)], C.c_int),
+    "mlx_mlp_destroy": ([C.c_void_p], C.c_int),
+    "mlx_mlp_num_params": ([C.c_void_p], C.c_longlong),
+    "mlx_mlp_set_params": ([C.c_void_p, _f32p, C.c_longlong], C.c_int),
+    "mlx_mlp_get_params": ([C.c_void_p, _f32p, C.c_longlong], C.c_int),
+    "mlx_mlp_forward": ([C.c_void_p, _f32p, C.c_int32, _f32p], C.c_int),
+    "mlx_mlp_loss_grad": ([C.c_void_p, _f32p, _f32p, C.c_int32, _f32p, _f32p], C.c_int),
+    "mlx_mlp_train": ([C.c_void_p, _f32p, _f32p, C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_uint64, _f32p],
+                      C.c_int),
     "mlx_stvk_residual_noalloc": ([C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p], C.c_int),
     "mlx_greedy_coloring": ([_i32p, C.c_int32, C.c_int32, _i32p, _i32p], C.c_int),
