@@ -310,6 +310,32 @@ int mlx_mlp_loss_grad(mlx_mlp* mlp, const float* x, const float* target, int32_t
 int mlx_mlp_train(mlx_mlp* mlp, const float* x, const float* target, int32_t n_samples, int32_t batch, int32_t epochs,
                   float lr, uint64_t seed, float* losses);
 
+/* Learned warm start of the resident stepper's first layer (its rigid
+ * clusters).  No counterpart in the reference.  For every cluster, right
+ * after makeRigidsFromConnectivity, 44 features are formed on the device: its
+ * COM velocity, angular velocity, COM displacement from the positions given
+ * to mlx_sim_init and the rotation vector of its deformation from them (FP64
+ * polar decomposition), and for the 4 clusters nearest at rest their
+ * relative velocities, COM distance change and mass ratio.  7 outputs act on
+ * the layer: a COM-velocity and angular-velocity correction applied before
+ * the symplectic rigid step, and the cluster's starting boundary multiplier
+ * (0 in the reference).
+ *   mode 1: `net` (44 -> 7) maps normalised features
+ *           ((f - feature_mean) / feature_std) to normalised outputs
+ *           (denormalised with output_mean / output_std);
+ *   mode 2: `corrections` (num_clusters x 7, output units) are applied;
+ *   mode 0: nothing is applied.
+ * With `record` every step keeps its raw features and the targets -- the
+ * corrections that would have put each cluster on the best-fit rigid motion
+ * to its final positions, and its mean final boundary multiplier -- for
+ * mlx_sim_warm_start_fetch.  The stop rules are unchanged: a warm start
+ * changes the iterations needed to reach the residual, not the residual. */
+int mlx_sim_warm_start(mlx_solver* solver, int32_t record, int32_t mode, mlx_mlp* net, const float* feature_mean,
+                       const float* feature_std, const float* output_mean, const float* output_std,
+                       const float* corrections, int32_t* num_clusters);
+int mlx_sim_warm_start_fetch(mlx_solver* solver, float* features, float* targets, int32_t capacity,
+                             int32_t* num_clusters);
+
 /* ---- allocation-free residual ------------------------------------------
  * No counterpart in the reference.  The elastic constraint residual of
  * simpleEvaluateAllConstraintResiduals (StVK Voigt tets, no contacts) on

@@ -547,6 +547,29 @@ struct mlx_mlp {
   Mlp impl;
 };
 
+namespace mlx {
+// Forward of `batch` device rows on stream `s` (which may be capturing);
+// *y / *ld receive the device output rows and their stride.
+int mlp_forward_on_stream(mlx_mlp* m, const float* d_x, int batch, cudaStream_t s, const float** y, int* ld) {
+  if (!m) return set_error(MLX_ERR_ARGUMENT, "null perceptron");
+  Mlp& p = m->impl;
+  cudaStream_t own = p.stream;
+  p.stream = s;
+  const int rc = p.forward_dev(d_x, batch);
+  p.stream = own;
+  if (y) *y = p.Y;
+  if (ld) *ld = p.Np.back();
+  return rc;
+}
+int mlp_dims(const mlx_mlp* m, int* n_in, int* n_out, int* max_batch) {
+  if (!m) return set_error(MLX_ERR_ARGUMENT, "null perceptron");
+  *n_in = m->impl.n_in;
+  *n_out = m->impl.n_out;
+  *max_batch = m->impl.max_batch;
+  return MLX_OK;
+}
+}  // namespace mlx
+
 extern "C" {
 
 int mlx_mlp_create(int32_t n_in, int32_t n_hidden, int32_t n_hidden_layers, int32_t n_out, int32_t max_batch,

@@ -19,6 +19,7 @@
 #include "contacts.cuh"
 #include "monitor.cuh"
 #include "partition.h"
+#include "warmstart.cuh"
 #include "solver.h"
 
 #include <algorithm>
@@ -198,6 +199,26 @@ struct LayerWork {
   DevBuf bodies, lamB;
 };
 
+// Learned warm start of the resident stepper (warmstart.cuh).
+struct WarmStartState {
+  int record = 0;            // keep features and targets of every step
+  int mode = 0;              // 0 off, 1 perceptron, 2 given corrections
+  mlx_mlp* net = nullptr;
+  int col = -1, nb = 0;
+  const float* y = nullptr;  // rows of corrections (device) and their stride
+  int ld = 0;
+  WsStatic S{};
+  DevBuf d_static, d_rest, d_norm, d_own, d_raw, d_feat, d_rec, d_target, d_corr;
+  void reset() {
+    record = mode = 0;
+    net = nullptr;
+    col = -1;
+    nb = 0;
+    y = nullptr;
+    ld = 0;
+  }
+};
+
 // Per-call bookkeeping of the layer loop (the scalars layerSolve threads
 // through projectGS, xpbdLayer3D.m:94-232).
 struct RunState {
@@ -306,6 +327,13 @@ struct Solver final : SolverBase {
     std::vector<double> ra;
     int total_it = 0;
   } sim_last;
+  WarmStartState ws;
+  std::vector<double> sim_p0;  // positions given to mlx_sim_init (the rest configuration)
+  int ws_configure(int record, int mode, mlx_mlp* net, const float* fmean, const float* fstd, const float* omean,
+                   const float* ostd, const float* corrections, int32_t* nb) override;
+  int ws_fetch(float* features, float* targets, int cap, int32_t* nb) override;
+  int ws_after_make_rigids(const LayerWork& w);
+  int ws_after_lamb_reset(const LayerWork& w);
   int find_contacts(const mlx_obstacle* obs, int nobs, const double* p, int max_contacts, int32_t* vids,
                     double* normals, double* points, double* comp, int32_t* K) override;
   int sim_set_obstacles(const mlx_obstacle* obs, int nobs, double restitution) override;
@@ -583,10 +611,8 @@ int Solver<R>::create(const mlx_mesh_desc* md) {
   CU(cudaMemcpyAsync(d_s2e.p, s2e.data(), sizeof(int) * T, cudaMemcpyHostToDevice, stream));
   if (!pinned.empty())
     CU(cudaMemcpyAsync(d_pin_dofs.p, pinned.data(), sizeof(int) * pinned.size(), cudaMemcpyHostToDevice, stream));
-  if (cluster_ok) {
-    vid_sorted = vid;
-    vowner = mp.vowner;
-  }
+  vid_sorted = vid;
+  if (cluster_ok) vowner = mp.vowner;
   CU(cudaStreamSynchronize(stream));
   return MLX_OK;
 }
@@ -1072,6 +1098,10 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
       k_make_rigids<R><<<ls.nb, 256, 0, stream>>>(L, w.bodies.as<Body>(), p, resv, d_vmass.as<double>(), ri);
       CU(cudaGetLastError());
       ++st.launches;
+      if (&w == &sim_work && col == ws.col && layer == 0 && (ws.record || ws.mode)) {
+        CHECK(ws_after_make_rigids(w));
+        st.launches += ws.mode == 1 ? 8 : 4;
+      }
     }
     k_release_elastic<R><<<blocks_for(N, 256), 256, 0, stream>>>(p, resv, L.vert_rigid, N, hR);
     CU(cudaGetLastError());
@@ -1099,6 +1129,10 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
       if (!capturing) CHECK(w.lamB.ensure(sizeof(double) * ls.n_bnd));
       else if (w.lamB.bytes < sizeof(double) * ls.n_bnd) return set_error(MLX_ERR_ARGUMENT, "boundary buffer not reserved");
       CU(cudaMemsetAsync(w.lamB.p, 0, sizeof(double) * ls.n_bnd, stream));
+      if (&w == &sim_work && col == ws.col && layer == 0 && ws.mode) {
+        CHECK(ws_after_lamb_reset(w));
+        ++st.launches;
+      }
     }
     const int* dlist = dint + ls.o_list;
     const bool bodyWork = (ls.nb > 0 && (L.any_boundary || (P->use_rigid_contacts && L.any_rigid_contact))) ||
@@ -1731,6 +1765,8 @@ int Solver<R>::sim_setup(const mlx_layer_desc* ld, const mlx_solve_params* P, co
   CHECK(d_stage.ensure(sizeof(double) * (2 * n3 + np)));
   double* hs = h_stage.as<double>();
   std::memcpy(hs, p0, sizeof(double) * n3);
+  sim_p0.assign(p0, p0 + n3);
+  ws.reset();
   if (v0) std::memcpy(hs + n3, v0, sizeof(double) * n3);
   else std::memset(hs + n3, 0, sizeof(double) * n3);
   for (size_t i = 0; i < np; ++i) hs[2 * n3 + i] = p0[pinned[i]];
@@ -1956,6 +1992,152 @@ int Solver<R>::sim_monitor(double* ra, int cap, int32_t* len, int32_t* total_it,
 }
 
 template <typename R>
+int Solver<R>::ws_after_make_rigids(const LayerWork& w) {
+  const int nb = ws.nb;
+  k_ws_own<R><<<nb, 256, 0, stream>>>(ws.S, w.bodies.as<Body>(), pos(), ws.d_own.as<float>(), ws.d_rec.as<double>());
+  const float* nrm = ws.d_norm.as<float>();
+  const float* om = nrm + 2 * kWsFeat;
+  const float* os = om + kWsOut;
+  k_ws_features<<<blocks_for(nb, 128), 128, 0, stream>>>(ws.S, ws.d_own.as<float>(), nrm, nrm + kWsFeat,
+                                                         ws.d_raw.as<float>(),
+                                                         ws.mode == 1 ? ws.d_feat.as<float>() : nullptr);
+  CU(cudaGetLastError());
+  if (ws.mode == 0) return MLX_OK;
+  if (ws.mode == 1) {
+    CHECK(mlp_forward_on_stream(ws.net, ws.d_feat.as<float>(), nb, stream, &ws.y, &ws.ld));
+  } else {
+    ws.y = ws.d_corr.as<float>();
+    ws.ld = kWsOut;
+  }
+  k_ws_apply_velocity<<<blocks_for(nb, 128), 128, 0, stream>>>(nb, w.bodies.as<Body>(), ws.y, ws.ld, om, os);
+  CU(cudaGetLastError());
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::ws_after_lamb_reset(const LayerWork& w) {
+  const float* om = ws.d_norm.as<float>() + 2 * kWsFeat;
+  k_ws_apply_lambda<<<ws.nb, 128, 0, stream>>>(ws.S, w.lamB.as<double>(), ws.y, ws.ld, om, om + kWsOut);
+  CU(cudaGetLastError());
+  return MLX_OK;
+}
+
+// Sets up the warm start on the first layer of the resident stepper (its
+// rigid clusters): rest data and nearest neighbours of the clusters, the
+// normalisation of features (mean, std: 44 each) and outputs (7 each), the
+// perceptron (mode 1) or fixed corrections (mode 2, clusters x 7 in output
+// units), and whether every step keeps its features and targets.
+template <typename R>
+int Solver<R>::ws_configure(int record, int mode, mlx_mlp* net, const float* fmean, const float* fstd,
+                            const float* omean, const float* ostd, const float* corrections, int32_t* nb_out) {
+  if (!sim.ready) return set_error(MLX_ERR_ARGUMENT, "mlx_sim_init first");
+  if (mode < 0 || mode > 2) return set_error(MLX_ERR_ARGUMENT, "warm start mode must be 0, 1 or 2");
+  DeviceGuard g(device);
+  const int col = sim.ld.num_layers > 0 ? sim.ld.layers_map[0] - 1 : -1;
+  if (col < 0 || sim_work.cache.size() <= (size_t)col || sim_work.cache[col]->nb == 0)
+    return set_error(MLX_ERR_ARGUMENT, "the first layer has no rigid clusters to warm-start");
+  LayerStatic& ls = *sim_work.cache[col];
+  const int nb = ls.nb;
+  if (mode == 1) {
+    int ni = 0, no = 0, mb = 0;
+    CHECK(mlp_dims(net, &ni, &no, &mb));
+    if (ni != kWsFeat || no != kWsOut || mb < nb)
+      return set_error(MLX_ERR_ARGUMENT, "the perceptron must map 44 features to 7 outputs for every cluster");
+    if (!fmean || !fstd || !omean || !ostd) return set_error(MLX_ERR_ARGUMENT, "normalisation arrays are NULL");
+  }
+  if (mode == 2 && !corrections) return set_error(MLX_ERR_ARGUMENT, "corrections are NULL");
+  ws.reset();
+  // rest positions and per-cluster rest data
+  std::vector<double4> rest(N);
+  for (int v = 0; v < N; ++v) rest[v] = make_double4(sim_p0[3 * v], sim_p0[3 * v + 1], sim_p0[3 * v + 2], 0);
+  CHECK(ws.d_rest.ensure(sizeof(double4) * N));
+  CU(cudaMemcpyAsync(ws.d_rest.p, rest.data(), sizeof(double4) * N, cudaMemcpyHostToDevice, stream));
+  // d_static: nbr int[nb*4] | rest_com[nb*3] | rest_cinv[nb*9] | mass[nb]
+  const size_t o_com = ((size_t)nb * kWsNbr * sizeof(int) + 15) / 16 * 16;
+  const size_t o_cinv = o_com + sizeof(double) * 3 * nb, o_mass = o_cinv + sizeof(double) * 9 * nb;
+  CHECK(ws.d_static.ensure(o_mass + sizeof(double) * nb));
+  char* base = static_cast<char*>(ws.d_static.p);
+  const int* dint = ls.dev.as<int>();
+  WsStatic S{};
+  S.nb = nb;
+  S.body_vert_off = dint + ls.o_bvo;
+  S.body_verts = dint + ls.o_bv;
+  S.bnd_off = dint + ls.o_bo;
+  S.nbr = reinterpret_cast<const int*>(base);
+  S.rest_com = reinterpret_cast<const double*>(base + o_com);
+  S.rest_cinv = reinterpret_cast<const double*>(base + o_cinv);
+  S.mass = reinterpret_cast<const double*>(base + o_mass);
+  S.rest = ws.d_rest.as<double4>();
+  S.vmass = d_vmass.as<double>();
+  k_ws_rest<<<nb, 256, 0, stream>>>(S, reinterpret_cast<double*>(base + o_com),
+                                    reinterpret_cast<double*>(base + o_cinv), reinterpret_cast<double*>(base + o_mass));
+  CU(cudaGetLastError());
+  std::vector<double> com(3 * (size_t)nb);
+  CU(cudaMemcpyAsync(com.data(), base + o_com, sizeof(double) * 3 * nb, cudaMemcpyDeviceToHost, stream));
+  CU(cudaStreamSynchronize(stream));
+  // the kWsNbr clusters nearest at rest (ties: lower index)
+  std::vector<int> nbr((size_t)nb * kWsNbr, -1);
+  std::vector<std::pair<double, int>> d;
+  for (int b = 0; b < nb; ++b) {
+    d.clear();
+    for (int c = 0; c < nb; ++c) {
+      if (c == b) continue;
+      const double dx = com[3 * c] - com[3 * b], dy = com[3 * c + 1] - com[3 * b + 1], dz = com[3 * c + 2] - com[3 * b + 2];
+      d.emplace_back(dx * dx + dy * dy + dz * dz, c);
+    }
+    const size_t k = std::min<size_t>(kWsNbr, d.size());
+    std::partial_sort(d.begin(), d.begin() + k, d.end());
+    for (size_t q = 0; q < k; ++q) nbr[(size_t)b * kWsNbr + q] = d[q].second;
+  }
+  CU(cudaMemcpyAsync(base, nbr.data(), sizeof(int) * nbr.size(), cudaMemcpyHostToDevice, stream));
+  // normalisation: fmean | fstd | omean | ostd (identity when not given)
+  std::vector<float> nrm(2 * kWsFeat + 2 * kWsOut);
+  for (int i = 0; i < kWsFeat; ++i) {
+    nrm[i] = fmean ? fmean[i] : 0.f;
+    nrm[kWsFeat + i] = fstd ? fstd[i] : 1.f;
+  }
+  for (int i = 0; i < kWsOut; ++i) {
+    nrm[2 * kWsFeat + i] = (mode == 1 && omean) ? omean[i] : 0.f;
+    nrm[2 * kWsFeat + kWsOut + i] = (mode == 1 && ostd) ? ostd[i] : 1.f;
+  }
+  CHECK(ws.d_norm.ensure(sizeof(float) * nrm.size()));
+  CU(cudaMemcpyAsync(ws.d_norm.p, nrm.data(), sizeof(float) * nrm.size(), cudaMemcpyHostToDevice, stream));
+  CHECK(ws.d_own.ensure(sizeof(float) * kWsOwn * nb));
+  CHECK(ws.d_raw.ensure(sizeof(float) * kWsFeat * nb));
+  CHECK(ws.d_feat.ensure(sizeof(float) * kWsFeat * nb));
+  CHECK(ws.d_rec.ensure(sizeof(double) * kWsRec * nb));
+  CHECK(ws.d_target.ensure(sizeof(float) * kWsOut * nb));
+  CHECK(ws.d_corr.ensure(sizeof(float) * kWsOut * nb));
+  CU(cudaMemsetAsync(ws.d_target.p, 0, sizeof(float) * kWsOut * nb, stream));
+  if (mode == 2)
+    CU(cudaMemcpyAsync(ws.d_corr.p, corrections, sizeof(float) * kWsOut * nb, cudaMemcpyHostToDevice, stream));
+  CU(cudaStreamSynchronize(stream));
+  ws.S = S;
+  ws.record = record;
+  ws.mode = mode;
+  ws.net = net;
+  ws.col = col;
+  ws.nb = nb;
+  if (sim.graph) { cudaGraphExecDestroy(sim.graph); sim.graph = nullptr; }
+  if (nb_out) *nb_out = nb;
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::ws_fetch(float* features, float* targets, int cap, int32_t* nb) {
+  if (ws.nb == 0) return set_error(MLX_ERR_ARGUMENT, "warm start not configured");
+  if (nb) *nb = ws.nb;
+  if (cap < ws.nb) return set_error(MLX_ERR_LIMIT, "capacity below the number of clusters");
+  DeviceGuard g(device);
+  if (features)
+    CU(cudaMemcpyAsync(features, ws.d_raw.p, sizeof(float) * kWsFeat * ws.nb, cudaMemcpyDeviceToHost, stream));
+  if (targets)
+    CU(cudaMemcpyAsync(targets, ws.d_target.p, sizeof(float) * kWsOut * ws.nb, cudaMemcpyDeviceToHost, stream));
+  CU(cudaStreamSynchronize(stream));
+  return MLX_OK;
+}
+
+template <typename R>
 int Solver<R>::sim_contact_count(int32_t* n) {
   if (!n) return set_error(MLX_ERR_ARGUMENT, "null argument");
   *n = 0;
@@ -2112,6 +2294,12 @@ int Solver<R>::sim_issue_step(long long* launches, bool capturing) {
     st.launches += 4;
   }
   CHECK(run_layers(&sim.ld, &sim.P, nullptr, cd, st, capturing, sim_work, dc));
+  if (ws.nb > 0 && ws.record) {
+    k_ws_targets<R><<<ws.nb, 256, 0, stream>>>(ws.S, p, d_oldp.as<R4<R>>(), ws.d_rec.as<double>(),
+                                                sim_work.lamB.as<double>(), h, ws.d_target.as<float>());
+    CU(cudaGetLastError());
+    ++st.launches;
+  }
   if (sim.P.compute_residuals) {
     sim_last.valid = true;
     sim_last.device = devmon;
@@ -2366,6 +2554,17 @@ int mlx_sim_monitor(mlx_solver* s, double* residuals, int32_t capacity, int32_t*
                     double* run_until, int32_t* status) {
   if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
   return s->impl->sim_monitor(residuals, capacity, len, total_iterations, run_until, status);
+}
+int mlx_sim_warm_start(mlx_solver* s, int32_t record, int32_t mode, mlx_mlp* net, const float* feature_mean,
+                       const float* feature_std, const float* output_mean, const float* output_std,
+                       const float* corrections, int32_t* num_clusters) {
+  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+  return s->impl->ws_configure(record, mode, net, feature_mean, feature_std, output_mean, output_std, corrections,
+                               num_clusters);
+}
+int mlx_sim_warm_start_fetch(mlx_solver* s, float* features, float* targets, int32_t capacity, int32_t* num_clusters) {
+  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+  return s->impl->ws_fetch(features, targets, capacity, num_clusters);
 }
 int mlx_sim_contact_count(mlx_solver* s, int32_t* n) {
   if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");

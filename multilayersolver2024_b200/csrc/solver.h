@@ -2,6 +2,7 @@
 // solver implementations.
 #pragma once
 
+#include <cuda_runtime.h>
 #include <string>
 #include "../../include/mlxpbd.h"
 
@@ -31,8 +32,14 @@ struct SolverBase {
   virtual int sim_contact_count(int32_t* n) = 0;
   virtual int sim_monitor(double* ra, int cap, int32_t* len, int32_t* total_it, double* run_until,
                           int32_t* status) = 0;
+  virtual int ws_configure(int record, int mode, mlx_mlp* net, const float* fmean, const float* fstd,
+                           const float* omean, const float* ostd, const float* corrections, int32_t* nb) = 0;
+  virtual int ws_fetch(float* features, float* targets, int cap, int32_t* nb) = 0;
 };
 
 SolverBase* make_solver(const mlx_mesh_desc* md, int* rc);
+
+int mlp_forward_on_stream(mlx_mlp* m, const float* d_x, int batch, cudaStream_t s, const float** y, int* ld);
+int mlp_dims(const mlx_mlp* m, int* n_in, int* n_out, int* max_batch);
 
 }  // namespace mlx

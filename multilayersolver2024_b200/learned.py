@@ -71,3 +71,46 @@ class Mlp:
             self.close()
         except Exception:
             pass
+
+
+def collect_warm_start_data(sim, steps, graph=True):
+    """Runs `steps` resident steps with recording on (plain solve, mode 0) and
+    returns the stacked features (rows x 44), targets (rows x 7) and the
+    projectGS iterations of every step (when the step monitors residuals)."""
+    sim.warm_start(record=True, mode=0)
+    feats, tgts, iters = [], [], []
+    for _ in range(steps):
+        sim.step(1, graph=graph)
+        f, t = sim.warm_start_records()
+        feats.append(f)
+        tgts.append(t)
+        try:
+            iters.append(sim.monitor()[1])
+        except Exception:
+            iters.append(None)
+    return np.concatenate(feats), np.concatenate(tgts), iters
+
+
+def normalisation(a, floor=1e-6):
+    a = np.asarray(a, np.float64)
+    return a.mean(0).astype(np.float32), np.maximum(a.std(0), floor).astype(np.float32)
+
+
+def fit_warm_start(features, targets, epochs=200, lr=2e-3, batch=None, seed=0, hidden=128, layers=3, max_batch=4096):
+    """Trains the warm-start perceptron (44 -> 7) on normalised features and
+    targets with the library's tensor-core kernels.  Returns the network, the
+    feature and output normalisations and the per-epoch losses."""
+    fn, on = normalisation(features), normalisation(targets)
+    x = (features - fn[0]) / fn[1]
+    y = (targets - on[0]) / on[1]
+    n = x.shape[0]
+    b = batch or min(max(128, n // 8 // 128 * 128), max_batch)
+    b = min(b, n)
+    net = Mlp(44, 7, n_hidden=hidden, n_hidden_layers=layers, max_batch=max(max_batch, b), seed=seed)
+    losses = net.train(x, y, batch=b, epochs=epochs, lr=lr, seed=seed)
+    return net, fn, on, losses
+
+
+def predict(net, fn, on, features):
+    """Denormalised outputs of the warm-start network."""
+    return net.forward((features - fn[0]) / fn[1]) * on[1] + on[0]

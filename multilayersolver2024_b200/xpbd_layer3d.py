@@ -205,6 +205,37 @@ class ResidentSim:
                                                             C.byref(it), C.byref(ru), C.byref(st)), self._lib)
         return ra[:min(n.value, capacity)].copy(), it.value, ru.value, st.value
 
+    def warm_start(self, record=False, mode=0, net=None, feature_norm=None, output_norm=None, corrections=None):
+        """Learned warm start (``mlx_sim_warm_start``): mode 0 off, 1 the
+        perceptron ``net`` with feature / output normalisation ((mean, std)
+        pairs of 44 and 7 values), 2 fixed ``corrections`` (clusters x 7).
+        ``record`` keeps every step's features and targets.  Returns the
+        number of clusters."""
+        from ._lib import f32
+        fm, fs = (None, None) if feature_norm is None else (np.ascontiguousarray(feature_norm[0], np.float32),
+                                                          np.ascontiguousarray(feature_norm[1], np.float32))
+        om, osd = (None, None) if output_norm is None else (np.ascontiguousarray(output_norm[0], np.float32),
+                                                           np.ascontiguousarray(output_norm[1], np.float32))
+        corr = None if corrections is None else np.ascontiguousarray(corrections, np.float32)
+        self._ws_keep = (net, fm, fs, om, osd, corr)
+        nb = C.c_int32(0)
+        check("mlx_sim_warm_start", self._lib.mlx_sim_warm_start(
+            self.solver.handle, int(bool(record)), int(mode), net.handle if net is not None else None, f32(fm),
+            f32(fs), f32(om), f32(osd), f32(corr), C.byref(nb)), self._lib)
+        self._ws_nb = nb.value
+        return nb.value
+
+    def warm_start_records(self):
+        """Features (clusters x 44) and targets (clusters x 7) of the last step."""
+        from ._lib import f32
+        nb = self._ws_nb
+        feat = np.zeros((nb, 44), np.float32)
+        tgt = np.zeros((nb, 7), np.float32)
+        n = C.c_int32(0)
+        check("mlx_sim_warm_start_fetch", self._lib.mlx_sim_warm_start_fetch(self.solver.handle, f32(feat), f32(tgt),
+                                                                              nb, C.byref(n)), self._lib)
+        return feat, tgt
+
     def contact_count(self):
         """Contact vertices of the last step."""
         n = C.c_int32(0)

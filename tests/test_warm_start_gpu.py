@@ -1,0 +1,136 @@
+"""The learned warm start of the coarse (rigid-cluster) layer.
+
+  * features and targets: the rotation vector of every cluster's deformation
+    (FP64 polar decomposition on the device) and the velocity targets
+    (Kabsch fit of the converged step) against a numpy restatement that uses
+    an SVD for the polar factor (rtol 1e-4 in FP32 storage);
+  * mode 2 with zero corrections is bit-identical to the plain solve;
+  * the network, trained by the library's tensor-core kernels on records of
+    the solver itself, predicts held-out targets better than the plain solve's
+    implicit prediction (no correction), and a warm-started run reaches the
+    same residual with positions within 1e-3 of the bounding-box diagonal of
+    the plain run.
+"""
+import numpy as np
+import pytest
+
+from multilayersolver2024_b200 import _lib, scenes
+from multilayersolver2024_b200.learned import collect_warm_start_data, fit_warm_start, predict
+from multilayersolver2024_b200.mesh3d import Mesh3D, to_lame
+from multilayersolver2024_b200.xpbd_layer3d import ResidentSim, Solver, XpbdLayer3D, find_boundary_vertices
+
+pytestmark = pytest.mark.gpu
+
+
+def _scene(seed=5, dims=(16, 4, 4), cluster=2):
+    rng = np.random.default_rng(seed)
+    V, T, cube = scenes.generate_beam(*dims, 0.1)
+    E = np.exp(rng.uniform(np.log(1e4), np.log(1e6), T.shape[0]))
+    m = Mesh3D.from_arrays(V, T, *to_lame(0.35, E), energy_type=_lib.MLX_ENERGY_NEOHOOKEAN)
+    m.pin(np.nonzero(np.isclose(V[:, 0], 0.0))[0] + 1)
+    forced = np.zeros(m.T, bool)
+    forced[m.pinnedTets - 1] = True
+    coarse = scenes.cluster_rigid_sets(cube, dims, cluster, forced)
+    sets = np.asfortranarray(np.stack([np.zeros(m.T, np.int32), coarse], 1))
+    v0 = np.zeros_like(m.p)
+    v0[2::3] = -1.5 * V[:, 0] / V[:, 0].max()
+    return m, sets, v0
+
+
+def _sim(m, sets, v0, residuals=True, h=1.0 / 60.0):
+    it = XpbdLayer3D()
+    it.setLayers([50, 0])
+    it.iterations = [3, 6]
+    it.customRigidSets = sets
+    it.precision = _lib.MLX_FP32
+    it.computeResiduals = residuals
+    it.runUntilResSmallerThan = 1e-4 if residuals else -1.0
+    it.hangingStop = 3000
+    ls = find_boundary_vertices(m, sets, [0, int(sets[:, 1].max())])
+    s = Solver(m, precision=_lib.MLX_FP32, material="lame")
+    return ResidentSim(s, it, ls, h, p0=m.p, v0=v0), ls
+
+
+def _polar(F):
+    U, _, Vt = np.linalg.svd(F)
+    R = U @ Vt
+    if np.linalg.det(R) < 0:
+        U[:, -1] *= -1
+        R = U @ Vt
+    return R
+
+
+def _log(R):
+    th = np.arccos(np.clip(0.5 * (np.trace(R) - 1), -1, 1))
+    v = np.array([R[2, 1] - R[1, 2], R[0, 2] - R[2, 0], R[1, 0] - R[0, 1]])
+    return v * (0.5 if th < 1e-6 else 0.5 * th / np.sin(th))
+
+
+def test_features_and_targets_match_numpy(gpu):
+    m, sets, v0 = _scene()
+    h = 1.0 / 60.0
+    sim, ls = _sim(m, sets, v0, residuals=False, h=h)
+    sim.warm_start(record=True, mode=0)
+    mass = m.mass[0::3]
+    body = ls.vertexRigidBody[:, 1]
+    X = m.p.reshape(-1, 3)
+    checked = 0
+    for step in range(3):
+        x0 = sim.state()[0].reshape(-1, 3)
+        sim.step(1, graph=True)
+        x1 = sim.state()[0].reshape(-1, 3)
+        feat, tgt = sim.warm_start_records()
+        for b in range(0, feat.shape[0], 3):
+            ids = np.nonzero(body == b + 1)[0]
+            w = mass[ids][:, None]
+            C = (w * X[ids]).sum(0) / w.sum()
+            c0 = (w * x0[ids]).sum(0) / w.sum()
+            # own features: displacement and the rotation of the deformation from rest
+            np.testing.assert_allclose(feat[b, 6:9], c0 - C, rtol=1e-3, atol=1e-6)
+            A = ((x0[ids] - c0) * w).T @ (X[ids] - C)
+            F = A @ np.linalg.inv(((X[ids] - C) * w).T @ (X[ids] - C))
+            np.testing.assert_allclose(feat[b, 9:12], _log(_polar(F)), rtol=1e-3, atol=2e-5)
+            # targets: Kabsch fit of the step, as velocity corrections
+            c1 = (w * x1[ids]).sum(0) / w.sum()
+            R = _polar(((x1[ids] - c1) * w).T @ (x0[ids] - c0))
+            np.testing.assert_allclose(tgt[b, 0:3], (c1 - c0) / h - feat[b, 0:3], rtol=1e-3, atol=1e-4)
+            np.testing.assert_allclose(tgt[b, 3:6], _log(R) / h - feat[b, 3:6], rtol=1e-3, atol=2e-3)
+            checked += 1
+    assert checked > 10
+
+
+def test_zero_corrections_are_the_plain_solve(gpu):
+    m, sets, v0 = _scene()
+    a, _ = _sim(m, sets, v0, residuals=False)
+    b, _ = _sim(m, sets, v0, residuals=False)
+    nb = a.warm_start(record=False, mode=0)
+    b.warm_start(record=False, mode=2, corrections=np.zeros((nb, 7), np.float32))
+    for _ in range(3):
+        a.step(1, graph=True)
+        b.step(1, graph=True)
+        np.testing.assert_array_equal(a.state()[0], b.state()[0])
+
+
+def test_trained_network_beats_no_correction(gpu):
+    m, sets, v0 = _scene()
+    train, _ = _sim(m, sets, v0)
+    f, t, plain_iters = collect_warm_start_data(train, 40)
+    nb = f.shape[0] // 40
+    ftr, ttr, fte, tte = f[:30 * nb], t[:30 * nb], f[30 * nb:], t[30 * nb:]
+    net, fn, on, losses = fit_warm_start(ftr, ttr, epochs=300, lr=2e-3, batch=128)
+    assert losses[-1] < losses[0]
+    pred = predict(net, fn, on, fte)
+    mse_net = ((pred[:, :6] - tte[:, :6]) ** 2).mean()
+    mse_zero = (tte[:, :6] ** 2).mean()
+    assert mse_net < 0.7 * mse_zero, (mse_net, mse_zero)
+    # warm-started run: same residual target, positions close to the plain run
+    plain, _ = _sim(m, sets, v0)
+    warm, _ = _sim(m, sets, v0)
+    warm.warm_start(record=False, mode=1, net=net, feature_norm=fn, output_norm=on)
+    d = m.bbox_diagonal()
+    for _ in range(5):
+        plain.step(1, graph=True)
+        warm.step(1, graph=True)
+        ra, _, _, status = warm.monitor()
+        assert status == 0 and abs(ra[-1]) <= 1e-4
+        assert np.abs(warm.state()[0] - plain.state()[0]).max() / d <= 1e-3
