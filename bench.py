@@ -267,27 +267,60 @@ def run_ours(args, rank, world, local):
     # monitor and stop rules on the device (conditional graph nodes) ----
     to_res = None
     if not args.no_residual_leg:
-        sc3 = make_scene()
-        m3 = sc3.mesh
-        integ3 = make_integrator(sc3, MLX_FP32)
-        integ3.computeResiduals = True
-        integ3.runUntilResSmallerThan = 1e-4
-        integ3.hangingStop = args.residual_cap
-        solver3 = Solver(m3, precision=MLX_FP32, device=local, material="lame")
-        sim3 = ResidentSim(solver3, integ3, ls, sc3.h, p0=m3.p, v0=np.zeros_like(m3.p))
-        sim3.add_velocity(sc3.impulse[0], sc3.impulse[1])
-        iters, ms_steps, finals, reached = [], [], [], []
-        for _ in range(args.residual_steps):
-            ms_steps.append(sim3.step(1, graph=True, timed=True))
-            ra, it_total, _, status = sim3.monitor()
-            iters.append(int(it_total))
-            finals.append(float(ra[-1]))
-            reached.append(bool(abs(ra[-1]) <= 1e-4))
-        solver3.close()
+        from multilayersolver2024_b200 import scenes as _scenes
+        from multilayersolver2024_b200.learned import collect_warm_start_data, fit_warm_start
+
+        def residual_sim(scene):
+            integ3 = make_integrator(scene, MLX_FP32)
+            integ3.computeResiduals = True
+            integ3.runUntilResSmallerThan = 1e-4
+            integ3.hangingStop = args.residual_cap
+            sets3 = scene.custom_sets
+            ls3 = find_boundary_vertices(scene.mesh, sets3,
+                                         [int(sets3[:, c].max(initial=0)) for c in range(sets3.shape[1])])
+            solver3 = Solver(scene.mesh, precision=MLX_FP32, device=local, material="lame")
+            sim3 = ResidentSim(solver3, integ3, ls3, scene.h, p0=scene.mesh.p, v0=np.zeros_like(scene.mesh.p))
+            sim3.add_velocity(scene.impulse[0], scene.impulse[1])
+            return solver3, sim3
+
+        def run_leg(sim3, n):
+            iters, ms_steps, finals = [], [], []
+            for _ in range(n):
+                ms_steps.append(sim3.step(1, graph=True, timed=True))
+                ra, it_total, _, status = sim3.monitor()
+                iters.append(int(it_total))
+                finals.append(float(ra[-1]))
+            return {"iterations_per_step": iters, "ms_per_step": ms_steps,
+                    "steps_per_s": len(ms_steps) / (sum(ms_steps) / 1000.0), "final_residual": finals,
+                    "reached": [bool(abs(r) <= 1e-4) for r in finals]}
+
+        solver_p, sim_p = residual_sim(make_scene())
+        plain_leg = run_leg(sim_p, args.residual_steps)
+        p_plain = sim_p.state()[0]
+        solver_p.close()
+        learned_leg = None
+        if CONFIG == 2 and args.learned_train_steps > 0:
+            # the warm start's network is trained on another seed of the same
+            # scene class, then steps the benchmark scene
+            solver_t, sim_t = residual_sim(_scenes.config2(seed=3))
+            ftr, ttr, _ = collect_warm_start_data(sim_t, args.learned_train_steps)
+            solver_t.close()
+            t0 = time.perf_counter()
+            net, fn, on, losses = fit_warm_start(ftr, ttr, epochs=300, lr=2e-3, batch=128)
+            train_s = time.perf_counter() - t0
+            solver_w, sim_w = residual_sim(make_scene())
+            sim_w.warm_start(record=False, mode=1, net=net, feature_norm=fn, output_norm=on)
+            learned_leg = run_leg(sim_w, args.residual_steps)
+            learned_leg.update({
+                "training": {"samples": int(ftr.shape[0]), "steps_recorded": args.learned_train_steps,
+                             "scene": "config2 seed 3", "epochs": 300, "seconds": train_s,
+                             "loss_first_last": [float(losses[0]), float(losses[-1])]},
+                "max_position_deviation_from_plain": float(np.abs(sim_w.state()[0] - p_plain).max()
+                                                           / make_scene().mesh.bbox_diagonal())})
+            solver_w.close()
+            net.close()
         to_res = {"run_until": 1e-4, "hanging_stop": args.residual_cap, "steps": args.residual_steps,
-                  "iterations_per_step": iters, "ms_per_step": ms_steps,
-                  "steps_per_s": len(ms_steps) / (sum(ms_steps) / 1000.0), "final_residual": finals,
-                  "reached": reached,
+                  **plain_leg, "learned_warm_start": learned_leg,
                   "monitor": "device (layers as conditional IF nodes, projectGS as conditional WHILE nodes)"}
 
     line = None
@@ -365,7 +398,9 @@ def main():
                     "(on by default for config 3)")
     ap.add_argument("--no-autotune", action="store_true", help="never run the autotuner (profiling runs)")
     ap.add_argument("--no-residual-leg", action="store_true", help="skip the iterations-to-residual-1e-4 leg")
-    ap.add_argument("--residual-steps", type=int, default=2)
+    ap.add_argument("--residual-steps", type=int, default=4)
+    ap.add_argument("--learned-train-steps", type=int, default=16,
+                    help="recorded steps (another seed) the warm-start network is trained on; 0 skips that leg")
     ap.add_argument("--residual-cap", type=int, default=15000,
                     help="hangingStop of the residual leg (bounds the iterations of a step)")
     args = ap.parse_args()
