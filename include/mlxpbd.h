@@ -287,6 +287,19 @@ int mlx_sim_monitor(mlx_solver* solver, double* residuals, int32_t capacity, int
 /* Number of contacts of the last resident step (reads one int from the device). */
 int mlx_sim_contact_count(mlx_solver* solver, int32_t* num_contact_vertices);
 
+/* ---- preconditioned conjugate gradients ---------------------------------
+ * solvePCG(iterations, Afun, b, zeros, preconditioner)
+ * (2d/tools/solver/solvePCG.m:1-56) on the device for the linearly implicit
+ * system of the mesh, A = M + h^2 K0: lumped masses and the linear-elasticity
+ * stiffness at the rest shape from each tet's DmInv, volume, mu and lambda
+ * (the system quickSolve3D.m:170 hands to solvePCG, without damping, at the
+ * rest tangent), restricted to the unpinned DOFs; preconditioner: the 3x3
+ * block-Jacobi inverse of A.  b and x are 3N (pinned components of x are 0);
+ * resvec (optional, `iterations` values) receives ||A x - b|| after every
+ * iteration, as solvePCG's second output.  Needs mu and lambda in the mesh
+ * description. */
+int mlx_pcg_solve(mlx_solver* solver, double h, const double* b, int32_t iterations, double* x, double* resvec);
+
 /* ---- learned warm start: the perceptron ----------------------------------
  * No counterpart in the reference.  n_in -> n_hidden (GELU) x
  * n_hidden_layers -> n_out, BF16 weights and activations with FP32

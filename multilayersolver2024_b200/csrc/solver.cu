@@ -20,6 +20,7 @@
 #include "monitor.cuh"
 #include "partition.h"
 #include "warmstart.cuh"
+#include "pcg.cuh"
 #include "solver.h"
 
 #include <algorithm>
@@ -328,6 +329,13 @@ struct Solver final : SolverBase {
     int total_it = 0;
   } sim_last;
   WarmStartState ws;
+  // PCG on the linearly implicit system (pcg.cuh); host copies of the
+  // material kept from create (sorted order), device data built on first use
+  std::vector<double> pcg_G, pcg_vol, pcg_lame;
+  bool pcg_ready = false;
+  DevBuf d_pcg_G, d_pcg_vol, d_pcg_lame, d_pcg_vt, d_pcg_pin, d_pcg_vec, d_pcg_P, d_pcg_part, d_pcg_sc, d_pcg_res;
+  int pcg_setup();
+  int pcg_solve(double h, const double* b, int iterations, double* x, double* resvec) override;
   std::vector<double> sim_p0;  // positions given to mlx_sim_init (the rest configuration)
   int ws_configure(int record, int mode, mlx_mlp* net, const float* fmean, const float* fstd, const float* omean,
                    const float* ostd, const float* corrections, int32_t* nb) override;
@@ -613,6 +621,18 @@ int Solver<R>::create(const mlx_mesh_desc* md) {
     CU(cudaMemcpyAsync(d_pin_dofs.p, pinned.data(), sizeof(int) * pinned.size(), cudaMemcpyHostToDevice, stream));
   vid_sorted = vid;
   if (cluster_ok) vowner = mp.vowner;
+  if (md->mu && md->lambda) {
+    pcg_G.resize(9 * (size_t)T);
+    pcg_vol.resize(T);
+    pcg_lame.resize(2 * (size_t)T);
+    for (int sidx = 0; sidx < T; ++sidx) {
+      const int e = s2e[sidx];
+      for (int j = 0; j < 9; ++j) pcg_G[9 * (size_t)sidx + j] = md->DmInv[9 * (size_t)e + j];
+      pcg_vol[sidx] = md->volume[e];
+      pcg_lame[2 * (size_t)sidx] = md->mu[e];
+      pcg_lame[2 * (size_t)sidx + 1] = md->lambda[e];
+    }
+  }
   CU(cudaStreamSynchronize(stream));
   return MLX_OK;
 }
@@ -2138,6 +2158,116 @@ int Solver<R>::ws_fetch(float* features, float* targets, int cap, int32_t* nb) {
 }
 
 template <typename R>
+int Solver<R>::pcg_setup() {
+  if (pcg_ready) return MLX_OK;
+  if (pcg_vol.empty()) return set_error(MLX_ERR_UNSUPPORTED, "the PCG system needs mu and lambda in the mesh description");
+  std::vector<int> off(N + 1, 0);
+  for (int sidx = 0; sidx < T; ++sidx) {
+    const int4 q = vid_sorted[sidx];
+    for (int v : {q.x, q.y, q.z, q.w}) ++off[v + 1];
+  }
+  for (int v = 0; v < N; ++v) off[v + 1] += off[v];
+  std::vector<int2> vt(off[N]);
+  {
+    std::vector<int> f(off.begin(), off.end() - 1);
+    for (int sidx = 0; sidx < T; ++sidx) {
+      const int4 q = vid_sorted[sidx];
+      const int vv[4] = {q.x, q.y, q.z, q.w};
+      for (int k = 0; k < 4; ++k) vt[f[vv[k]]++] = make_int2(sidx, k);
+    }
+  }
+  std::vector<unsigned char> pm(N, 0);
+  for (int d : pinned) pm[d / 3] |= (unsigned char)(1u << (d % 3));
+  CHECK(d_pcg_G.ensure(sizeof(double) * pcg_G.size()));
+  CHECK(d_pcg_vol.ensure(sizeof(double) * T));
+  CHECK(d_pcg_lame.ensure(sizeof(double) * 2 * (size_t)T));
+  CHECK(d_pcg_vt.ensure(sizeof(int) * (N + 1) + sizeof(int2) * vt.size()));
+  CHECK(d_pcg_pin.ensure(N));
+  CU(cudaMemcpyAsync(d_pcg_G.p, pcg_G.data(), sizeof(double) * pcg_G.size(), cudaMemcpyHostToDevice, stream));
+  CU(cudaMemcpyAsync(d_pcg_vol.p, pcg_vol.data(), sizeof(double) * T, cudaMemcpyHostToDevice, stream));
+  CU(cudaMemcpyAsync(d_pcg_lame.p, pcg_lame.data(), sizeof(double) * 2 * (size_t)T, cudaMemcpyHostToDevice, stream));
+  // CSR: vt pairs first (8-byte aligned), then the offsets
+  CU(cudaMemcpyAsync(d_pcg_vt.p, vt.data(), sizeof(int2) * vt.size(), cudaMemcpyHostToDevice, stream));
+  CU(cudaMemcpyAsync(static_cast<char*>(d_pcg_vt.p) + sizeof(int2) * vt.size(), off.data(), sizeof(int) * (N + 1),
+                     cudaMemcpyHostToDevice, stream));
+  CU(cudaMemcpyAsync(d_pcg_pin.p, pm.data(), N, cudaMemcpyHostToDevice, stream));
+  CHECK(d_pcg_vec.ensure(sizeof(double4) * 7 * (size_t)N));
+  CHECK(d_pcg_P.ensure(sizeof(double) * 9 * (size_t)N));
+  CHECK(d_pcg_part.ensure(sizeof(double) * 2 * 296));
+  CHECK(d_pcg_sc.ensure(sizeof(PcgScalars)));
+  CU(cudaStreamSynchronize(stream));
+  pcg_ready = true;
+  return MLX_OK;
+}
+
+// solvePCG (2d/tools/solver/solvePCG.m) with x0 = 0 for A = M + h^2 K0 on
+// the unpinned DOFs and the block-Jacobi preconditioner (pcg.cuh).  The
+// iteration runs as stream work only; alpha and beta stay on the device.
+template <typename R>
+int Solver<R>::pcg_solve(double h, const double* b, int iterations, double* x, double* resvec) {
+  if (!b || !x) return set_error(MLX_ERR_ARGUMENT, "null argument");
+  if (iterations < 0 || !(h > 0)) return set_error(MLX_ERR_ARGUMENT, "need iterations >= 0 and h > 0");
+  DeviceGuard g(device);
+  CHECK(pcg_setup());
+  const size_t npairs = (d_pcg_vt.bytes - sizeof(int) * (N + 1)) / sizeof(int2);
+  PcgOp op;
+  op.N = N;
+  op.vt = d_pcg_vt.as<int2>();
+  op.vt_off = reinterpret_cast<const int*>(static_cast<const char*>(d_pcg_vt.p) + sizeof(int2) * npairs);
+  op.vid = d_vid.as<int4>();
+  op.G = d_pcg_G.as<double>();
+  op.vol = d_pcg_vol.as<double>();
+  op.lame = d_pcg_lame.as<double>();
+  op.vmass = d_vmass.as<double>();
+  op.pin = d_pcg_pin.as<unsigned char>();
+  op.h2 = h * h;
+  double4* V = d_pcg_vec.as<double4>();
+  double4 *db = V, *dx = V + N, *dr = V + 2 * (size_t)N, *dz = V + 3 * (size_t)N, *dd = V + 4 * (size_t)N,
+          *dAp = V + 5 * (size_t)N, *dtmp = V + 6 * (size_t)N;
+  double* P = d_pcg_P.as<double>();
+  double* part = d_pcg_part.as<double>();
+  PcgScalars* sc = d_pcg_sc.as<PcgScalars>();
+  CHECK(d_pcg_res.ensure(sizeof(double) * std::max(iterations, 1)));
+  double* dres = resvec ? d_pcg_res.as<double>() : nullptr;
+  const int nb = blocks_for(N, 256), nred = std::min(nb, 296);
+  CHECK(d_stage.ensure(sizeof(double) * 3 * (size_t)N));
+  CU(cudaMemcpyAsync(d_stage.p, b, sizeof(double) * 3 * (size_t)N, cudaMemcpyHostToDevice, stream));
+  k_load_vec<double><<<nb, 256, 0, stream>>>(d_stage.as<double>(), dtmp, N);
+  k_pcg_mask<<<nb, 256, 0, stream>>>(N, op.pin, dtmp, db);               // b on the unpinned DOFs
+  CU(cudaMemsetAsync(dx, 0, sizeof(double4) * N, stream));               // x = x0 = 0
+  CU(cudaMemcpyAsync(dr, db, sizeof(double4) * N, cudaMemcpyDeviceToDevice, stream));  // r = b - A x0
+  k_pcg_block_jacobi<<<nb, 256, 0, stream>>>(op, P);
+  k_pcg_precond<<<nb, 256, 0, stream>>>(N, P, op.pin, dr, dz);           // z = P r
+  CU(cudaMemcpyAsync(dd, dz, sizeof(double4) * N, cudaMemcpyDeviceToDevice, stream));  // d = z
+  k_pcg_dot2<<<nred, 256, 0, stream>>>(N, dr, dz, nullptr, nullptr, part);
+  k_pcg_scalars<<<1, 256, 0, stream>>>(part, nred, 0, sc, nullptr, 0);    // rTz = r'z
+  for (int i = 0; i < iterations; ++i) {
+    k_pcg_apply<<<nb, 256, 0, stream>>>(op, dd, dAp);                    // Ap = A d
+    k_pcg_dot2<<<nred, 256, 0, stream>>>(N, dd, dAp, nullptr, nullptr, part);
+    k_pcg_scalars<<<1, 256, 0, stream>>>(part, nred, 1, sc, nullptr, 0);  // alpha = rTz / d'Ap
+    k_pcg_step<<<nb, 256, 0, stream>>>(N, sc, dd, dAp, dx, dr);         // x += alpha d, r -= alpha Ap
+    k_pcg_precond<<<nb, 256, 0, stream>>>(N, P, op.pin, dr, dz);         // z = P r
+    k_pcg_dot2<<<nred, 256, 0, stream>>>(N, dr, dz, nullptr, nullptr, part);
+    k_pcg_scalars<<<1, 256, 0, stream>>>(part, nred, 2, sc, nullptr, 0);  // beta, rTz = r'z
+    k_pcg_direction<<<nb, 256, 0, stream>>>(N, sc, dz, dd);              // d = z + beta d
+    if (dres) {                                                          // resvec(i) = ||A x - b||
+      k_pcg_apply<<<nb, 256, 0, stream>>>(op, dx, dAp);
+      k_pcg_sub<<<nb, 256, 0, stream>>>(N, dAp, db, dtmp);
+      k_pcg_dot2<<<nred, 256, 0, stream>>>(N, dtmp, dtmp, nullptr, nullptr, part);
+      k_pcg_scalars<<<1, 256, 0, stream>>>(part, nred, 3, sc, dres, i);
+      // the next iteration's A d overwrites dAp after this use
+    }
+  }
+  CU(cudaGetLastError());
+  k_store_pos<double><<<nb, 256, 0, stream>>>(dx, d_stage.as<double>(), N);
+  CU(cudaMemcpyAsync(x, d_stage.p, sizeof(double) * 3 * (size_t)N, cudaMemcpyDeviceToHost, stream));
+  if (resvec && iterations > 0)
+    CU(cudaMemcpyAsync(resvec, dres, sizeof(double) * iterations, cudaMemcpyDeviceToHost, stream));
+  CU(cudaStreamSynchronize(stream));
+  return MLX_OK;
+}
+
+template <typename R>
 int Solver<R>::sim_contact_count(int32_t* n) {
   if (!n) return set_error(MLX_ERR_ARGUMENT, "null argument");
   *n = 0;
@@ -2565,6 +2695,10 @@ int mlx_sim_warm_start(mlx_solver* s, int32_t record, int32_t mode, mlx_mlp* net
 int mlx_sim_warm_start_fetch(mlx_solver* s, float* features, float* targets, int32_t capacity, int32_t* num_clusters) {
   if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
   return s->impl->ws_fetch(features, targets, capacity, num_clusters);
+}
+int mlx_pcg_solve(mlx_solver* s, double h, const double* b, int32_t iterations, double* x, double* resvec) {
+  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+  return s->impl->pcg_solve(h, b, iterations, x, resvec);
 }
 int mlx_sim_contact_count(mlx_solver* s, int32_t* n) {
   if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");

@@ -35,6 +35,7 @@ struct SolverBase {
   virtual int ws_configure(int record, int mode, mlx_mlp* net, const float* fmean, const float* fstd,
                            const float* omean, const float* ostd, const float* corrections, int32_t* nb) = 0;
   virtual int ws_fetch(float* features, float* targets, int cap, int32_t* nb) = 0;
+  virtual int pcg_solve(double h, const double* b, int iterations, double* x, double* resvec) = 0;
 };
 
 SolverBase* make_solver(const mlx_mesh_desc* md, int* rc);
