@@ -41,6 +41,10 @@ WORKLOADS = {
         "3352014 tets) merged into one mesh (colours overlaid as Mesh3D.mergeMesh), E log-uniform [1e4,1e6], "
         "nu=0.35, coarse 4^3-cube rigid clusters (5 it) + fine layer (10 it), dt=1/60, bases pinned, "
         "seeded surface impulses, per-colour tiles autotuned"),
+    4: ("config4: contact-heavy drop, 32 StVK boxes of 12^3 cubes (70304 vertices, 331776 tets), E=5e5, nu=0.3, "
+        "seeded rotations and heights 0.5-3 m over a ground plane + 4 analytic spheres (r 0.3-0.6 m), contacts "
+        "detected on the device every step, 3 layers (4^3-cube clusters 1 it, 2^3-cube clusters 4 it, fine 10 it), "
+        "contact resistance 0.9, dt=1/120; timed after the boxes have landed"),
 }
 WORKLOAD = WORKLOADS[2]
 
@@ -123,7 +127,13 @@ CONFIG = 2
 
 def make_scene():
     from multilayersolver2024_b200 import scenes
-    return scenes.config3() if CONFIG == 3 else scenes.config2()
+    return {2: scenes.config2, 3: scenes.config3, 4: scenes.config4}[CONFIG]()
+
+
+def start_velocity(scene, m):
+    """Velocity at t = 0: the scene's seeded impulse, if it has one."""
+    if scene.impulse is not None:
+        m.v[scene.impulse[0] - 1] += scene.impulse[1]
 
 
 def make_integrator(scene, precision):
@@ -134,26 +144,41 @@ def make_integrator(scene, precision):
     integ.iterations = list(scene.iterations)
     integ.customRigidSets = scene.custom_sets
     integ.precision = precision
+    integ.contactResistance = scene.settings.get("contactResistance", integ.contactResistance)
     return integ
 
 
-def cpu_port_steps_per_s(nsteps, threads):
+def cpu_port_steps_per_s(nsteps, threads, state=None):
     """The oracle (FP64 C++ restatement of the reference path, all given host
-    threads) on the same workload: steps/s over `nsteps` steps."""
+    threads) on the same workload: steps/s over `nsteps` steps, from the
+    scene's t = 0 state or from `state` = (positions, velocities)."""
     from oracle import oracle as O
     from multilayersolver2024_b200.xpbd_layer3d import ContactSet, StepCache
     O.load().orc_set_threads(threads)
     sc = make_scene()
     integ = make_integrator(sc, 1)
     m = sc.mesh
-    m.v[sc.impulse[0] - 1] += sc.impulse[1]
+    start_velocity(sc, m)
+    if state is not None:
+        m.p, m.v = (a.copy() for a in state)
     cache = StepCache()
-    O.integrate(integ, m, sc.h, ContactSet(), cache, 1)  # warm-up (frame 1)
+
+    def contacts():
+        # simulate3D's loop: the finders on the step-start positions
+        return O.find_contacts(sc.contact_finders, m.p) if sc.contact_finders else ContactSet()
+
+    O.integrate(integ, m, sc.h, contacts(), cache, 1)  # warm-up (frame 1)
     t0 = time.perf_counter()
     for frame in range(2, nsteps + 2):
-        O.integrate(integ, m, sc.h, ContactSet(), cache, frame)
+        O.integrate(integ, m, sc.h, contacts(), cache, frame)
     dt = time.perf_counter() - t0
     return nsteps / dt, dt
+
+
+# untimed steps of the device stepper that bring a scene into its timed phase
+# (config 4: the boxes have landed on the obstacles after 150 steps, 1.25 s)
+ADVANCE = {4: 150}
+_PHASE = {}
 
 
 def run_reference(args, rank, world):
@@ -171,7 +196,9 @@ def run_reference(args, rank, world):
             "config": {"workload": WORKLOAD, "solver": "plain multi-layer, CPU port"},
             "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "port",
                              "sample": f"{total} consecutive steps of the full workload (oracle restatement; "
-                                       "MATLAB, the reference's runtime, is not installed)"},
+                                       "MATLAB, the reference's runtime, is not installed)"
+                                       + (", from t = 0 with the oracle contact finders every step" if CONFIG == 4
+                                          else "")},
             "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -209,7 +236,15 @@ def run_ours(args, rank, world, local):
     ls = find_boundary_vertices(m, sets, [int(sets[:, c].max(initial=0)) for c in range(sets.shape[1])])
     solver = Solver(m, precision=MLX_FP32, device=local, material="lame")
     sim = ResidentSim(solver, integ, ls, sc.h, p0=m.p, v0=np.zeros_like(m.p))
-    sim.add_velocity(sc.impulse[0], sc.impulse[1])
+    if sc.impulse is not None:
+        sim.add_velocity(sc.impulse[0], sc.impulse[1])
+    if sc.contact_finders:
+        sim.set_obstacles(sc.contact_finders, restitution=1e-2)
+    advance = ADVANCE.get(CONFIG, 0)
+    if advance:
+        sim.step(advance, graph=True)
+        torch.cuda.synchronize()
+        _PHASE["state"] = tuple(a.copy() for a in sim.state()[:2])
     tuned = None
     if args.autotune:
         before, after = sim.autotune(reps=5)
@@ -220,6 +255,7 @@ def run_ours(args, rank, world, local):
         sim.step(1, graph=True)
     torch.cuda.synchronize()
     sim.sweep_stats(reset=True)
+    contacts_at_start = sim.contact_count() if sc.contact_finders else None
 
     clocks = ClockSampler(local)
     clocks.start()
@@ -234,6 +270,7 @@ def run_ours(args, rank, world, local):
     barrier()
     clocks.stop()
     sweep_ms, sweep_bytes, sweep_launches = sim.sweep_stats(reset=True)
+    contacts_at_end = sim.contact_count() if sc.contact_finders else None
     max_ms = max_over_ranks(total_ms)
     value = args.steps * world / (max_ms / 1000.0)
     launches_per_step = sim.launches_per_step
@@ -245,23 +282,40 @@ def run_ours(args, rank, world, local):
     m2 = sc2.mesh
     integ2 = make_integrator(sc2, MLX_FP32)
     cache = StepCache()
-    m2.v[sc2.impulse[0] - 1] += sc2.impulse[1]
+    start_velocity(sc2, m2)
+    if advance:
+        m2.p, m2.v = (a.copy() for a in _PHASE["state"])
+    from multilayersolver2024_b200.contacts import find_contacts
+    contact_bytes = []
+
+    def e2e_step(frame):
+        # simulate3D's step: the finders on the step-start positions (on the
+        # device, mlx_find_contacts), then integrate (mlx_layer_solve)
+        cs = find_contacts(integ2.solver(m2), sc2.contact_finders, m2.p) if sc2.contact_finders else ContactSet()
+        contact_bytes.append(cs.vertex_ids.size)
+        integ2.integrate(m2, sc2.h, cs, cache, frame)
+
     e2e_steps = 0 if args.no_e2e else max(3, min(args.steps, 20 if CONFIG == 2 else 3))
     for frame in range(1, 3 if e2e_steps else 1):  # warm-up: solver creation and layer caches
-        integ2.integrate(m2, sc2.h, ContactSet(), cache, frame)
+        e2e_step(frame)
     barrier()
+    contact_bytes.clear()
     e2e_s = 1e-30
     for frame in range(3, 3 + e2e_steps):
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        integ2.integrate(m2, sc2.h, ContactSet(), cache, frame)
+        e2e_step(frame)
         e2e_s += time.perf_counter() - t0
     barrier()
     e2e_s = max_over_ranks(e2e_s)
     N, T = m2.N, m2.T
-    h2d = 8 * (3 * 3 * N + 6 * T + m2.pinnedDOFs.size)
-    d2h = 8 * 3 * N
+    K = float(np.mean(contact_bytes)) if contact_bytes else 0.0
+    # layer solve: xi, oldp, v in (3 x 3N), lambda (6T), pinned x, contacts
+    # (normal, point, compliance, id: 7 x 8 + 4 bytes each); detection:
+    # positions in (3N), contact lists back
+    h2d = 8 * (3 * 3 * N + 6 * T + m2.pinnedDOFs.size) + 60 * K + (8 * 3 * N if sc2.contact_finders else 0)
+    d2h = 8 * 3 * N + (60 * K if sc2.contact_finders else 0)
 
     # ---- iterations to residual 1e-4: the same workload with the residual
     # monitor and stop rules on the device (conditional graph nodes) ----
@@ -279,8 +333,15 @@ def run_ours(args, rank, world, local):
             ls3 = find_boundary_vertices(scene.mesh, sets3,
                                          [int(sets3[:, c].max(initial=0)) for c in range(sets3.shape[1])])
             solver3 = Solver(scene.mesh, precision=MLX_FP32, device=local, material="lame")
-            sim3 = ResidentSim(solver3, integ3, ls3, scene.h, p0=scene.mesh.p, v0=np.zeros_like(scene.mesh.p))
-            sim3.add_velocity(scene.impulse[0], scene.impulse[1])
+            if advance:
+                p0, v0 = _PHASE["state"]
+            else:
+                p0, v0 = scene.mesh.p, np.zeros_like(scene.mesh.p)
+            sim3 = ResidentSim(solver3, integ3, ls3, scene.h, p0=p0, v0=v0)
+            if scene.impulse is not None and not advance:
+                sim3.add_velocity(scene.impulse[0], scene.impulse[1])
+            if scene.contact_finders:
+                sim3.set_obstacles(scene.contact_finders, restitution=1e-2)
             return solver3, sim3
 
         def run_leg(sim3, n):
@@ -332,10 +393,12 @@ def run_ours(args, rank, world, local):
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
-            sps, dt = cpu_port_steps_per_s(args.cpu_steps, threads)
+            sps, dt = cpu_port_steps_per_s(args.cpu_steps, threads, _PHASE.get("state"))
             cpu = {"value": sps, "unit": "steps/s", "cores": threads, "kind": "port",
                    "sample": f"{args.cpu_steps} steps of the full workload after 1 warm-up step "
-                             f"({dt:.1f} s, FP64 oracle restatement, OpenMP over the tets of a colour)"}
+                             f"({dt:.1f} s, FP64 oracle restatement, OpenMP over the tets of a colour"
+                             + (", from the same landed state, oracle contact finders every step)" if advance
+                                else ")")}
         line = {
             "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
@@ -343,7 +406,9 @@ def run_ours(args, rank, world, local):
             "config": {"workload": WORKLOAD, "solver": "plain multi-layer (no warm-start)",
                        "iterations_per_step": int(sum(sc.iterations)), "precision": "FP32 bulk, FP64 rigid bodies",
                        "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}",
-                       "graph": "one CUDA graph per step", "autotune": tuned},
+                       "graph": "one CUDA graph per step", "autotune": tuned,
+                       "untimed_advance_steps": advance,
+                       "contacts_first_last_timed_step": [contacts_at_start, contacts_at_end]},
             "roofline": {"bound": "hbm", "kernel": sweep_kernel,
                          "launch_path": solver.launch_path,
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -358,7 +423,8 @@ def run_ours(args, rank, world, local):
                          "avg_launch_us": 1000.0 * sweep_ms / max(sweep_launches, 1)},
             "cpu_baseline": cpu,
             "e2e": None if not e2e_steps else {"value": e2e_steps * world / e2e_s, "unit": "steps/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "api": "XpbdLayer3D.integrate -> mlx_layer_solve"},
+                    "d2h_bytes_per_step": d2h, "api": "XpbdLayer3D.integrate -> mlx_layer_solve"
+                    + (" (+ mlx_find_contacts on the step-start positions)" if sc.contact_finders else "")},
             "to_residual": to_res,
             "gpu_launches": int(launches_per_step * args.steps),
             "clocks": clocks.summary(),
@@ -392,8 +458,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-API leg (profiling runs)")
-    ap.add_argument("--config", type=int, choices=[2, 3], default=2,
-                    help="2: the plain multi-layer block (default); 3: the 256-scene batch")
+    ap.add_argument("--config", type=int, choices=[2, 3, 4], default=2,
+                    help="2: the plain multi-layer block (default); 3: the 256-scene batch; 4: the contact-heavy drop")
     ap.add_argument("--autotune", action="store_true", help="run the per-colour tile autotuner before timing "
                     "(on by default for config 3)")
     ap.add_argument("--no-autotune", action="store_true", help="never run the autotuner (profiling runs)")

@@ -13,6 +13,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "tet_kernels.cuh"
 
 namespace mlx {
 
@@ -38,6 +39,12 @@ __device__ __forceinline__ double ddot3(double a0, double a1, double a2, double 
   return dadd(dadd(dmul(a0, b0), dmul(a1, b1)), dmul(a2, b2));
 }
 
+// contactInfo3D.xpbdContactCompliance of an obstacle's contacts: one value
+// per finder (the sphere finder leaves contactInfo3D's default).
+__device__ __forceinline__ double obstacle_compliance(const Obstacle& o) {
+  return o.type == OBS_SPHERE ? 1e-4 : o.compliance;
+}
+
 // Contact of a point with one obstacle: PlaneContactFinder3D.findContacts
 // (3d/contact/PlaneContactFinder3D.m:34-75), SphereContactFinder.findContacts
 // (3d/contact/SphereContactFinder.m:24-71), PlatformContactDetector.findContacts
@@ -50,14 +57,14 @@ __device__ __forceinline__ bool obstacle_contact(const Obstacle& o, double x, do
     phi = dsub(ddot3(x, y, z, o.n[0], o.n[1], o.n[2]), o.D);
     if (!(phi <= 0.0)) return false;
     n = d3(o.n[0], o.n[1], o.n[2]);
-    comp = o.compliance;
+    comp = obstacle_compliance(o);
   } else if (o.type == OBS_SPHERE) {
     const double dx = dsub(o.c[0], x), dy = dsub(o.c[1], y), dz = dsub(o.c[2], z);
     const double d = __dsqrt_rn(dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz)));
     if (!(d <= o.radius)) return false;
     phi = dsub(d, o.radius);
     n = d3(__ddiv_rn(dsub(x, o.c[0]), d), __ddiv_rn(dsub(y, o.c[1]), d), __ddiv_rn(dsub(z, o.c[2]), d));
-    comp = 1e-4;  // the sphere finder leaves contactInfo3D's default compliance
+    comp = obstacle_compliance(o);
   } else {
     const double ex = dsub(x, o.c[0]), ey = dsub(y, o.c[1]), ez = dsub(z, o.c[2]);
     double dots[3], ad[3];
@@ -75,7 +82,7 @@ __device__ __forceinline__ bool obstacle_contact(const Obstacle& o, double x, do
     phi = -ad[k];
     const double s = dots[k] > 0 ? 1.0 : (dots[k] < 0 ? -1.0 : 0.0);
     n = d3(s * o.dir[3 * k], s * o.dir[3 * k + 1], s * o.dir[3 * k + 2]);
-    comp = o.compliance;
+    comp = obstacle_compliance(o);
   }
   pt = d3(dsub(x, dmul(n.x, phi)), dsub(y, dmul(n.y, phi)), dsub(z, dmul(n.z, phi)));
   return true;
@@ -90,6 +97,7 @@ struct DevContacts {
   const int* cidx;         // [N] index of the vertex in verts, or -1
   const int* count;        // [1] number of contact vertices
   double* lambda;          // [count * nobs] contact multipliers of the current layer
+  const int* obs_count;    // [nobs] contacts of each obstacle (its finder's list length)
 };
 
 // Bit masks of every vertex at the step-start positions.
@@ -245,6 +253,70 @@ __global__ void k_contact_velocity(const DevContacts dc, const R4<R>* __restrict
   const double mn = fmin(-ek * vt, 0.0);
   vel[v] = make_r4<R>((R)(vn.x + n.x * (-vn.x + mn)), (R)(vn.y + n.y * (-vn.y + mn)), (R)(vn.z + n.z * (-vn.z + mn)),
                       u.w);
+}
+
+// Length of each finder's contact list: the vertices whose mask has bit f
+// (integer atomics, so the counts are exact).  `counts` is zeroed before.
+__global__ void __launch_bounds__(256) k_obstacle_counts(const unsigned* __restrict__ mask, int N, int nobs,
+                                                         int* __restrict__ counts) {
+  __shared__ int s[32];
+  if (threadIdx.x < 32) s[threadIdx.x] = 0;
+  __syncthreads();
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < N; v += gridDim.x * blockDim.x) {
+    unsigned m = mask[v];
+    while (m) {
+      atomicAdd(&s[__ffs(m) - 1], 1);
+      m &= m - 1;
+    }
+  }
+  __syncthreads();
+  if ((int)threadIdx.x < nobs && s[threadIdx.x]) atomicAdd(&counts[threadIdx.x], s[threadIdx.x]);
+}
+
+// The contact part of simpleEvaluateAllConstraintResiduals
+// (xpbdLayer3D.m:546-586) for the device contacts, one partial sum per
+// block.  The reference's correction term is the K x 1 x K implicit expansion
+// of (compliance/h^2) (1x1xK) times lambda (Kx1) (xpbdLayer3D.m:581-583), so
+// contact k meets the compliance of every contact j of the step; the
+// compliances are one value per obstacle, so contact k's K terms are
+// obs_count[g] copies of its term with obstacle g's compliance.
+template <typename R>
+__global__ void __launch_bounds__(256) k_contact_residual_partials(const DevContacts dc, const R4<R>* __restrict__ pos,
+                                                                   const R4<R>* __restrict__ x0,
+                                                                   double contact_resistance, double inv_h2_d,
+                                                                   double* __restrict__ partials) {
+  __shared__ double comp[32];
+  __shared__ int cnt[32];
+  if ((int)threadIdx.x < dc.nobs) {
+    comp[threadIdx.x] = obstacle_compliance(dc.obs[threadIdx.x]);
+    cnt[threadIdx.x] = dc.obs_count[threadIdx.x];
+  }
+  __syncthreads();
+  const int K = *dc.count;
+  double acc[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < K; i += gridDim.x * blockDim.x) {
+    const int v = dc.verts[i];
+    const unsigned m = dc.mask[v];
+    const R4<R> p = ldcg_r4(pos + v);
+    const R4<R> s0 = x0[v];
+    for (int f = 0; f < dc.nobs; ++f) {
+      if (!((m >> f) & 1u)) continue;
+      D3 n, c;
+      double cf;
+      obstacle_contact(dc.obs[f], (double)s0.x, (double)s0.y, (double)s0.z, n, c, cf);
+      double phi = n.x * ((double)p.x - c.x) + n.y * ((double)p.y - c.y) + n.z * ((double)p.z - c.z);
+      if (phi > 0) phi = 0;
+      const double a = fabs(contact_resistance * phi);
+      const double lk = dc.lambda[(size_t)i * dc.nobs + f];
+      for (int g = 0; g < dc.nobs; ++g) {
+        if (!cnt[g]) continue;
+        const double r = a - fmin(a, fabs((comp[g] * inv_h2_d) * lk));
+        acc[0] += (double)cnt[g] * (r * r);
+      }
+    }
+  }
+  block_sum<1>(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc[0];
 }
 
 }  // namespace mlx

@@ -276,7 +276,11 @@ struct Solver final : SolverBase {
   static constexpr int kDefaultTile = 64;
   std::vector<std::vector<int>> tiles;  // [column][colour], 0 = default
   int sim_autotune(int reps, double* before_ms, double* after_ms) override;
-  int residual(const ContactData& cd, double contact_resistance, double h, double* out);
+  int residual(const ContactData& cd, double contact_resistance, double h, double* out,
+               const DevContacts* dc = nullptr);
+  // the device contacts' partial sums of the residual (stream work only)
+  int contact_residual_partials(const DevContacts& dc, double contact_resistance, double h, double* partials,
+                                int* nblocks);
   int norm_resv(double* out);
   int validate_layers(const mlx_layer_desc* ld, const mlx_solve_params* P);
   int upload_contacts(const mlx_contacts* K, ContactData& cd);
@@ -300,6 +304,8 @@ struct Solver final : SolverBase {
   std::vector<Obstacle> sim_obs;
   double sim_restitution = 1e-2;
   DevBuf d_obs, d_cmask, d_cverts, d_cidx, d_cscan, d_clam_dev;
+  // buffers of mlx_find_contacts, kept across calls (they only grow)
+  DevBuf fc_ob, fc_mask, fc_verts, fc_scan, fc_x, fc_pos, fc_vid, fc_out;
   DevContacts dev_contacts() const {
     DevContacts dc{};
     dc.nobs = (int)sim_obs.size();
@@ -309,6 +315,7 @@ struct Solver final : SolverBase {
     dc.verts = d_cverts.as<int>();
     dc.cidx = d_cidx.as<int>();
     dc.count = d_cscan.as<int>() + blocks_for(N, 256);
+    dc.obs_count = dc.count + 2;
     dc.lambda = d_clam_dev.as<double>();
     return dc;
   }
@@ -320,7 +327,7 @@ struct Solver final : SolverBase {
   int cond_handle(cudaGraphConditionalHandle* h);
   int cond_begin(cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type, cudaStream_t body);
   int cond_end(cudaStream_t parent);
-  int residual_dev(double* out);
+  int residual_dev(double* out, const DevContacts& dc);
   int norm_resv_dev(double* out);
   int sim_monitor(double* ra, int cap, int32_t* len, int32_t* total_it, double* run_until, int32_t* status) override;
   struct {
@@ -890,7 +897,8 @@ int Solver<R>::launch_color(int c, const LayerStatic& ls, const int* dlist, R h,
 }
 
 template <typename R>
-int Solver<R>::residual(const ContactData& cd, double contact_resistance, double h, double* out) {
+int Solver<R>::residual(const ContactData& cd, double contact_resistance, double h, double* out,
+                        const DevContacts* dc) {
   const int bs = 256;
   int tetBlocks = std::min(blocks_for(T, bs), 592);
   int cBlocks = cd.K > 0 ? std::min(blocks_for(cd.K, bs), 64) : 0;
@@ -909,7 +917,9 @@ int Solver<R>::residual(const ContactData& cd, double contact_resistance, double
       k_residual_partials<R, MAT_STVK_LAME><<<tetBlocks + cBlocks, bs, 0, stream>>>(td, pos(), cd, contact_resistance, inv_h2, inv_h, inv_h2_d, tetBlocks, partials);
   }
   CU(cudaGetLastError());
-  k_finish_norm<256><<<1, 256, 0, stream>>>(partials, tetBlocks + cBlocks, d_scalar.as<double>());
+  int dBlocks = 0;
+  if (dc && dc->nobs) CHECK(contact_residual_partials(*dc, contact_resistance, h, partials + tetBlocks + cBlocks, &dBlocks));
+  k_finish_norm<256><<<1, 256, 0, stream>>>(partials, tetBlocks + cBlocks + dBlocks, d_scalar.as<double>());
   CU(cudaGetLastError());
   CU(cudaMemcpyAsync(h_scalar.p, d_scalar.p, sizeof(double), cudaMemcpyDeviceToHost, stream));
   CU(cudaStreamSynchronize(stream));
@@ -994,8 +1004,8 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
   // is a conditional IF node and its projectGS loop a conditional WHILE node
   // (monitor.cuh).  Kernels keep plain stream order there.
   const bool devmon = capturing && P->compute_residuals;
-  if (devmon && (cd.K > 0 || dc.nobs))
-    return set_error(MLX_ERR_UNSUPPORTED, "device residual monitoring does not cover contacts");
+  if (devmon && cd.K > 0)
+    return set_error(MLX_ERR_UNSUPPORTED, "device residual monitoring covers device-detected contacts only");
   struct Guard {
     Solver* s;
     cudaStream_t outer;
@@ -1240,7 +1250,8 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
       }
       bool endLayer = false;
       if (devmon) {
-        CHECK(residual_dev(&mon()->res));
+        CHECK(residual_dev(&mon()->res, dc));
+        if (dc.nobs) ++st.launches;
         k_mon_iter_end<<<1, 1, 0, stream>>>(mon(), h_while_cur, ld->iterations[layer], isLast ? 1 : 0, mp);
         CU(cudaGetLastError());
         st.launches += 3;
@@ -1251,8 +1262,8 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
         CU(cudaStreamSynchronize(stream));
         auto t0 = std::chrono::steady_clock::now();
         double newRes = 0;
-        CHECK(residual(cd, P->contact_resistance, h, &newRes));
-        st.launches += 2;
+        CHECK(residual(cd, P->contact_resistance, h, &newRes, &dc));
+        st.launches += dc.nobs ? 3 : 2;
         std::vector<double>& ra = st.residualArray;
         ra.push_back(newRes);
         double lastResidual = std::fabs(ra[ra.size() - 2]);
@@ -1328,7 +1339,7 @@ int Solver<R>::cond_end(cudaStream_t parent) {
 }
 
 template <typename R>
-int Solver<R>::residual_dev(double* out) {
+int Solver<R>::residual_dev(double* out, const DevContacts& dc) {
   const int bs = 256;
   const int tetBlocks = std::min(blocks_for(T, bs), 592);
   ContactData cd{};
@@ -1347,8 +1358,22 @@ int Solver<R>::residual_dev(double* out) {
       k_residual_partials<R, MAT_STVK_LAME><<<tetBlocks, bs, 0, stream>>>(td, pos(), cd, 0.0, inv_h2, inv_h, inv_h2_d, tetBlocks, partials);
   }
   CU(cudaGetLastError());
-  k_finish_norm<256><<<1, 256, 0, stream>>>(partials, tetBlocks, out);
+  int dBlocks = 0;
+  if (dc.nobs) CHECK(contact_residual_partials(dc, sim.P.contact_resistance, sim.P.h, partials + tetBlocks, &dBlocks));
+  k_finish_norm<256><<<1, 256, 0, stream>>>(partials, tetBlocks + dBlocks, out);
   CU(cudaGetLastError());
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::contact_residual_partials(const DevContacts& dc, double contact_resistance, double h,
+                                         double* partials, int* nblocks) {
+  // the number of contacts is only known on the device: a fixed grid strides over it
+  const int blocks = std::max(1, std::min(blocks_for(N, 256), 64));
+  k_contact_residual_partials<R><<<blocks, 256, 0, stream>>>(dc, pos(), d_oldp.as<R4<R>>(), contact_resistance,
+                                                             1.0 / (h * h), partials);
+  CU(cudaGetLastError());
+  *nblocks = blocks;
   return MLX_OK;
 }
 
@@ -1952,6 +1977,9 @@ int Solver<R>::detect_contacts(const R4<R>* x0) {
   k_compact_scan<<<1, 1024, 0, stream>>>(scan, nb, nullptr, scan + nb);
   k_compact_scatter<<<nb, 256, 0, stream>>>(d_cmask.as<unsigned>(), N, -1, scan, d_cverts.as<int>(),
                                             d_cidx.as<int>());
+  // finder list lengths (the residual's K x K expansion counts them)
+  CU(cudaMemsetAsync(scan + nb + 2, 0, sizeof(int) * nobs, stream));
+  k_obstacle_counts<<<std::min(nb, 296), 256, 0, stream>>>(d_cmask.as<unsigned>(), N, nobs, scan + nb + 2);
   CU(cudaGetLastError());
   return MLX_OK;
 }
@@ -1969,10 +1997,10 @@ int Solver<R>::sim_set_obstacles(const mlx_obstacle* obs, int nobs, double resti
     CHECK(d_cmask.ensure(sizeof(unsigned) * N));
     CHECK(d_cverts.ensure(sizeof(int) * N));
     CHECK(d_cidx.ensure(sizeof(int) * N));
-    CHECK(d_cscan.ensure(sizeof(int) * (blocks_for(N, 256) + 2)));
+    CHECK(d_cscan.ensure(sizeof(int) * (blocks_for(N, 256) + 2 + MLX_MAX_OBSTACLES)));
     CHECK(d_clam_dev.ensure(sizeof(double) * (size_t)N * o.size()));
     CU(cudaMemcpyAsync(d_obs.p, o.data(), sizeof(Obstacle) * o.size(), cudaMemcpyHostToDevice, stream));
-    CU(cudaMemsetAsync(d_cscan.p, 0, sizeof(int) * (blocks_for(N, 256) + 2), stream));
+    CU(cudaMemsetAsync(d_cscan.p, 0, sizeof(int) * (blocks_for(N, 256) + 2 + MLX_MAX_OBSTACLES), stream));
     CU(cudaStreamSynchronize(stream));
   }
   if (sim.graph) { cudaGraphExecDestroy(sim.graph); sim.graph = nullptr; }
@@ -2290,7 +2318,8 @@ int Solver<R>::find_contacts(const mlx_obstacle* obs, int nobs, const double* p,
   DeviceGuard g(device);
   const int nb = blocks_for(N, 256);
   const size_t cap = (size_t)N * o.size();
-  DevBuf dob, dmask, dverts, dscan, dx, dvid, dout, dpos;
+  DevBuf &dob = fc_ob, &dmask = fc_mask, &dverts = fc_verts, &dscan = fc_scan, &dx = fc_x, &dvid = fc_vid,
+         &dout = fc_out, &dpos = fc_pos;
   CHECK(dob.ensure(sizeof(Obstacle) * o.size()));
   CHECK(dmask.ensure(sizeof(unsigned) * N));
   CHECK(dverts.ensure(sizeof(int) * cap));
@@ -2325,15 +2354,16 @@ int Solver<R>::find_contacts(const mlx_obstacle* obs, int nobs, const double* p,
   if (total > max_contacts) return set_error(MLX_ERR_LIMIT, "more contacts than max_contacts");
   if (total == 0) return MLX_OK;
   if (!vids || !normals || !points || !comp) return set_error(MLX_ERR_ARGUMENT, "null output array");
-  std::vector<double> h(7 * cap);
+  // the list's rows hold `total` entries each out of `cap`: copy those only
   CU(cudaMemcpyAsync(vids, dvid.p, sizeof(int) * total, cudaMemcpyDeviceToHost, stream));
-  CU(cudaMemcpyAsync(h.data(), dout.p, sizeof(double) * 7 * cap, cudaMemcpyDeviceToHost, stream));
-  CU(cudaStreamSynchronize(stream));
   for (int d = 0; d < 3; ++d) {
-    std::memcpy(normals + (size_t)d * total, h.data() + (size_t)d * cap, sizeof(double) * total);
-    std::memcpy(points + (size_t)d * total, h.data() + 3 * cap + (size_t)d * cap, sizeof(double) * total);
+    CU(cudaMemcpyAsync(normals + (size_t)d * total, out + (size_t)d * cap, sizeof(double) * total,
+                       cudaMemcpyDeviceToHost, stream));
+    CU(cudaMemcpyAsync(points + (size_t)d * total, out + (3 + (size_t)d) * cap, sizeof(double) * total,
+                       cudaMemcpyDeviceToHost, stream));
   }
-  std::memcpy(comp, h.data() + 6 * cap, sizeof(double) * total);
+  CU(cudaMemcpyAsync(comp, out + 6 * cap, sizeof(double) * total, cudaMemcpyDeviceToHost, stream));
+  CU(cudaStreamSynchronize(stream));
   return MLX_OK;
 }
 
@@ -2421,7 +2451,7 @@ int Solver<R>::sim_issue_step(long long* launches, bool capturing) {
     // contacts of the step-start positions (simulate3D detects on mesh3D.p
     // before integrate; oldp holds those positions now)
     CHECK(detect_contacts(d_oldp.as<R4<R>>()));
-    st.launches += 4;
+    st.launches += 5;
   }
   CHECK(run_layers(&sim.ld, &sim.P, nullptr, cd, st, capturing, sim_work, dc));
   if (ws.nb > 0 && ws.record) {

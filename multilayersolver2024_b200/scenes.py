@@ -179,3 +179,59 @@ def config3(seed: int = 3, n_scenes: int = 256, tmin=2000, tmax=40000, cluster=4
                impulse=(np.concatenate(imp_dofs).astype(np.int32), np.concatenate(imp_dv)))
     sc.settings["parts"] = meshes
     return sc
+
+
+def config4(seed: int = 4, n_boxes: int = 32, cubes: int = 12, grid=(8, 4), spacing=2.0, n_spheres: int = 4,
+            coarse: int = 4, mid: int = 2, drop=(0.5, 3.0)) -> Scene:
+    """Contact-heavy drop: `n_boxes` StVK boxes of cubes^3 cubes (0.1 m, 6 tets
+    per cube; 32 x 10,368 tets by default), E = 5e5 Pa, nu = 0.3, with seeded
+    rotations, over a ground plane z = 0 and `n_spheres` analytic spheres
+    (radius in [0.3, 0.6] m, half sunk in the ground under seeded boxes).  A
+    box's lowest possible point (its half diagonal below its centre) starts a
+    seeded height in `drop` m above what lies under it.  Three layers:
+    coarse^3-cube rigid clusters, mid^3-cube rigid clusters, then the fine
+    layer; 15 iterations split as the reference's cube drop example splits
+    its own (1 and 4 rigid-layer iterations, the rest fine) with its contact
+    resistance 0.9 (3d/examples/XPBD/cubeDrop_xpbd.m:27-35) and the finders'
+    default contact compliance 1e-4; dt = 1/120, 500 steps.  Boxes sit on a
+    grid `spacing` m apart, so they meet the obstacles and not each other.
+    Returns the merged mesh; `contact_finders` holds the obstacles."""
+    from .contacts import PlaneContactFinder3D, SphereContactFinder, rotation_matrix_degrees
+    rng = np.random.default_rng(seed)
+    half = cubes * 0.1 / 2
+    xy = [np.array([(k % grid[0]) * spacing, ((k // grid[0]) % grid[1]) * spacing]) for k in range(n_boxes)]
+    finders = [PlaneContactFinder3D([0.0, 0.0, 1.0], [0.0, 0.0, 0.0])]
+    base = np.zeros(n_boxes)
+    for k in rng.choice(n_boxes, size=min(n_spheres, n_boxes), replace=False):
+        r = rng.uniform(0.3, 0.6)
+        x, y = xy[k] + rng.uniform(-0.3, 0.3, 2)
+        finders.append(SphereContactFinder(r, [x, y, 0.5 * r]))
+        base[k] = 1.5 * r
+    meshes, sets_c, sets_m = [], [], []
+    nb_c = nb_m = 0
+    for k in range(n_boxes):
+        V, T, cube = generate_beam(cubes, cubes, cubes, 0.1)
+        R = rotation_matrix_degrees(rng.uniform(0, 360, 3))
+        c = np.array([xy[k][0], xy[k][1], base[k] + rng.uniform(*drop) + half * np.sqrt(3.0)])
+        V = (V - half) @ R.T + c
+        m = Mesh3D.from_arrays(V, T, *to_lame(0.3, 5e5), rho=1000.0, alpha1=0.0,
+                               energy_type=_lib.MLX_ENERGY_STVK_VOIGT)
+        none = np.zeros(m.T, dtype=bool)
+        sc = cluster_rigid_sets(cube, (cubes, cubes, cubes), coarse, none)
+        sm = cluster_rigid_sets(cube, (cubes, cubes, cubes), mid, none)
+        sc[sc > 0] += nb_c
+        sm[sm > 0] += nb_m
+        nb_c = int(max(nb_c, sc.max(initial=0)))
+        nb_m = int(max(nb_m, sm.max(initial=0)))
+        sets_c.append(sc)
+        sets_m.append(sm)
+        meshes.append(m)
+    mesh = merge_meshes(meshes)
+    # sorted columns: [fine (0), mid (25), coarse (50)]
+    custom = np.asfortranarray(np.stack([np.zeros(mesh.T, np.int32), np.concatenate(sets_m),
+                                         np.concatenate(sets_c)], 1).astype(np.int32))
+    sc = Scene(f"config4_drop_{n_boxes}_boxes_{cubes}c", mesh, 1.0 / 120.0, 500, [50, 25, 0], [1, 4, 10],
+               gravity=-9.81, custom_sets=custom, contact_finders=finders)
+    sc.settings["parts"] = meshes
+    sc.settings["contactResistance"] = 0.9
+    return sc

@@ -8,7 +8,9 @@ analytic obstacles, against the oracle's finders and integrate.
     step, projected in every layer, contactVelocityUpdate after the step)
     against the oracle integrate fed with the oracle finders' lists of the
     step-start positions: FP64 <= 1e-9, FP32 <= 1e-4 of the bounding-box
-    diagonal over 8 steps, rigid contacts on and off.
+    diagonal over 8 steps, rigid contacts on and off;
+  * the residual monitor (device and host) with those contacts: residual
+    arrays, iteration counts and positions against the oracle, FP64.
 """
 import numpy as np
 import pytest
@@ -102,3 +104,51 @@ def test_resident_stepper_with_obstacles_matches_oracle(gpu, oracle, precision, 
             assert abs(sim.contact_count() - nref[k]) <= max(2, nref[k] // 10)
         err = np.abs(sim.state()[0] - ref[k]).max() / d
         assert err <= tol, f"step {k}: {err:.3e}"
+
+
+@pytest.mark.parametrize("graph", [True, False])
+@pytest.mark.parametrize("run_until,hanging_stop", [(-1.0, 400), (0.03, 400), (1e-7, 60)])
+def test_monitored_steps_with_obstacles_match_oracle(gpu, oracle, graph, run_until, hanging_stop):
+    """Residual monitor with device contacts (the contact rows of
+    simpleEvaluateAllConstraintResiduals, K x K expansion included): the
+    residual array, the iteration count, runUntil and the positions of every
+    step against the oracle fed with its finders' lists, FP64, graph (device
+    monitor) and host monitor."""
+    h, steps = 0.01, 6
+    m, sets, v0 = _falling_scene()
+
+    def integ():
+        it = _integ(sets, _lib.MLX_FP64, True)
+        it.computeResiduals = True
+        it.runUntilResSmallerThan = run_until
+        it.hangingStop = hanging_stop
+        return it
+
+    oracle.load().orc_set_threads(8)
+    mo, _, _ = _falling_scene()
+    mo.v = v0.copy()
+    io = integ()
+    cache = StepCache()
+    ref = []
+    for frame in range(1, steps + 1):
+        cs = oracle.find_contacts(_finders(), mo.p)
+        ra, iters = oracle.integrate(io, mo, h, cs, cache, frame)
+        ref.append((mo.p.copy(), np.asarray(ra, float), int(iters), float(io.runUntilResSmallerThan),
+                    np.unique(cs.vertex_ids).size))
+    assert max(r[4] for r in ref) > 10
+    ls = find_boundary_vertices(m, sets, [0, int(sets[:, 1].max())])
+    s = Solver(m, precision=_lib.MLX_FP64, material="blocks")
+    sim = ResidentSim(s, integ(), ls, h, p0=m.p, v0=v0)
+    sim.set_obstacles(_finders(), restitution=1e-2)
+    d = m.bbox_diagonal()
+    for k in range(steps):
+        sim.step(1, graph=graph)
+        ra, iters, ru, status = sim.monitor()
+        p_ref, ra_ref, it_ref, ru_ref, _ = ref[k]
+        assert status == 0
+        assert iters == it_ref, f"step {k}: {iters} iterations, oracle {it_ref}"
+        assert ra.size == ra_ref.size
+        np.testing.assert_allclose(ra, ra_ref, rtol=0, atol=1e-9 * max(np.abs(ra_ref).max(), 1e-300))
+        assert ru == pytest.approx(ru_ref, rel=1e-9, abs=0)
+        err = np.abs(sim.state()[0] - p_ref).max() / d
+        assert err <= 1e-9, f"step {k}: {err:.3e}"
