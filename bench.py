@@ -240,7 +240,7 @@ def run_ours(args, rank, world, local):
         sim.add_velocity(sc.impulse[0], sc.impulse[1])
     if sc.contact_finders:
         sim.set_obstacles(sc.contact_finders, restitution=1e-2)
-    advance = ADVANCE.get(CONFIG, 0)
+    advance = ADVANCE.get(CONFIG, 0) if args.advance is None else args.advance
     if advance:
         sim.step(advance, graph=True)
         torch.cuda.synchronize()
@@ -465,6 +465,9 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="never run the autotuner (profiling runs)")
     ap.add_argument("--no-residual-leg", action="store_true", help="skip the iterations-to-residual-1e-4 leg")
     ap.add_argument("--residual-steps", type=int, default=4)
+    ap.add_argument("--advance", type=int, default=None,
+                    help="untimed steps before the warm-up (default: 150 for config 4, which lands the boxes; "
+                    "0 for the others)")
     ap.add_argument("--learned-train-steps", type=int, default=16,
                     help="recorded steps (another seed) the warm-start network is trained on; 0 skips that leg")
     ap.add_argument("--residual-cap", type=int, default=15000,

@@ -136,7 +136,8 @@ typedef struct mlx_contacts {
 /* Per-step vectors of layerSolve. */
 typedef struct mlx_solve_inputs {
   const double* xi;                    /* 3N                                  */
-  const double* lambdai;               /* T x 6 column-major                  */
+  const double* lambdai;               /* T x 6 column-major; NULL = zeros    */
+                                       /* (what integrate passes)             */
   const double* oldp;                  /* 3N                                  */
   const double* old_oldp;              /* 3N (accepted; unused by the path)   */
   const double* f;                     /* 3N (accepted; unused by the path)   */

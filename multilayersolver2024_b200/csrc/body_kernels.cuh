@@ -1,11 +1,16 @@
 // body_kernels.cuh -- rigid-layer kernels (FP64 body state on every path).
 //
-// One CTA owns one rigid body: its vertex, boundary-vertex and rigid-contact
-// lists are contiguous CSR ranges, the per-body sums of the reference's
-// accumarray calls become fixed-order block reductions (deterministic), and
-// the body update (expRodrigues, R <- dR R, I <- R I0 R') runs on thread 0
-// between two barriers.  Elastic contacts, which touch no body, ride in the
-// extra CTAs of the same launch.
+// One thread group owns one rigid body: its vertex, boundary-vertex and
+// rigid-contact lists are contiguous CSR ranges, the per-body sums of the
+// reference's accumarray calls become fixed-order reductions over the group
+// (deterministic), and the body update (expRodrigues, R <- dR R,
+// I <- R I0 R') runs on the group's first thread between two barriers.  In
+// the per-body kernels the group is a whole CTA for a body of more than
+// kSmallBody vertices and one warp otherwise (eight bodies per 256-thread
+// CTA), chosen per body from its own size, so a body's arithmetic never
+// depends on the other bodies of the layer (a scene steps bit-identically
+// alone or inside a batch).  Elastic contacts, which touch no body, ride in
+// the extra CTAs of the same launch.
 #pragma once
 
 #include "common.cuh"
@@ -30,7 +35,53 @@ struct LayerDev {
   int n_ec_groups;          // elastic contacts grouped by vertex
   const int* ec_off;        // [n_ec_groups+1]
   const int* ec_ids;        // contact ids, ascending inside a group
+  int n_items;              // CTAs of the per-body kernels
+  const int* items;         // [n_items][kItemInts]: see body_of_item
 };
+
+// Bodies of at most kSmallBody vertices are owned by one warp.
+constexpr int kSmallBody = 128;
+constexpr int kBodyThreads = 256;                 // CTA size of the per-body kernels
+constexpr int kItemInts = kBodyThreads / 32;      // one body per warp, or one large body
+constexpr int kLargeItem = -2;                    // item[1] marking a CTA-wide body
+
+// Deterministic sum of NV doubles over a warp (xor butterfly: at every stage
+// both lanes of a pair add the same two operands, so all lanes hold the same
+// bits).
+template <int NV>
+__device__ __forceinline__ void warp_sum(double (&v)[NV]) {
+#pragma unroll
+  for (int q = 0; q < NV; ++q)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+}
+
+// The thread group that owns a body.
+struct CtaGroup {
+  __device__ __forceinline__ int rank() const { return threadIdx.x; }
+  __device__ __forceinline__ int size() const { return blockDim.x; }
+  __device__ __forceinline__ void sync() const { __syncthreads(); }
+  template <int NV> __device__ __forceinline__ void sum(double (&v)[NV]) const { block_sum<NV>(v); }
+};
+struct WarpGroup {
+  __device__ __forceinline__ int rank() const { return threadIdx.x & 31; }
+  __device__ __forceinline__ int size() const { return 32; }
+  __device__ __forceinline__ void sync() const { __syncwarp(); }
+  template <int NV> __device__ __forceinline__ void sum(double (&v)[NV]) const { warp_sum<NV>(v); }
+};
+
+// Body of this thread in a per-body kernel (kBodyThreads threads per CTA):
+// item[1] == kLargeItem gives body item[0] to the whole CTA (returns 1);
+// otherwise warp w owns body item[w] (returns 0; -1 = no body).
+__device__ __forceinline__ int body_of_item(const LayerDev& L, int& b) {
+  const int* it = L.items + (size_t)kItemInts * blockIdx.x;
+  if (it[1] == kLargeItem) {
+    b = it[0];
+    return 1;
+  }
+  b = it[threadIdx.x >> 5];
+  return 0;
+}
 
 __device__ __forceinline__ D3 solve3_piv(const double* Mcm, D3 b) {
   double A[3][3], bb[3] = {b.x, b.y, b.z}, x[3];
@@ -94,16 +145,13 @@ __device__ __forceinline__ void store_xyz(R4<R>* pos, int v, D3 x) {
 // RigidBody3D.matComputeRigidBodyProperties3D (RigidBody3D.m:198-247):
 // mass, COM, COM velocity, inertia, angular momentum and omega = I \ L, with
 // the residual velocity as vertex velocity; writes ri = p - COM.
-template <typename R>
-__global__ void __launch_bounds__(256) k_make_rigids(LayerDev L, Body* __restrict__ bodies,
-                                                     const R4<R>* __restrict__ pos,
-                                                     const R4<R>* __restrict__ resv,
-                                                     const double* __restrict__ vmass,
-                                                     double4* __restrict__ ri) {
-  int b = blockIdx.x;
+template <typename R, typename G>
+__device__ __forceinline__ void make_rigid(const LayerDev& L, int b, Body* __restrict__ bodies,
+                                           const R4<R>* __restrict__ pos, const R4<R>* __restrict__ resv,
+                                           const double* __restrict__ vmass, double4* __restrict__ ri, const G& g) {
   int beg = L.body_vert_off[b], end = L.body_vert_off[b + 1];
   double s[7] = {0, 0, 0, 0, 0, 0, 0};
-  for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+  for (int i = beg + g.rank(); i < end; i += g.size()) {
     int v = L.body_verts[i];
     double m = vmass[v];
     R4<R> p = pos[v], u = resv[v];
@@ -111,11 +159,11 @@ __global__ void __launch_bounds__(256) k_make_rigids(LayerDev L, Body* __restric
     s[1] += (double)p.x * m; s[2] += (double)p.y * m; s[3] += (double)p.z * m;
     s[4] += (double)u.x * m; s[5] += (double)u.y * m; s[6] += (double)u.z * m;
   }
-  block_sum<7>(s);
+  g.template sum<7>(s);
   double M = s[0];
   D3 com = d3(s[1] / M, s[2] / M, s[3] / M), cdot = d3(s[4] / M, s[5] / M, s[6] / M);
   double t[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // Ixx Iyy Izz Ixy Ixz Iyz Lx Ly Lz
-  for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+  for (int i = beg + g.rank(); i < end; i += g.size()) {
     int v = L.body_verts[i];
     double m = vmass[v];
     R4<R> p = pos[v], u = resv[v];
@@ -132,8 +180,8 @@ __global__ void __launch_bounds__(256) k_make_rigids(LayerDev L, Body* __restric
     D3 c = cross(r, vd);
     t[6] += m * c.x; t[7] += m * c.y; t[8] += m * c.z;
   }
-  block_sum<9>(t);
-  if (threadIdx.x == 0) {
+  g.template sum<9>(t);
+  if (g.rank() == 0) {
     Body& B = bodies[b];
     double I0[9] = {t[0], t[3], t[4], t[3], t[1], t[5], t[4], t[5], t[2]};
     D3 w = solve3_piv(I0, d3(t[6], t[7], t[8]));
@@ -151,6 +199,17 @@ __global__ void __launch_bounds__(256) k_make_rigids(LayerDev L, Body* __restric
   }
 }
 
+template <typename R>
+__global__ void __launch_bounds__(kBodyThreads) k_make_rigids(LayerDev L, Body* __restrict__ bodies,
+                                                              const R4<R>* __restrict__ pos,
+                                                              const R4<R>* __restrict__ resv,
+                                                              const double* __restrict__ vmass,
+                                                              double4* __restrict__ ri) {
+  int b;
+  if (body_of_item(L, b)) make_rigid<R>(L, b, bodies, pos, resv, vmass, ri, CtaGroup{});
+  else if (b >= 0) make_rigid<R>(L, b, bodies, pos, resv, vmass, ri, WarpGroup{});
+}
+
 // Release all elastic residual (xpbdLayer3D.m:138-139).
 template <typename R>
 __global__ void k_release_elastic(R4<R>* __restrict__ pos, R4<R>* __restrict__ resv,
@@ -165,15 +224,11 @@ __global__ void k_release_elastic(R4<R>* __restrict__ pos, R4<R>* __restrict__ r
 // RigidBody3D.rigidSymplecticImperativeStep (RigidBody3D.m:174-179), the
 // re-placement of rigid vertices (xpbdLayer3D.m:147) and the residual rebase
 // resv = R_step resv - (x - xprev)/h (xpbdLayer3D.m:149-158).
-template <typename R>
-__global__ void __launch_bounds__(256) k_rigid_step(LayerDev L, Body* __restrict__ bodies,
-                                                    R4<R>* __restrict__ pos,
-                                                    const R4<R>* __restrict__ xprev,
-                                                    R4<R>* __restrict__ resv,
-                                                    const double4* __restrict__ ri, double h) {
-  __shared__ Body sb;
-  int b = blockIdx.x;
-  if (threadIdx.x == 0) {
+template <typename R, typename G>
+__device__ __forceinline__ void rigid_step(const LayerDev& L, int b, Body* __restrict__ bodies, R4<R>* __restrict__ pos,
+                                           const R4<R>* __restrict__ xprev, R4<R>* __restrict__ resv,
+                                           const double4* __restrict__ ri, double h, Body& sb, const G& g) {
+  if (g.rank() == 0) {
     Body B = bodies[b];
     for (int d = 0; d < 3; ++d) B.com[d] += h * B.comdot[d];
     double dR[9], tmp[9];
@@ -185,9 +240,9 @@ __global__ void __launch_bounds__(256) k_rigid_step(LayerDev L, Body* __restrict
     bodies[b] = B;
     sb = B;
   }
-  __syncthreads();
+  g.sync();
   int beg = L.body_vert_off[b], end = L.body_vert_off[b + 1];
-  for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+  for (int i = beg + g.rank(); i < end; i += g.size()) {
     int v = L.body_verts[i];
     D3 x = body_point(sb, ri[v]);
     R4<R> p = pos[v];
@@ -200,6 +255,18 @@ __global__ void __launch_bounds__(256) k_rigid_step(LayerDev L, Body* __restrict
     double rz = ((double)q.z - (double)xp.z) / h;
     resv[v] = make_r4<R>((R)(rot.x - rx), (R)(rot.y - ry), (R)(rot.z - rz), 0);
   }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kBodyThreads) k_rigid_step(LayerDev L, Body* __restrict__ bodies,
+                                                             R4<R>* __restrict__ pos,
+                                                             const R4<R>* __restrict__ xprev,
+                                                             R4<R>* __restrict__ resv,
+                                                             const double4* __restrict__ ri, double h) {
+  __shared__ Body sb[kItemInts];
+  int b;
+  if (body_of_item(L, b)) rigid_step<R>(L, b, bodies, pos, xprev, resv, ri, h, sb[0], CtaGroup{});
+  else if (b >= 0) rigid_step<R>(L, b, bodies, pos, xprev, resv, ri, h, sb[threadIdx.x >> 5], WarpGroup{});
 }
 
 // rigidGeneralizedInverseMass (3d/constraints/rigidGeneralizedInverseMass.m):
@@ -266,26 +333,26 @@ __device__ __forceinline__ void elastic_contact_group(const LayerDev& L, int g, 
 // penaltyConstraint.projectRigid :30-63), Jacobi style as in the reference.
 // All bodies are updated whenever the layer has any boundary vertex / rigid
 // contact, as the reference's vectorised update does.
-template <typename R, typename P>
+template <typename R, typename P, typename G = CtaGroup>
 __device__ __forceinline__ void body_iteration(const LayerDev& L, int b, Body* __restrict__ bodies,
                                                const P& pos, const double4* __restrict__ ri,
                                                const double* __restrict__ vmass, double* __restrict__ lamB,
                                                const ContactData& cd, double h, double boundary_compliance,
                                                double contact_resistance, int use_rigid_contacts, Body& sb,
                                                double* invI, const DevContacts& dc = DevContacts{},
-                                               const R4<R>* __restrict__ x0 = nullptr) {
-  if (threadIdx.x == 0) {
+                                               const R4<R>* __restrict__ x0 = nullptr, const G g = G{}) {
+  if (g.rank() == 0) {
     sb = bodies[b];
     inverse3(sb.I, invI);
   }
-  __syncthreads();
+  g.sync();
   bool dirty = false;
   if (L.any_boundary) {
     double s[6] = {0, 0, 0, 0, 0, 0};
     int beg = L.bnd_off[b], end = L.bnd_off[b + 1];
     double invM = 1.0 / sb.mass;
     D3 com = d3(sb.com[0], sb.com[1], sb.com[2]);
-    for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+    for (int i = beg + g.rank(); i < end; i += g.size()) {
       int v = L.bnd_verts[i];
       R4<R> p = pos.ld(v);
       D3 pE = d3((double)p.x, (double)p.y, (double)p.z);
@@ -306,13 +373,13 @@ __device__ __forceinline__ void body_iteration(const LayerDev& L, int b, Body* _
       D3 dw = cross(r, d3(pp.x / h, pp.y / h, pp.z / h));
       s[3] += dw.x; s[4] += dw.y; s[5] += dw.z;
     }
-    block_sum<6>(s);
-    if (threadIdx.x == 0) {
+    g.template sum<6>(s);
+    if (g.rank() == 0) {
       apply_increments(sb, s, h);
       inverse3(sb.I, invI);
     }
-    __syncthreads();
-    for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+    g.sync();
+    for (int i = beg + g.rank(); i < end; i += g.size()) {
       int v = L.bnd_verts[i];
       store_xyz<R>(pos, v, body_point(sb, ri[v]));
     }
@@ -320,12 +387,12 @@ __device__ __forceinline__ void body_iteration(const LayerDev& L, int b, Body* _
   }
   if (use_rigid_contacts && L.any_rigid_contact) {
     pos.fence();
-    __syncthreads();
+    g.sync();
     double s[6] = {0, 0, 0, 0, 0, 0};
     int beg = L.rc_off[b], end = L.rc_off[b + 1];
     double invM = 1.0 / sb.mass, h2 = h * h;
     D3 com = d3(sb.com[0], sb.com[1], sb.com[2]);
-    for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+    for (int i = beg + g.rank(); i < end; i += g.size()) {
       int k = L.rc_ids[i];
       int v = cd.vid[k];
       R4<R> p = pos.ld(v);
@@ -346,10 +413,10 @@ __device__ __forceinline__ void body_iteration(const LayerDev& L, int b, Body* _
       D3 cr = cross(r, pp);
       s[3] += (1 / h) * cr.x; s[4] += (1 / h) * cr.y; s[5] += (1 / h) * cr.z;
     }
-    block_sum<6>(s);
-    if (threadIdx.x == 0) apply_increments(sb, s, h);
-    __syncthreads();
-    for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+    g.template sum<6>(s);
+    if (g.rank() == 0) apply_increments(sb, s, h);
+    g.sync();
+    for (int i = beg + g.rank(); i < end; i += g.size()) {
       int v = cd.vid[L.rc_ids[i]];
       store_xyz<R>(pos, v, body_point(sb, ri[v]));
     }
@@ -358,12 +425,12 @@ __device__ __forceinline__ void body_iteration(const LayerDev& L, int b, Body* _
   if (use_rigid_contacts && dc.nobs) {
     // contacts detected on the device: the body's vertices carry finder masks
     pos.fence();
-    __syncthreads();
+    g.sync();
     double s[6] = {0, 0, 0, 0, 0, 0};
     const int beg = L.body_vert_off[b], end = L.body_vert_off[b + 1];
     const double invM = 1.0 / sb.mass, h2 = h * h;
     const D3 com = d3(sb.com[0], sb.com[1], sb.com[2]);
-    for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+    for (int i = beg + g.rank(); i < end; i += g.size()) {
       const int v = L.body_verts[i];
       const unsigned m = dc.mask[v];
       if (!m) continue;
@@ -391,51 +458,59 @@ __device__ __forceinline__ void body_iteration(const LayerDev& L, int b, Body* _
         s[3] += (1 / h) * cr.x; s[4] += (1 / h) * cr.y; s[5] += (1 / h) * cr.z;
       }
     }
-    block_sum<6>(s);
-    if (threadIdx.x == 0) apply_increments(sb, s, h);
-    __syncthreads();
-    for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+    g.template sum<6>(s);
+    if (g.rank() == 0) apply_increments(sb, s, h);
+    g.sync();
+    for (int i = beg + g.rank(); i < end; i += g.size()) {
       const int v = L.body_verts[i];
       if (dc.mask[v]) store_xyz<R>(pos, v, body_point(sb, ri[v]));
     }
     dirty = true;
   }
-  if (dirty && threadIdx.x == 0) bodies[b] = sb;
+  if (dirty && g.rank() == 0) bodies[b] = sb;
   pos.fence();
-  __syncthreads();
+  g.sync();
 }
 
 // One iteration's body phase as its own launch: CTAs [0, nb) run one body
 // each, the remaining CTAs the elastic contact groups.
 template <typename R>
-__global__ void __launch_bounds__(256) k_iterate_bodies(LayerDev L, Body* __restrict__ bodies,
-                                                        R4<R>* __restrict__ pos,
-                                                        const double4* __restrict__ ri,
-                                                        const double* __restrict__ vmass,
-                                                        double* __restrict__ lamB, ContactData cd,
-                                                        double h, double boundary_compliance,
-                                                        double contact_resistance, int use_rigid_contacts,
-                                                        DevContacts dc, const R4<R>* __restrict__ x0) {
-  __shared__ Body sb;
-  __shared__ double invI[9];
+__global__ void __launch_bounds__(kBodyThreads) k_iterate_bodies(LayerDev L, Body* __restrict__ bodies,
+                                                                 R4<R>* __restrict__ pos,
+                                                                 const double4* __restrict__ ri,
+                                                                 const double* __restrict__ vmass,
+                                                                 double* __restrict__ lamB, ContactData cd,
+                                                                 double h, double boundary_compliance,
+                                                                 double contact_resistance, int use_rigid_contacts,
+                                                                 DevContacts dc, const R4<R>* __restrict__ x0) {
+  __shared__ Body sb[kItemInts];
+  __shared__ double invI[kItemInts][9];
   pdl_launch_dependents();
   pdl_wait();
-  int b = blockIdx.x;
-  if (b >= L.nb) {
+  const int nbc = L.nb > 0 ? L.n_items : 0;  // CTAs [0, nbc) work on bodies
+  if ((int)blockIdx.x >= nbc) {
     const GlobalPos<R> gp{pos};
+    const int e = (int)blockIdx.x - nbc;
     if (dc.nobs) {
       // device-detected contacts: elastic ones are those of non-rigid vertices
-      const int n = *dc.count, stride = (gridDim.x - L.nb) * blockDim.x;
-      for (int i = (b - L.nb) * blockDim.x + threadIdx.x; i < n; i += stride)
+      const int n = *dc.count, stride = (gridDim.x - nbc) * blockDim.x;
+      for (int i = e * blockDim.x + threadIdx.x; i < n; i += stride)
         if (L.vert_body[dc.verts[i]] == 0) elastic_contacts_of_vertex<R>(dc, i, gp, x0, h, contact_resistance);
       return;
     }
-    int g = (b - L.nb) * blockDim.x + threadIdx.x;
+    int g = e * blockDim.x + threadIdx.x;
     if (g < L.n_ec_groups) elastic_contact_group<R>(L, g, gp, cd, h, contact_resistance);
     return;
   }
-  body_iteration<R>(L, b, bodies, GlobalPos<R>{pos}, ri, vmass, lamB, cd, h, boundary_compliance, contact_resistance,
-                    use_rigid_contacts, sb, invI, dc, x0);
+  int b;
+  if (body_of_item(L, b)) {
+    body_iteration<R>(L, b, bodies, GlobalPos<R>{pos}, ri, vmass, lamB, cd, h, boundary_compliance,
+                      contact_resistance, use_rigid_contacts, sb[0], invI[0], dc, x0, CtaGroup{});
+  } else if (b >= 0) {
+    const int w = threadIdx.x >> 5;
+    body_iteration<R>(L, b, bodies, GlobalPos<R>{pos}, ri, vmass, lamB, cd, h, boundary_compliance,
+                      contact_resistance, use_rigid_contacts, sb[w], invI[w], dc, x0, WarpGroup{});
+  }
 }
 
 // xi(pinnedDOFs) = pinnedx (xpbdLayer3D.m:333)
@@ -452,20 +527,18 @@ __global__ void k_pin(R4<R>* __restrict__ pos, const int* __restrict__ dofs,
 
 // End of projectGS / layer: rotateAllVerts (xpbdLayer3D.m:344, 508-513) and,
 // for a rigid layer, rotateResidual by dR = R_proj R_step' (:217-221, 234-241).
-template <typename R>
-__global__ void __launch_bounds__(256) k_finish_layer(LayerDev L, const Body* __restrict__ bodies,
-                                                      R4<R>* __restrict__ pos, R4<R>* __restrict__ resv,
-                                                      const double4* __restrict__ ri, int rigid_layer) {
-  __shared__ Body sb;
-  __shared__ double dR[9];
-  int b = blockIdx.x;
-  if (threadIdx.x == 0) {
+template <typename R, typename G>
+__device__ __forceinline__ void finish_layer(const LayerDev& L, int b, const Body* __restrict__ bodies,
+                                             R4<R>* __restrict__ pos, R4<R>* __restrict__ resv,
+                                             const double4* __restrict__ ri, int rigid_layer, Body& sb, double* dR,
+                                             const G& g) {
+  if (g.rank() == 0) {
     sb = bodies[b];
     mm3_bt(sb.R, sb.Rstep, dR);
   }
-  __syncthreads();
+  g.sync();
   int beg = L.body_vert_off[b], end = L.body_vert_off[b + 1];
-  for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+  for (int i = beg + g.rank(); i < end; i += g.size()) {
     int v = L.body_verts[i];
     store_xyz<R>(pos, v, body_point(sb, ri[v]));
     if (rigid_layer) {
@@ -473,6 +546,21 @@ __global__ void __launch_bounds__(256) k_finish_layer(LayerDev L, const Body* __
       D3 r = mv3(dR, d3((double)u.x, (double)u.y, (double)u.z));
       resv[v] = make_r4<R>((R)r.x, (R)r.y, (R)r.z, 0);
     }
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kBodyThreads) k_finish_layer(LayerDev L, const Body* __restrict__ bodies,
+                                                               R4<R>* __restrict__ pos, R4<R>* __restrict__ resv,
+                                                               const double4* __restrict__ ri, int rigid_layer) {
+  __shared__ Body sb[kItemInts];
+  __shared__ double dR[kItemInts][9];
+  int b;
+  if (body_of_item(L, b)) {
+    finish_layer<R>(L, b, bodies, pos, resv, ri, rigid_layer, sb[0], dR[0], CtaGroup{});
+  } else if (b >= 0) {
+    const int w = threadIdx.x >> 5;
+    finish_layer<R>(L, b, bodies, pos, resv, ri, rigid_layer, sb[w], dR[w], WarpGroup{});
   }
 }
 

@@ -174,6 +174,8 @@ struct LayerStatic {
   std::vector<int> packed;       // body_vert_off | body_verts | bnd_off | bnd_verts | list | vert_body
   size_t o_bvo = 0, o_bv = 0, o_bo = 0, o_bnd = 0, o_list = 0, o_vb = 0, o_cstart = 0, o_ccount = 0;
   int n_bnd = 0;
+  size_t o_items = 0;  // CTAs of the per-body kernels (body_kernels.cuh body_of_item)
+  int n_items = 0;
   std::vector<int> tile;  // block size of each colour kernel (0 = default), set by the autotuner
   // cluster kernel: (colour, part) ranges of the elastic tets, colours with work
   size_t o_cloff = 0, o_clcol = 0, o_cllb = 0;
@@ -304,6 +306,9 @@ struct Solver final : SolverBase {
   std::vector<Obstacle> sim_obs;
   double sim_restitution = 1e-2;
   DevBuf d_obs, d_cmask, d_cverts, d_cidx, d_cscan, d_clam_dev;
+  // pinned staging of the per-layer contact lists of mlx_layer_solve
+  PinnedBuf h_cpack;
+  size_t cpack_used = 0;
   // buffers of mlx_find_contacts, kept across calls (they only grow)
   DevBuf fc_ob, fc_mask, fc_verts, fc_scan, fc_x, fc_pos, fc_vid, fc_out;
   DevContacts dev_contacts() const {
@@ -814,6 +819,24 @@ int Solver<R>::build_static(const mlx_layer_desc* ld, int col, LayerStatic& ls, 
   for (int c = 0; c < C; ++c) cstart[c] = ls.identity_list ? color_off[c] : ls.color_start[c];
   ls.o_cstart = put(cstart);
   ls.o_ccount = put(ls.color_count);
+  // CTAs of the per-body kernels: a body of more than kSmallBody vertices
+  // alone, the others kItemInts per CTA (one warp each) in body order
+  {
+    std::vector<int> items, small;
+    for (int b = 0; b < nb; ++b) {
+      if (bvo[b + 1] - bvo[b] > kSmallBody) {
+        items.push_back(b);
+        items.push_back(kLargeItem);
+        for (int q = 2; q < kItemInts; ++q) items.push_back(-1);
+      } else {
+        small.push_back(b);
+      }
+    }
+    for (size_t i = 0; i < small.size(); i += kItemInts)
+      for (int q = 0; q < kItemInts; ++q) items.push_back(i + q < small.size() ? small[i + q] : -1);
+    ls.n_items = (int)(items.size() / kItemInts);
+    ls.o_items = put(items);
+  }
   if (cluster_ok) {
     // the elastic list (or the identity) is in sorted order, which is
     // (colour, part) order on the cluster path
@@ -1054,8 +1077,9 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
     L.vert_body = dint + ls.o_vb;
     L.vert_rigid = ls.dev_rigid.as<unsigned char>();
     L.any_boundary = ls.n_bnd > 0;
+    L.n_items = ls.n_items;
+    L.items = dint + ls.o_items;
     // contact lists of this layer
-    std::vector<int> cpack;
     if (nK > 0) {
       const int32_t* rid = ls.rid.data();
       std::vector<int> rc_off(ls.nb + 1, 0), rc_ids;
@@ -1092,13 +1116,22 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
           if (group_of[k] >= 0) ec_ids[f[group_of[k]]++] = k;
       }
       size_t o_rco = 0, o_rci = rc_off.size(), o_eco = o_rci + rc_ids.size(), o_eci = o_eco + ec_off.size();
-      cpack.reserve(o_eci + ec_ids.size());
-      cpack.insert(cpack.end(), rc_off.begin(), rc_off.end());
-      cpack.insert(cpack.end(), rc_ids.begin(), rc_ids.end());
-      cpack.insert(cpack.end(), ec_off.begin(), ec_off.end());
-      cpack.insert(cpack.end(), ec_ids.begin(), ec_ids.end());
-      CHECK(d_cgroups.ensure(sizeof(int) * cpack.size()));
-      CU(cudaMemcpyAsync(d_cgroups.p, cpack.data(), sizeof(int) * cpack.size(), cudaMemcpyHostToDevice, stream));
+      // the lists go through pinned memory that no copy in flight reads: each
+      // layer of a call takes a new range (reset once the call has synchronised)
+      const size_t need = o_eci + ec_ids.size();
+      if (cpack_used + need > h_cpack.bytes / sizeof(int)) {
+        CU(cudaStreamSynchronize(stream));
+        CHECK(h_cpack.ensure(sizeof(int) * std::max(need, 2 * (h_cpack.bytes / sizeof(int)))));
+        cpack_used = 0;
+      }
+      int* cpack = h_cpack.as<int>() + cpack_used;
+      cpack_used += need;
+      std::copy(rc_off.begin(), rc_off.end(), cpack + o_rco);
+      std::copy(rc_ids.begin(), rc_ids.end(), cpack + o_rci);
+      std::copy(ec_off.begin(), ec_off.end(), cpack + o_eco);
+      std::copy(ec_ids.begin(), ec_ids.end(), cpack + o_eci);
+      CHECK(d_cgroups.ensure(sizeof(int) * need));
+      CU(cudaMemcpyAsync(d_cgroups.p, cpack, sizeof(int) * need, cudaMemcpyHostToDevice, stream));
       const int* dc = d_cgroups.as<int>();
       L.rc_off = dc + o_rco;
       L.rc_ids = dc + o_rci;
@@ -1125,7 +1158,7 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
     if (ls.nb > 0) {
       if (!capturing) CHECK(w.bodies.ensure(sizeof(Body) * ls.nb));
       else if (w.bodies.bytes < sizeof(Body) * ls.nb) return set_error(MLX_ERR_ARGUMENT, "body buffer not reserved");
-      k_make_rigids<R><<<ls.nb, 256, 0, stream>>>(L, w.bodies.as<Body>(), p, resv, d_vmass.as<double>(), ri);
+      k_make_rigids<R><<<ls.n_items, kBodyThreads, 0, stream>>>(L, w.bodies.as<Body>(), p, resv, d_vmass.as<double>(), ri);
       CU(cudaGetLastError());
       ++st.launches;
       if (&w == &sim_work && col == ws.col && layer == 0 && (ws.record || ws.mode)) {
@@ -1137,7 +1170,7 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
     CU(cudaGetLastError());
     ++st.launches;
     if (rigidLayer && ls.nb > 0) {
-      k_rigid_step<R><<<ls.nb, 256, 0, stream>>>(L, w.bodies.as<Body>(), p, xprev, resv, ri, h);
+      k_rigid_step<R><<<ls.n_items, kBodyThreads, 0, stream>>>(L, w.bodies.as<Body>(), p, xprev, resv, ri, h);
       CU(cudaGetLastError());
       ++st.launches;
     }
@@ -1169,7 +1202,8 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
                           L.n_ec_groups > 0 || dc.nobs > 0;
     // device-detected contacts: their number is only known on the device, so
     // the extra CTAs stride over it
-    const int ecBlocks = dc.nobs ? std::max(1, std::min(blocks_for(N, 128), 592)) : blocks_for(L.n_ec_groups, 128);
+    const int ecBlocks = dc.nobs ? std::max(1, std::min(blocks_for(N, kBodyThreads), 296))
+                                 : blocks_for(L.n_ec_groups, kBodyThreads);
     bool stopSolve = false;
     if ((persistent || (cluster_ok && ls.cl_ok)) && !P->compute_residuals && !dc.nobs) {
       // fixed iteration count: the whole projectGS loop of the layer in one launch
@@ -1191,11 +1225,10 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
         st.totalIterations += iters;
       }
       if (ls.nb > 0) {
-        k_finish_layer<R><<<ls.nb, 256, 0, stream>>>(L, w.bodies.as<Body>(), p, resv, ri, rigidLayer ? 1 : 0);
+        k_finish_layer<R><<<ls.n_items, kBodyThreads, 0, stream>>>(L, w.bodies.as<Body>(), p, resv, ri, rigidLayer ? 1 : 0);
         CU(cudaGetLastError());
         ++st.launches;
       }
-      if (nK > 0) CU(cudaStreamSynchronize(stream));  // cpack is a pageable host source
       continue;
     }
     cudaGraphConditionalHandle h_while_cur = 0;
@@ -1230,7 +1263,7 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
         tev_used += 2;
       }
       if (bodyWork) {
-        cudaLaunchConfig_t cfg = pdl_config(ls.nb + ecBlocks, 128);
+        cudaLaunchConfig_t cfg = pdl_config((ls.nb > 0 ? ls.n_items : 0) + ecBlocks, kBodyThreads);
         cudaLaunchAttribute attr = pdl_attr();
         cfg.attrs = &attr;
         cfg.numAttrs = pdl ? 1 : 0;
@@ -1285,12 +1318,11 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
       if (endLayer || stopSolve) break;
     }
     if (ls.nb > 0) {
-      k_finish_layer<R><<<ls.nb, 256, 0, stream>>>(L, w.bodies.as<Body>(), p, resv, ri, rigidLayer ? 1 : 0);
+      k_finish_layer<R><<<ls.n_items, kBodyThreads, 0, stream>>>(L, w.bodies.as<Body>(), p, resv, ri, rigidLayer ? 1 : 0);
       CU(cudaGetLastError());
       ++st.launches;
     }
     if (devmon) CHECK(cond_end(outer));  // end of the layer's IF body
-    if (nK > 0) CU(cudaStreamSynchronize(stream));  // cpack is a pageable host source
     if (stopSolve) break;
   }
   return MLX_OK;
@@ -1649,8 +1681,8 @@ template <typename R>
 int Solver<R>::layer_solve(const mlx_layer_desc* ld, const mlx_solve_params* P, const mlx_contacts* K,
                            const mlx_solve_inputs* in, mlx_solve_outputs* out) {
   if (!ld || !P || !in || !out) return set_error(MLX_ERR_ARGUMENT, "null argument");
-  if (!in->xi || !in->lambdai || !in->oldp || !in->residualv || !out->xi)
-    return set_error(MLX_ERR_ARGUMENT, "xi, lambdai, oldp, residualv and out->xi are required");
+  if (!in->xi || !in->oldp || !in->residualv || !out->xi)
+    return set_error(MLX_ERR_ARGUMENT, "xi, oldp, residualv and out->xi are required");
   if (!pinned.empty() && !in->pinnedx) return set_error(MLX_ERR_ARGUMENT, "pinnedx is NULL");
   CHECK(validate_layers(ld, P));
   if (in->residual_in_len < 1 && P->compute_residuals)
@@ -1659,23 +1691,29 @@ int Solver<R>::layer_solve(const mlx_layer_desc* ld, const mlx_solve_params* P, 
   DeviceGuard g(device);
   const size_t n3 = 3 * (size_t)N, n6 = 6 * (size_t)T, np = pinned.size();
   // ---- upload per-call vectors (one pinned staging copy) ----
-  size_t nst = n3 * 3 + n6 + np;
+  // Staged: xi, residualv, oldp when damping reads it, lambdai unless NULL
+  // (all zeros, what integrate passes), the pinned values.
+  const size_t o_old = 2 * n3, o_lam = o_old + (damp ? n3 : 0), o_pin = o_lam + (in->lambdai ? n6 : 0);
+  const size_t nst = std::max<size_t>(o_pin + np, n3 + (out->lambdai ? n6 : 0));
   CHECK(h_stage.ensure(sizeof(double) * nst));
   CHECK(d_stage.ensure(sizeof(double) * nst));
   double* hs = h_stage.as<double>();
   std::memcpy(hs, in->xi, sizeof(double) * n3);
-  std::memcpy(hs + n3, in->oldp, sizeof(double) * n3);
-  std::memcpy(hs + 2 * n3, in->residualv, sizeof(double) * n3);
-  std::memcpy(hs + 3 * n3, in->lambdai, sizeof(double) * n6);
-  if (np) std::memcpy(hs + 3 * n3 + n6, in->pinnedx, sizeof(double) * np);
-  CU(cudaMemcpyAsync(d_stage.p, hs, sizeof(double) * nst, cudaMemcpyHostToDevice, stream));
+  std::memcpy(hs + n3, in->residualv, sizeof(double) * n3);
+  if (damp) std::memcpy(hs + o_old, in->oldp, sizeof(double) * n3);
+  if (in->lambdai) std::memcpy(hs + o_lam, in->lambdai, sizeof(double) * n6);
+  if (np) std::memcpy(hs + o_pin, in->pinnedx, sizeof(double) * np);
+  CU(cudaMemcpyAsync(d_stage.p, hs, sizeof(double) * (o_pin + np), cudaMemcpyHostToDevice, stream));
   double* ds = d_stage.as<double>();
   const int bs = 256;
   k_load_pos<R><<<blocks_for(N, bs), bs, 0, stream>>>(ds, d_mass3.as<double>(), pos(), N);
-  if (damp) k_load_vec<R><<<blocks_for(N, bs), bs, 0, stream>>>(ds + n3, d_oldp.as<R4<R>>(), N);
-  k_load_vec<R><<<blocks_for(N, bs), bs, 0, stream>>>(ds + 2 * n3, d_resv.as<R4<R>>(), N);
-  k_load_lambda<R><<<blocks_for(T, bs), bs, 0, stream>>>(ds + 3 * n3, d_s2e.as<int>(), d_lambda.as<R>(), T);
-  if (np) k_cast<R><<<blocks_for((long long)np, bs), bs, 0, stream>>>(ds + 3 * n3 + n6, d_pinx.as<R>(), (int)np);
+  k_load_vec<R><<<blocks_for(N, bs), bs, 0, stream>>>(ds + n3, d_resv.as<R4<R>>(), N);
+  if (damp) k_load_vec<R><<<blocks_for(N, bs), bs, 0, stream>>>(ds + o_old, d_oldp.as<R4<R>>(), N);
+  if (in->lambdai)
+    k_load_lambda<R><<<blocks_for(T, bs), bs, 0, stream>>>(ds + o_lam, d_s2e.as<int>(), d_lambda.as<R>(), T);
+  else
+    CU(cudaMemsetAsync(d_lambda.p, 0, sizeof(R) * n6, stream));
+  if (np) k_cast<R><<<blocks_for((long long)np, bs), bs, 0, stream>>>(ds + o_pin, d_pinx.as<R>(), (int)np);
   CU(cudaGetLastError());
   ContactData cd;
   CHECK(upload_contacts(K, cd));
@@ -1693,6 +1731,7 @@ int Solver<R>::layer_solve(const mlx_layer_desc* ld, const mlx_solve_params* P, 
   CU(cudaGetLastError());
   CU(cudaMemcpyAsync(hs, ds, sizeof(double) * (out->lambdai ? n3 + n6 : n3), cudaMemcpyDeviceToHost, stream));
   CU(cudaStreamSynchronize(stream));
+  cpack_used = 0;  // no copy of the contact lists is in flight now
   CHECK(check_gsync());
   std::memcpy(out->xi, hs, sizeof(double) * n3);
   if (out->lambdai) std::memcpy(out->lambdai, hs + n3, sizeof(double) * n6);

@@ -316,7 +316,9 @@ def call_layer_solve(fn, solver_or_desc, layer_desc, params, contacts, xi, lambd
     N3 = xi.size
     keep = []
     arr = lambda a, dt=np.float64: keep.append(np.ascontiguousarray(a, dt)) or keep[-1]
-    xi_ = arr(xi); lam_ = _F(lambdai, np.float64); keep.append(lam_)
+    xi_ = arr(xi)
+    lam_ = None if lambdai is None else _F(lambdai, np.float64)  # None: zeros
+    keep.append(lam_)
     oldp_ = arr(oldp); oo_ = arr(oldOldp); f_ = arr(f); rv_ = arr(residualv)
     px_ = arr(pinnedx if pinnedx is not None else np.zeros(0)); rin = arr(residual_in)
     inp = SolveInputs()
@@ -327,6 +329,8 @@ def call_layer_solve(fn, solver_or_desc, layer_desc, params, contacts, xi, lambd
     cap = residual_capacity or (rin.size + 1 + max(0, params.hanging_stop if params.hanging_stop >= 0 else 0) +
                                 sum(int(layer_desc.iterations[i]) for i in range(layer_desc.num_layers)) + 100000)
     out_xi = np.zeros(N3)
+    if want_lambda and lam_ is None:
+        raise ValueError("want_lambda needs lambdai")
     out_lam = np.zeros(lam_.shape, order="F") if want_lambda else None
     out_res = np.zeros(cap)
     out = SolveOutputs()
@@ -372,13 +376,13 @@ def contact_velocity_update(normals, vertex_ids, v, h, gravity, dim=3, restituti
     if K == 0:
         return v
     e = np.full(K, restitution)
-    dofs = (np.asarray(vertex_ids, np.int64)[:, None] * dim - np.arange(dim - 1, -1, -1)[None, :]) - 1
-    vn = v[dofs]
+    rows = np.asarray(vertex_ids, np.int64).ravel() - 1  # the dofs of vertex k are row k of v as (N, dim)
+    vn = v.reshape(-1, dim)[rows]
     e[np.linalg.norm(vn, axis=1) <= 2 * gravity * h] = 0
     vt = np.sum(normals * vn, axis=1)
     dv = normals * (-vn + np.minimum(-e * vt, 0)[:, None])
     v = v.copy()
-    v[dofs] = vn + dv
+    v.reshape(-1, dim)[rows] = vn + dv  # repeated vertices: the last contact's value stays
     return v
 
 
@@ -483,6 +487,19 @@ class XpbdLayer3D:
         check("mlx_layer_solve", rc, lib)
         return res[0], res[1], res[2], res[3]
 
+    def _boundary_vertices(self, mesh, sets, num_rigids):
+        """findBoundaryVertices of this step's sets.  Fixed custom sets give
+        the same result every step, so it is kept while they and the mesh
+        stay the same."""
+        if self.customRigidSets is None:
+            return find_boundary_vertices(mesh, sets, num_rigids)
+        c = getattr(self, "_fbv", None)
+        if c is not None and c[0] is mesh and c[1].shape == sets.shape and np.array_equal(c[1], sets):
+            return c[2]
+        ls = find_boundary_vertices(mesh, sets, num_rigids)
+        self._fbv = (mesh, sets.copy(), ls)
+        return ls
+
     def integrate(self, mesh: Mesh3D, h: float, contacts: ContactSet, cache: StepCache, frame: int):
         """xpbdLayer3D.integrate (xpbdLayer3D.m:621-745)."""
         assert len(self.layers) and len(self.iterations)
@@ -497,7 +514,7 @@ class XpbdLayer3D:
         f = f + self.CustomForce
         mesh.f = f
         sets, numRigids = self.buildLayers(mesh, cache, h)
-        ls = find_boundary_vertices(mesh, sets, numRigids)
+        ls = self._boundary_vertices(mesh, sets, numRigids)
         cache.layers = ls.isRigidElement
         cache.oldOldp = cache.oldp
         cache.oldp = mesh.p.copy()
@@ -506,7 +523,7 @@ class XpbdLayer3D:
         up = mesh.unpinnedDOFs - 1
         resv[up] = resv[up] + h * f[up] / mesh.mass[up]
         resv = (1 - self.airDrag) * resv
-        lambdai = np.zeros((mesh.T, 6), order="F")
+        lambdai = None  # zeros(T, 6) (xpbdLayer3D.m:666): the library zeroes them on the device
         residualArray = np.array([0.0])
         ld, keep = pack_layer_desc(ls, self.layersMap, self.iterations)
         cts, keep2 = pack_contacts(contacts.normals, contacts.points, contacts.vertex_ids, contacts.compliance)
