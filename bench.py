@@ -206,7 +206,7 @@ def run_reference(args, rank, world):
 
 def run_ours(args, rank, world, local):
     import torch
-    from multilayersolver2024_b200 import MLX_FP32, StepCache, XpbdLayer3D, load
+    from multilayersolver2024_b200 import MLX_ENERGY_NEOHOOKEAN, MLX_FP32, StepCache, XpbdLayer3D, load
     from multilayersolver2024_b200.xpbd_layer3d import ContactSet, ResidentSim, Solver, find_boundary_vertices
 
     torch.cuda.set_device(local)
@@ -311,10 +311,13 @@ def run_ours(args, rank, world, local):
     e2e_s = max_over_ranks(e2e_s)
     N, T = m2.N, m2.T
     K = float(np.mean(contact_bytes)) if contact_bytes else 0.0
-    # layer solve: xi, oldp, v in (3 x 3N), lambda (6T), pinned x, contacts
-    # (normal, point, compliance, id: 7 x 8 + 4 bytes each); detection:
-    # positions in (3N), contact lists back
-    h2d = 8 * (3 * 3 * N + 6 * T + m2.pinnedDOFs.size) + 60 * K + (8 * 3 * N if sc2.contact_finders else 0)
+    # layer solve: xi and v in (2 x 3N; oldp too when the material is
+    # damped; lambdai is passed as zeros, NULL), pinned x, contacts (normal,
+    # point, compliance, id: 7 x 8 + 4 bytes each); detection: positions in
+    # (3N), contact lists back
+    damped = m2.energy_type != MLX_ENERGY_NEOHOOKEAN and bool(np.any(np.asarray(m2.alpha1) != 0))
+    h2d = (8 * ((3 if damped else 2) * 3 * N + m2.pinnedDOFs.size) + 60 * K
+           + (8 * 3 * N if sc2.contact_finders else 0))
     d2h = 8 * 3 * N + (60 * K if sc2.contact_finders else 0)
 
     # ---- iterations to residual 1e-4: the same workload with the residual
