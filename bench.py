@@ -390,8 +390,13 @@ def run_ours(args, rank, world, local):
     line = None
     if rank == 0:
         peak, peak_kind = measured_peak_hbm()
-        sweep_kernel = ("k_layer_cluster (whole projectGS loop of a layer)" if solver.launch_path.startswith("cluster")
-                        else "k_project_color (all colours of a sweep)")
+        if solver.launch_path.startswith("cluster"):
+            sweep_kernel = "k_layer_cluster (whole projectGS loop of a layer)"
+        elif "CTAs each owning whole components" in solver.launch_path:
+            sweep_kernel = ("k_layer_groups (whole projectGS loop of each body-free layer; algorithmic bytes without "
+                            "vertex records, which stay in shared memory) + k_project_color (layers with bodies)")
+        else:
+            sweep_kernel = "k_project_color (all colours of a sweep)"
         achieved = (sweep_bytes / (sweep_ms / 1000.0)) / 1e9 if sweep_ms > 0 else None
         cpu = None
         if world == 1 and not args.no_cpu_baseline:

@@ -16,6 +16,7 @@
 #include "body_kernels.cuh"
 #include "persistent.cuh"
 #include "cluster.cuh"
+#include "groups.cuh"
 #include "contacts.cuh"
 #include "monitor.cuh"
 #include "partition.h"
@@ -176,6 +177,10 @@ struct LayerStatic {
   int n_bnd = 0;
   size_t o_items = 0;  // CTAs of the per-body kernels (body_kernels.cuh body_of_item)
   int n_items = 0;
+  // component-group path (groups.cuh): (colour, group) ranges of the elastic tets
+  bool gr_ok = false;
+  int gr_one = 0;
+  size_t o_goff = 0;
   std::vector<int> tile;  // block size of each colour kernel (0 = default), set by the autotuner
   // cluster kernel: (colour, part) ranges of the elastic tets, colours with work
   size_t o_cloff = 0, o_clcol = 0, o_cllb = 0;
@@ -383,6 +388,21 @@ struct Solver final : SolverBase {
   std::vector<int> vowner;        // part owning each vertex
   long long cl_budget = 0;        // dynamic shared memory a CTA may use
   int plan_cluster(const mlx_mesh_desc* md, MeshPartition& mp);
+  // Component-group path (groups.cuh): a fixed-iteration layer without rigid
+  // bodies or host contacts runs as one launch, one CTA per group of
+  // consecutive vertex-disconnected components (records in shared memory).
+  // Chosen at mlx_create when the components are contiguous vertex and tet
+  // ranges, every group fits in a CTA's shared memory and the estimated sweep
+  // is shorter than with colour launches; MLXPBD_GROUPS=0 turns it off, =1
+  // skips the estimate.
+  bool groups_ok = false;
+  int gr_G = 0;
+  size_t gr_smem = 0;
+  std::vector<int> tgroup_sorted;  // group of each tet, sorted order
+  DevBuf d_gv0, d_tloc, d_gpin;
+  int plan_groups(const mlx_mesh_desc* md);
+  int launch_groups(const LayerStatic& ls, const int* dint, const mlx_solve_params* P, int iterations,
+                    const DevContacts& dc);
   int build_cluster_slots(LayerStatic& ls, const std::vector<int>& list);
   int launch_cluster(const LayerStatic& ls, const int* dint, const LayerDev& L, const ContactData& cd,
                      const mlx_solve_params* P, int iterations, bool body_work, LayerWork& w);
@@ -410,6 +430,7 @@ struct Solver final : SolverBase {
   double sweep_ms = 0, sweep_bytes = 0;
   long long sweep_launches = 0;
   double bytes_per_tet() const;
+  double group_bytes_per_tet() const;
   int record_event(cudaEvent_t e, bool capturing);
   int enable_sweep_timing(int on) override;
   int sweep_stats(double* ms, double* bytes, long long* launches, int reset) override;
@@ -427,6 +448,9 @@ struct Solver final : SolverBase {
   long long sim_launches_per_step() const override { return sim.launches_per_step; }
   std::string launch_path() const override {
     if (persistent) return "persistent cooperative kernel per layer (" + std::to_string(persist_ctas) + " CTAs)";
+    if (groups_ok && !cluster_ok)
+      return "body-free layers: one launch, " + std::to_string(gr_G) + " CTAs each owning whole components "
+             "(records in shared memory); other layers: one launch per colour (programmatic dependent launches)";
     if (cluster_ok)
       return "cluster kernel per layer: " + std::to_string(cl_size) + " CTAs x " + std::to_string(cl_threads) +
              " threads, vertex slots" + (cl_lam_slots ? " and multipliers" : "") + " in shared memory";
@@ -633,6 +657,7 @@ int Solver<R>::create(const mlx_mesh_desc* md) {
     CU(cudaMemcpyAsync(d_pin_dofs.p, pinned.data(), sizeof(int) * pinned.size(), cudaMemcpyHostToDevice, stream));
   vid_sorted = vid;
   if (cluster_ok) vowner = mp.vowner;
+  CHECK(plan_groups(md));
   if (md->mu && md->lambda) {
     pcg_G.resize(9 * (size_t)T);
     pcg_vol.resize(T);
@@ -737,6 +762,202 @@ int Solver<R>::plan_cluster(const mlx_mesh_desc* md, MeshPartition& mp) {
 }
 
 template <typename R>
+static const void* group_kernel(int mat_kind, bool damp) {
+  switch (mat_kind) {
+    case MAT_NH: return (const void*)k_layer_groups<R, MAT_NH, false>;
+    case MAT_STVK_BLOCKS:
+      return damp ? (const void*)k_layer_groups<R, MAT_STVK_BLOCKS, true>
+                  : (const void*)k_layer_groups<R, MAT_STVK_BLOCKS, false>;
+    default:
+      return damp ? (const void*)k_layer_groups<R, MAT_STVK_LAME, true>
+                  : (const void*)k_layer_groups<R, MAT_STVK_LAME, false>;
+  }
+}
+
+// Groups of consecutive vertex-disconnected components for the
+// component-group path: components must be ascending, contiguous vertex and
+// element ranges (a merged batch is).  A colour phase of a group costs about
+// one dependent chain of a tet projection (~2 us) per pass of the CTA over
+// the group's tets of that colour, so groups take components in order while
+// every colour still fits in one pass (and the records in shared memory); a
+// larger component stands alone.  The path is taken when the slowest group's
+// sweep is estimated shorter than the colour launches' (one dependent launch
+// per colour, ~2.6 us, plus the colour's bytes at ~6.5 TB/s).
+template <typename R>
+int Solver<R>::plan_groups(const mlx_mesh_desc* md) {
+  groups_ok = false;
+  const char* env = std::getenv("MLXPBD_GROUPS");
+  const bool off = env && std::string(env) == "0", force = env && std::string(env) == "1";
+  if (off || cluster_ok || persistent || T == 0) return MLX_OK;
+  // components (union-find over the tets' corners)
+  std::vector<int> parent(N);
+  for (int v = 0; v < N; ++v) parent[v] = v;
+  auto find = [&](int v) {
+    while (parent[v] != v) {
+      parent[v] = parent[parent[v]];
+      v = parent[v];
+    }
+    return v;
+  };
+  for (int e = 0; e < T; ++e) {
+    const int a = find(md->t[e] - 1);
+    for (int k = 1; k < 4; ++k) {
+      const int b = find(md->t[e + (size_t)k * T] - 1);
+      if (a != b) parent[std::max(a, b)] = std::min(a, b);
+    }
+  }
+  // component index of each vertex in order of first appearance; contiguous
+  // vertex ranges means the index never decreases along the vertices
+  std::vector<int> vcomp(N), cv0;
+  {
+    std::vector<int> label(N, -1);
+    for (int v = 0; v < N; ++v) {
+      const int r = find(v);
+      if (label[r] < 0) {
+        label[r] = (int)cv0.size();
+        cv0.push_back(v);
+      }
+      vcomp[v] = label[r];
+      if (v > 0 && vcomp[v] < vcomp[v - 1]) return MLX_OK;
+    }
+  }
+  const int ncomp = (int)cv0.size();
+  cv0.push_back(N);
+  // tets of every (component, colour)
+  std::vector<int> ccol((size_t)ncomp * C, 0), colcount(C, 0);
+  int lastc = 0;
+  for (int e = 0; e < T; ++e) {
+    const int c = vcomp[md->t[e] - 1];
+    if (c < lastc) return MLX_OK;  // elements are not grouped by component
+    lastc = c;
+    ++ccol[(size_t)c * C + md->element_color[e] - 1];
+    ++colcount[md->element_color[e] - 1];
+  }
+  int optin = 0, sms = 0;
+  CU(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+  CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  const void* fn = group_kernel<R>(mat_kind, damp);
+  cudaFuncAttributes fa;
+  CU(cudaFuncGetAttributes(&fa, fn));
+  const long long budget = (long long)optin - (long long)fa.sharedSizeBytes - 1024;
+  const long long vmax = budget / (long long)sizeof(R4<R>);
+  std::vector<int> gv0{0}, acc(C, 0);
+  long long gv = 0, max_gv = 0, max_passes = 0;
+  auto passes = [&]() {
+    long long n = 0;
+    for (int q = 0; q < C; ++q) n += (acc[q] + kGroupThreads - 1) / kGroupThreads;
+    return n;
+  };
+  for (int c = 0; c < ncomp; ++c) {
+    const long long nv = cv0[c + 1] - cv0[c];
+    if (nv > vmax) return MLX_OK;
+    bool fits = gv + nv <= vmax;
+    for (int q = 0; q < C && fits; ++q) fits = acc[q] + ccol[(size_t)c * C + q] <= kGroupThreads;
+    if (gv > 0 && !fits) {
+      gv0.push_back(cv0[c]);
+      max_gv = std::max(max_gv, gv);
+      max_passes = std::max(max_passes, passes());
+      std::fill(acc.begin(), acc.end(), 0);
+      gv = 0;
+    }
+    for (int q = 0; q < C; ++q) acc[q] += ccol[(size_t)c * C + q];
+    gv += nv;
+  }
+  gv0.push_back(N);
+  max_gv = std::max(max_gv, gv);
+  max_passes = std::max(max_passes, passes());
+  const int G = (int)gv0.size() - 1;
+  // estimated sweeps (us); one CTA per SM, so more groups than SMs run in waves
+  const double t_groups = 2.0 * (double)max_passes * (double)((G + sms - 1) / sms);
+  double t_colours = 0;
+  for (int q = 0; q < C; ++q)
+    if (colcount[q]) t_colours += 2.6 + (double)colcount[q] * (double)bytes_per_tet() / 6.5e6;
+  if (!force && t_groups >= t_colours) return MLX_OK;
+  // each group's pins must be one range of the pinned list, in group order
+  // (true when the list is ascending); a group applies its range in order
+  std::vector<int> gpin(G + 1, 0);
+  {
+    int lastg = 0;
+    for (size_t i = 0; i < pinned.size(); ++i) {
+      const int g = (int)(std::upper_bound(gv0.begin(), gv0.end(), pinned[i] / 3) - gv0.begin()) - 1;
+      if (g < lastg) return MLX_OK;
+      lastg = g;
+      ++gpin[g + 1];
+    }
+    for (int q = 0; q < G; ++q) gpin[q + 1] += gpin[q];
+  }
+  // group of every tet (sorted order) and its corner slots
+  tgroup_sorted.assign(T, 0);
+  std::vector<int4> tloc(T);
+  for (int sidx = 0; sidx < T; ++sidx) {
+    const int4 v = vid_sorted[sidx];
+    const int g = (int)(std::upper_bound(gv0.begin(), gv0.end(), v.x) - gv0.begin()) - 1;
+    tgroup_sorted[sidx] = g;
+    const int b = gv0[g];
+    tloc[sidx] = make_int4(v.x - b, v.y - b, v.z - b, v.w - b);
+  }
+  gr_smem = (size_t)max_gv * sizeof(R4<R>);
+  CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(gr_smem, 16)));
+  CHECK(d_gv0.ensure(sizeof(int) * gv0.size()));
+  CHECK(d_tloc.ensure(sizeof(int4) * (size_t)T));
+  CHECK(d_gpin.ensure(sizeof(int) * gpin.size()));
+  CU(cudaMemcpyAsync(d_gv0.p, gv0.data(), sizeof(int) * gv0.size(), cudaMemcpyHostToDevice, stream));
+  CU(cudaMemcpyAsync(d_tloc.p, tloc.data(), sizeof(int4) * (size_t)T, cudaMemcpyHostToDevice, stream));
+  CU(cudaMemcpyAsync(d_gpin.p, gpin.data(), sizeof(int) * gpin.size(), cudaMemcpyHostToDevice, stream));
+  CU(cudaStreamSynchronize(stream));
+  gr_G = G;
+  groups_ok = true;
+  return MLX_OK;
+}
+
+template <typename R>
+int Solver<R>::launch_groups(const LayerStatic& ls, const int* dint, const mlx_solve_params* P, int iterations,
+                             const DevContacts& dc) {
+  GroupArgs ga;
+  ga.list = ls.identity_list ? nullptr : dint + ls.o_list;
+  ga.off = dint + ls.o_goff;
+  ga.gv0 = d_gv0.as<int>();
+  ga.tloc = d_tloc.as<int4>();
+  ga.pin_off = d_gpin.as<int>();
+  ga.pin_dofs = d_pin_dofs.as<int>();
+  ga.C = C;
+  ga.G = gr_G;
+  ga.iterations = iterations;
+  ga.one_per_thread = ls.gr_one;
+  const R hR = (R)P->h;
+  const R inv_h2 = R(1) / (hR * hR), inv_h = R(1) / hR;
+  TetData<R> td = tets();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(gr_G);
+  cfg.blockDim = dim3(kGroupThreads);
+  cfg.dynamicSmemBytes = gr_smem;
+  cfg.stream = stream;
+  const R4<R>* oldp = d_oldp.as<R4<R>>();
+  const R* pv = d_pinx.as<R>();
+  const double h = P->h, cr = P->contact_resistance;
+  cudaError_t e;
+  switch (mat_kind) {
+    case MAT_NH:
+      e = cudaLaunchKernelEx(&cfg, k_layer_groups<R, MAT_NH, false>, td, ga, pos(), oldp, inv_h2, inv_h, dc, oldp, h,
+                             cr, pv);
+      break;
+    case MAT_STVK_BLOCKS:
+      e = damp ? cudaLaunchKernelEx(&cfg, k_layer_groups<R, MAT_STVK_BLOCKS, true>, td, ga, pos(), oldp, inv_h2,
+                                    inv_h, dc, oldp, h, cr, pv)
+               : cudaLaunchKernelEx(&cfg, k_layer_groups<R, MAT_STVK_BLOCKS, false>, td, ga, pos(), oldp, inv_h2,
+                                    inv_h, dc, oldp, h, cr, pv);
+      break;
+    default:
+      e = damp ? cudaLaunchKernelEx(&cfg, k_layer_groups<R, MAT_STVK_LAME, true>, td, ga, pos(), oldp, inv_h2,
+                                    inv_h, dc, oldp, h, cr, pv)
+               : cudaLaunchKernelEx(&cfg, k_layer_groups<R, MAT_STVK_LAME, false>, td, ga, pos(), oldp, inv_h2,
+                                    inv_h, dc, oldp, h, cr, pv);
+  }
+  if (e != cudaSuccess) return set_error(MLX_ERR_CUDA, std::string("group layer launch: ") + cudaGetErrorString(e));
+  return MLX_OK;
+}
+
+template <typename R>
 int Solver<R>::build_static(const mlx_layer_desc* ld, int col, LayerStatic& ls, bool capturing) {
   const uint8_t* isE = ld->is_elastic_element + (size_t)T * col;
   const uint8_t* isR = ld->is_rigid_element + (size_t)T * col;
@@ -836,6 +1057,44 @@ int Solver<R>::build_static(const mlx_layer_desc* ld, int col, LayerStatic& ls, 
       for (int q = 0; q < kItemInts; ++q) items.push_back(i + q < small.size() ? small[i + q] : -1);
     ls.n_items = (int)(items.size() / kItemInts);
     ls.o_items = put(items);
+  }
+  // (colour, group) ranges of the elastic tets for the component-group path:
+  // within a colour the elastic tets are in element order, so each group's
+  // are one range when the groups are ascending element ranges
+  ls.gr_ok = false;
+  if (groups_ok) {
+    const int G = gr_G;
+    std::vector<int> goff((size_t)C * G + 1, 0);
+    bool mono = true;
+    int maxr = 0;
+    for (int c = 0; c < C && mono; ++c) {
+      const int b = ls.identity_list ? color_off[c] : ls.color_start[c];
+      const int n = ls.color_count[c];
+      int last = -1;
+      for (int q = 0; q < n; ++q) {
+        const int sidx = ls.identity_list ? b + q : list[b + q];
+        const int g = tgroup_sorted[sidx];
+        if (g < last) { mono = false; break; }
+        last = g;
+        ++goff[(size_t)c * G + g + 1];
+      }
+    }
+    if (mono) {
+      for (size_t q = 1; q < goff.size(); ++q) maxr = std::max(maxr, goff[q]);
+      // counts -> starts (in list positions, or sorted ids for the identity)
+      for (int c = 0; c < C; ++c) {
+        int run = ls.identity_list ? color_off[c] : ls.color_start[c];
+        for (int g = 0; g < G; ++g) {
+          const int cnt = goff[(size_t)c * G + g + 1];
+          goff[(size_t)c * G + g] = run;
+          run += cnt;
+        }
+      }
+      goff[(size_t)C * G] = ls.identity_list ? T : (int)list.size();
+      ls.gr_one = maxr <= kGroupThreads ? 1 : 0;
+      ls.o_goff = put(goff);
+      ls.gr_ok = true;
+    }
   }
   if (cluster_ok) {
     // the elastic list (or the identity) is in sorted order, which is
@@ -1228,6 +1487,27 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
         k_finish_layer<R><<<ls.n_items, kBodyThreads, 0, stream>>>(L, w.bodies.as<Body>(), p, resv, ri, rigidLayer ? 1 : 0);
         CU(cudaGetLastError());
         ++st.launches;
+      }
+      continue;
+    }
+    if (groups_ok && ls.gr_ok && ls.nb == 0 && nK == 0 && !P->compute_residuals) {
+      // a body-free layer with a fixed iteration count: one launch, a CTA per
+      // group of components
+      const int iters = std::max(ld->iterations[layer], 0);
+      if (iters > 0) {
+        const bool timed = sweep_timing && tev_used + 2 <= tev.size();
+        if (timed) CHECK(record_event(tev[tev_used], capturing));
+        CHECK(launch_groups(ls, dint, P, iters, dc));
+        if (timed) {
+          double b = 0;
+          for (int c = 0; c < C; ++c) b += ls.color_count[c] * (group_bytes_per_tet() + (ls.identity_list ? 0.0 : 4.0));
+          CHECK(record_event(tev[tev_used + 1], capturing));
+          tev_bytes[tev_used / 2] = b * iters + 2.0 * (double)N * sizeof(R4<R>);
+          tev_launches[tev_used / 2] = 1;
+          tev_used += 2;
+        }
+        ++st.launches;
+        st.totalIterations += iters;
       }
       continue;
     }
@@ -2416,6 +2696,19 @@ double Solver<R>::bytes_per_tet() const {
   const double vol = mat_kind == MAT_NH ? 0 : r;  // Neo-Hookean compliances include the volume
   double b = 16 + 9 * r + vol + mat_stride(mat_kind) * r + 2 * nl * r + 8 * 4 * r;
   if (damp) b += 4 * 4 * r;
+  return b;
+}
+
+template <typename R>
+double Solver<R>::group_bytes_per_tet() const {
+  // the component-group path keeps the vertex records in shared memory: per
+  // tet projection, corner slots, DmInv, volume, material and lambda read +
+  // write (+ vertex ids and four step-start records with Rayleigh damping)
+  const double r = sizeof(R);
+  const int nl = mat_kind == MAT_NH ? 2 : 6;
+  const double vol = mat_kind == MAT_NH ? 0 : r;
+  double b = 16 + 9 * r + vol + mat_stride(mat_kind) * r + 2 * nl * r;
+  if (damp) b += 16 + 4 * 4 * r;
   return b;
 }
 
