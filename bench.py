@@ -41,6 +41,9 @@ WORKLOADS = {
         "3352014 tets) merged into one mesh (colours overlaid as Mesh3D.mergeMesh), E log-uniform [1e4,1e6], "
         "nu=0.35, coarse 4^3-cube rigid clusters (5 it) + fine layer (10 it), dt=1/60, bases pinned, "
         "seeded surface impulses, per-colour tiles autotuned"),
+    5: ("config5: learned warm-start workload, Neo-Hookean block 64x32x32 cubes (70785 vertices, 393216 tets), "
+        "E log-uniform [1e4,1e7], nu [0.25,0.45], 3 layers (8^3-cube clusters 5 it, 4^3-cube clusters 5 it, fine 10 it), "
+        "dt=1/60, base pinned, seeded surface impulse at t=0"),
     4: ("config4: contact-heavy drop, 32 StVK boxes of 12^3 cubes (70304 vertices, 331776 tets), E=5e5, nu=0.3, "
         "seeded rotations and heights 0.5-3 m over a ground plane + 4 analytic spheres (r 0.3-0.6 m), contacts "
         "detected on the device every step, 3 layers (4^3-cube clusters 1 it, 2^3-cube clusters 4 it, fine 10 it), "
@@ -127,7 +130,14 @@ CONFIG = 2
 
 def make_scene():
     from multilayersolver2024_b200 import scenes
-    return {2: scenes.config2, 3: scenes.config3, 4: scenes.config4}[CONFIG]()
+    return {2: scenes.config2, 3: scenes.config3, 4: scenes.config4, 5: scenes.config5}[CONFIG]()
+
+
+def make_training_scene():
+    """Another seed of the workload's scene class (other materials and
+    impulse): the warm start's network is trained on its solver records."""
+    from multilayersolver2024_b200 import scenes
+    return {2: lambda: scenes.config2(seed=3), 5: lambda: scenes.config5(seed=6)}[CONFIG]()
 
 
 def start_velocity(scene, m):
@@ -324,7 +334,6 @@ def run_ours(args, rank, world, local):
     # monitor and stop rules on the device (conditional graph nodes) ----
     to_res = None
     if not args.no_residual_leg:
-        from multilayersolver2024_b200 import scenes as _scenes
         from multilayersolver2024_b200.learned import collect_warm_start_data, fit_warm_start
 
         def residual_sim(scene):
@@ -363,10 +372,10 @@ def run_ours(args, rank, world, local):
         p_plain = sim_p.state()[0]
         solver_p.close()
         learned_leg = None
-        if CONFIG == 2 and args.learned_train_steps > 0:
+        if CONFIG in (2, 5) and args.learned_train_steps > 0:
             # the warm start's network is trained on another seed of the same
             # scene class, then steps the benchmark scene
-            solver_t, sim_t = residual_sim(_scenes.config2(seed=3))
+            solver_t, sim_t = residual_sim(make_training_scene())
             ftr, ttr, _ = collect_warm_start_data(sim_t, args.learned_train_steps)
             solver_t.close()
             t0 = time.perf_counter()
@@ -377,7 +386,8 @@ def run_ours(args, rank, world, local):
             learned_leg = run_leg(sim_w, args.residual_steps)
             learned_leg.update({
                 "training": {"samples": int(ftr.shape[0]), "steps_recorded": args.learned_train_steps,
-                             "scene": "config2 seed 3", "epochs": 300, "seconds": train_s,
+                             "scene": f"config{CONFIG} seed {3 if CONFIG == 2 else 6}", "epochs": 300,
+                             "seconds": train_s,
                              "loss_first_last": [float(losses[0]), float(losses[-1])]},
                 "max_position_deviation_from_plain": float(np.abs(sim_w.state()[0] - p_plain).max()
                                                            / make_scene().mesh.bbox_diagonal())})
@@ -466,8 +476,9 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-API leg (profiling runs)")
-    ap.add_argument("--config", type=int, choices=[2, 3, 4], default=2,
-                    help="2: the plain multi-layer block (default); 3: the 256-scene batch; 4: the contact-heavy drop")
+    ap.add_argument("--config", type=int, choices=[2, 3, 4, 5], default=2,
+                    help="2: the plain multi-layer block (default); 3: the 256-scene batch; 4: the contact-heavy drop; "
+                    "5: the learned warm-start workload (64x32x32, 3 layers)")
     ap.add_argument("--autotune", action="store_true", help="run the per-colour tile autotuner before timing "
                     "(on by default for config 3)")
     ap.add_argument("--no-autotune", action="store_true", help="never run the autotuner (profiling runs)")

@@ -122,6 +122,32 @@ def config2(seed: int = 2, nx=64, ny=16, nz=16, cluster=8) -> Scene:
                  impulse=(dofs, dv.ravel()))
 
 
+def config5(seed: int = 5, nx=64, ny=32, nz=32, coarse=8, mid=4) -> Scene:
+    """The learned warm start's workload: the config-2 scene class at
+    64x32x32 cubes (70,785 vertices, 393,216 tets), per-tet E log-uniform in
+    [1e4, 1e7], nu uniform in [0.25, 0.45], Neo-Hookean, base pinned, seeded
+    surface impulse; three layers -- coarse^3-cube clusters (5 iterations),
+    mid^3-cube clusters (5), fine (10) -- dt = 1/60.  Other seeds give the
+    training scenes (other materials and impulses)."""
+    rng = np.random.default_rng(seed)
+    V, T, cube = generate_beam(nx, ny, nz, 0.1)
+    nt = T.shape[0]
+    E = np.exp(rng.uniform(np.log(1e4), np.log(1e7), nt))
+    nu = rng.uniform(0.25, 0.45, nt)
+    mu, lam = to_lame(nu, E)
+    m = Mesh3D.from_arrays(V, T, mu, lam, rho=1000.0, alpha1=0.0, energy_type=_lib.MLX_ENERGY_NEOHOOKEAN)
+    m.pin(np.nonzero(np.isclose(V[:, 2], 0.0))[0] + 1)
+    forced = np.zeros(nt, dtype=bool)
+    forced[m.pinnedTets - 1] = True
+    sc = cluster_rigid_sets(cube, (nx, ny, nz), coarse, forced)
+    sm = cluster_rigid_sets(cube, (nx, ny, nz), mid, forced)
+    sets = np.asfortranarray(np.stack([np.zeros(nt, np.int32), sm, sc], 1))  # sorted columns: [fine, mid, coarse]
+    patch, dv = _surface_impulse(rng, V, nz * 0.1)
+    dofs = np.stack([patch * 3 + 1, patch * 3 + 2, patch * 3 + 3], 1).ravel().astype(np.int32)
+    return Scene(f"config5_nh_block_{nx}x{ny}x{nz}", m, 1.0 / 60.0, 300, [50, 25, 0], [5, 5, 10], custom_sets=sets,
+                 impulse=(dofs, dv.ravel()))
+
+
 def _surface_impulse(rng, V, top_z, radius=0.4):
     """A seeded velocity on a patch of the top surface (0-based vertex ids)."""
     top = np.nonzero(np.isclose(V[:, 2], top_z))[0]
