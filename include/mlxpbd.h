@@ -301,6 +301,25 @@ int mlx_sim_contact_count(mlx_solver* solver, int32_t* num_contact_vertices);
  * description. */
 int mlx_pcg_solve(mlx_solver* solver, double h, const double* b, int32_t iterations, double* x, double* resvec);
 
+/* xpbdLayer3D.buildLayers (3d/integrator/xpbdLayer3D.m:601-619) followed by
+ * xpbdLayer2D.findBoundaryVertices (2d/integrator/xpbdLayer2D.m:551-569) on
+ * the device, replacing mexEdiffNorm3D + sort + mexUnionFindByVertice and
+ * the mask computation of the host.  ordering 0: strain-rate order of p and
+ * oldp (3N each, host) with the mesh's DmInv (9 values per element, as in
+ * mlx_mesh_desc; copied to the device once per pointer) and step h;
+ * ordering 1: `order` (T, 1-based element ids, e.g. a random permutation).
+ * sorted_layers: ascending layer percentages (num_layers); forced_elastic:
+ * T flags (pinned tets).  Outputs (host, column-major, one column per sorted
+ * layer): rigidBodySetsPerLayer (T x L, 0 = elastic, bodies numbered by
+ * their smallest element), numRigids (L), isElasticElement (T x L),
+ * isBoundaryVertex, isRigidVertex (N x L), vertexRigidBody (N x L); the four
+ * mask outputs may be NULL.  Results are the bits of the host builder. */
+int mlx_build_layers(mlx_solver* solver, const double* p, const double* oldp, double h, int32_t ordering,
+                     const int32_t* order, const double* DmInv, const double* sorted_layers, int32_t num_layers,
+                     const uint8_t* forced_elastic, int32_t* rigid_body_sets, int32_t* num_rigids,
+                     uint8_t* is_elastic_element, uint8_t* is_boundary_vertex, uint8_t* is_rigid_vertex,
+                     int32_t* vertex_rigid_body);
+
 /* ---- learned warm start: the perceptron ----------------------------------
  * No counterpart in the reference.  n_in -> n_hidden (GELU) x
  * n_hidden_layers -> n_out, BF16 weights and activations with FP32

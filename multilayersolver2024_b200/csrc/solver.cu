@@ -17,12 +17,16 @@
 #include "persistent.cuh"
 #include "cluster.cuh"
 #include "groups.cuh"
+#include "layers_dev.cuh"
 #include "contacts.cuh"
 #include "monitor.cuh"
 #include "partition.h"
 #include "warmstart.cuh"
 #include "pcg.cuh"
 #include "solver.h"
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <cstddef>
@@ -401,6 +405,15 @@ struct Solver final : SolverBase {
   std::vector<int> tgroup_sorted;  // group of each tet, sorted order
   DevBuf d_gv0, d_tloc, d_gpin;
   int plan_groups(const mlx_mesh_desc* md);
+  // buildLayers + findBoundaryVertices on the device (layers_dev.cuh)
+  DevBuf lb_p, lb_oldp, lb_dminv, lb_norms, lb_norms_sorted, lb_elems, lb_order, lb_rank, lb_forced, lb_parent,
+      lb_rep, lb_root, lb_flag, lb_scan, lb_sets, lb_key, lb_touch, lb_isE, lb_isBV, lb_isRV, lb_body, lb_small,
+      lb_tmp;
+  const double* lb_dminv_src = nullptr;  // host DmInv the device copy was made from
+  int build_layers(const double* p, const double* oldp, double h, int ordering, const int32_t* order,
+                   const double* dminv, const double* sorted_layers, int L, const uint8_t* forced, int32_t* sets,
+                   int32_t* num_rigids, uint8_t* is_elastic, uint8_t* is_boundary, uint8_t* is_rigid_vertex,
+                   int32_t* vertex_body) override;
   int launch_groups(const LayerStatic& ls, const int* dint, const mlx_solve_params* P, int iterations,
                     const DevContacts& dc);
   int build_cluster_slots(LayerStatic& ls, const std::vector<int>& list);
@@ -954,6 +967,132 @@ int Solver<R>::launch_groups(const LayerStatic& ls, const int* dint, const mlx_s
                                     inv_h, dc, oldp, h, cr, pv);
   }
   if (e != cudaSuccess) return set_error(MLX_ERR_CUDA, std::string("group layer launch: ") + cudaGetErrorString(e));
+  return MLX_OK;
+}
+
+__global__ void k_iota(int* __restrict__ a, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = i;
+}
+__global__ void k_last_count(const int* __restrict__ scan, const int* __restrict__ flag, int T, int* __restrict__ out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *out = T > 0 ? scan[T - 1] + flag[T - 1] : 0;
+}
+
+template <typename R>
+int Solver<R>::build_layers(const double* p, const double* oldp, double h, int ordering, const int32_t* order,
+                            const double* dminv, const double* sorted_layers, int L, const uint8_t* forced,
+                            int32_t* sets, int32_t* num_rigids, uint8_t* is_elastic, uint8_t* is_boundary,
+                            uint8_t* is_rigid_vertex, int32_t* vertex_body) {
+  if (!sorted_layers || !forced || !sets || !num_rigids || L < 1)
+    return set_error(MLX_ERR_ARGUMENT, "bad layer-builder arguments");
+  if (ordering == 0 && (!p || !oldp || !dminv || !(h > 0)))
+    return set_error(MLX_ERR_ARGUMENT, "strain-rate ordering needs p, oldp, DmInv and h > 0");
+  if (ordering == 1 && !order) return set_error(MLX_ERR_ARGUMENT, "ordering 1 needs the order");
+  if (ordering != 0 && ordering != 1) return set_error(MLX_ERR_ARGUMENT, "ordering must be 0 or 1");
+  for (int l = 1; l < L; ++l)
+    if (sorted_layers[l] < sorted_layers[l - 1]) return set_error(MLX_ERR_ARGUMENT, "layers must be ascending");
+  if (T == 0 || N == 0) {
+    for (int l = 0; l < L; ++l) num_rigids[l] = 0;
+    return MLX_OK;
+  }
+  DeviceGuard g(device);
+  const int bs = 256, tb = blocks_for(T, bs), nbk = blocks_for(N, bs);
+  CHECK(lb_order.ensure(sizeof(int) * std::max(T, 1)));
+  CHECK(lb_rank.ensure(sizeof(int) * std::max(T, 1)));
+  CHECK(lb_forced.ensure(std::max(T, 1)));
+  CHECK(lb_parent.ensure(sizeof(int) * std::max(T, 1)));
+  CHECK(lb_root.ensure(sizeof(int) * std::max(T, 1)));
+  CHECK(lb_flag.ensure(sizeof(int) * std::max(T, 1)));
+  CHECK(lb_scan.ensure(sizeof(int) * std::max(T, 1)));
+  CHECK(lb_sets.ensure(sizeof(int32_t) * std::max<size_t>((size_t)T * L, 1)));
+  CHECK(lb_isE.ensure(std::max<size_t>((size_t)T * L, 1)));
+  CHECK(lb_rep.ensure(sizeof(int) * std::max(N, 1)));
+  CHECK(lb_key.ensure(sizeof(int) * std::max(N, 1)));
+  CHECK(lb_touch.ensure(sizeof(int) * std::max(N, 1)));
+  CHECK(lb_isBV.ensure(std::max<size_t>((size_t)N * L, 1)));
+  CHECK(lb_isRV.ensure(std::max<size_t>((size_t)N * L, 1)));
+  CHECK(lb_body.ensure(sizeof(int32_t) * std::max<size_t>((size_t)N * L, 1)));
+  CHECK(lb_small.ensure(sizeof(int) * (size_t)(L + 1)));
+  int* err = lb_small.as<int>() + L;
+  CU(cudaMemsetAsync(lb_small.p, 0, sizeof(int) * (size_t)(L + 1), stream));
+  CU(cudaMemcpyAsync(lb_forced.p, forced, T, cudaMemcpyHostToDevice, stream));
+  const int4* vid = d_vid.as<int4>();
+  const int* s2e_d = d_s2e.as<int>();
+  // ---- the order ----
+  if (ordering == 0) {
+    CHECK(lb_p.ensure(sizeof(double) * 3 * (size_t)N));
+    CHECK(lb_oldp.ensure(sizeof(double) * 3 * (size_t)N));
+    CHECK(lb_norms.ensure(sizeof(double) * std::max(T, 1)));
+    CHECK(lb_norms_sorted.ensure(sizeof(double) * std::max(T, 1)));
+    CHECK(lb_elems.ensure(sizeof(int) * std::max(T, 1)));
+    if (dminv != lb_dminv_src || !lb_dminv.p) {
+      CHECK(lb_dminv.ensure(sizeof(double) * 9 * (size_t)T));
+      CU(cudaMemcpyAsync(lb_dminv.p, dminv, sizeof(double) * 9 * (size_t)T, cudaMemcpyHostToDevice, stream));
+      lb_dminv_src = dminv;
+    }
+    CU(cudaMemcpyAsync(lb_p.p, p, sizeof(double) * 3 * (size_t)N, cudaMemcpyHostToDevice, stream));
+    CU(cudaMemcpyAsync(lb_oldp.p, oldp, sizeof(double) * 3 * (size_t)N, cudaMemcpyHostToDevice, stream));
+    const double inv_h2 = 1.0 / (h * h);
+    k_strain_rate_norms<<<tb, bs, 0, stream>>>(vid, s2e_d, T, lb_dminv.as<double>(), lb_p.as<double>(),
+                                               lb_oldp.as<double>(), inv_h2, lb_norms.as<double>(),
+                                               lb_elems.as<int>());
+    CU(cudaGetLastError());
+    // stable ascending sort of (measure, element): the order of sort(...,"ascend")
+    size_t tmp = 0;
+    CU(cub::DeviceRadixSort::SortPairs(nullptr, tmp, lb_norms.as<double>(), lb_norms_sorted.as<double>(),
+                                       lb_elems.as<int>(), lb_order.as<int>(), T, 0, 64, stream));
+    CHECK(lb_tmp.ensure(std::max<size_t>(tmp, 16)));
+    CU(cub::DeviceRadixSort::SortPairs(lb_tmp.p, tmp, lb_norms.as<double>(), lb_norms_sorted.as<double>(),
+                                       lb_elems.as<int>(), lb_order.as<int>(), T, 0, 64, stream));
+  } else {
+    std::vector<int> o(T);
+    for (int q = 0; q < T; ++q) {
+      o[q] = order[q] - 1;
+      if (o[q] < 0 || o[q] >= T) return set_error(MLX_ERR_ARGUMENT, "order entry out of range");
+    }
+    CU(cudaMemcpyAsync(lb_order.p, o.data(), sizeof(int) * (size_t)T, cudaMemcpyHostToDevice, stream));
+    CU(cudaStreamSynchronize(stream));  // o is a pageable host source
+  }
+  k_order_rank<<<tb, bs, 0, stream>>>(lb_order.as<int>(), T, lb_rank.as<int>());
+  CU(cudaGetLastError());
+  size_t stmp = 0;
+  CU(cub::DeviceScan::ExclusiveSum(nullptr, stmp, lb_flag.as<int>(), lb_scan.as<int>(), T, stream));
+  if (lb_tmp.bytes < stmp) CHECK(lb_tmp.ensure(stmp));
+  // ---- every layer ----
+  for (int l = 0; l < L; ++l) {
+    const int end = std::min((int)std::floor((sorted_layers[l] / 100.0) * T), T);
+    int32_t* sl = lb_sets.as<int32_t>() + (size_t)T * l;
+    CU(cudaMemsetAsync(lb_rep.p, 0x7f, sizeof(int) * (size_t)N, stream));
+    k_uf_init<<<tb, bs, 0, stream>>>(lb_rank.as<int>(), lb_forced.as<uint8_t>(), T, end, lb_parent.as<int>());
+    k_uf_rep<<<tb, bs, 0, stream>>>(vid, s2e_d, T, lb_parent.as<int>(), lb_rep.as<int>());
+    k_uf_unite<<<tb, bs, 0, stream>>>(vid, s2e_d, T, lb_parent.as<int>(), lb_rep.as<int>(), err);
+    k_uf_roots<<<tb, bs, 0, stream>>>(T, lb_parent.as<int>(), lb_root.as<int>(), lb_flag.as<int>(), err);
+    CU(cudaGetLastError());
+    size_t st2 = lb_tmp.bytes;
+    CU(cub::DeviceScan::ExclusiveSum(lb_tmp.p, st2, lb_flag.as<int>(), lb_scan.as<int>(), T, stream));
+    k_uf_label<<<tb, bs, 0, stream>>>(T, lb_root.as<int>(), lb_scan.as<int>(), sl);
+    k_last_count<<<1, 32, 0, stream>>>(lb_scan.as<int>(), lb_flag.as<int>(), T, lb_small.as<int>() + l);
+    // findBoundaryVertices of this layer
+    CU(cudaMemsetAsync(lb_key.p, 0xff, sizeof(int) * (size_t)N, stream));
+    CU(cudaMemsetAsync(lb_touch.p, 0, sizeof(int) * (size_t)N, stream));
+    k_bv_keys<<<tb, bs, 0, stream>>>(vid, s2e_d, T, sl, lb_key.as<int>(), lb_touch.as<int>());
+    k_bv_masks<<<nbk, bs, 0, stream>>>(N, T, sl, lb_key.as<int>(), lb_touch.as<int>(),
+                                       lb_isBV.as<uint8_t>() + (size_t)N * l, lb_isRV.as<uint8_t>() + (size_t)N * l,
+                                       lb_body.as<int32_t>() + (size_t)N * l);
+    k_elastic_mask<<<tb, bs, 0, stream>>>(T, sl, lb_isE.as<uint8_t>() + (size_t)T * l);
+    CU(cudaGetLastError());
+  }
+  std::vector<int> small(L + 1);
+  CU(cudaMemcpyAsync(small.data(), lb_small.p, sizeof(int) * (size_t)(L + 1), cudaMemcpyDeviceToHost, stream));
+  CU(cudaMemcpyAsync(sets, lb_sets.p, sizeof(int32_t) * (size_t)T * L, cudaMemcpyDeviceToHost, stream));
+  if (is_elastic) CU(cudaMemcpyAsync(is_elastic, lb_isE.p, (size_t)T * L, cudaMemcpyDeviceToHost, stream));
+  if (is_boundary) CU(cudaMemcpyAsync(is_boundary, lb_isBV.p, (size_t)N * L, cudaMemcpyDeviceToHost, stream));
+  if (is_rigid_vertex) CU(cudaMemcpyAsync(is_rigid_vertex, lb_isRV.p, (size_t)N * L, cudaMemcpyDeviceToHost, stream));
+  if (vertex_body)
+    CU(cudaMemcpyAsync(vertex_body, lb_body.p, sizeof(int32_t) * (size_t)N * L, cudaMemcpyDeviceToHost, stream));
+  CU(cudaStreamSynchronize(stream));
+  if (small[L]) return set_error(MLX_ERR_LIMIT, "union-find step bound reached");
+  for (int l = 0; l < L; ++l) num_rigids[l] = small[l];
   return MLX_OK;
 }
 
@@ -3057,6 +3196,16 @@ int mlx_sim_warm_start(mlx_solver* s, int32_t record, int32_t mode, mlx_mlp* net
 int mlx_sim_warm_start_fetch(mlx_solver* s, float* features, float* targets, int32_t capacity, int32_t* num_clusters) {
   if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
   return s->impl->ws_fetch(features, targets, capacity, num_clusters);
+}
+int mlx_build_layers(mlx_solver* s, const double* p, const double* oldp, double h, int32_t ordering,
+                     const int32_t* order, const double* DmInv, const double* sorted_layers, int32_t num_layers,
+                     const uint8_t* forced_elastic, int32_t* rigid_body_sets, int32_t* num_rigids,
+                     uint8_t* is_elastic_element, uint8_t* is_boundary_vertex, uint8_t* is_rigid_vertex,
+                     int32_t* vertex_rigid_body) {
+  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+  return s->impl->build_layers(p, oldp, h, ordering, order, DmInv, sorted_layers, num_layers, forced_elastic,
+                               rigid_body_sets, num_rigids, is_elastic_element, is_boundary_vertex, is_rigid_vertex,
+                               vertex_rigid_body);
 }
 int mlx_pcg_solve(mlx_solver* s, double h, const double* b, int32_t iterations, double* x, double* resvec) {
   if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");

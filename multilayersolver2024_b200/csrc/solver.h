@@ -36,6 +36,10 @@ struct SolverBase {
                            const float* omean, const float* ostd, const float* corrections, int32_t* nb) = 0;
   virtual int ws_fetch(float* features, float* targets, int cap, int32_t* nb) = 0;
   virtual int pcg_solve(double h, const double* b, int iterations, double* x, double* resvec) = 0;
+  virtual int build_layers(const double* p, const double* oldp, double h, int ordering, const int32_t* order,
+                           const double* dminv, const double* sorted_layers, int L, const uint8_t* forced,
+                           int32_t* sets, int32_t* num_rigids, uint8_t* is_elastic, uint8_t* is_boundary,
+                           uint8_t* is_rigid_vertex, int32_t* vertex_body) = 0;
 };
 
 SolverBase* make_solver(const mlx_mesh_desc* md, int* rc);

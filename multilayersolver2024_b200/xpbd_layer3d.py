@@ -53,6 +53,40 @@ def find_boundary_vertices(mesh: Mesh3D, sets: np.ndarray, num_rigids) -> LayerS
     return LayerSet(sets, np.asarray(num_rigids, np.int32), _F(sets != 0, np.uint8), ela, bnd, rig, vb)
 
 
+def build_layers_device(solver, mesh: Mesh3D, p, oldp, h, sorted_layers, forced, order=None, dminv=None) -> LayerSet:
+    """buildLayers + findBoundaryVertices on the device (``mlx_build_layers``):
+    strain-rate order of p / oldp (with the mesh's DmInv, or `dminv`), or the
+    given 1-based `order`; the same bits as the host builder."""
+    lib = solver._lib
+    sl = np.ascontiguousarray(sorted_layers, np.float64)
+    L, T, N = sl.size, mesh.T, mesh.N
+    fe = np.ascontiguousarray(forced, np.uint8)
+    sets = np.zeros((T, L), np.int32, order="F")
+    nr = np.zeros(L, np.int32)
+    ela = np.zeros((T, L), np.uint8, order="F")
+    bnd = np.zeros((N, L), np.uint8, order="F")
+    rig = np.zeros((N, L), np.uint8, order="F")
+    vb = np.zeros((N, L), np.int32, order="F")
+    if order is None:
+        pp, op = np.ascontiguousarray(p, np.float64), np.ascontiguousarray(oldp, np.float64)
+        if dminv is not None:
+            dm = np.ascontiguousarray(dminv, np.float64)
+        else:
+            # kept on the mesh: the library copies DmInv to the device once per host pointer
+            if getattr(mesh, "_dminv_c", None) is None or mesh._dminv_c.base is not None:
+                mesh._dminv_c = np.ascontiguousarray(mesh.DmInv, np.float64).copy()
+            dm = mesh._dminv_c
+        check("mlx_build_layers", lib.mlx_build_layers(solver.handle, f64(pp), f64(op), float(h), 0, None, f64(dm),
+                                                       f64(sl), L, u8(fe), i32(sets), i32(nr), u8(ela), u8(bnd),
+                                                       u8(rig), i32(vb)), lib)
+    else:
+        o = np.ascontiguousarray(order, np.int32)
+        check("mlx_build_layers", lib.mlx_build_layers(solver.handle, None, None, float(h), 1, i32(o), None,
+                                                       f64(sl), L, u8(fe), i32(sets), i32(nr), u8(ela), u8(bnd),
+                                                       u8(rig), i32(vb)), lib)
+    return LayerSet(sets, nr, _F(sets != 0, np.uint8), ela, bnd, rig, vb)
+
+
 def strain_rate_norms(mesh: Mesh3D, p, oldp, h) -> np.ndarray:
     lib = load()
     out = np.zeros(mesh.T)
@@ -414,6 +448,9 @@ class XpbdLayer3D:
         self.airDrag = 0.0
         self.useRigidContacts = True
         self.StopAtImprovementPercent = 0.0
+        # where buildLayers runs for strain-rate / random layers: "device"
+        # (mlx_build_layers) or "host" (the native host helpers)
+        self.layerBuilder = "device"
         self.pinnedx = None
         # fixed rigid sets per sorted layer column (LayerOrderingType 4, "custom")
         self.customRigidSets = None
@@ -513,8 +550,16 @@ class XpbdLayer3D:
         f[2::3] = f[2::3] + mesh.mass[2::3] * self.Gravity
         f = f + self.CustomForce
         mesh.f = f
-        sets, numRigids = self.buildLayers(mesh, cache, h)
-        ls = self._boundary_vertices(mesh, sets, numRigids)
+        if self.customRigidSets is None and self.layerBuilder == "device":
+            # buildLayers and findBoundaryVertices in one device call
+            forced = np.zeros(mesh.T, np.uint8)
+            forced[mesh.pinnedTets - 1] = 1
+            order = self.rng.permutation(mesh.T).astype(np.int32) + 1 if self.LayerOrderingType == 1 else None
+            ls = build_layers_device(self.solver(mesh), mesh, mesh.p, cache.oldp, h, self.sortedLayers, forced,
+                                     order)
+        else:
+            sets, numRigids = self.buildLayers(mesh, cache, h)
+            ls = self._boundary_vertices(mesh, sets, numRigids)
         cache.layers = ls.isRigidElement
         cache.oldOldp = cache.oldp
         cache.oldp = mesh.p.copy()
