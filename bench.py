@@ -397,6 +397,38 @@ def run_ours(args, rank, world, local):
                   **plain_leg, "learned_warm_start": learned_leg,
                   "monitor": "device (layers as conditional IF nodes, projectGS as conditional WHILE nodes)"}
 
+    # ---- buildLayers for strain-rate layers (the reference's default
+    # ordering): on the device against the native host helpers ----
+    layer_builder = None
+    if not args.no_e2e:
+        from multilayersolver2024_b200.xpbd_layer3d import (build_layers_device, find_boundary_vertices as fbv,
+                                                            strain_rate_norms, union_find_layers)
+        sc5 = make_scene()
+        m5 = sc5.mesh
+        rng = np.random.default_rng(0)
+        oldp5 = m5.p + rng.normal(0, 1e-3, m5.p.size)
+        p5 = oldp5 + rng.normal(0, 1e-3, m5.p.size)
+        forced5 = np.zeros(m5.T, np.uint8)
+        forced5[m5.pinnedTets - 1] = 1
+        pct = [0.0, 25.0, 50.0]
+        reps = 5 if m5.T < 1_000_000 else 2
+        build_layers_device(solver, m5, p5, oldp5, sc5.h, pct, forced5)  # warm-up (DmInv copy)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            dev = build_layers_device(solver, m5, p5, oldp5, sc5.h, pct, forced5)
+        dev_ms = (time.perf_counter() - t0) * 1000.0 / reps
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            order5 = np.argsort(strain_rate_norms(m5, p5, oldp5, sc5.h), kind="stable").astype(np.int32) + 1
+            sets5, nr5 = union_find_layers(m5, order5, pct, forced5)
+            host = fbv(m5, sets5, nr5)
+        host_ms = (time.perf_counter() - t0) * 1000.0 / reps
+        layer_builder = {"layers_pct": pct, "device_ms": dev_ms, "host_ms": host_ms,
+                         "identical": bool(np.array_equal(dev.rigidBodySetsPerLayer, host.rigidBodySetsPerLayer)
+                                           and np.array_equal(dev.vertexRigidBody, host.vertexRigidBody)),
+                         "api": "mlx_build_layers (host buffers in and out) vs mlx_strain_rate_norms + stable "
+                                "argsort + mlx_union_find_layers + mlx_find_boundary_vertices"}
+
     line = None
     if rank == 0:
         peak, peak_kind = measured_peak_hbm()
@@ -444,6 +476,7 @@ def run_ours(args, rank, world, local):
                     "d2h_bytes_per_step": d2h, "api": "XpbdLayer3D.integrate -> mlx_layer_solve"
                     + (" (+ mlx_find_contacts on the step-start positions)" if sc.contact_finders else "")},
             "to_residual": to_res,
+            "layer_builder": layer_builder,
             "gpu_launches": int(launches_per_step * args.steps),
             "clocks": clocks.summary(),
             "state_finite": finite,

@@ -255,10 +255,28 @@ struct Solver final : SolverBase {
       d_contacts, d_cvid, d_clam, d_cgroups;
   PinnedBuf h_stage, h_scalar, h_cstage;
   LayerWork work, sim_work;
+  // mlx_layer_solve's layer loop as a CUDA graph, replayed while calls keep
+  // one shape: no residual monitoring, no contact list, the same layer
+  // columns, iteration counts, parameters and layer masks (so every cached
+  // layer static, and with it every kernel argument, is unchanged).
+  // MLXPBD_HOST_GRAPH=0 turns it off.
+  struct HostGraph {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<int> lkey;
+    std::vector<unsigned char> pkey;
+    long long launches = 0, iterations = 0;
+  } hg;
+  bool host_graph_on = true;
+  void drop_host_graph() {
+    if (hg.exec) cudaGraphExecDestroy(hg.exec);
+    hg.exec = nullptr;
+  }
+  bool statics_hit(const mlx_layer_desc* ld, const LayerWork& w) const;
 
   ~Solver() override {
     for (cudaEvent_t e : tev) cudaEventDestroy(e);
     if (sim.graph) cudaGraphExecDestroy(sim.graph);
+    if (hg.exec) cudaGraphExecDestroy(hg.exec);
     if (cs_if) cudaStreamDestroy(cs_if);
     if (cs_while) cudaStreamDestroy(cs_while);
     if (stream) cudaStreamDestroy(stream);
@@ -652,6 +670,8 @@ int Solver<R>::create(const mlx_mesh_desc* md) {
     persistent = e && std::string(e) == "1";
     const char* q = std::getenv("MLXPBD_PDL");
     pdl = !(q && std::string(q) == "0");
+    const char* hgv = std::getenv("MLXPBD_HOST_GRAPH");
+    host_graph_on = !(hgv && std::string(hgv) == "0");
     const char* n = std::getenv("MLXPBD_PERSIST_CTAS");
     int sms = 0;
     CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
@@ -1094,6 +1114,30 @@ int Solver<R>::build_layers(const double* p, const double* oldp, double h, int o
   if (small[L]) return set_error(MLX_ERR_LIMIT, "union-find step bound reached");
   for (int l = 0; l < L; ++l) num_rigids[l] = small[l];
   return MLX_OK;
+}
+
+// Whether every layer of `ld` finds its static data cached in `w` unchanged
+// (the check build_static makes, plus the rigid-element count).
+template <typename R>
+bool Solver<R>::statics_hit(const mlx_layer_desc* ld, const LayerWork& w) const {
+  for (int layer = 0; layer < ld->num_layers; ++layer) {
+    const int col = ld->layers_map[layer] - 1;
+    if (col < 0 || col >= (int)w.cache.size() || !w.cache[col]) return false;
+    const LayerStatic& ls = *w.cache[col];
+    const uint8_t* isE = ld->is_elastic_element + (size_t)T * col;
+    const uint8_t* isR = ld->is_rigid_element + (size_t)T * col;
+    const int32_t* rid = ld->vertex_rigid_body + (size_t)N * col;
+    const uint8_t* isBV = ld->is_boundary_vertex + (size_t)N * col;
+    const uint8_t* isRV = ld->is_rigid_vertex + (size_t)N * col;
+    if (!(ls.valid && ls.nb == ld->num_rigids[col] && std::memcmp(ls.isE.data(), isE, T) == 0 &&
+          std::memcmp(ls.isBV.data(), isBV, N) == 0 && std::memcmp(ls.isRV.data(), isRV, N) == 0 &&
+          std::memcmp(ls.rid.data(), rid, sizeof(int32_t) * N) == 0))
+      return false;
+    int nre = 0;
+    for (int e = 0; e < T; ++e) nre += isR[e] != 0;
+    if (nre != ls.n_rigid_elements) return false;
+  }
+  return true;
 }
 
 template <typename R>
@@ -2142,7 +2186,49 @@ int Solver<R>::layer_solve(const mlx_layer_desc* ld, const mlx_solve_params* P, 
   st.runUntil = P->run_until;
   st.sumNonMon = in->sum_non_monitored_time;
   CHECK(reset_gsync());
-  CHECK(run_layers(ld, P, K, cd, st, false, work));
+  const bool graphable = host_graph_on && !P->compute_residuals && cd.K == 0 && !sweep_timing;
+  std::vector<int> lkey;
+  std::vector<unsigned char> pkey;
+  if (graphable) {
+    lkey = {ld->num_layers, ld->num_columns};
+    for (int l = 0; l < ld->num_layers; ++l) {
+      lkey.push_back(ld->layers_map[l]);
+      lkey.push_back(ld->iterations[l]);
+    }
+    pkey.assign(reinterpret_cast<const unsigned char*>(P), reinterpret_cast<const unsigned char*>(P) + sizeof(*P));
+  }
+  if (graphable && lkey == hg.lkey && pkey == hg.pkey && statics_hit(ld, work)) {
+    // the same shape as the previous call, whose uncaptured run built every
+    // layer static: record the loop once, then replay it
+    if (!hg.exec) {
+      cudaGraph_t graph = nullptr;
+      CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      RunState cs = st;
+      const int rc = run_layers(ld, P, K, cd, cs, true, work);
+      const cudaError_t e = cudaStreamEndCapture(stream, &graph);
+      if (rc != MLX_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+      }
+      if (e != cudaSuccess) return set_error(MLX_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+      const cudaError_t ei = cudaGraphInstantiate(&hg.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ei != cudaSuccess) {
+        hg.exec = nullptr;
+        return set_error(MLX_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ei));
+      }
+      hg.launches = cs.launches - st.launches;
+      hg.iterations = cs.totalIterations - st.totalIterations;
+    }
+    CU(cudaGraphLaunch(hg.exec, stream));
+    st.launches += hg.launches;
+    st.totalIterations += hg.iterations;
+  } else {
+    drop_host_graph();
+    CHECK(run_layers(ld, P, K, cd, st, false, work));
+    hg.lkey = lkey;
+    hg.pkey = pkey;
+  }
   CU(cudaMemcpyAsync(h_gsync.p, d_gsync.p, sizeof(unsigned int) * 4, cudaMemcpyDeviceToHost, stream));
   // ---- download ----
   k_store_pos<R><<<blocks_for(N, bs), bs, 0, stream>>>(pos(), ds, N);

@@ -108,3 +108,29 @@ def test_forced_single_component_matches_oracle(gpu, monkeypatch, oracle):
     ref = _oracle_run(scenes.config1(), 20, oracle)
     d = scenes.config1().mesh.bbox_diagonal()
     assert max(np.abs(a - b).max() / d for a, b in zip(got, ref)) <= 1e-9
+
+
+def test_host_layer_solve_graph_replay_is_bit_identical(gpu, monkeypatch):
+    """mlx_layer_solve replays its layer loop from a CUDA graph while calls
+    keep one shape (fixed iterations, no contacts, same masks): integrate
+    over several frames equals the uncaptured loop bit for bit, with
+    bodies, boundary glue and pins (config 2 class at reduced size)."""
+    from multilayersolver2024_b200.xpbd_layer3d import ContactSet, StepCache
+
+    def run(flag):
+        monkeypatch.setenv("MLXPBD_HOST_GRAPH", flag)
+        sc = scenes.config2(seed=4, nx=16, ny=4, nz=4, cluster=4)
+        m = sc.mesh
+        m.v[sc.impulse[0] - 1] += sc.impulse[1]
+        it = _integ(sc, _lib.MLX_FP32)
+        cache = StepCache()
+        out = []
+        for frame in range(1, 7):
+            it.integrate(m, sc.h, ContactSet(), cache, frame)
+            out.append(m.p.copy())
+        for s in it._solvers.values():
+            s.close()
+        return out
+    a, b = run("1"), run("0")
+    for k in range(len(a)):
+        np.testing.assert_array_equal(a[k], b[k], err_msg=f"frame {k + 1}")
