@@ -360,8 +360,13 @@ def call_layer_solve(fn, solver_or_desc, layer_desc, params, contacts, xi, lambd
     inp.residualv, inp.pinnedx, inp.residual_in = f64(rv_), f64(px_), f64(rin)
     inp.residual_in_len = rin.size
     inp.sum_non_monitored_time = sum_non_monitored_time
-    cap = residual_capacity or (rin.size + 1 + max(0, params.hanging_stop if params.hanging_stop >= 0 else 0) +
-                                sum(int(layer_desc.iterations[i]) for i in range(layer_desc.num_layers)) + 100000)
+    if residual_capacity:
+        cap = residual_capacity
+    elif not params.compute_residuals:
+        cap = rin.size + 1  # the residual array comes back as it went in
+    else:
+        cap = (rin.size + 1 + max(0, params.hanging_stop if params.hanging_stop >= 0 else 0) +
+               sum(int(layer_desc.iterations[i]) for i in range(layer_desc.num_layers)) + 100000)
     out_xi = np.zeros(N3)
     if want_lambda and lam_ is None:
         raise ValueError("want_lambda needs lambdai")
@@ -564,10 +569,11 @@ class XpbdLayer3D:
         cache.oldOldp = cache.oldp
         cache.oldp = mesh.p.copy()
         xi = mesh.p.copy()
-        resv = mesh.v.copy()
-        up = mesh.unpinnedDOFs - 1
-        resv[up] = resv[up] + h * f[up] / mesh.mass[up]
-        resv = (1 - self.airDrag) * resv
+        # resv(unpinned) += h f / m: the same quotients, formed for every DOF
+        # and zeroed at the pinned ones (cheaper than two gathers and a scatter)
+        dv = h * f / mesh.mass
+        dv[mesh.pinnedDOFs - 1] = 0.0
+        resv = (1 - self.airDrag) * (mesh.v + dv)
         lambdai = None  # zeros(T, 6) (xpbdLayer3D.m:666): the library zeroes them on the device
         residualArray = np.array([0.0])
         ld, keep = pack_layer_desc(ls, self.layersMap, self.iterations)
