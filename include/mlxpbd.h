@@ -122,6 +122,16 @@ typedef struct mlx_solve_params {
   int32_t last_layer_give_up_enabled;
   int32_t use_gravity_constraints;
   int32_t use_rigid_contacts;
+  int32_t contact_coloring;            /* 0: the reference's order -- elastic
+                                          contacts after the colour sweep
+                                          (xpbdLayer3D.m:315-341); 1: each
+                                          vertex's elastic contacts in the
+                                          first colour phase whose tets do not
+                                          touch the vertex (after the sweep
+                                          when every colour does).  No
+                                          counterpart in the reference; device-
+                                          detected contacts only
+                                          (mlx_sim_set_obstacles). */
 } mlx_solve_params;
 
 /* Step-start contacts (xpbdLayer3D.m:675-681; contactInfo3D.m:32-55). */

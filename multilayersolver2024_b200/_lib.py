@@ -66,6 +66,7 @@ class SolveParams(C.Structure):
         ("compute_residuals", C.c_int32), ("hanging_stop", C.c_int32),
         ("give_up_enabled", C.c_int32), ("last_layer_give_up_enabled", C.c_int32),
         ("use_gravity_constraints", C.c_int32), ("use_rigid_contacts", C.c_int32),
+        ("contact_coloring", C.c_int32),
     ]
 
 

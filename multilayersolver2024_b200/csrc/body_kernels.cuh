@@ -495,7 +495,9 @@ __global__ void __launch_bounds__(kBodyThreads) k_iterate_bodies(LayerDev L, Bod
       // device-detected contacts: elastic ones are those of non-rigid vertices
       const int n = *dc.count, stride = (gridDim.x - nbc) * blockDim.x;
       for (int i = e * blockDim.x + threadIdx.x; i < n; i += stride)
-        if (L.vert_body[dc.verts[i]] == 0) elastic_contacts_of_vertex<R>(dc, i, gp, x0, h, contact_resistance);
+        // (with contact_coloring only the vertices no colour phase took)
+        if (L.vert_body[dc.verts[i]] == 0 && (!dc.colored || dc.vcc[dc.verts[i]] == dc.C))
+          elastic_contacts_of_vertex<R>(dc, i, gp, x0, h, contact_resistance);
       return;
     }
     int g = e * blockDim.x + threadIdx.x;

@@ -98,6 +98,14 @@ struct DevContacts {
   const int* count;        // [1] number of contact vertices
   double* lambda;          // [count * nobs] contact multipliers of the current layer
   const int* obs_count;    // [nobs] contacts of each obstacle (its finder's list length)
+  // contact_coloring: vertex v's elastic contacts run in colour phase vcc[v]
+  // (C: after the sweep); cbucket lists the step's contact vertices by that
+  // colour, colour c at [coff[c], coff[c + 1])
+  int colored;
+  int C;
+  const int* vcc;          // [N]
+  const int* cbucket;      // [count]
+  const int* coff;         // [C + 2]
 };
 
 // Bit masks of every vertex at the step-start positions.
@@ -317,6 +325,60 @@ __global__ void __launch_bounds__(256) k_contact_residual_partials(const DevCont
   }
   block_sum<1>(acc);
   if (threadIdx.x == 0) partials[blockIdx.x] = acc[0];
+}
+
+// contact_coloring, per step: the contact vertices bucketed by their colour
+// phase (counts, offsets, scatter).  The order inside a bucket is free: a
+// bucket holds distinct vertices, each projected by one thread.
+__global__ void k_cc_hist(const DevContacts dc, int* __restrict__ hist) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < *dc.count) atomicAdd(hist + dc.vcc[dc.verts[i]], 1);
+}
+__global__ void k_cc_offsets(const int* __restrict__ hist, int nb, int* __restrict__ off, int* __restrict__ cur) {
+  if (blockIdx.x || threadIdx.x) return;
+  int run = 0;
+  for (int c = 0; c < nb; ++c) {
+    off[c] = run;
+    cur[c] = run;
+    run += hist[c];
+  }
+  off[nb] = run;
+}
+__global__ void k_cc_scatter(const DevContacts dc, int* __restrict__ cur, int* __restrict__ bucket) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < *dc.count) {
+    const int v = dc.verts[i];
+    bucket[atomicAdd(cur + dc.vcc[v], 1)] = v;
+  }
+}
+
+// One colour of the sweep with the elastic contacts of that colour phase
+// (contact_coloring): CTAs [0, tet_blocks) project the colour's tets exactly
+// as k_project_color, the remaining CTAs the contacts of the vertices in
+// bucket `colour` (no tet of this colour touches them) that are elastic in
+// this layer.
+template <typename R, int MAT, bool DAMP>
+__global__ void __launch_bounds__(kMaxColorTile) k_project_color_cc(TetData<R> td, const int* __restrict__ list,
+                                                          int begin, int count, R4<R>* __restrict__ pos,
+                                                          const R4<R>* __restrict__ oldp, R inv_h2, R inv_h,
+                                                          int tet_blocks, DevContacts dc, int colour,
+                                                          const int* __restrict__ vert_body,
+                                                          const R4<R>* __restrict__ x0, double h,
+                                                          double contact_resistance) {
+  pdl_launch_dependents();
+  if ((int)blockIdx.x < tet_blocks) {
+    project_color_tet<R, MAT, DAMP>(td, list, begin, count, blockIdx.x * blockDim.x + threadIdx.x, pos, oldp, inv_h2,
+                                    inv_h);
+    return;
+  }
+  pdl_wait();
+  const GlobalPos<R> gp{pos};
+  const int b = (int)blockIdx.x - tet_blocks, stride = ((int)gridDim.x - tet_blocks) * blockDim.x;
+  const int end = dc.coff[colour + 1];
+  for (int q = dc.coff[colour] + b * blockDim.x + threadIdx.x; q < end; q += stride) {
+    const int v = dc.cbucket[q];
+    if (vert_body[v] == 0) elastic_contacts_of_vertex<R>(dc, dc.cidx[v], gp, x0, h, contact_resistance);
+  }
 }
 
 }  // namespace mlx

@@ -136,9 +136,11 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
       have = true;
     }
   };
+  // colours with no tet of this group are skipped, unless contact colouring
+  // may have put contacts in them
   auto next_colour = [&](int c) {
     ++c;
-    while (c < ga.C && ga.off[c * ga.G + g + 1] == ga.off[c * ga.G + g]) ++c;
+    while (c < ga.C && !dc.colored && ga.off[c * ga.G + g + 1] == ga.off[c * ga.G + g]) ++c;
     return c;
   };
   if (ga.one_per_thread) fetch(next_colour(-1));
@@ -160,11 +162,18 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
           project_group<R, MAT, DAMP>(td, t, l, rec, oldp, inv_h2, inv_h);
         }
       }
+      if (dc.colored) {
+        // contact_coloring: the contacts of this colour phase touch no tet of
+        // the colour, so they join its phase
+        for (int i = crange[0] + tid; i < crange[1]; i += nthr)
+          if (dc.vcc[dc.verts[i]] == c) elastic_contacts_of_vertex<R>(dc, i, sp, x0, h, contact_resistance);
+      }
       __syncthreads();
     }
     if (dc.nobs) {
       for (int i = crange[0] + tid; i < crange[1]; i += nthr)
-        elastic_contacts_of_vertex<R>(dc, i, sp, x0, h, contact_resistance);
+        if (!dc.colored || dc.vcc[dc.verts[i]] == dc.C)
+          elastic_contacts_of_vertex<R>(dc, i, sp, x0, h, contact_resistance);
       __syncthreads();
     }
     const int p0 = ga.pin_off[g], p1 = ga.pin_off[g + 1];

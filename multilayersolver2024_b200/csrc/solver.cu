@@ -299,7 +299,8 @@ struct Solver final : SolverBase {
   R4<R>* pos() const { return d_pos.as<R4<R>>(); }
 
   int build_static(const mlx_layer_desc* ld, int col, LayerStatic& ls, bool capturing);
-  int launch_color(int c, const LayerStatic& ls, const int* dlist, R h, int bs_override = 0);
+  int launch_color(int c, const LayerStatic& ls, const int* dlist, R h, int bs_override = 0,
+                   const DevContacts* cc = nullptr, const int* vert_body = nullptr, double hd = 0, double cr = 0);
   // per-colour tile autotuner of the resident stepper (block size of each
   // colour kernel, chosen by timing; kept per layer column)
   static constexpr int kDefaultTile = 64;
@@ -333,6 +334,10 @@ struct Solver final : SolverBase {
   std::vector<Obstacle> sim_obs;
   double sim_restitution = 1e-2;
   DevBuf d_obs, d_cmask, d_cverts, d_cidx, d_cscan, d_clam_dev;
+  // contact_coloring: colour phase of each vertex's contacts, the step's
+  // buckets and their offsets / cursors / counts
+  DevBuf d_vcc, d_cbucket, d_coff, d_ccur, d_chist;
+  int contact_colours();
   // pinned staging of the per-layer contact lists of mlx_layer_solve
   PinnedBuf h_cpack;
   size_t cpack_used = 0;
@@ -349,6 +354,11 @@ struct Solver final : SolverBase {
     dc.count = d_cscan.as<int>() + blocks_for(N, 256);
     dc.obs_count = dc.count + 2;
     dc.lambda = d_clam_dev.as<double>();
+    dc.colored = sim.P.contact_coloring ? 1 : 0;
+    dc.C = C;
+    dc.vcc = d_vcc.as<int>();
+    dc.cbucket = d_cbucket.as<int>();
+    dc.coff = d_coff.as<int>();
     return dc;
   }
   int detect_contacts(const R4<R>* x0);  // stream work only (captured in the step)
@@ -1321,9 +1331,10 @@ int Solver<R>::build_static(const mlx_layer_desc* ld, int col, LayerStatic& ls, 
 }
 
 template <typename R>
-int Solver<R>::launch_color(int c, const LayerStatic& ls, const int* dlist, R h, int bs_override) {
+int Solver<R>::launch_color(int c, const LayerStatic& ls, const int* dlist, R h, int bs_override,
+                            const DevContacts* cc, const int* vert_body, double hd, double cr) {
   int count = ls.color_count[c];
-  if (count == 0) return MLX_OK;
+  if (count == 0 && !cc) return MLX_OK;
   const int bs = bs_override > 0 ? bs_override : (ls.tile.empty() || ls.tile[c] <= 0 ? kDefaultTile : ls.tile[c]);
   R inv_h2 = R(1) / (h * h), inv_h = R(1) / h;
   TetData<R> td = tets();
@@ -1341,6 +1352,33 @@ int Solver<R>::launch_color(int c, const LayerStatic& ls, const int* dlist, R h,
   cfg.attrs = attr;
   cfg.numAttrs = pdl ? 1 : 0;
   cudaError_t e;
+  if (cc) {
+    // contact_coloring: extra CTAs for the elastic contacts of this colour
+    // phase (their number is known on the device only: a fixed grid strides)
+    const int tb = blocks_for(count, bs);
+    const int extra = std::max(1, std::min(32, blocks_for(N, bs) / std::max(C, 1) + 1));
+    cfg.gridDim = dim3(tb + extra);
+    const R4<R>* x0 = d_oldp.as<R4<R>>();
+    switch (mat_kind) {
+      case MAT_NH:
+        e = cudaLaunchKernelEx(&cfg, k_project_color_cc<R, MAT_NH, false>, td, list, begin, count, p, oldp, inv_h2,
+                               inv_h, tb, *cc, c, vert_body, x0, hd, cr);
+        break;
+      case MAT_STVK_BLOCKS:
+        e = damp ? cudaLaunchKernelEx(&cfg, k_project_color_cc<R, MAT_STVK_BLOCKS, true>, td, list, begin, count, p,
+                                      oldp, inv_h2, inv_h, tb, *cc, c, vert_body, x0, hd, cr)
+                 : cudaLaunchKernelEx(&cfg, k_project_color_cc<R, MAT_STVK_BLOCKS, false>, td, list, begin, count, p,
+                                      oldp, inv_h2, inv_h, tb, *cc, c, vert_body, x0, hd, cr);
+        break;
+      default:
+        e = damp ? cudaLaunchKernelEx(&cfg, k_project_color_cc<R, MAT_STVK_LAME, true>, td, list, begin, count, p,
+                                      oldp, inv_h2, inv_h, tb, *cc, c, vert_body, x0, hd, cr)
+                 : cudaLaunchKernelEx(&cfg, k_project_color_cc<R, MAT_STVK_LAME, false>, td, list, begin, count, p,
+                                      oldp, inv_h2, inv_h, tb, *cc, c, vert_body, x0, hd, cr);
+    }
+    if (e != cudaSuccess) return set_error(MLX_ERR_CUDA, std::string("colour launch: ") + cudaGetErrorString(e));
+    return MLX_OK;
+  }
   switch (mat_kind) {
     case MAT_NH:
       e = cudaLaunchKernelEx(&cfg, k_project_color<R, MAT_NH, false>, td, list, begin, count, p, oldp, inv_h2, inv_h);
@@ -1713,8 +1751,8 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
       long long sweep_l = 0;
       double sweep_b = 0;
       for (int c = 0; c < C; ++c) {
-        if (ls.color_count[c] == 0) continue;
-        CHECK(launch_color(c, ls, dlist, hR));
+        if (ls.color_count[c] == 0 && !dc.colored) continue;
+        CHECK(launch_color(c, ls, dlist, hR, 0, dc.colored ? &dc : nullptr, L.vert_body, h, P->contact_resistance));
         ++st.launches;
         ++sweep_l;
         sweep_b += ls.color_count[c] * (bytes_per_tet() + (ls.identity_list ? 0.0 : 4.0));
@@ -2150,6 +2188,8 @@ int Solver<R>::layer_solve(const mlx_layer_desc* ld, const mlx_solve_params* P, 
   CHECK(validate_layers(ld, P));
   if (in->residual_in_len < 1 && P->compute_residuals)
     return set_error(MLX_ERR_ARGUMENT, "residual_in must hold at least the initial entry");
+  if (P->contact_coloring && K && K->num_contacts > 0)
+    return set_error(MLX_ERR_UNSUPPORTED, "contact_coloring needs device-detected contacts (mlx_sim_set_obstacles)");
 
   DeviceGuard g(device);
   const size_t n3 = 3 * (size_t)N, n6 = 6 * (size_t)T, np = pinned.size();
@@ -2525,6 +2565,45 @@ int Solver<R>::detect_contacts(const R4<R>* x0) {
   CU(cudaMemsetAsync(scan + nb + 2, 0, sizeof(int) * nobs, stream));
   k_obstacle_counts<<<std::min(nb, 296), 256, 0, stream>>>(d_cmask.as<unsigned>(), N, nobs, scan + nb + 2);
   CU(cudaGetLastError());
+  if (sim.P.contact_coloring) {
+    const DevContacts dc = dev_contacts();
+    CU(cudaMemsetAsync(d_chist.p, 0, sizeof(int) * (size_t)(C + 1), stream));
+    k_cc_hist<<<nb, 256, 0, stream>>>(dc, d_chist.as<int>());
+    k_cc_offsets<<<1, 32, 0, stream>>>(d_chist.as<int>(), C + 1, d_coff.as<int>(), d_ccur.as<int>());
+    k_cc_scatter<<<nb, 256, 0, stream>>>(dc, d_ccur.as<int>(), d_cbucket.as<int>());
+    CU(cudaGetLastError());
+  }
+  return MLX_OK;
+}
+
+// contact_coloring: the colour phase of each vertex's elastic contacts is the
+// first colour none of the vertex's tets has (C when every colour does), and
+// the buffers of the per-step buckets.
+template <typename R>
+int Solver<R>::contact_colours() {
+  if (d_vcc.p) return MLX_OK;
+  const int words = (C + 64) / 64;
+  std::vector<uint64_t> used((size_t)N * words, 0);
+  for (int c = 0; c < C; ++c)
+    for (int s = color_off[c]; s < color_off[c + 1]; ++s) {
+      const int4 v = vid_sorted[s];
+      for (int k : {v.x, v.y, v.z, v.w}) used[(size_t)k * words + c / 64] |= 1ull << (c % 64);
+    }
+  std::vector<int> vcc(N, C);
+  for (int v = 0; v < N; ++v)
+    for (int c = 0; c < C; ++c)
+      if (!((used[(size_t)v * words + c / 64] >> (c % 64)) & 1ull)) {
+        vcc[v] = c;
+        break;
+      }
+  CHECK(d_vcc.ensure(sizeof(int) * (size_t)N));
+  CHECK(d_cbucket.ensure(sizeof(int) * (size_t)N));
+  CHECK(d_coff.ensure(sizeof(int) * (size_t)(C + 2)));
+  CHECK(d_ccur.ensure(sizeof(int) * (size_t)(C + 1)));
+  CHECK(d_chist.ensure(sizeof(int) * (size_t)(C + 1)));
+  CU(cudaMemcpyAsync(d_vcc.p, vcc.data(), sizeof(int) * (size_t)N, cudaMemcpyHostToDevice, stream));
+  CU(cudaMemsetAsync(d_coff.p, 0, sizeof(int) * (size_t)(C + 2), stream));
+  CU(cudaStreamSynchronize(stream));
   return MLX_OK;
 }
 
@@ -2544,6 +2623,7 @@ int Solver<R>::sim_set_obstacles(const mlx_obstacle* obs, int nobs, double resti
     CHECK(d_cscan.ensure(sizeof(int) * (blocks_for(N, 256) + 2 + MLX_MAX_OBSTACLES)));
     CHECK(d_clam_dev.ensure(sizeof(double) * (size_t)N * o.size()));
     CU(cudaMemcpyAsync(d_obs.p, o.data(), sizeof(Obstacle) * o.size(), cudaMemcpyHostToDevice, stream));
+    CHECK(contact_colours());
     CU(cudaMemsetAsync(d_cscan.p, 0, sizeof(int) * (blocks_for(N, 256) + 2 + MLX_MAX_OBSTACLES), stream));
     CU(cudaStreamSynchronize(stream));
   }
@@ -3008,7 +3088,7 @@ int Solver<R>::sim_issue_step(long long* launches, bool capturing) {
     // contacts of the step-start positions (simulate3D detects on mesh3D.p
     // before integrate; oldp holds those positions now)
     CHECK(detect_contacts(d_oldp.as<R4<R>>()));
-    st.launches += 5;
+    st.launches += sim.P.contact_coloring ? 8 : 5;
   }
   CHECK(run_layers(&sim.ld, &sim.P, nullptr, cd, st, capturing, sim_work, dc));
   if (ws.nb > 0 && ws.record) {

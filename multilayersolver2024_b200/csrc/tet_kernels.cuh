@@ -444,11 +444,9 @@ __device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepc
 // (ids, DmInv, volume, material) is loaded before waiting on the previous
 // colour; positions and multipliers after.
 template <typename R, int MAT, bool DAMP>
-__global__ void __launch_bounds__(kMaxColorTile) k_project_color(TetData<R> td, const int* __restrict__ list,
-                                                       int begin, int count, R4<R>* __restrict__ pos,
-                                                       const R4<R>* __restrict__ oldp, R inv_h2, R inv_h) {
-  pdl_launch_dependents();
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void project_color_tet(const TetData<R>& td, const int* __restrict__ list, int begin,
+                                                  int count, int i, R4<R>* __restrict__ pos,
+                                                  const R4<R>* __restrict__ oldp, R inv_h2, R inv_h) {
   const bool active = i < count;
   const int T = td.T;
   int s = 0;
@@ -493,6 +491,15 @@ __global__ void __launch_bounds__(kMaxColorTile) k_project_color(TetData<R> td, 
   stcg_r4(pos + v.y, make_r4<R>(X[1].x, X[1].y, X[1].z, minv[1]));
   stcg_r4(pos + v.z, make_r4<R>(X[2].x, X[2].y, X[2].z, minv[2]));
   stcg_r4(pos + v.w, make_r4<R>(X[3].x, X[3].y, X[3].z, minv[3]));
+}
+
+template <typename R, int MAT, bool DAMP>
+__global__ void __launch_bounds__(kMaxColorTile) k_project_color(TetData<R> td, const int* __restrict__ list,
+                                                       int begin, int count, R4<R>* __restrict__ pos,
+                                                       const R4<R>* __restrict__ oldp, R inv_h2, R inv_h) {
+  pdl_launch_dependents();
+  project_color_tet<R, MAT, DAMP>(td, list, begin, count, blockIdx.x * blockDim.x + threadIdx.x, pos, oldp, inv_h2,
+                                  inv_h);
 }
 
 // ---------------------------------------------------------------------------

@@ -159,7 +159,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
   ld.is_rigid_vertex = isRV.data();
   ld.num_rigids = numRigids.data();
 
-  mlx_solve_params P;
+  mlx_solve_params P = {};  // contact_coloring 0: the reference's order
   P.h = scalar(a[10]);
   P.boundary_compliance = scalar(a[13]);
   P.contact_resistance = scalar(a[14]);

@@ -338,6 +338,7 @@ def make_params(integ: "XpbdLayer3D", h: float) -> SolveParams:
     P.last_layer_give_up_enabled = int(bool(integ.LastLayerGiveUpEnabled))
     P.use_gravity_constraints = int(bool(integ.useGravityConstraints))
     P.use_rigid_contacts = int(bool(integ.useRigidContacts))
+    P.contact_coloring = int(bool(getattr(integ, "contactColoring", False)))
     return P
 
 
@@ -456,6 +457,9 @@ class XpbdLayer3D:
         # where buildLayers runs for strain-rate / random layers: "device"
         # (mlx_build_layers) or "host" (the native host helpers)
         self.layerBuilder = "device"
+        # elastic contacts projected inside the colour sweep (mlx_solve_params
+        # contact_coloring); False keeps the reference's order
+        self.contactColoring = False
         self.pinnedx = None
         # fixed rigid sets per sorted layer column (LayerOrderingType 4, "custom")
         self.customRigidSets = None

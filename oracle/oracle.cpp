@@ -471,7 +471,28 @@ struct Solve {
   int K = 0;
   const double *cn = nullptr, *cp = nullptr, *ccomp = nullptr;
   const int32_t* cv = nullptr;
+  // contact_coloring: the colour phase of each vertex's elastic contacts --
+  // the first colour none of its tets has, numColors when every colour does
+  std::vector<int> ccol;
   Solve(const Mesh& mm, const mlx_solve_params& pp) : m(mm), P(pp) {}
+
+  void contact_colours() {
+    if (!ccol.empty()) return;
+    const int words = (m.numColors + 64) / 64;
+    std::vector<uint64_t> used((size_t)m.N * words, 0);
+    for (int e = 0; e < m.T; ++e)
+      for (int k = 0; k < 4; ++k) {
+        const int c = m.color[e] - 1;
+        used[(size_t)m.vid(e, k) * words + c / 64] |= 1ull << (c % 64);
+      }
+    ccol.assign(m.N, m.numColors);
+    for (int v = 0; v < m.N; ++v)
+      for (int c = 0; c < m.numColors; ++c)
+        if (!((used[(size_t)v * words + c / 64] >> (c % 64)) & 1ull)) {
+          ccol[v] = c;
+          break;
+        }
+  }
 
   void tet_gather(int e, const std::vector<double>& src, double* out) const {
     for (int k = 0; k < 4; ++k)
@@ -480,8 +501,8 @@ struct Solve {
 
   // xpbdLayer3D.stvkVoigtConstraints (xpbdLayer3D.m:347-379); the NH branch is
   // the per-colour loop of xpbdLayer2D.neoHookeanConstraints (:260-294).
-  void color_sweep(const std::vector<int>& elastic) {
-    if (elastic.empty()) return;
+  void color_sweep(const std::vector<int>& elastic, const int32_t* rid) {
+    if (elastic.empty() && !(P.contact_coloring && K > 0)) return;
     double h = P.h, h2 = h * h;
     std::vector<std::vector<int>> byColor(m.numColors);
     for (int e : elastic) byColor[m.color[e] - 1].push_back(e);
@@ -521,6 +542,8 @@ struct Solve {
         for (int k = 0; k < 4; ++k)
           for (int d = 0; d < 3; ++d) xi[3 * (size_t)m.vid(e, k) + d] = newx[12 * (size_t)q + 3 * k + d];
       }
+      // contact_coloring: the elastic contacts of this colour's free vertices
+      if (P.contact_coloring && K > 0) elastic_contacts(rid, c);
     }
   }
 
@@ -560,18 +583,23 @@ struct Solve {
     }
   }
 
-  // xpbdLayer3D.contactConstraints (:422-485) with penaltyConstraint
-  // projectElastic / projectRigid (penaltyConstraint.m:4-63).
-  void contacts(const int32_t* rid, Bodies& B, const std::vector<double>& ri) {
-    if (K == 0) return;
+  // The elastic branch of contactConstraints (xpbdLayer3D.m:426-438,
+  // penaltyConstraint.projectElastic): gather, project, scatter (last write
+  // wins).  colour < 0: every elastic contact; otherwise (contact_coloring)
+  // those whose vertex has that contact colour.
+  void elastic_contacts(const int32_t* rid, int colour) {
     double h = P.h, h2 = h * h, res = P.contact_resistance;
+    if (colour >= 0) contact_colours();  // (colour == numColors: the vertices no phase took)
+    auto mine = [&](int k) {
+      const int v = cv[k] - 1;
+      return rid[v] == 0 && (colour < 0 || ccol[v] == colour);
+    };
     std::vector<double> newx;
     std::vector<int> ev;
     std::vector<double> dls;
-    // elastic contacts: gather, project, scatter (last write wins)
     for (int k = 0; k < K; ++k) {
       int v = cv[k] - 1;
-      if (rid[v] != 0) continue;
+      if (!mine(k)) continue;
       V3 x = v3(xi[3 * v], xi[3 * v + 1], xi[3 * v + 2]);
       V3 n = v3(cn[k], cn[k + K], cn[k + 2 * K]);
       V3 c = v3(cp[k], cp[k + K], cp[k + 2 * K]);
@@ -592,8 +620,17 @@ struct Solve {
     {
       size_t i = 0;
       for (int k = 0; k < K; ++k)
-        if (rid[cv[k] - 1] == 0) contactLambdas[k] += dls[i++];
+        if (mine(k)) contactLambdas[k] += dls[i++];
     }
+  }
+
+  // xpbdLayer3D.contactConstraints (:422-485) with penaltyConstraint
+  // projectElastic / projectRigid (penaltyConstraint.m:4-63).
+  void contacts(const int32_t* rid, Bodies& B, const std::vector<double>& ri) {
+    if (K == 0) return;
+    double h = P.h, h2 = h * h, res = P.contact_resistance;
+    // elastic contacts (with contact_coloring only those no colour phase took)
+    elastic_contacts(rid, P.contact_coloring ? m.numColors : -1);
     if (!P.use_rigid_contacts) return;
     std::vector<int> rk;
     for (int k = 0; k < K; ++k)
@@ -1008,7 +1045,7 @@ int orc_layer_solve(const mlx_mesh_desc* md, const mlx_layer_desc* ld, const mlx
       ++it;
       if (it > kSafetyIterations) return fail(MLX_ERR_LIMIT, "iteration safety limit reached");
       ++S.totalIterations;
-      S.color_sweep(elastic);
+      S.color_sweep(elastic, rid);
       S.boundary(bverts, lamB, rid, B, ri);
       S.contacts(rid, B, ri);
       for (int q = 0; q < m.numPinned; ++q) S.xi[m.pinned[q] - 1] = in->pinnedx[q];
