@@ -52,6 +52,17 @@ WORKLOADS = {
 WORKLOAD = WORKLOADS[2]
 
 
+def max_over_ranks(x, dist, device="cuda"):
+    """The max of a per-rank float over the process group (the job's time is
+    its slowest rank's); `x` itself without a process group."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -232,12 +243,6 @@ def run_ours(args, rank, world, local):
         if dist:
             dist.barrier()
 
-    def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
     sc = make_scene()
     m = sc.mesh
@@ -281,7 +286,7 @@ def run_ours(args, rank, world, local):
     clocks.stop()
     sweep_ms, sweep_bytes, sweep_launches = sim.sweep_stats(reset=True)
     contacts_at_end = sim.contact_count() if sc.contact_finders else None
-    max_ms = max_over_ranks(total_ms)
+    max_ms = max_over_ranks(total_ms, dist)
     value = args.steps * world / (max_ms / 1000.0)
     launches_per_step = sim.launches_per_step
     p_gpu, _ = sim.state()
@@ -318,7 +323,7 @@ def run_ours(args, rank, world, local):
         e2e_step(frame)
         e2e_s += time.perf_counter() - t0
     barrier()
-    e2e_s = max_over_ranks(e2e_s)
+    e2e_s = max_over_ranks(e2e_s, dist)
     N, T = m2.N, m2.T
     K = float(np.mean(contact_bytes)) if contact_bytes else 0.0
     # layer solve: xi and v in (2 x 3N; oldp too when the material is
