@@ -485,11 +485,31 @@ class XpbdLayer3D:
             self._solvers[key] = s
         return s
 
+    @property
+    def customRigidSets(self):
+        """Fixed rigid sets per sorted layer column (T x Ls), or None.  Stored
+        as a read-only copy when assigned -- the value semantics of the
+        reference's MATLAB property: changing them means assigning them."""
+        return self._custom_sets
+
+    @customRigidSets.setter
+    def customRigidSets(self, sets):
+        if sets is None:
+            self._custom_sets = None
+        else:
+            a = np.array(sets, dtype=np.int32, order="F", copy=True)
+            a.flags.writeable = False
+            self._custom_sets = a
+        self._custom_counts = None
+
     def buildLayers(self, mesh: Mesh3D, cache: StepCache, h: float):
         """xpbdLayer3D.buildLayers (:601-619)."""
         if self.customRigidSets is not None:
-            sets = _F(self.customRigidSets, np.int32)
-            return sets, np.asarray([int(sets[:, c].max(initial=0)) for c in range(sets.shape[1])], np.int32)
+            sets = self.customRigidSets
+            if self._custom_counts is None:
+                self._custom_counts = np.asarray([int(sets[:, c].max(initial=0)) for c in range(sets.shape[1])],
+                                                 np.int32)
+            return sets, self._custom_counts
         if self.LayerOrderingType == 1:
             order = self.rng.permutation(mesh.T) + 1
         else:
@@ -540,10 +560,10 @@ class XpbdLayer3D:
         if self.customRigidSets is None:
             return find_boundary_vertices(mesh, sets, num_rigids)
         c = getattr(self, "_fbv", None)
-        if c is not None and c[0] is mesh and c[1].shape == sets.shape and np.array_equal(c[1], sets):
+        if c is not None and c[0] is mesh and c[1] is sets:  # the stored sets are read-only
             return c[2]
         ls = find_boundary_vertices(mesh, sets, num_rigids)
-        self._fbv = (mesh, sets.copy(), ls)
+        self._fbv = (mesh, sets, ls)
         return ls
 
     def integrate(self, mesh: Mesh3D, h: float, contacts: ContactSet, cache: StepCache, frame: int):
