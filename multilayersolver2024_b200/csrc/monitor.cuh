@@ -69,8 +69,8 @@ __global__ void k_mon_loop_begin(MonState* ms, cudaGraphConditionalHandle loop, 
 
 // End of one projectGS iteration: append the residual and apply
 // simpleMonitorError's rules (xpbdLayer3D.m:515-544), then the loop test.
-__global__ void k_mon_iter_end(MonState* ms, cudaGraphConditionalHandle loop, int iterations, int is_last,
-                               MonParams mp) {
+__device__ __forceinline__ void mon_iter_end(MonState* ms, cudaGraphConditionalHandle loop, int iterations,
+                                             int is_last, const MonParams& mp) {
   ms->it += 1;
   ms->total_iterations += 1;
   const double newRes = ms->res;
@@ -102,6 +102,11 @@ __global__ void k_mon_iter_end(MonState* ms, cudaGraphConditionalHandle loop, in
   const bool go = !(ms->end_layer || ms->stop) &&
                   (ms->it <= iterations || (!ms->stop && ms->run_until >= 0 && is_last));
   cudaGraphSetConditional(loop, go ? 1u : 0u);
+}
+
+__global__ void k_mon_iter_end(MonState* ms, cudaGraphConditionalHandle loop, int iterations, int is_last,
+                               MonParams mp) {
+  mon_iter_end(ms, loop, iterations, is_last, mp);
 }
 
 }  // namespace mlx

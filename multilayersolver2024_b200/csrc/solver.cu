@@ -670,7 +670,8 @@ int Solver<R>::create(const mlx_mesh_desc* md) {
   CHECK(d_ri.ensure(sizeof(double4) * N));
   CHECK(d_s2e.ensure(sizeof(int) * T));
   CHECK(d_partials.ensure(sizeof(double) * 1024));
-  CHECK(d_scalar.ensure(sizeof(double) * 8));
+  CHECK(d_scalar.ensure(sizeof(double) * 8));  // [0] residual, [1] norm of resv, [7] k_residual_monitor's ticket
+  CU(cudaMemsetAsync(d_scalar.p, 0, sizeof(double) * 8, stream));
   CHECK(h_scalar.ensure(sizeof(double) * 8));
   CHECK(d_gsync.ensure(sizeof(unsigned int) * 4));
   CHECK(h_gsync.ensure(sizeof(int) * 4));
@@ -1494,6 +1495,39 @@ int Solver<R>::upload_contacts(const mlx_contacts* K, ContactData& cd) {
   return MLX_OK;
 }
 
+// One monitored iteration's residual and stop rules in one launch (no device
+// contacts): every CTA writes its partial sum of the tets' residual terms;
+// the last CTA to finish (ticket) sums the partials in index order exactly
+// as k_finish_norm does, stores the norm and applies the monitor's rules,
+// then resets the ticket for the next iteration.
+template <typename R, int MAT>
+__global__ void __launch_bounds__(256) k_residual_monitor(TetData<R> td, const R4<R>* __restrict__ pos, R inv_h2,
+                                                          R inv_h, double inv_h2_d, double* __restrict__ partials,
+                                                          unsigned* __restrict__ ticket, MonState* ms,
+                                                          cudaGraphConditionalHandle loop, int iterations, int is_last,
+                                                          MonParams mp) {
+  double acc[1] = {residual_tets<R, MAT>(td, pos, inv_h2, inv_h, inv_h2_d, blockIdx.x * blockDim.x + threadIdx.x,
+                                         gridDim.x * blockDim.x)};
+  block_sum<1>(acc);
+  __shared__ int last;
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = acc[0];
+    __threadfence();
+    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double sum[1] = {0.0};
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) sum[0] += __ldcg(partials + i);
+  block_sum<1>(sum);
+  if (threadIdx.x == 0) {
+    ms->res = sqrt(sum[0]);
+    *ticket = 0;
+    mon_iter_end(ms, loop, iterations, is_last, mp);
+  }
+}
+
 // The layer loop of layerSolve (xpbdLayer3D.m:109-226) on the device-resident
 // state (pos, resv, oldp, lambda, pinned values).  With `capturing` set the
 // loop issues only stream work (no host synchronisation), so it can be
@@ -1784,6 +1818,33 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
         ++st.launches;
       }
       bool endLayer = false;
+      if (devmon && !dc.nobs) {
+        // residual, its norm and the stop rules in one launch
+        const int tb = std::min(blocks_for(T, 256), 592);
+        const R ih2 = R(1) / (hR * hR), ih = R(1) / hR;
+        TetData<R> td = tets();
+        double* parts = d_partials.as<double>();
+        unsigned* ticket = reinterpret_cast<unsigned*>(d_scalar.as<double>() + 7);
+        MonState* ms = mon();
+        const int its = ld->iterations[layer], il = isLast ? 1 : 0;
+        switch (mat_kind) {
+          case MAT_NH:
+            k_residual_monitor<R, MAT_NH><<<tb, 256, 0, stream>>>(td, pos(), ih2, ih, 1.0 / (h * h), parts, ticket, ms,
+                                                                  h_while_cur, its, il, mp);
+            break;
+          case MAT_STVK_BLOCKS:
+            k_residual_monitor<R, MAT_STVK_BLOCKS><<<tb, 256, 0, stream>>>(td, pos(), ih2, ih, 1.0 / (h * h), parts,
+                                                                           ticket, ms, h_while_cur, its, il, mp);
+            break;
+          default:
+            k_residual_monitor<R, MAT_STVK_LAME><<<tb, 256, 0, stream>>>(td, pos(), ih2, ih, 1.0 / (h * h), parts,
+                                                                         ticket, ms, h_while_cur, its, il, mp);
+        }
+        CU(cudaGetLastError());
+        ++st.launches;
+        CHECK(cond_end(cs_if));  // end of the WHILE body
+        break;
+      }
       if (devmon) {
         CHECK(residual_dev(&mon()->res, dc));
         if (dc.nobs) ++st.launches;

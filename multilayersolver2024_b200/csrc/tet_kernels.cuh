@@ -545,14 +545,14 @@ struct ContactData {
 // Residual partial sums over all tets (blocks [0, tetBlocks)) and all
 // contacts (the remaining blocks), one double per block
 // (simpleEvaluateAllConstraintResiduals, xpbdLayer3D.m:546-586).
+// This thread's sum of the tets' residual terms over the grid-stride range
+// starting at `first` (stride `stride`).
 template <typename R, int MAT>
-__global__ void __launch_bounds__(256) k_residual_partials(TetData<R> td, const R4<R>* __restrict__ pos,
-                                                           ContactData cd, double contact_resistance,
-                                                           R inv_h2, R inv_h, double inv_h2_d,
-                                                           int tetBlocks, double* __restrict__ partials) {
+__device__ __forceinline__ double residual_tets(const TetData<R>& td, const R4<R>* __restrict__ pos, R inv_h2,
+                                                R inv_h, double inv_h2_d, int first, int stride) {
   double acc[1] = {0.0};
-  if ((int)blockIdx.x < tetBlocks) {
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < td.T; s += tetBlocks * blockDim.x) {
+  {
+    for (int s = first; s < td.T; s += stride) {
       int4 v;
       R G[9], minv[4];
       V3<R> X[4];
@@ -577,6 +577,19 @@ __global__ void __launch_bounds__(256) k_residual_partials(TetData<R> td, const 
         acc[0] += stvk_residual<R>(X, G, vol, cm, lam);
       }
     }
+  }
+  return acc[0];
+}
+
+template <typename R, int MAT>
+__global__ void __launch_bounds__(256) k_residual_partials(TetData<R> td, const R4<R>* __restrict__ pos,
+                                                           ContactData cd, double contact_resistance,
+                                                           R inv_h2, R inv_h, double inv_h2_d,
+                                                           int tetBlocks, double* __restrict__ partials) {
+  double acc[1] = {0.0};
+  if ((int)blockIdx.x < tetBlocks) {
+    acc[0] = residual_tets<R, MAT>(td, pos, inv_h2, inv_h, inv_h2_d, blockIdx.x * blockDim.x + threadIdx.x,
+                                   tetBlocks * blockDim.x);
   } else {
     // contacts: the reference's correction term is the K x 1 x K implicit
     // expansion of (compliance/h^2) (1x1xK) times lambda (Kx1)
