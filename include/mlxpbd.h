@@ -311,6 +311,14 @@ int mlx_sim_contact_count(mlx_solver* solver, int32_t* num_contact_vertices);
  * description. */
 int mlx_pcg_solve(mlx_solver* solver, double h, const double* b, int32_t iterations, double* x, double* resvec);
 
+/* Diagnostic of the bounded device waits (no counterpart in the reference):
+ * one thread runs the wait the library's kernels use -- kind 0: the grid
+ * barrier of the persistent layer kernel, kind 1: the mbarrier wait of the
+ * tensor-core GEMM -- on a condition nothing satisfies, so it gives up after
+ * limit_ns (clamped to [1 ms, 2 s]) and *timed_out is set to 1.  Shows that a
+ * wait that runs out ends with a status and leaves the context usable. */
+int mlx_wait_probe(int32_t device, int32_t kind, int64_t limit_ns, int32_t* timed_out);
+
 /* xpbdLayer3D.buildLayers (3d/integrator/xpbdLayer3D.m:601-619) followed by
  * xpbdLayer2D.findBoundaryVertices (2d/integrator/xpbdLayer2D.m:551-569) on
  * the device, replacing mexEdiffNorm3D + sort + mexUnionFindByVertice and

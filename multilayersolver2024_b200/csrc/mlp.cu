@@ -61,12 +61,12 @@ __device__ __forceinline__ unsigned long long now_ns() {
 }
 
 // Waits for phase `parity` of the barrier; false when the wait gave up
-// after kWaitNs.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+// after limit_ns.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsigned long long limit_ns = kWaitNs) {
   const uint32_t a = smem_addr(bar);
   const unsigned long long t0 = now_ns();
   for (unsigned spin = 0;; ++spin) {
-    if ((spin & 1023u) == 1023u && now_ns() - t0 > kWaitNs) return false;
+    if ((spin & 1023u) == 1023u && now_ns() - t0 > limit_ns) return false;
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -349,6 +349,16 @@ __global__ void k_gather_grad(const float* __restrict__ dw, const float* __restr
 
 inline int pad_to(int x, int m) { return (x + m - 1) / m * m; }
 
+// Diagnostic of the bounded mbarrier wait the GEMM uses: thread 0 waits on a
+// barrier no thread arrives at, so the wait runs out after limit_ns.
+__global__ void k_probe_mbar_wait(unsigned long long limit_ns, int* timed_out) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x != 0) return;
+  mbar_init(&bar, 1);
+  *timed_out = mbar_wait(&bar, 0, limit_ns) ? 0 : 1;
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(&bar)) : "memory");
+}
+
 }  // namespace
 
 // The perceptron: n_in -> n_hidden (GELU) x n_layers_hidden -> n_out.
@@ -566,6 +576,25 @@ int mlp_dims(const mlx_mlp* m, int* n_in, int* n_out, int* max_batch) {
   *n_in = m->impl.n_in;
   *n_out = m->impl.n_out;
   *max_batch = m->impl.max_batch;
+  return MLX_OK;
+}
+}  // namespace mlx
+
+namespace mlx {
+int mlp_wait_probe(int device, long long limit_ns, int* timed_out) {
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (cudaSetDevice(device) != cudaSuccess) return set_error(MLX_ERR_ARGUMENT, "bad device");
+  int* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, sizeof(int));
+  if (e == cudaSuccess) {
+    k_probe_mbar_wait<<<1, 32>>>((unsigned long long)limit_ns, d);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(timed_out, d, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+  }
+  cudaSetDevice(prev);
+  if (e != cudaSuccess) return set_error(MLX_ERR_CUDA, std::string("mbarrier wait probe: ") + cudaGetErrorString(e));
   return MLX_OK;
 }
 }  // namespace mlx

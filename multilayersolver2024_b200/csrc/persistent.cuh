@@ -38,6 +38,26 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
+// Waits until *count >= target (acquire), giving up after limit_ns or when
+// another waiter has set *error (which a timeout here sets).  Returns false
+// when it gave up.
+__device__ __forceinline__ bool wait_count_ge(const unsigned* count, unsigned target, int* error,
+                                              unsigned long long limit_ns) {
+  if (ld_acquire_gpu(count) >= target) return true;
+  const unsigned long long t0 = global_ns();
+  unsigned spins = 0;
+  while (ld_acquire_gpu(count) < target) {
+    if ((++spins & 255u) == 0) {
+      if (*reinterpret_cast<volatile int*>(error)) return false;
+      if (global_ns() - t0 > limit_ns) {
+        atomicExch(error, 1);
+        return false;
+      }
+    }
+  }
+  return true;
+}
+
 // Grid-wide counting barrier with a bounded wait.  Barrier number `k`
 // (1, 2, ... within the launch) completes when the monotonic arrival counter
 // reaches k * gridDim.x.  The CTA barrier orders this CTA's writes before the
@@ -49,23 +69,9 @@ __device__ __forceinline__ bool grid_sync(const GridSync& g, unsigned& k) {
   ++k;
   __syncthreads();
   if (threadIdx.x == 0) {
-    ok = 1;
     const unsigned target = k * gridDim.x;
     red_release_add_gpu(g.count, 1u);
-    if (ld_acquire_gpu(g.count) < target) {
-      unsigned long long t0 = global_ns();
-      unsigned spins = 0;
-      while (ld_acquire_gpu(g.count) < target) {
-        if ((++spins & 255u) == 0) {
-          if (*reinterpret_cast<volatile int*>(g.error)) { ok = 0; break; }
-          if (global_ns() - t0 > kWaitNs) {
-            atomicExch(g.error, 1);
-            ok = 0;
-            break;
-          }
-        }
-      }
-    }
+    ok = wait_count_ge(g.count, target, g.error, kWaitNs) ? 1 : 0;
   }
   __syncthreads();
   return ok != 0;

@@ -1001,6 +1001,12 @@ int Solver<R>::launch_groups(const LayerStatic& ls, const int* dint, const mlx_s
   return MLX_OK;
 }
 
+// Diagnostic of the grid barrier's bounded wait: thread 0 waits for a count
+// nothing increments, so the wait runs out after limit_ns.
+__global__ void k_probe_grid_wait(unsigned* count, int* error, unsigned long long limit_ns, int* timed_out) {
+  if (threadIdx.x == 0) *timed_out = wait_count_ge(count, 1u, error, limit_ns) ? 0 : 1;
+}
+
 __global__ void k_iota(int* __restrict__ a, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) a[i] = i;
@@ -3434,6 +3440,31 @@ int mlx_build_layers(mlx_solver* s, const double* p, const double* oldp, double 
   return s->impl->build_layers(p, oldp, h, ordering, order, DmInv, sorted_layers, num_layers, forced_elastic,
                                rigid_body_sets, num_rigids, is_elastic_element, is_boundary_vertex, is_rigid_vertex,
                                vertex_rigid_body);
+}
+int mlx_wait_probe(int32_t device, int32_t kind, int64_t limit_ns, int32_t* timed_out) {
+  if (!timed_out) return set_error(MLX_ERR_ARGUMENT, "null argument");
+  if (kind != 0 && kind != 1) return set_error(MLX_ERR_ARGUMENT, "kind must be 0 (grid barrier) or 1 (mbarrier)");
+  limit_ns = std::max<int64_t>(1000000, std::min<int64_t>(limit_ns, 2000000000));
+  *timed_out = 0;
+  if (kind == 1) return mlx::mlp_wait_probe(device, (long long)limit_ns, timed_out);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (cudaSetDevice(device) != cudaSuccess) return set_error(MLX_ERR_ARGUMENT, "bad device");
+  unsigned* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, sizeof(unsigned) * 4);
+  if (e == cudaSuccess) {
+    cudaMemset(d, 0, sizeof(unsigned) * 4);
+    k_probe_grid_wait<<<1, 32>>>(d, reinterpret_cast<int*>(d + 1), (unsigned long long)limit_ns,
+                                 reinterpret_cast<int*>(d + 2));
+    e = cudaGetLastError();
+    int r = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&r, d + 2, sizeof(int), cudaMemcpyDeviceToHost);
+    *timed_out = r;
+    cudaFree(d);
+  }
+  cudaSetDevice(prev);
+  if (e != cudaSuccess) return set_error(MLX_ERR_CUDA, std::string("grid wait probe: ") + cudaGetErrorString(e));
+  return MLX_OK;
 }
 int mlx_pcg_solve(mlx_solver* s, double h, const double* b, int32_t iterations, double* x, double* resvec) {
   if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");

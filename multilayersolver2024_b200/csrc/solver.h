@@ -46,5 +46,6 @@ SolverBase* make_solver(const mlx_mesh_desc* md, int* rc);
 
 int mlp_forward_on_stream(mlx_mlp* m, const float* d_x, int batch, cudaStream_t s, const float** y, int* ld);
 int mlp_dims(const mlx_mlp* m, int* n_in, int* n_out, int* max_batch);
+int mlp_wait_probe(int device, long long limit_ns, int* timed_out);
 
 }  // namespace mlx
