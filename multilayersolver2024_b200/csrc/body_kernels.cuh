@@ -286,10 +286,28 @@ __device__ __forceinline__ void inverse3(const double* A, double* inv) {
   }
 }
 
-// Per-body update after an accumulation (xpbdLayer3D.m:401-414, 466-479).
-__device__ __forceinline__ void apply_increments(Body& B, const double* s, double h) {
+// Inverse of a body's world inertia (column-major) by its adjugate: one
+// division and independent products, a short dependent chain for the thread
+// that updates the body (the inertia of a cluster is well conditioned; the
+// results agree with a pivoted solve to rounding).
+__device__ __forceinline__ void inertia_inverse(const double* A, double* inv) {
+  const double a00 = A[0], a10 = A[1], a20 = A[2], a01 = A[3], a11 = A[4], a21 = A[5], a02 = A[6], a12 = A[7],
+               a22 = A[8];
+  const double c00 = a11 * a22 - a12 * a21, c01 = a12 * a20 - a10 * a22, c02 = a10 * a21 - a11 * a20;
+  const double c10 = a02 * a21 - a01 * a22, c11 = a00 * a22 - a02 * a20, c12 = a01 * a20 - a00 * a21;
+  const double c20 = a01 * a12 - a02 * a11, c21 = a02 * a10 - a00 * a12, c22 = a00 * a11 - a01 * a10;
+  const double r = 1.0 / (a00 * c00 + a01 * c01 + a02 * c02);
+  // inv(row, col) = C(col, row) / det, column-major
+  inv[0] = c00 * r; inv[1] = c01 * r; inv[2] = c02 * r;
+  inv[3] = c10 * r; inv[4] = c11 * r; inv[5] = c12 * r;
+  inv[6] = c20 * r; inv[7] = c21 * r; inv[8] = c22 * r;
+}
+
+// Per-body update after an accumulation (xpbdLayer3D.m:401-414, 466-479):
+// omega = I \ dL with I's inverse `invI` (the reference's solve, to rounding).
+__device__ __forceinline__ void apply_increments(Body& B, const double* s, double h, const double* invI) {
   for (int d = 0; d < 3; ++d) B.com[d] += s[d];
-  D3 w = solve3_piv(B.I, d3(s[3], s[4], s[5]));
+  D3 w = mv3(invI, d3(s[3], s[4], s[5]));
   double dR[9], tmp[9];
   exp_rodrigues(w, h, dR);
   mm3(dR, B.R, B.R);
@@ -343,7 +361,7 @@ __device__ __forceinline__ void body_iteration(const LayerDev& L, int b, Body* _
                                                const R4<R>* __restrict__ x0 = nullptr, const G g = G{}) {
   if (g.rank() == 0) {
     sb = bodies[b];
-    inverse3(sb.I, invI);
+    inertia_inverse(sb.I, invI);
   }
   g.sync();
   bool dirty = false;
@@ -375,8 +393,8 @@ __device__ __forceinline__ void body_iteration(const LayerDev& L, int b, Body* _
     }
     g.template sum<6>(s);
     if (g.rank() == 0) {
-      apply_increments(sb, s, h);
-      inverse3(sb.I, invI);
+      apply_increments(sb, s, h, invI);
+      inertia_inverse(sb.I, invI);
     }
     g.sync();
     for (int i = beg + g.rank(); i < end; i += g.size()) {
@@ -414,7 +432,7 @@ __device__ __forceinline__ void body_iteration(const LayerDev& L, int b, Body* _
       s[3] += (1 / h) * cr.x; s[4] += (1 / h) * cr.y; s[5] += (1 / h) * cr.z;
     }
     g.template sum<6>(s);
-    if (g.rank() == 0) apply_increments(sb, s, h);
+    if (g.rank() == 0) apply_increments(sb, s, h, invI);
     g.sync();
     for (int i = beg + g.rank(); i < end; i += g.size()) {
       int v = cd.vid[L.rc_ids[i]];
@@ -459,7 +477,7 @@ __device__ __forceinline__ void body_iteration(const LayerDev& L, int b, Body* _
       }
     }
     g.template sum<6>(s);
-    if (g.rank() == 0) apply_increments(sb, s, h);
+    if (g.rank() == 0) apply_increments(sb, s, h, invI);
     g.sync();
     for (int i = beg + g.rank(); i < end; i += g.size()) {
       const int v = L.body_verts[i];

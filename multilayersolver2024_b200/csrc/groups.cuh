@@ -105,8 +105,10 @@ __device__ __forceinline__ int lower_bound_dev(const int* a, int n, int x) {
 }
 
 // One launch = the whole projectGS loop of one body-free layer; CTA g owns
-// group g.  Dynamic shared memory: the records of the largest group.
-template <typename R, int MAT, bool DAMP>
+// group g.  Dynamic shared memory: the records of the largest group.  CC:
+// contacts coloured with the elastic constraints (a separate instantiation,
+// so the reference-order kernel carries none of that code).
+template <typename R, int MAT, bool DAMP, bool CC = false>
 __global__ void __launch_bounds__(kGroupThreads, 1)
     k_layer_groups(TetData<R> td, GroupArgs ga, R4<R>* __restrict__ pos, const R4<R>* __restrict__ oldp,
                    R inv_h2, R inv_h, DevContacts dc, const R4<R>* __restrict__ x0, double h,
@@ -140,7 +142,7 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
   // may have put contacts in them
   auto next_colour = [&](int c) {
     ++c;
-    while (c < ga.C && !dc.colored && ga.off[c * ga.G + g + 1] == ga.off[c * ga.G + g]) ++c;
+    while (c < ga.C && !CC && ga.off[c * ga.G + g + 1] == ga.off[c * ga.G + g]) ++c;
     return c;
   };
   if (ga.one_per_thread) fetch(next_colour(-1));
@@ -162,7 +164,7 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
           project_group<R, MAT, DAMP>(td, t, l, rec, oldp, inv_h2, inv_h);
         }
       }
-      if (dc.colored) {
+      if (CC) {
         // contact_coloring: the contacts of this colour phase touch no tet of
         // the colour, so they join its phase
         for (int i = crange[0] + tid; i < crange[1]; i += nthr)
@@ -172,8 +174,7 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
     }
     if (dc.nobs) {
       for (int i = crange[0] + tid; i < crange[1]; i += nthr)
-        if (!dc.colored || dc.vcc[dc.verts[i]] == dc.C)
-          elastic_contacts_of_vertex<R>(dc, i, sp, x0, h, contact_resistance);
+        if (!CC || dc.vcc[dc.verts[i]] == dc.C) elastic_contacts_of_vertex<R>(dc, i, sp, x0, h, contact_resistance);
       __syncthreads();
     }
     const int p0 = ga.pin_off[g], p1 = ga.pin_off[g + 1];

@@ -806,13 +806,20 @@ int Solver<R>::plan_cluster(const mlx_mesh_desc* md, MeshPartition& mp) {
 }
 
 template <typename R>
-static const void* group_kernel(int mat_kind, bool damp) {
+static const void* group_kernel(int mat_kind, bool damp, bool cc = false) {
   switch (mat_kind) {
-    case MAT_NH: return (const void*)k_layer_groups<R, MAT_NH, false>;
+    case MAT_NH:
+      return cc ? (const void*)k_layer_groups<R, MAT_NH, false, true> : (const void*)k_layer_groups<R, MAT_NH, false>;
     case MAT_STVK_BLOCKS:
+      if (cc)
+        return damp ? (const void*)k_layer_groups<R, MAT_STVK_BLOCKS, true, true>
+                    : (const void*)k_layer_groups<R, MAT_STVK_BLOCKS, false, true>;
       return damp ? (const void*)k_layer_groups<R, MAT_STVK_BLOCKS, true>
                   : (const void*)k_layer_groups<R, MAT_STVK_BLOCKS, false>;
     default:
+      if (cc)
+        return damp ? (const void*)k_layer_groups<R, MAT_STVK_LAME, true, true>
+                    : (const void*)k_layer_groups<R, MAT_STVK_LAME, false, true>;
       return damp ? (const void*)k_layer_groups<R, MAT_STVK_LAME, true>
                   : (const void*)k_layer_groups<R, MAT_STVK_LAME, false>;
   }
@@ -942,6 +949,8 @@ int Solver<R>::plan_groups(const mlx_mesh_desc* md) {
   }
   gr_smem = (size_t)max_gv * sizeof(R4<R>);
   CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(gr_smem, 16)));
+  CU(cudaFuncSetAttribute(group_kernel<R>(mat_kind, damp, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)std::max<size_t>(gr_smem, 16)));
   CHECK(d_gv0.ensure(sizeof(int) * gv0.size()));
   CHECK(d_tloc.ensure(sizeof(int4) * (size_t)T));
   CHECK(d_gpin.ensure(sizeof(int) * gpin.size()));
@@ -980,6 +989,27 @@ int Solver<R>::launch_groups(const LayerStatic& ls, const int* dint, const mlx_s
   const R* pv = d_pinx.as<R>();
   const double h = P->h, cr = P->contact_resistance;
   cudaError_t e;
+  if (dc.colored) {
+    switch (mat_kind) {
+      case MAT_NH:
+        e = cudaLaunchKernelEx(&cfg, k_layer_groups<R, MAT_NH, false, true>, td, ga, pos(), oldp, inv_h2, inv_h, dc,
+                               oldp, h, cr, pv);
+        break;
+      case MAT_STVK_BLOCKS:
+        e = damp ? cudaLaunchKernelEx(&cfg, k_layer_groups<R, MAT_STVK_BLOCKS, true, true>, td, ga, pos(), oldp,
+                                      inv_h2, inv_h, dc, oldp, h, cr, pv)
+                 : cudaLaunchKernelEx(&cfg, k_layer_groups<R, MAT_STVK_BLOCKS, false, true>, td, ga, pos(), oldp,
+                                      inv_h2, inv_h, dc, oldp, h, cr, pv);
+        break;
+      default:
+        e = damp ? cudaLaunchKernelEx(&cfg, k_layer_groups<R, MAT_STVK_LAME, true, true>, td, ga, pos(), oldp,
+                                      inv_h2, inv_h, dc, oldp, h, cr, pv)
+                 : cudaLaunchKernelEx(&cfg, k_layer_groups<R, MAT_STVK_LAME, false, true>, td, ga, pos(), oldp,
+                                      inv_h2, inv_h, dc, oldp, h, cr, pv);
+    }
+    if (e != cudaSuccess) return set_error(MLX_ERR_CUDA, std::string("group layer launch: ") + cudaGetErrorString(e));
+    return MLX_OK;
+  }
   switch (mat_kind) {
     case MAT_NH:
       e = cudaLaunchKernelEx(&cfg, k_layer_groups<R, MAT_NH, false>, td, ga, pos(), oldp, inv_h2, inv_h, dc, oldp, h,
