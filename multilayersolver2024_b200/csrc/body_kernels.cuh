@@ -492,8 +492,11 @@ __device__ __forceinline__ void body_iteration(const LayerDev& L, int b, Body* _
 
 // One iteration's body phase as its own launch: CTAs [0, nb) run one body
 // each, the remaining CTAs the elastic contact groups.
+// Three CTAs per SM (80 registers, a few spilled FP64 values): with many
+// small bodies a layer's CTAs then run in fewer waves, which measured faster
+// than the spill-free 126-register build (configs 2-4, 1-2 %).
 template <typename R>
-__global__ void __launch_bounds__(kBodyThreads) k_iterate_bodies(LayerDev L, Body* __restrict__ bodies,
+__global__ void __launch_bounds__(kBodyThreads, 3) k_iterate_bodies(LayerDev L, Body* __restrict__ bodies,
                                                                  R4<R>* __restrict__ pos,
                                                                  const double4* __restrict__ ri,
                                                                  const double* __restrict__ vmass,
