@@ -14,7 +14,11 @@ flushed between timed steps; `e2e` is steps/s through the public host API
 its inputs host->device and its positions back).  Multi-GPU runs are
 independent replicas (weak scaling): the step does not shard.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Other workloads (`--config`): 1 = `--replicas` copies of the 8x2x2
+single-layer cantilever merged into one mesh, 3 = the 256-scene batch, 4 = the
+contact-heavy drop, 5 = the learned warm start's block.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config C]
 """
 from __future__ import annotations
 
@@ -50,6 +54,14 @@ WORKLOADS = {
         "contact resistance 0.9, dt=1/120; timed after the boxes have landed"),
 }
 WORKLOAD = WORKLOADS[2]
+REPLICAS = 4096
+
+
+def config1_workload(copies):
+    nv, nt = 81 * copies, 192 * copies
+    return (f"config1: {copies} independent copies of the 8x2x2 StVK cantilever (81 vertices, 192 tets each; "
+            f"{nv} vertices, {nt} tets) merged into one mesh (colours overlaid as Mesh3D.mergeMesh), E=1e5, nu=0.3, "
+            "one layer [0] (20 it), dt=0.01, x=0 faces pinned, undamped")
 
 
 def max_over_ranks(x, dist, device="cuda"):
@@ -118,10 +130,10 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def profiled_dram_bytes_per_tet():
-    """DRAM bytes per projected tet of the colour kernel from the committed ncu
-    summary of this workload (profiles/k_project_color_config<N>.json), or None."""
-    f = ROOT / "profiles" / f"k_project_color_config{CONFIG}.json"
+def profiled_dram_bytes_per_tet(kernel="k_project_color"):
+    """DRAM bytes per projected tet of `kernel` from the committed ncu summary
+    of this workload (profiles/<kernel>_config<N>.json), or None."""
+    f = ROOT / "profiles" / f"{kernel}_config{CONFIG}.json"
     if f.exists():
         return float(json.loads(f.read_text())["dram_bytes_per_tet"])
     return None
@@ -141,6 +153,8 @@ CONFIG = 2
 
 def make_scene():
     from multilayersolver2024_b200 import scenes
+    if CONFIG == 1:
+        return scenes.config1_replicated(REPLICAS)
     return {2: scenes.config2, 3: scenes.config3, 4: scenes.config4, 5: scenes.config5}[CONFIG]()
 
 
@@ -445,6 +459,15 @@ def run_ours(args, rank, world, local):
         else:
             sweep_kernel = "k_project_color (all colours of a sweep)"
         achieved = (sweep_bytes / (sweep_ms / 1000.0)) / 1e9 if sweep_ms > 0 else None
+        groups_only = sweep_kernel.startswith("k_layer_groups") and all(n == 0 for n in sc.layers)
+        if groups_only and profiled_dram_bytes_per_tet("k_layer_groups") is not None:
+            # one launch = the whole projectGS loop of the layer: T x iterations projections
+            traffic = profiled_dram_bytes_per_tet("k_layer_groups") * m.T * sum(sc.iterations)
+        elif profiled_dram_bytes_per_tet() is not None:
+            traffic = (profiled_dram_bytes_per_tet() * sweep_bytes / solver_bytes_per_tet(m, MLX_FP32)
+                       / max(sweep_launches, 1))
+        else:
+            traffic = None
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
@@ -468,8 +491,7 @@ def run_ours(args, rank, world, local):
                          "launch_path": solver.launch_path,
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None,
-                         "traffic": (profiled_dram_bytes_per_tet() * sweep_bytes / solver_bytes_per_tet(m, MLX_FP32)
-                                     / max(sweep_launches, 1)) if profiled_dram_bytes_per_tet() else None,
+                         "traffic": traffic,
                          "traffic_note": "DRAM bytes per launch from one ncu capture (cold cache) scaled by the "
                                          "tets per launch; achieved uses algorithmic bytes",
                          "peak_kind": peak_kind, "bytes_per_tet": solver_bytes_per_tet(m, MLX_FP32),
@@ -486,6 +508,9 @@ def run_ours(args, rank, world, local):
             "clocks": clocks.summary(),
             "state_finite": finite,
         }
+        if CONFIG in (1, 3):
+            # independent scenes in the merged mesh
+            line["scene_steps_per_s"] = value * (REPLICAS if CONFIG == 1 else 256)
         print(json.dumps(line), flush=True)
     solver.close()
     if dist:
@@ -514,9 +539,11 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-API leg (profiling runs)")
-    ap.add_argument("--config", type=int, choices=[2, 3, 4, 5], default=2,
-                    help="2: the plain multi-layer block (default); 3: the 256-scene batch; 4: the contact-heavy drop; "
-                    "5: the learned warm-start workload (64x32x32, 3 layers)")
+    ap.add_argument("--config", type=int, choices=[1, 2, 3, 4, 5], default=2,
+                    help="1: copies of the single-layer cantilever (--replicas); 2: the plain multi-layer block "
+                    "(default); 3: the 256-scene batch; 4: the contact-heavy drop; 5: the learned warm-start "
+                    "workload (64x32x32, 3 layers)")
+    ap.add_argument("--replicas", type=int, default=4096, help="config 1: copies of the cantilever in the mesh")
     ap.add_argument("--autotune", action="store_true", help="run the per-colour tile autotuner before timing "
                     "(on by default for config 3)")
     ap.add_argument("--no-autotune", action="store_true", help="never run the autotuner (profiling runs)")
@@ -530,9 +557,10 @@ def main():
     ap.add_argument("--residual-cap", type=int, default=15000,
                     help="hangingStop of the residual leg (bounds the iterations of a step)")
     args = ap.parse_args()
-    global CONFIG, WORKLOAD
+    global CONFIG, WORKLOAD, REPLICAS
     CONFIG = args.config
-    WORKLOAD = WORKLOADS[CONFIG]
+    REPLICAS = max(1, args.replicas)
+    WORKLOAD = config1_workload(REPLICAS) if CONFIG == 1 else WORKLOADS[CONFIG]
     if CONFIG == 3:
         args.autotune = True
         args.cpu_steps = min(args.cpu_steps, 1)

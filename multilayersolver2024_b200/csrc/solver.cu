@@ -893,7 +893,10 @@ int Solver<R>::plan_groups(const mlx_mesh_desc* md) {
   const long long budget = (long long)optin - (long long)fa.sharedSizeBytes - 1024;
   const long long vmax = budget / (long long)sizeof(R4<R>);
   std::vector<int> gv0{0}, acc(C, 0);
-  long long gv = 0, max_gv = 0, max_passes = 0;
+  long long gv = 0, max_gv = 0, max_passes = 0, gt = 0;
+  // a group closes once it holds T / SMs tets, so many small components
+  // spread over all SMs instead of filling fewer CTAs to the colour limit
+  const long long target = ((long long)T + sms - 1) / sms;
   auto passes = [&]() {
     long long n = 0;
     for (int q = 0; q < C; ++q) n += (acc[q] + kGroupThreads - 1) / kGroupThreads;
@@ -904,14 +907,18 @@ int Solver<R>::plan_groups(const mlx_mesh_desc* md) {
     if (nv > vmax) return MLX_OK;
     bool fits = gv + nv <= vmax;
     for (int q = 0; q < C && fits; ++q) fits = acc[q] + ccol[(size_t)c * C + q] <= kGroupThreads;
-    if (gv > 0 && !fits) {
+    if (gv > 0 && (!fits || gt >= target)) {
       gv0.push_back(cv0[c]);
       max_gv = std::max(max_gv, gv);
       max_passes = std::max(max_passes, passes());
       std::fill(acc.begin(), acc.end(), 0);
       gv = 0;
+      gt = 0;
     }
-    for (int q = 0; q < C; ++q) acc[q] += ccol[(size_t)c * C + q];
+    for (int q = 0; q < C; ++q) {
+      acc[q] += ccol[(size_t)c * C + q];
+      gt += ccol[(size_t)c * C + q];
+    }
     gv += nv;
   }
   gv0.push_back(N);

@@ -94,6 +94,30 @@ def config1(energy=_lib.MLX_ENERGY_STVK_VOIGT) -> Scene:
     return Scene("config1_cantilever_8x2x2", m, 0.01, 200, [0], [20])
 
 
+def config1_replicated(copies: int = 16384, per_row: int = 128, energy=_lib.MLX_ENERGY_STVK_VOIGT) -> Scene:
+    """`copies` independent copies of the config-1 cantilever in one mesh, laid
+    out as Mesh3D.mergeMesh lays out its parts (vertices and tets
+    concatenated, tets offset by the vertices before them, colours overlaid:
+    first-fit colouring of disjoint parts gives every part its solo colours).
+    Copies sit on a grid in the y-z plane, 0.4 m apart, `per_row` per row;
+    every copy's x = 0 face is pinned.  Settings as config1 (one layer [0],
+    20 iterations, dt = 0.01, undamped); the rigid sets are given (all zero)
+    so a step builds no layers."""
+    V1, T1, _ = generate_beam(8, 2, 2, 0.1)
+    n1, t1 = V1.shape[0], T1.shape[0]
+    k = np.arange(copies)
+    off = np.stack([np.zeros(copies), 0.4 * (k % per_row), 0.4 * (k // per_row)], 1)
+    V = (V1[None, :, :] + off[:, None, :]).reshape(-1, 3)
+    T = (T1[None, :, :].astype(np.int64) + (n1 * k)[:, None, None]).reshape(-1, 4).astype(np.int32)
+    mu, lam = to_lame(0.3, 1e5)
+    m = Mesh3D.from_arrays(V, T, mu, lam, rho=1000.0, alpha1=0.0, energy_type=energy)
+    m.pin(np.nonzero(np.isclose(V[:, 0], 0.0))[0] + 1)
+    m.part_vertex_offsets = n1 * np.arange(copies + 1)
+    m.part_tet_offsets = t1 * np.arange(copies + 1)
+    sets = np.zeros((m.T, 1), np.int32, order="F")
+    return Scene(f"config1_cantilever_8x2x2_x{copies}", m, 0.01, 200, [0], [20], custom_sets=sets)
+
+
 def config2(seed: int = 2, nx=64, ny=16, nz=16, cluster=8) -> Scene:
     """Plain multi-layer Neo-Hookean block: 64x16x16 cubes (18,785 vertices,
     98,304 tets), per-tet E log-uniform in [1e4, 1e7], nu uniform in

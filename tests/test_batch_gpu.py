@@ -8,7 +8,11 @@ per-colour tile autotuner.
     independent, bodies are reduced per body);
   * the autotuner changes no result bit (it only changes block sizes);
   * a small batch matches the FP64 oracle within the FP32 tolerance 1e-4 of
-    each scene's bounding-box diagonal.
+    each scene's bounding-box diagonal;
+  * copies of the config-1 cantilever in one mesh: the copy at the origin is
+    bit-identical to the cantilever stepped alone, and every copy matches the
+    FP64 oracle's solo cantilever (shifted) within the FP32 tolerance 1e-3 of
+    its bounding-box diagonal that the 200-step solo cantilever is held to.
 """
 import numpy as np
 import pytest
@@ -86,3 +90,20 @@ def test_autotuner_keeps_results(gpu):
     for s in range(3):
         sim.step(1, graph=True)
         np.testing.assert_array_equal(sim.state()[0], ref[s])
+
+
+def test_replicated_cantilevers(gpu, oracle):
+    k, steps = 64, 10
+    batch = scenes.config1_replicated(k, per_row=8)
+    got, _ = _resident_run(batch, steps, _lib.MLX_FP32)
+    solo, _ = _resident_run(scenes.config1_replicated(1), steps, _lib.MLX_FP32)
+    n3 = solo[0].size
+    for s in range(steps):
+        np.testing.assert_array_equal(got[s][:n3], solo[s], err_msg=f"step {s}")
+    ref = _oracle_run(scenes.config1(), steps, oracle)
+    d = scenes.config1().mesh.bbox_diagonal()
+    err = 0.0
+    for c in range(k):
+        shift = np.tile([0.0, 0.4 * (c % 8), 0.4 * (c // 8)], n3 // 3)
+        err = max(err, max(np.abs(g[c * n3:(c + 1) * n3] - shift - r).max() / d for g, r in zip(got, ref)))
+    assert err <= 1e-3, f"{err:.3e}"

@@ -10,7 +10,8 @@ the colour launches: positions bit-identical at every step, for
   * damped StVK blocks (step-start positions read for the damping term),
     FP32 and FP64;
   * the single-component cantilever of config 1 with the path forced, FP64,
-    which also matches the oracle.
+    which also matches the oracle;
+  * 64 copies of that cantilever in one mesh, FP32.
 """
 import numpy as np
 import pytest
@@ -87,6 +88,11 @@ def test_drop_with_device_contacts(gpu, monkeypatch):
         return scenes.config4(seed=11, n_boxes=3, cubes=4, grid=(3, 1), spacing=1.5, n_spheres=1, coarse=2, mid=2,
                               drop=(0.005, 0.015))
     _same(monkeypatch, small, 30, _lib.MLX_FP32, v0z=-1.0)
+
+
+def test_replicated_cantilevers(gpu, monkeypatch):
+    """64 copies of the config-1 cantilever: one CTA owns many whole copies."""
+    _same(monkeypatch, lambda: scenes.config1_replicated(64, per_row=8), 5, _lib.MLX_FP32)
 
 
 def _damped_blocks():
