@@ -438,6 +438,32 @@ int mlx_find_boundary_vertices(const int32_t* t, int32_t num_tets,
                                uint8_t* is_rigid_vertex,
                                int32_t* vertex_rigid_body);
 
+/* The per-step vector arithmetic of xpbdLayer3D.integrate around layerSolve,
+ * each phase one fused pass over the DOFs (split over host threads for large
+ * meshes), with the reference's operation order so results are the same
+ * doubles as the element-wise MATLAB expressions.
+ *
+ * mlx_any_nan: any(isnan(x)) of the step-start check (xpbdLayer3D.m:629).
+ * Returns 1 or 0 (0 for n <= 0), or minus MLX_ERR_ARGUMENT for a NULL x.
+ *
+ * mlx_integrate_begin (xpbdLayer3D.m:638-643, 662-664): forces
+ * f = [0, 0, mass_z * gravity] + custom force (`custom_force_vec` of
+ * num_dofs values, or the scalar `custom_force` when it is NULL) and the
+ * residual velocity (1 - air_drag) * (v + h f / mass) with the h f / mass
+ * term left out at the 1-based `pinned_dofs`.  f and residualv may not alias
+ * the inputs.
+ *
+ * mlx_integrate_end (xpbdLayer3D.m:737): v = (xi - oldp) / h.  v may alias
+ * neither input. */
+int32_t mlx_any_nan(int64_t n, const double* x);
+int mlx_integrate_begin(int32_t num_dofs, double h, double gravity, double air_drag,
+                        double custom_force, const double* custom_force_vec,
+                        const double* mass, const double* v,
+                        const int32_t* pinned_dofs, int32_t num_pinned,
+                        double* f, double* residualv);
+int mlx_integrate_end(int32_t num_dofs, double h, const double* xi, const double* oldp,
+                      double* v);
+
 #ifdef __cplusplus
 }
 #endif

@@ -178,6 +178,10 @@ SIGNATURES = {
                               C.c_int),
     "mlx_find_boundary_vertices": ([_i32p, C.c_int32, C.c_int32, _i32p, C.c_int32, _u8p, _u8p, _u8p, _i32p],
                                    C.c_int),
+    "mlx_any_nan": ([C.c_int64, _f64p], C.c_int32),
+    "mlx_integrate_begin": ([C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, _f64p, _f64p, _f64p, _i32p,
+                             C.c_int32, _f64p, _f64p], C.c_int),
+    "mlx_integrate_end": ([C.c_int32, C.c_double, _f64p, _f64p, _f64p], C.c_int),
 }
 
 _lib = None

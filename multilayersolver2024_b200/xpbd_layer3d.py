@@ -368,7 +368,7 @@ def call_layer_solve(fn, solver_or_desc, layer_desc, params, contacts, xi, lambd
     else:
         cap = (rin.size + 1 + max(0, params.hanging_stop if params.hanging_stop >= 0 else 0) +
                sum(int(layer_desc.iterations[i]) for i in range(layer_desc.num_layers)) + 100000)
-    out_xi = np.zeros(N3)
+    out_xi = np.empty(N3)  # every value is written
     if want_lambda and lam_ is None:
         raise ValueError("want_lambda needs lambdai")
     out_lam = np.zeros(lam_.shape, order="F") if want_lambda else None
@@ -408,6 +408,15 @@ class ContactSet:
         return ContactSet(np.concatenate([s.normals for s in sets]), np.concatenate([s.points for s in sets]),
                           np.concatenate([s.vertex_ids for s in sets]).astype(np.int32),
                           np.concatenate([s.compliance for s in sets]))
+
+
+def _any_nan(lib, x) -> bool:
+    """any(isnan(x)) (xpbdLayer3D.m:629) in one native pass."""
+    x = np.ascontiguousarray(x, np.float64)
+    r = lib.mlx_any_nan(x.size, f64(x))
+    if r < 0:
+        check("mlx_any_nan", -r, lib)
+    return bool(r)
 
 
 def contact_velocity_update(normals, vertex_ids, v, h, gravity, dim=3, restitution=1e-5):
@@ -566,18 +575,38 @@ class XpbdLayer3D:
         self._fbv = (mesh, sets, ls)
         return ls
 
+    def _layer_desc(self, ls):
+        """pack_layer_desc of this step, kept while the layer set object, the
+        layers map and the iteration counts stay the same."""
+        key = (tuple(np.ravel(self.layersMap).tolist()), tuple(np.ravel(self.iterations).tolist()))
+        c = getattr(self, "_ld", None)
+        if c is not None and c[0] is ls and c[1] == key:
+            return c[2], c[3]
+        ld, keep = pack_layer_desc(ls, self.layersMap, self.iterations)
+        self._ld = (ls, key, ld, keep)
+        return ld, keep
+
     def integrate(self, mesh: Mesh3D, h: float, contacts: ContactSet, cache: StepCache, frame: int):
         """xpbdLayer3D.integrate (xpbdLayer3D.m:621-745)."""
         assert len(self.layers) and len(self.iterations)
         assert self.boundaryCompliance < 1e-5
         sumNonMonitoredTime = 0.0
-        if cache.oldp is None or np.any(np.isnan(cache.oldp)) or frame == 1:
+        lib = load()
+        if cache.oldp is None or frame == 1 or _any_nan(lib, cache.oldp):
             cache.oldp = mesh.p.copy()
             self.pinnedx = mesh.p[mesh.pinnedDOFs - 1].copy()
         tic = time.perf_counter()
-        f = np.zeros(3 * mesh.N)
-        f[2::3] = f[2::3] + mesh.mass[2::3] * self.Gravity
-        f = f + self.CustomForce
+        # forces and residual velocity (xpbdLayer3D.m:638-643, 662-664) in one
+        # native pass; the pinned DOFs get no h f / m term
+        n3 = 3 * mesh.N
+        f, resv = np.empty(n3), np.empty(n3)
+        cf = self.CustomForce
+        cfv = None if np.ndim(cf) == 0 else np.ascontiguousarray(np.broadcast_to(cf, (n3,)), np.float64)
+        pins = np.ascontiguousarray(mesh.pinnedDOFs, np.int32)
+        check("mlx_integrate_begin", lib.mlx_integrate_begin(
+            n3, float(h), float(self.Gravity), float(self.airDrag), float(cf) if cfv is None else 0.0, f64(cfv),
+            f64(np.ascontiguousarray(mesh.mass, np.float64)), f64(np.ascontiguousarray(mesh.v, np.float64)),
+            i32(pins), pins.size, f64(f), f64(resv)), lib)
         mesh.f = f
         if self.customRigidSets is None and self.layerBuilder == "device":
             # buildLayers and findBoundaryVertices in one device call
@@ -592,17 +621,11 @@ class XpbdLayer3D:
         cache.layers = ls.isRigidElement
         cache.oldOldp = cache.oldp
         cache.oldp = mesh.p.copy()
-        xi = mesh.p.copy()
-        # resv(unpinned) += h f / m: the same quotients, formed for every DOF
-        # and zeroed at the pinned ones (cheaper than two gathers and a scatter)
-        dv = h * f / mesh.mass
-        dv[mesh.pinnedDOFs - 1] = 0.0
-        resv = (1 - self.airDrag) * (mesh.v + dv)
+        xi = mesh.p  # layerSolve only reads it; mesh.p is replaced by its result
         lambdai = None  # zeros(T, 6) (xpbdLayer3D.m:666): the library zeroes them on the device
         residualArray = np.array([0.0])
-        ld, keep = pack_layer_desc(ls, self.layersMap, self.iterations)
+        ld, keep = self._layer_desc(ls)
         cts, keep2 = pack_contacts(contacts.normals, contacts.points, contacts.vertex_ids, contacts.compliance)
-        lib = load()
         rc, res = call_layer_solve(lib.mlx_layer_solve, self.solver(mesh).handle, ld, make_params(self, h), cts,
                                    xi, lambdai, cache.oldp, cache.oldOldp, f, resv, self.pinnedx, residualArray,
                                    sumNonMonitoredTime)
@@ -610,7 +633,9 @@ class XpbdLayer3D:
         xi, sumNonMonitoredTime, residualArray, self.runUntilResSmallerThan = res[0], res[1], res[2], res[3]
         self.last_total_iterations = res[5]
         cache.residualArray = residualArray[1:]
-        mesh.v = (xi - cache.oldp) / h
+        v = np.empty(n3)
+        check("mlx_integrate_end", lib.mlx_integrate_end(n3, float(h), f64(xi), f64(cache.oldp), f64(v)), lib)
+        mesh.v = v
         mesh.p = xi
         mesh.v = contact_velocity_update(contacts.normals, contacts.vertex_ids, mesh.v, h, self.Gravity, 3, 1e-2)
         integrate_forces = time.perf_counter() - tic - sumNonMonitoredTime
