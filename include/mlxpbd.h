@@ -464,6 +464,17 @@ int mlx_integrate_begin(int32_t num_dofs, double h, double gravity, double air_d
 int mlx_integrate_end(int32_t num_dofs, double h, const double* xi, const double* oldp,
                       double* v);
 
+/* xpbdLayer2D.contactVelocityUpdate (2d/integrator/xpbdLayer2D.m:577-603),
+ * called after the step with the step-start contacts (xpbdLayer3D.m:740):
+ * normals K x dim column-major, 1-based vertex ids (the first column of
+ * contactVertexID), v of num_dofs = dim x vertices values; the updated
+ * velocities go to v_out, which may be v itself.  A vertex with several
+ * contacts keeps its last contact's value. */
+int mlx_contact_velocity_update(int32_t num_contacts, const double* normals,
+                                const int32_t* vertex_ids, int32_t dim, int64_t num_dofs,
+                                const double* v, double h, double gravity,
+                                double restitution, double* v_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -182,6 +182,8 @@ SIGNATURES = {
     "mlx_integrate_begin": ([C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, _f64p, _f64p, _f64p, _i32p,
                              C.c_int32, _f64p, _f64p], C.c_int),
     "mlx_integrate_end": ([C.c_int32, C.c_double, _f64p, _f64p, _f64p], C.c_int),
+    "mlx_contact_velocity_update": ([C.c_int32, _f64p, _i32p, C.c_int32, C.c_int64, _f64p, C.c_double, C.c_double,
+                                     C.c_double, _f64p], C.c_int),
 }
 
 _lib = None

@@ -85,13 +85,14 @@ def find_contacts(solver, finders, p):
     p = np.ascontiguousarray(p, dtype=np.float64)
     N = p.size // 3
     cap = max(N * n, 1)
-    ids = np.zeros(cap, np.int32)
-    nrm = np.zeros(3 * cap)
-    pts = np.zeros(3 * cap)
-    comp = np.zeros(cap)
+    # only the first K rows (3K values) are written and read
+    ids = np.empty(cap, np.int32)
+    nrm = np.empty(3 * cap)
+    pts = np.empty(3 * cap)
+    comp = np.empty(cap)
     K = C.c_int32(0)
     check("mlx_find_contacts", lib.mlx_find_contacts(solver.handle, C.cast(arr, C.c_void_p), n, f64(p), cap, i32(ids),
                                                      f64(nrm), f64(pts), f64(comp), C.byref(K)), lib)
     k = K.value
-    return ContactSet(nrm[:3 * k].reshape(3, k).T.copy(), pts[:3 * k].reshape(3, k).T.copy(), ids[:k].copy(),
-                      comp[:k].copy())
+    # K x 3 column-major views of the written rows, the layout layerSolve takes
+    return ContactSet(nrm[:3 * k].reshape(3, k).T, pts[:3 * k].reshape(3, k).T, ids[:k], comp[:k])

@@ -1,7 +1,7 @@
 // host_integrate.cpp -- the per-step vector arithmetic of
 // xpbdLayer3D.integrate around layerSolve (xpbdLayer3D.m:621-745) on the host:
 // the NaN check of the step-start positions, forces and residual velocity
-// before the solve, the velocity update after it.  Each is one fused pass
+// before the solve, the velocity update and contactVelocityUpdate after it.  Each is one fused pass
 // over the DOFs with the reference's operation order (the same doubles as
 // its element-wise expressions); meshes of more than 2^16 DOFs are split
 // over the host threads.
@@ -9,6 +9,8 @@
 #include <atomic>
 #include <cmath>
 #include <cstdint>
+#include <cstring>
+#include <memory>
 #include <thread>
 #include <vector>
 
@@ -21,11 +23,12 @@ namespace {
 
 constexpr long long kGrain = 1 << 16;  // DOFs per thread at least
 
-// fn(begin, end) over [0, n), on up to hardware_concurrency() threads.
+// fn(begin, end) over [0, n), on up to hardware_concurrency() threads of at
+// least `grain` items each.
 template <typename F>
-void parallel_ranges(long long n, F fn) {
+void parallel_ranges(long long n, F fn, long long grain = kGrain) {
   const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const long long nt = std::min<long long>(hw, (n + kGrain - 1) / kGrain);
+  const long long nt = std::min<long long>(hw, (n + grain - 1) / grain);
   if (nt <= 1) {
     if (n > 0) fn(0LL, n);
     return;
@@ -103,6 +106,46 @@ int mlx_integrate_end(int32_t num_dofs, double h, const double* xi, const double
   parallel_ranges(num_dofs, [&](long long a, long long b) {
     for (long long i = a; i < b; ++i) v[i] = (xi[i] - oldp[i]) / h;
   });
+  return MLX_OK;
+}
+
+// xpbdLayer2D.contactVelocityUpdate (2d/integrator/xpbdLayer2D.m:577-603):
+// per contact, the vertex's velocity vn (read before any write), e = 0 when
+// |vn| <= 2 gravity h, else the restitution; vn + n .* (-vn + min(-e (n . vn), 0))
+// written back in contact order, so a repeated vertex keeps its last contact's
+// value as MATLAB's v(dofs) = ... does.
+int mlx_contact_velocity_update(int32_t num_contacts, const double* normals, const int32_t* vertex_ids, int32_t dim,
+                                int64_t num_dofs, const double* v, double h, double gravity, double restitution,
+                                double* v_out) {
+  if (num_contacts < 0 || num_dofs < 0) return set_error(MLX_ERR_ARGUMENT, "negative size");
+  if (dim != 2 && dim != 3) return set_error(MLX_ERR_ARGUMENT, "dim must be 2 or 3");
+  if (num_dofs % dim) return set_error(MLX_ERR_ARGUMENT, "num_dofs is not a multiple of dim");
+  if (num_dofs > 0 && (!v || !v_out)) return set_error(MLX_ERR_ARGUMENT, "v and v_out are required");
+  if (num_contacts > 0 && (!normals || !vertex_ids)) return set_error(MLX_ERR_ARGUMENT, "normals and vertex_ids are required");
+  const long long nv = num_dofs / dim, K = num_contacts;
+  for (long long k = 0; k < K; ++k)
+    if (vertex_ids[k] < 1 || vertex_ids[k] > nv) return set_error(MLX_ERR_ARGUMENT, "contact vertex id out of range");
+  std::unique_ptr<double[]> nvel(new double[(size_t)K * dim]);
+  const double thresh = 2 * gravity * h;
+  const bool can_stop = thresh >= 0;  // |vn| <= a negative threshold never holds
+  parallel_ranges(K, [&](long long a, long long b) {
+    for (long long k = a; k < b; ++k) {
+      const double* vk = v + (size_t)(vertex_ids[k] - 1) * dim;
+      double sq = vk[0] * vk[0], vt = normals[k] * vk[0];
+      for (int c = 1; c < dim; ++c) {
+        sq = sq + vk[c] * vk[c];
+        vt = vt + normals[k + c * K] * vk[c];
+      }
+      const double e = can_stop && std::sqrt(sq) <= thresh ? 0.0 : restitution;
+      const double m = std::min(-e * vt, 0.0);
+      for (int c = 0; c < dim; ++c) nvel[(size_t)k * dim + c] = vk[c] + normals[k + c * K] * (-vk[c] + m);
+    }
+  }, kGrain / 8);  // scattered reads: threads pay off sooner
+  if (v_out != v) std::memcpy(v_out, v, sizeof(double) * (size_t)num_dofs);
+  for (long long k = 0; k < K; ++k) {
+    double* o = v_out + (size_t)(vertex_ids[k] - 1) * dim;
+    for (int c = 0; c < dim; ++c) o[c] = nvel[(size_t)k * dim + c];
+  }
   return MLX_OK;
 }
 

@@ -420,19 +420,21 @@ def _any_nan(lib, x) -> bool:
 
 
 def contact_velocity_update(normals, vertex_ids, v, h, gravity, dim=3, restitution=1e-5):
-    """xpbdLayer2D.contactVelocityUpdate (2d/integrator/xpbdLayer2D.m:577-603)."""
+    """xpbdLayer2D.contactVelocityUpdate (2d/integrator/xpbdLayer2D.m:577-603)
+    in one native pass (``mlx_contact_velocity_update``); returns a new array
+    (`v` itself without contacts)."""
     K = normals.shape[0]
     if K == 0:
         return v
-    e = np.full(K, restitution)
-    rows = np.asarray(vertex_ids, np.int64).ravel() - 1  # the dofs of vertex k are row k of v as (N, dim)
-    vn = v.reshape(-1, dim)[rows]
-    e[np.linalg.norm(vn, axis=1) <= 2 * gravity * h] = 0
-    vt = np.sum(normals * vn, axis=1)
-    dv = normals * (-vn + np.minimum(-e * vt, 0)[:, None])
-    v = v.copy()
-    v.reshape(-1, dim)[rows] = vn + dv  # repeated vertices: the last contact's value stays
-    return v
+    lib = load()
+    n = np.asfortranarray(np.asarray(normals, np.float64).reshape(K, dim))
+    ids = np.ascontiguousarray(vertex_ids, np.int32).ravel()[:K]
+    vin = np.ascontiguousarray(v, np.float64)
+    out = np.empty(vin.size)
+    check("mlx_contact_velocity_update", lib.mlx_contact_velocity_update(K, f64(n), i32(ids), dim, vin.size, f64(vin),
+                                                                         float(h), float(gravity), float(restitution),
+                                                                         f64(out)), lib)
+    return out
 
 
 class XpbdLayer3D:

@@ -69,3 +69,66 @@ def test_argument_errors(lib):
                                    f64(np.empty(n3)), f64(np.empty(n3))) == _lib.MLX_ERR_ARGUMENT
     assert lib.mlx_integrate_end(n3, 0.01, None, f64(a), f64(np.empty(n3))) == _lib.MLX_ERR_ARGUMENT
     assert lib.mlx_any_nan(3, None) == -_lib.MLX_ERR_ARGUMENT
+
+
+def _cvu_reference(normals, ids, v, h, gravity, dim, restitution):
+    """contactVelocityUpdate (2d/integrator/xpbdLayer2D.m:577-603) restated in
+    numpy: gather, threshold, normal response, last write wins."""
+    K = normals.shape[0]
+    e = np.full(K, restitution)
+    rows = ids.astype(np.int64) - 1
+    vn = v.reshape(-1, dim)[rows]
+    e[np.linalg.norm(vn, axis=1) <= 2 * gravity * h] = 0
+    vt = np.sum(normals * vn, axis=1)
+    dv = normals * (-vn + np.minimum(-e * vt, 0)[:, None])
+    out = v.copy()
+    for k in range(K):  # explicit contact order: a repeated vertex keeps its last contact
+        out.reshape(-1, dim)[rows[k]] = vn[k] + dv[k]
+    return out
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("gravity", [-9.81, 9.81])
+def test_contact_velocity_update_equals_the_reference_expressions(lib, dim, gravity):
+    rng = np.random.default_rng(dim)
+    nv, K = 500, 700  # more contacts than vertices: repeated vertices
+    v = rng.normal(0, 0.5, dim * nv)
+    ids = rng.integers(1, nv + 1, K).astype(np.int32)
+    n = rng.normal(0, 1, (K, dim))
+    n /= np.linalg.norm(n, axis=1)[:, None]
+    h, e = 1.0 / 60.0, 1e-2
+    ref = _cvu_reference(n, ids, v, h, gravity, dim, e)
+    nf = np.asfortranarray(n)
+    out = np.empty_like(v)
+    assert lib.mlx_contact_velocity_update(K, f64(nf), i32(ids), dim, v.size, f64(v), h, gravity, e,
+                                           f64(out)) == _lib.MLX_OK
+    np.testing.assert_array_equal(out, ref)
+    w = v.copy()  # in place
+    assert lib.mlx_contact_velocity_update(K, f64(nf), i32(ids), dim, w.size, f64(w), h, gravity, e,
+                                           f64(w)) == _lib.MLX_OK
+    np.testing.assert_array_equal(w, ref)
+    from multilayersolver2024_b200.xpbd_layer3d import contact_velocity_update
+    np.testing.assert_array_equal(contact_velocity_update(n, ids, v, h, gravity, dim, e), ref)
+
+
+def test_contact_velocity_update_matches_the_oracle(lib, oracle):
+    rng = np.random.default_rng(5)
+    nv, K = 300, 400
+    v = rng.normal(0, 0.5, 3 * nv)
+    ids = rng.integers(1, nv + 1, K).astype(np.int32)
+    n = rng.normal(0, 1, (K, 3))
+    n /= np.linalg.norm(n, axis=1)[:, None]
+    from multilayersolver2024_b200.xpbd_layer3d import contact_velocity_update
+    got = contact_velocity_update(n, ids, v, 1 / 120, -9.81, 3, 1e-2)
+    ref = oracle.contact_velocity_update(n, ids, v.copy(), 1 / 120, -9.81, 1e-2)
+    np.testing.assert_array_equal(got, ref)
+
+
+def test_contact_velocity_update_errors(lib):
+    v = np.zeros(9)
+    n = np.asfortranarray(np.ones((1, 3)))
+    assert lib.mlx_contact_velocity_update(1, f64(n), i32(np.array([4], np.int32)), 3, 9, f64(v), 0.01, -9.8, 0.0,
+                                           f64(v)) == _lib.MLX_ERR_ARGUMENT
+    assert lib.mlx_contact_velocity_update(1, f64(n), i32(np.array([1], np.int32)), 4, 9, f64(v), 0.01, -9.8, 0.0,
+                                           f64(v)) == _lib.MLX_ERR_ARGUMENT
+    assert lib.mlx_contact_velocity_update(0, None, None, 3, 9, f64(v), 0.01, -9.8, 0.0, f64(v)) == _lib.MLX_OK
