@@ -324,7 +324,7 @@ def run_ours(args, rank, world, local):
         contact_bytes.append(cs.vertex_ids.size)
         integ2.integrate(m2, sc2.h, cs, cache, frame)
 
-    e2e_steps = 0 if args.no_e2e else max(3, min(args.steps, 20 if CONFIG == 2 else 3))
+    e2e_steps = 0 if args.no_e2e else max(3, min(args.steps, {2: 20, 3: 3}.get(CONFIG, 10)))
     for frame in range(1, 3 if e2e_steps else 1):  # warm-up: solver creation and layer caches
         e2e_step(frame)
     barrier()

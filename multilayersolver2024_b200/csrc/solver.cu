@@ -117,12 +117,14 @@ struct DevBuf {
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() { if (p) cudaFree(p); }
-  int ensure(size_t n) {
+  // grow: a buffer whose size changes from call to call (contact lists)
+  // takes half as much again, so a slowly growing size reallocates rarely
+  int ensure(size_t n, bool grow = false) {
     if (n <= bytes && p) return MLX_OK;
     if (p) cudaFree(p);
     p = nullptr;
     bytes = 0;
-    size_t want = std::max<size_t>(n, 256);
+    size_t want = std::max<size_t>(grow ? n + n / 2 : n, 256);
     cudaError_t e = cudaMalloc(&p, want);
     if (e != cudaSuccess) return set_error(MLX_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e));
     bytes = want;
@@ -137,12 +139,12 @@ struct PinnedBuf {
   PinnedBuf(const PinnedBuf&) = delete;
   PinnedBuf& operator=(const PinnedBuf&) = delete;
   ~PinnedBuf() { if (p) cudaFreeHost(p); }
-  int ensure(size_t n) {
+  int ensure(size_t n, bool grow = false) {
     if (n <= bytes && p) return MLX_OK;
     if (p) cudaFreeHost(p);
     p = nullptr;
     bytes = 0;
-    size_t want = std::max<size_t>(n, 256);
+    size_t want = std::max<size_t>(grow ? n + n / 2 : n, 256);
     cudaError_t e = cudaMallocHost(&p, want);
     if (e != cudaSuccess) return set_error(MLX_ERR_ALLOC, std::string("cudaMallocHost: ") + cudaGetErrorString(e));
     bytes = want;
@@ -1517,10 +1519,10 @@ int Solver<R>::upload_contacts(const mlx_contacts* K, ContactData& cd) {
     return set_error(MLX_ERR_ARGUMENT, "contact arrays are NULL");
   for (int k = 0; k < nK; ++k)
     if (K->vertex_ids[k] < 1 || K->vertex_ids[k] > N) return set_error(MLX_ERR_ARGUMENT, "contact vertex id out of range");
-  CHECK(h_cstage.ensure(sizeof(double) * 7 * nK + sizeof(int) * nK));
-  CHECK(d_contacts.ensure(sizeof(double) * 7 * nK));
-  CHECK(d_cvid.ensure(sizeof(int) * nK));
-  CHECK(d_clam.ensure(sizeof(double) * nK));
+  CHECK(h_cstage.ensure(sizeof(double) * 7 * nK + sizeof(int) * nK, true));
+  CHECK(d_contacts.ensure(sizeof(double) * 7 * nK, true));
+  CHECK(d_cvid.ensure(sizeof(int) * nK, true));
+  CHECK(d_clam.ensure(sizeof(double) * nK, true));
   double* hc = h_cstage.as<double>();
   std::memcpy(hc, K->normals, sizeof(double) * 3 * nK);
   std::memcpy(hc + 3 * nK, K->point_colliders, sizeof(double) * 3 * nK);
@@ -1688,7 +1690,7 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
       std::copy(rc_ids.begin(), rc_ids.end(), cpack + o_rci);
       std::copy(ec_off.begin(), ec_off.end(), cpack + o_eco);
       std::copy(ec_ids.begin(), ec_ids.end(), cpack + o_eci);
-      CHECK(d_cgroups.ensure(sizeof(int) * need));
+      CHECK(d_cgroups.ensure(sizeof(int) * need, true));
       CU(cudaMemcpyAsync(d_cgroups.p, cpack, sizeof(int) * need, cudaMemcpyHostToDevice, stream));
       const int* dc = d_cgroups.as<int>();
       L.rc_off = dc + o_rco;
