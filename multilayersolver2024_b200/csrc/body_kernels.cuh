@@ -32,9 +32,10 @@ struct LayerDev {
   int any_rigid_contact;    // the layer has at least one rigid contact
   const int* vert_body;     // [N] 1-based body of each vertex, 0 = elastic
   const unsigned char* vert_rigid;  // [N] isRigidVertex
-  int n_ec_groups;          // elastic contacts grouped by vertex
+  int n_ec_groups;          // elastic contacts grouped by vertex, ascending vertex
   const int* ec_off;        // [n_ec_groups+1]
   const int* ec_ids;        // contact ids, ascending inside a group
+  const int* ec_vert;       // [n_ec_groups] the vertex of each group
   int n_items;              // CTAs of the per-body kernels
   const int* items;         // [n_items][kItemInts]: see body_of_item
 };
@@ -315,33 +316,12 @@ __device__ __forceinline__ void apply_increments(Body& B, const double* s, doubl
   mm3(B.R, tmp, B.I);
 }
 
-// Elastic contacts of one vertex (contactConstraints elastic branch,
-// xpbdLayer3D.m:426-438 + penaltyConstraint.projectElastic :4-28): every
-// contact of the group reads the same step-start position, each updates its
-// multiplier, and the last one's position is kept (MATLAB's scatter).
+// Elastic contacts of one vertex of the layer's host contact list
+// (elastic_contact_list_group over the layer's vertex groups).
 template <typename R, typename P>
 __device__ __forceinline__ void elastic_contact_group(const LayerDev& L, int g, const P& pos,
                                                       const ContactData& cd, double h, double contact_resistance) {
-  double h2 = h * h;
-  int k0 = L.ec_off[g], k1 = L.ec_off[g + 1];
-  int v = cd.vid[L.ec_ids[k0]];
-  R4<R> p = pos.ld(v);
-  D3 x = d3((double)p.x, (double)p.y, (double)p.z);
-  double minv = (double)p.w;
-  D3 xn = x;
-  for (int q = k0; q < k1; ++q) {
-    int k = L.ec_ids[q];
-    D3 n = d3(cd.normal[k], cd.normal[cd.K + k], cd.normal[2 * cd.K + k]);
-    D3 c = d3(cd.point[k], cd.point[cd.K + k], cd.point[2 * cd.K + k]);
-    double phi = dot(n, x - c);
-    if (phi > 0) phi = 0;
-    double C = contact_resistance * phi;
-    double aT = cd.compliance[k] / h2;
-    double dl = (-C - aT * cd.lambda[k]) / (2 * minv + aT);
-    cd.lambda[k] += dl;
-    xn = d3(x.x + minv * (dl * n.x), x.y + minv * (dl * n.y), x.z + minv * (dl * n.z));
-  }
-  pos.st(v, make_r4<R>((R)xn.x, (R)xn.y, (R)xn.z, p.w));
+  elastic_contact_list_group<R>(L.ec_off, L.ec_ids, g, pos, cd, h, contact_resistance);
 }
 
 // One iteration of one rigid body, run by a whole CTA: the rigid-elastic glue

@@ -88,6 +88,37 @@ __device__ __forceinline__ bool obstacle_contact(const Obstacle& o, double x, do
   return true;
 }
 
+// Elastic contacts of one vertex from a host contact list (contactConstraints
+// elastic branch, xpbdLayer3D.m:426-438 + penaltyConstraint.projectElastic
+// :4-28): contacts ids[off[g] .. off[g+1]) all touch one vertex; every one
+// reads the same step-start position, each updates its multiplier, and the
+// last one's position is kept (MATLAB's scatter).
+template <typename R, typename P>
+__device__ __forceinline__ void elastic_contact_list_group(const int* __restrict__ off, const int* __restrict__ ids,
+                                                           int g, const P& pos, const ContactData& cd, double h,
+                                                           double contact_resistance) {
+  double h2 = h * h;
+  int k0 = off[g], k1 = off[g + 1];
+  int v = cd.vid[ids[k0]];
+  R4<R> p = pos.ld(v);
+  D3 x = d3((double)p.x, (double)p.y, (double)p.z);
+  double minv = (double)p.w;
+  D3 xn = x;
+  for (int q = k0; q < k1; ++q) {
+    int k = ids[q];
+    D3 n = d3(cd.normal[k], cd.normal[cd.K + k], cd.normal[2 * cd.K + k]);
+    D3 c = d3(cd.point[k], cd.point[cd.K + k], cd.point[2 * cd.K + k]);
+    double phi = dot(n, x - c);
+    if (phi > 0) phi = 0;
+    double C = contact_resistance * phi;
+    double aT = cd.compliance[k] / h2;
+    double dl = (-C - aT * cd.lambda[k]) / (2 * minv + aT);
+    cd.lambda[k] += dl;
+    xn = d3(x.x + minv * (dl * n.x), x.y + minv * (dl * n.y), x.z + minv * (dl * n.z));
+  }
+  pos.st(v, make_r4<R>((R)xn.x, (R)xn.y, (R)xn.z, p.w));
+}
+
 // Contacts of the resident stepper for the current step.
 struct DevContacts {
   int nobs;                // 0: no obstacles

@@ -20,8 +20,9 @@
 //    slots, DmInv, material, lambda read and write) are loaded before the
 //    barrier that precedes its colour when every colour of the group fits in
 //    one pass of the CTA;
-//  * the contact phase (device-detected contacts of the group's vertices) and
-//    the pinning phase run on the same records.
+//  * the contact phase (device-detected contacts of the group's vertices, or
+//    the vertex groups of a host contact list) and the pinning phase run on
+//    the same records.
 //
 // The per-tet arithmetic is tet_update of the other paths and every vertex
 // sees the same sequence of updates, so results are bit-identical to the
@@ -46,6 +47,17 @@ struct GroupArgs {
   const int* pin_dofs;   // 0-based DOFs, ascending
   int C, G, iterations;
   int one_per_thread;    // no (colour, group) range exceeds blockDim.x
+};
+
+// The elastic contacts of a host contact list grouped by vertex, groups in
+// ascending vertex order (off / ids as elastic_contact_list_group takes them,
+// vert[g] the vertex of group g).
+struct HostContactGroups {
+  ContactData cd;
+  const int* off;
+  const int* ids;
+  const int* vert;
+  int n;
 };
 
 // The records of one group, addressed by vertex id.
@@ -105,14 +117,17 @@ __device__ __forceinline__ int lower_bound_dev(const int* a, int n, int x) {
 }
 
 // One launch = the whole projectGS loop of one body-free layer; CTA g owns
-// group g.  Dynamic shared memory: the records of the largest group.  CC:
-// contacts coloured with the elastic constraints (a separate instantiation,
-// so the reference-order kernel carries none of that code).
-template <typename R, int MAT, bool DAMP, bool CC = false>
+// group g.  Dynamic shared memory: the records of the largest group.  CMODE
+// (each a separate instantiation, so the reference-order kernel carries none
+// of the other code): 0 = no contacts or device-detected contacts after the
+// sweep; 1 = device contacts coloured with the elastic constraints; 2 = a
+// host contact list (`hc`) after the sweep.
+template <typename R, int MAT, bool DAMP, int CMODE = 0>
 __global__ void __launch_bounds__(kGroupThreads, 1)
     k_layer_groups(TetData<R> td, GroupArgs ga, R4<R>* __restrict__ pos, const R4<R>* __restrict__ oldp,
                    R inv_h2, R inv_h, DevContacts dc, const R4<R>* __restrict__ x0, double h,
-                   double contact_resistance, const R* __restrict__ pin_vals) {
+                   double contact_resistance, const R* __restrict__ pin_vals, HostContactGroups hc) {
+  constexpr bool CC = CMODE == 1, HC = CMODE == 2;
   extern __shared__ __align__(32) unsigned char gr_smem[];
   R4<R>* rec = reinterpret_cast<R4<R>*>(gr_smem);
   __shared__ int crange[2];
@@ -125,6 +140,11 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
     const int n = *dc.count;
     crange[0] = lower_bound_dev(dc.verts, n, v0);
     crange[1] = lower_bound_dev(dc.verts, n, v0 + nv);
+  }
+  if (HC && tid == 0) {
+    // the host list's vertex groups are ascending by vertex: the group's are one range
+    crange[0] = lower_bound_dev(hc.vert, hc.n, v0);
+    crange[1] = lower_bound_dev(hc.vert, hc.n, v0 + nv);
   }
   TetRest<R, MAT> cur;
   int4 slot = make_int4(0, 0, 0, 0);
@@ -175,6 +195,11 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
     if (dc.nobs) {
       for (int i = crange[0] + tid; i < crange[1]; i += nthr)
         if (!CC || dc.vcc[dc.verts[i]] == dc.C) elastic_contacts_of_vertex<R>(dc, i, sp, x0, h, contact_resistance);
+      __syncthreads();
+    }
+    if (HC) {
+      for (int q = crange[0] + tid; q < crange[1]; q += nthr)
+        elastic_contact_list_group<R>(hc.off, hc.ids, q, sp, hc.cd, h, contact_resistance);
       __syncthreads();
     }
     const int p0 = ga.pin_off[g], p1 = ga.pin_off[g + 1];

@@ -445,7 +445,7 @@ struct Solver final : SolverBase {
                    int32_t* num_rigids, uint8_t* is_elastic, uint8_t* is_boundary, uint8_t* is_rigid_vertex,
                    int32_t* vertex_body) override;
   int launch_groups(const LayerStatic& ls, const int* dint, const mlx_solve_params* P, int iterations,
-                    const DevContacts& dc);
+                    const DevContacts& dc, const HostContactGroups* hc = nullptr);
   int build_cluster_slots(LayerStatic& ls, const std::vector<int>& list);
   int launch_cluster(const LayerStatic& ls, const int* dint, const LayerDev& L, const ContactData& cd,
                      const mlx_solve_params* P, int iterations, bool body_work, LayerWork& w);
@@ -807,24 +807,26 @@ int Solver<R>::plan_cluster(const mlx_mesh_desc* md, MeshPartition& mp) {
   return MLX_OK;
 }
 
-template <typename R>
-static const void* group_kernel(int mat_kind, bool damp, bool cc = false) {
+template <typename R, int CM>
+static const void* group_kernel_mode(int mat_kind, bool damp) {
   switch (mat_kind) {
     case MAT_NH:
-      return cc ? (const void*)k_layer_groups<R, MAT_NH, false, true> : (const void*)k_layer_groups<R, MAT_NH, false>;
+      return (const void*)k_layer_groups<R, MAT_NH, false, CM>;
     case MAT_STVK_BLOCKS:
-      if (cc)
-        return damp ? (const void*)k_layer_groups<R, MAT_STVK_BLOCKS, true, true>
-                    : (const void*)k_layer_groups<R, MAT_STVK_BLOCKS, false, true>;
-      return damp ? (const void*)k_layer_groups<R, MAT_STVK_BLOCKS, true>
-                  : (const void*)k_layer_groups<R, MAT_STVK_BLOCKS, false>;
+      return damp ? (const void*)k_layer_groups<R, MAT_STVK_BLOCKS, true, CM>
+                  : (const void*)k_layer_groups<R, MAT_STVK_BLOCKS, false, CM>;
     default:
-      if (cc)
-        return damp ? (const void*)k_layer_groups<R, MAT_STVK_LAME, true, true>
-                    : (const void*)k_layer_groups<R, MAT_STVK_LAME, false, true>;
-      return damp ? (const void*)k_layer_groups<R, MAT_STVK_LAME, true>
-                  : (const void*)k_layer_groups<R, MAT_STVK_LAME, false>;
+      return damp ? (const void*)k_layer_groups<R, MAT_STVK_LAME, true, CM>
+                  : (const void*)k_layer_groups<R, MAT_STVK_LAME, false, CM>;
   }
+}
+
+// The group kernel of a material; mode as k_layer_groups' CMODE.
+template <typename R>
+static const void* group_kernel(int mat_kind, bool damp, int mode = 0) {
+  if (mode == 1) return group_kernel_mode<R, 1>(mat_kind, damp);
+  if (mode == 2) return group_kernel_mode<R, 2>(mat_kind, damp);
+  return group_kernel_mode<R, 0>(mat_kind, damp);
 }
 
 // Groups of consecutive vertex-disconnected components for the
@@ -958,8 +960,9 @@ int Solver<R>::plan_groups(const mlx_mesh_desc* md) {
   }
   gr_smem = (size_t)max_gv * sizeof(R4<R>);
   CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(gr_smem, 16)));
-  CU(cudaFuncSetAttribute(group_kernel<R>(mat_kind, damp, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)std::max<size_t>(gr_smem, 16)));
+  for (int mode = 1; mode <= 2; ++mode)
+    CU(cudaFuncSetAttribute(group_kernel<R>(mat_kind, damp, mode), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)std::max<size_t>(gr_smem, 16)));
   CHECK(d_gv0.ensure(sizeof(int) * gv0.size()));
   CHECK(d_tloc.ensure(sizeof(int4) * (size_t)T));
   CHECK(d_gpin.ensure(sizeof(int) * gpin.size()));
@@ -972,9 +975,31 @@ int Solver<R>::plan_groups(const mlx_mesh_desc* md) {
   return MLX_OK;
 }
 
+// k_layer_groups<R, material, damping, CM> on a launch configuration.
+template <typename R, int CM>
+static cudaError_t launch_group_kernel(cudaLaunchConfig_t* cfg, int mat_kind, bool damp, TetData<R> td, GroupArgs ga,
+                                       R4<R>* p, const R4<R>* oldp, R inv_h2, R inv_h, const DevContacts& dc,
+                                       double h, double cr, const R* pv, const HostContactGroups& hc) {
+  switch (mat_kind) {
+    case MAT_NH:
+      return cudaLaunchKernelEx(cfg, k_layer_groups<R, MAT_NH, false, CM>, td, ga, p, oldp, inv_h2, inv_h, dc, oldp, h,
+                                cr, pv, hc);
+    case MAT_STVK_BLOCKS:
+      return damp ? cudaLaunchKernelEx(cfg, k_layer_groups<R, MAT_STVK_BLOCKS, true, CM>, td, ga, p, oldp, inv_h2,
+                                       inv_h, dc, oldp, h, cr, pv, hc)
+                  : cudaLaunchKernelEx(cfg, k_layer_groups<R, MAT_STVK_BLOCKS, false, CM>, td, ga, p, oldp, inv_h2,
+                                       inv_h, dc, oldp, h, cr, pv, hc);
+    default:
+      return damp ? cudaLaunchKernelEx(cfg, k_layer_groups<R, MAT_STVK_LAME, true, CM>, td, ga, p, oldp, inv_h2,
+                                       inv_h, dc, oldp, h, cr, pv, hc)
+                  : cudaLaunchKernelEx(cfg, k_layer_groups<R, MAT_STVK_LAME, false, CM>, td, ga, p, oldp, inv_h2,
+                                       inv_h, dc, oldp, h, cr, pv, hc);
+  }
+}
+
 template <typename R>
 int Solver<R>::launch_groups(const LayerStatic& ls, const int* dint, const mlx_solve_params* P, int iterations,
-                             const DevContacts& dc) {
+                             const DevContacts& dc, const HostContactGroups* hc) {
   GroupArgs ga;
   ga.list = ls.identity_list ? nullptr : dint + ls.o_list;
   ga.off = dint + ls.o_goff;
@@ -997,45 +1022,12 @@ int Solver<R>::launch_groups(const LayerStatic& ls, const int* dint, const mlx_s
   const R4<R>* oldp = d_oldp.as<R4<R>>();
   const R* pv = d_pinx.as<R>();
   const double h = P->h, cr = P->contact_resistance;
-  cudaError_t e;
-  if (dc.colored) {
-    switch (mat_kind) {
-      case MAT_NH:
-        e = cudaLaunchKernelEx(&cfg, k_layer_groups<R, MAT_NH, false, true>, td, ga, pos(), oldp, inv_h2, inv_h, dc,
-                               oldp, h, cr, pv);
-        break;
-      case MAT_STVK_BLOCKS:
-        e = damp ? cudaLaunchKernelEx(&cfg, k_layer_groups<R, MAT_STVK_BLOCKS, true, true>, td, ga, pos(), oldp,
-                                      inv_h2, inv_h, dc, oldp, h, cr, pv)
-                 : cudaLaunchKernelEx(&cfg, k_layer_groups<R, MAT_STVK_BLOCKS, false, true>, td, ga, pos(), oldp,
-                                      inv_h2, inv_h, dc, oldp, h, cr, pv);
-        break;
-      default:
-        e = damp ? cudaLaunchKernelEx(&cfg, k_layer_groups<R, MAT_STVK_LAME, true, true>, td, ga, pos(), oldp,
-                                      inv_h2, inv_h, dc, oldp, h, cr, pv)
-                 : cudaLaunchKernelEx(&cfg, k_layer_groups<R, MAT_STVK_LAME, false, true>, td, ga, pos(), oldp,
-                                      inv_h2, inv_h, dc, oldp, h, cr, pv);
-    }
-    if (e != cudaSuccess) return set_error(MLX_ERR_CUDA, std::string("group layer launch: ") + cudaGetErrorString(e));
-    return MLX_OK;
-  }
-  switch (mat_kind) {
-    case MAT_NH:
-      e = cudaLaunchKernelEx(&cfg, k_layer_groups<R, MAT_NH, false>, td, ga, pos(), oldp, inv_h2, inv_h, dc, oldp, h,
-                             cr, pv);
-      break;
-    case MAT_STVK_BLOCKS:
-      e = damp ? cudaLaunchKernelEx(&cfg, k_layer_groups<R, MAT_STVK_BLOCKS, true>, td, ga, pos(), oldp, inv_h2,
-                                    inv_h, dc, oldp, h, cr, pv)
-               : cudaLaunchKernelEx(&cfg, k_layer_groups<R, MAT_STVK_BLOCKS, false>, td, ga, pos(), oldp, inv_h2,
-                                    inv_h, dc, oldp, h, cr, pv);
-      break;
-    default:
-      e = damp ? cudaLaunchKernelEx(&cfg, k_layer_groups<R, MAT_STVK_LAME, true>, td, ga, pos(), oldp, inv_h2,
-                                    inv_h, dc, oldp, h, cr, pv)
-               : cudaLaunchKernelEx(&cfg, k_layer_groups<R, MAT_STVK_LAME, false>, td, ga, pos(), oldp, inv_h2,
-                                    inv_h, dc, oldp, h, cr, pv);
-  }
+  HostContactGroups none{};
+  const HostContactGroups& hg_ = hc ? *hc : none;
+  const cudaError_t e =
+      dc.colored ? launch_group_kernel<R, 1>(&cfg, mat_kind, damp, td, ga, pos(), oldp, inv_h2, inv_h, dc, h, cr, pv, hg_)
+      : hc       ? launch_group_kernel<R, 2>(&cfg, mat_kind, damp, td, ga, pos(), oldp, inv_h2, inv_h, dc, h, cr, pv, hg_)
+                 : launch_group_kernel<R, 0>(&cfg, mat_kind, damp, td, ga, pos(), oldp, inv_h2, inv_h, dc, h, cr, pv, hg_);
   if (e != cudaSuccess) return set_error(MLX_ERR_CUDA, std::string("group layer launch: ") + cudaGetErrorString(e));
   return MLX_OK;
 }
@@ -1656,29 +1648,30 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
           if (b > 0) rc_ids[f[b - 1]++] = k;
         }
       }
-      // elastic contacts grouped by vertex (groups in first-occurrence order)
-      std::vector<int> first(N, -1), ec_cnt;
-      std::vector<int> group_of(nK, -1);
+      // elastic contacts grouped by vertex, groups in ascending vertex order
+      // (a vertex's contacts keep their list order; groups are independent)
+      std::vector<int> vcnt(N, 0), ec_off{0}, ec_vert, ec_ids;
       for (int k = 0; k < nK; ++k) {
-        int v = K->vertex_ids[k] - 1;
-        if (rid[v] != 0) continue;
-        if (first[v] < 0) { first[v] = (int)ec_cnt.size(); ec_cnt.push_back(0); }
-        group_of[k] = first[v];
-        ++ec_cnt[first[v]];
+        const int v = K->vertex_ids[k] - 1;
+        if (rid[v] == 0) ++vcnt[v];
       }
-      int ng = (int)ec_cnt.size();
-      std::vector<int> ec_off(ng + 1, 0), ec_ids;
-      for (int q = 0; q < ng; ++q) ec_off[q + 1] = ec_off[q] + ec_cnt[q];
+      for (int v = 0; v < N; ++v)
+        if (vcnt[v]) {
+          ec_vert.push_back(v);
+          ec_off.push_back(ec_off.back() + vcnt[v]);
+          vcnt[v] = ec_off[ec_off.size() - 2];  // now the group's next free slot
+        }
+      const int ng = (int)ec_vert.size();
       ec_ids.resize(ec_off[ng]);
-      {
-        std::vector<int> f(ec_off.begin(), ec_off.end() - 1);
-        for (int k = 0; k < nK; ++k)
-          if (group_of[k] >= 0) ec_ids[f[group_of[k]]++] = k;
+      for (int k = 0; k < nK; ++k) {
+        const int v = K->vertex_ids[k] - 1;
+        if (rid[v] == 0) ec_ids[vcnt[v]++] = k;
       }
-      size_t o_rco = 0, o_rci = rc_off.size(), o_eco = o_rci + rc_ids.size(), o_eci = o_eco + ec_off.size();
+      size_t o_rco = 0, o_rci = rc_off.size(), o_eco = o_rci + rc_ids.size(), o_eci = o_eco + ec_off.size(),
+             o_ecv = o_eci + ec_ids.size();
       // the lists go through pinned memory that no copy in flight reads: each
       // layer of a call takes a new range (reset once the call has synchronised)
-      const size_t need = o_eci + ec_ids.size();
+      const size_t need = o_ecv + ec_vert.size();
       if (cpack_used + need > h_cpack.bytes / sizeof(int)) {
         CU(cudaStreamSynchronize(stream));
         CHECK(h_cpack.ensure(sizeof(int) * std::max(need, 2 * (h_cpack.bytes / sizeof(int)))));
@@ -1690,6 +1683,7 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
       std::copy(rc_ids.begin(), rc_ids.end(), cpack + o_rci);
       std::copy(ec_off.begin(), ec_off.end(), cpack + o_eco);
       std::copy(ec_ids.begin(), ec_ids.end(), cpack + o_eci);
+      std::copy(ec_vert.begin(), ec_vert.end(), cpack + o_ecv);
       CHECK(d_cgroups.ensure(sizeof(int) * need, true));
       CU(cudaMemcpyAsync(d_cgroups.p, cpack, sizeof(int) * need, cudaMemcpyHostToDevice, stream));
       const int* dc = d_cgroups.as<int>();
@@ -1699,6 +1693,7 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
       L.n_ec_groups = ng;
       L.ec_off = dc + o_eco;
       L.ec_ids = dc + o_eci;
+      L.ec_vert = dc + o_ecv;
     }
     const bool rigidLayer = ls.n_rigid_elements > 0;
     R4<R>* p = pos();
@@ -1791,14 +1786,15 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
       }
       continue;
     }
-    if (groups_ok && ls.gr_ok && ls.nb == 0 && nK == 0 && !P->compute_residuals) {
+    if (groups_ok && ls.gr_ok && ls.nb == 0 && !P->compute_residuals) {
       // a body-free layer with a fixed iteration count: one launch, a CTA per
       // group of components
       const int iters = std::max(ld->iterations[layer], 0);
       if (iters > 0) {
         const bool timed = sweep_timing && tev_used + 2 <= tev.size();
         if (timed) CHECK(record_event(tev[tev_used], capturing));
-        CHECK(launch_groups(ls, dint, P, iters, dc));
+        const HostContactGroups hcg{cd, L.ec_off, L.ec_ids, L.ec_vert, L.n_ec_groups};
+        CHECK(launch_groups(ls, dint, P, iters, dc, nK > 0 ? &hcg : nullptr));
         if (timed) {
           double b = 0;
           for (int c = 0; c < C; ++c) b += ls.color_count[c] * (group_bytes_per_tet() + (ls.identity_list ? 0.0 : 4.0));

@@ -6,7 +6,8 @@ the colour launches: positions bit-identical at every step, for
     layer (the cluster layer keeps the colour launches, the fine layer takes
     the group path), FP32;
   * the contact-heavy drop at reduced size (device contacts in the group
-    kernel's contact phase), FP32;
+    kernel's contact phase), FP32, and the same drop through the host API
+    (the finders' contact list grouped by vertex in the group kernel);
   * damped StVK blocks (step-start positions read for the damping term),
     FP32 and FP64;
   * the single-component cantilever of config 1 with the path forced, FP64,
@@ -93,6 +94,42 @@ def test_drop_with_device_contacts(gpu, monkeypatch):
 def test_replicated_cantilevers(gpu, monkeypatch):
     """64 copies of the config-1 cantilever: one CTA owns many whole copies."""
     _same(monkeypatch, lambda: scenes.config1_replicated(64, per_row=8), 5, _lib.MLX_FP32)
+
+
+def test_host_contact_lists_on_the_group_path(gpu, monkeypatch):
+    """simulate3D's loop through the host API (finders, then integrate ->
+    mlx_layer_solve with the contact list): the body-free layer runs on the
+    group path with the list's vertex groups, and every frame's positions
+    and velocities equal the colour launches' bit for bit."""
+    from multilayersolver2024_b200.contacts import find_contacts
+    from multilayersolver2024_b200.xpbd_layer3d import StepCache
+
+    def run(flag):
+        monkeypatch.setenv("MLXPBD_GROUPS", flag)
+        sc = scenes.config4(seed=11, n_boxes=3, cubes=4, grid=(3, 1), spacing=1.5, n_spheres=1, coarse=2, mid=2,
+                            drop=(0.005, 0.015))
+        m = sc.mesh
+        m.v[2::3] = -1.0
+        it = _integ(sc, _lib.MLX_FP32)
+        cache = StepCache()
+        out, counts = [], []
+        for frame in range(1, 31):
+            cs = find_contacts(it.solver(m), sc.contact_finders, m.p)
+            counts.append(int(cs.vertex_ids.size))
+            it.integrate(m, sc.h, cs, cache, frame)
+            out.append((m.p.copy(), m.v.copy()))
+        paths = [s.launch_path for s in it._solvers.values()]
+        for s in it._solvers.values():
+            s.close()
+        return out, counts, paths
+
+    a, ca, pa = run("1")
+    b, cb, pb = run("0")
+    assert any(GROUP_PATH in p for p in pa) and not any(GROUP_PATH in p for p in pb)
+    assert max(ca) > 100 and ca == cb
+    for k in range(len(a)):
+        np.testing.assert_array_equal(a[k][0], b[k][0], err_msg=f"positions, frame {k + 1}")
+        np.testing.assert_array_equal(a[k][1], b[k][1], err_msg=f"velocities, frame {k + 1}")
 
 
 def _damped_blocks():
