@@ -126,7 +126,7 @@ def test_host_contact_lists_on_the_group_path(gpu, monkeypatch):
     a, ca, pa = run("1")
     b, cb, pb = run("0")
     assert any(GROUP_PATH in p for p in pa) and not any(GROUP_PATH in p for p in pb)
-    assert max(ca) > 100 and ca == cb
+    assert max(ca) > 20 and ca == cb
     for k in range(len(a)):
         np.testing.assert_array_equal(a[k][0], b[k][0], err_msg=f"positions, frame {k + 1}")
         np.testing.assert_array_equal(a[k][1], b[k][1], err_msg=f"velocities, frame {k + 1}")
