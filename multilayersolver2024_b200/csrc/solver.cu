@@ -36,6 +36,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 using namespace mlx;
@@ -152,6 +153,27 @@ struct PinnedBuf {
   }
   template <typename T> T* as() const { return static_cast<T*>(p); }
 };
+
+// memcpy between host buffers, split over up to 8 host threads when it is
+// large (the staging of a call's host vectors into pinned memory and back).
+static void host_copy(void* dst, const void* src, size_t bytes) {
+  constexpr size_t kGrain = size_t(512) << 10;
+  const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t nt = std::min<size_t>(std::min<size_t>(hw, 8), bytes / kGrain);
+  if (nt <= 1) {
+    if (bytes) std::memcpy(dst, src, bytes);
+    return;
+  }
+  const size_t chunk = (bytes + nt - 1) / nt;
+  std::vector<std::thread> th;
+  th.reserve(nt - 1);
+  for (size_t t = 1; t < nt; ++t) {
+    const size_t a = t * chunk, b = std::min(bytes, a + chunk);
+    if (a < b) th.emplace_back([=] { std::memcpy(static_cast<char*>(dst) + a, static_cast<const char*>(src) + a, b - a); });
+  }
+  std::memcpy(dst, src, std::min(bytes, chunk));
+  for (std::thread& x : th) x.join();
+}
 
 struct DeviceGuard {
   int prev = -1;
@@ -1516,9 +1538,9 @@ int Solver<R>::upload_contacts(const mlx_contacts* K, ContactData& cd) {
   CHECK(d_cvid.ensure(sizeof(int) * nK, true));
   CHECK(d_clam.ensure(sizeof(double) * nK, true));
   double* hc = h_cstage.as<double>();
-  std::memcpy(hc, K->normals, sizeof(double) * 3 * nK);
-  std::memcpy(hc + 3 * nK, K->point_colliders, sizeof(double) * 3 * nK);
-  std::memcpy(hc + 6 * nK, K->compliance, sizeof(double) * nK);
+  host_copy(hc, K->normals, sizeof(double) * 3 * nK);
+  host_copy(hc + 3 * nK, K->point_colliders, sizeof(double) * 3 * nK);
+  host_copy(hc + 6 * nK, K->compliance, sizeof(double) * nK);
   int* hv = reinterpret_cast<int*>(hc + 7 * nK);
   for (int k = 0; k < nK; ++k) hv[k] = K->vertex_ids[k] - 1;
   CU(cudaMemcpyAsync(d_contacts.p, hc, sizeof(double) * 7 * nK, cudaMemcpyHostToDevice, stream));
@@ -2304,13 +2326,26 @@ int Solver<R>::layer_solve(const mlx_layer_desc* ld, const mlx_solve_params* P, 
   CHECK(h_stage.ensure(sizeof(double) * nst));
   CHECK(d_stage.ensure(sizeof(double) * nst));
   double* hs = h_stage.as<double>();
-  std::memcpy(hs, in->xi, sizeof(double) * n3);
-  std::memcpy(hs + n3, in->residualv, sizeof(double) * n3);
-  if (damp) std::memcpy(hs + o_old, in->oldp, sizeof(double) * n3);
-  if (in->lambdai) std::memcpy(hs + o_lam, in->lambdai, sizeof(double) * n6);
-  if (np) std::memcpy(hs + o_pin, in->pinnedx, sizeof(double) * np);
-  CU(cudaMemcpyAsync(d_stage.p, hs, sizeof(double) * (o_pin + np), cudaMemcpyHostToDevice, stream));
   double* ds = d_stage.as<double>();
+  // vectors of a MB or more go up one by one, each copy overlapping the
+  // staging of the next
+  const bool piecewise = sizeof(double) * n3 >= (size_t(1) << 20);
+  size_t sent = 0;
+  auto stage = [&](size_t off, const double* src, size_t n) -> int {
+    host_copy(hs + off, src, sizeof(double) * n);
+    if (piecewise) {
+      CU(cudaMemcpyAsync(ds + sent, hs + sent, sizeof(double) * (off + n - sent), cudaMemcpyHostToDevice, stream));
+      sent = off + n;
+    }
+    return MLX_OK;
+  };
+  CHECK(stage(0, in->xi, n3));
+  CHECK(stage(n3, in->residualv, n3));
+  if (damp) CHECK(stage(o_old, in->oldp, n3));
+  if (in->lambdai) CHECK(stage(o_lam, in->lambdai, n6));
+  if (np) CHECK(stage(o_pin, in->pinnedx, np));
+  if (o_pin + np > sent)
+    CU(cudaMemcpyAsync(ds + sent, hs + sent, sizeof(double) * (o_pin + np - sent), cudaMemcpyHostToDevice, stream));
   const int bs = 256;
   k_load_pos<R><<<blocks_for(N, bs), bs, 0, stream>>>(ds, d_mass3.as<double>(), pos(), N);
   k_load_vec<R><<<blocks_for(N, bs), bs, 0, stream>>>(ds + n3, d_resv.as<R4<R>>(), N);
@@ -2381,8 +2416,8 @@ int Solver<R>::layer_solve(const mlx_layer_desc* ld, const mlx_solve_params* P, 
   CU(cudaStreamSynchronize(stream));
   cpack_used = 0;  // no copy of the contact lists is in flight now
   CHECK(check_gsync());
-  std::memcpy(out->xi, hs, sizeof(double) * n3);
-  if (out->lambdai) std::memcpy(out->lambdai, hs + n3, sizeof(double) * n6);
+  host_copy(out->xi, hs, sizeof(double) * n3);
+  if (out->lambdai) host_copy(out->lambdai, hs + n3, sizeof(double) * n6);
   int n = (int)st.residualArray.size();
   if (out->residual) {
     if (n > out->residual_capacity) return set_error(MLX_ERR_ARGUMENT, "residual capacity too small");
