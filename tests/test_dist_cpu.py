@@ -60,3 +60,17 @@ def test_reference_arm_two_ranks():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["kind"] == "port"
+
+
+def test_reference_arm_replicated_cantilevers():
+    """The reference arm on the replicated config-1 workload: one line whose
+    workload names the copies and their sizes."""
+    cmd = [sys.executable, "bench.py", "--impl", "reference", "--config", "1", "--replicas", "16", "--steps", "1",
+           "--warmup", "0"]
+    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["value"] > 0
+    assert d["config"]["workload"].startswith("config1: 16 independent copies") and "3072 tets" in d["config"]["workload"]
