@@ -11,6 +11,7 @@
 #include <cstdint>
 #include <cstring>
 #include <memory>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -38,19 +39,19 @@ void parallel_ranges(long long n, F fn, long long grain = kGrain) {
   th.reserve((size_t)nt - 1);
   for (long long t = 1; t < nt; ++t) {
     const long long a = t * chunk, b = std::min(n, a + chunk);
-    if (a < b) th.emplace_back(fn, a, b);
+    if (a >= b) continue;
+    try {
+      th.emplace_back(fn, a, b);
+    } catch (const std::system_error&) {
+      fn(a, b);  // no thread to be had: this one runs the range
+    }
   }
   fn(0LL, std::min(n, chunk));
   for (std::thread& x : th) x.join();
 }
 
-}  // namespace
-
-extern "C" {
-
-int32_t mlx_any_nan(int64_t n, const double* x) {
-  if (n <= 0) return 0;
-  if (!x) return -set_error(MLX_ERR_ARGUMENT, "x is NULL");  // negative: 1 means found
+// any(isnan(x)) over n > 0 values: 1 or 0.
+int any_nan_impl(long long n, const double* x) {
   std::atomic<int> found{0};
   parallel_ranges(n, [&](long long a, long long b) {
     for (long long i = a; i < b; i += 4096) {
@@ -67,46 +68,64 @@ int32_t mlx_any_nan(int64_t n, const double* x) {
   return found.load();
 }
 
+}  // namespace
+
+extern "C" {
+
+int32_t mlx_any_nan(int64_t n, const double* x) {
+  if (n <= 0) return 0;
+  if (!x) return -set_error(MLX_ERR_ARGUMENT, "x is NULL");  // negative: 1 means found
+  try {
+    return any_nan_impl(n, x);
+  } catch (...) {
+    return -set_error(MLX_ERR_ALLOC, "host resource exhausted");
+  }
+}
+
 // f(3:3:end) = f(3:3:end) + mass(3:3:end) * Gravity on a reset force, then
 // f = f + CustomForce (xpbdLayer3D.m:638-643); residualVelocity = v, plus
 // h * f ./ mass on the unpinned DOFs, times (1 - airDrag) (:662-664).
 int mlx_integrate_begin(int32_t num_dofs, double h, double gravity, double air_drag, double custom_force,
                         const double* custom_force_vec, const double* mass, const double* v,
                         const int32_t* pinned_dofs, int32_t num_pinned, double* f, double* residualv) {
-  if (num_dofs < 0 || num_pinned < 0) return set_error(MLX_ERR_ARGUMENT, "negative size");
-  if (num_dofs % 3) return set_error(MLX_ERR_ARGUMENT, "num_dofs is not a multiple of 3");
-  if (num_dofs == 0) return MLX_OK;
-  if (!mass || !v || !f || !residualv) return set_error(MLX_ERR_ARGUMENT, "mass, v, f and residualv are required");
-  if (num_pinned > 0 && !pinned_dofs) return set_error(MLX_ERR_ARGUMENT, "pinned_dofs is NULL");
-  for (int32_t i = 0; i < num_pinned; ++i)
-    if (pinned_dofs[i] < 1 || pinned_dofs[i] > num_dofs) return set_error(MLX_ERR_ARGUMENT, "pinned DOF out of range");
-  const double keep = 1.0 - air_drag;
-  parallel_ranges(num_dofs, [&](long long a, long long b) {
-    for (long long i = a; i < b; ++i) {
-      const double g = (i % 3 == 2) ? 0.0 + mass[i] * gravity : 0.0;
-      const double fi = g + (custom_force_vec ? custom_force_vec[i] : custom_force);
-      f[i] = fi;
-      residualv[i] = keep * (v[i] + h * fi / mass[i]);
+  return mlx::guarded([&]() -> int {
+    if (num_dofs < 0 || num_pinned < 0) return set_error(MLX_ERR_ARGUMENT, "negative size");
+    if (num_dofs % 3) return set_error(MLX_ERR_ARGUMENT, "num_dofs is not a multiple of 3");
+    if (num_dofs == 0) return MLX_OK;
+    if (!mass || !v || !f || !residualv) return set_error(MLX_ERR_ARGUMENT, "mass, v, f and residualv are required");
+    if (num_pinned > 0 && !pinned_dofs) return set_error(MLX_ERR_ARGUMENT, "pinned_dofs is NULL");
+    for (int32_t i = 0; i < num_pinned; ++i)
+      if (pinned_dofs[i] < 1 || pinned_dofs[i] > num_dofs) return set_error(MLX_ERR_ARGUMENT, "pinned DOF out of range");
+    const double keep = 1.0 - air_drag;
+    parallel_ranges(num_dofs, [&](long long a, long long b) {
+      for (long long i = a; i < b; ++i) {
+        const double g = (i % 3 == 2) ? 0.0 + mass[i] * gravity : 0.0;
+        const double fi = g + (custom_force_vec ? custom_force_vec[i] : custom_force);
+        f[i] = fi;
+        residualv[i] = keep * (v[i] + h * fi / mass[i]);
+      }
+    });
+    // pinned DOFs: the velocity alone (the reference adds h f / m on the
+    // unpinned ones only)
+    for (int32_t i = 0; i < num_pinned; ++i) {
+      const int32_t d = pinned_dofs[i] - 1;
+      residualv[d] = keep * v[d];
     }
+    return MLX_OK;
   });
-  // pinned DOFs: the velocity alone (the reference adds h f / m on the
-  // unpinned ones only)
-  for (int32_t i = 0; i < num_pinned; ++i) {
-    const int32_t d = pinned_dofs[i] - 1;
-    residualv[d] = keep * v[d];
-  }
-  return MLX_OK;
 }
 
 // mesh3D.v = (xi - cache.oldp) ./ h (xpbdLayer3D.m:737).
 int mlx_integrate_end(int32_t num_dofs, double h, const double* xi, const double* oldp, double* v) {
-  if (num_dofs < 0) return set_error(MLX_ERR_ARGUMENT, "negative size");
-  if (num_dofs == 0) return MLX_OK;
-  if (!xi || !oldp || !v) return set_error(MLX_ERR_ARGUMENT, "xi, oldp and v are required");
-  parallel_ranges(num_dofs, [&](long long a, long long b) {
-    for (long long i = a; i < b; ++i) v[i] = (xi[i] - oldp[i]) / h;
+  return mlx::guarded([&]() -> int {
+    if (num_dofs < 0) return set_error(MLX_ERR_ARGUMENT, "negative size");
+    if (num_dofs == 0) return MLX_OK;
+    if (!xi || !oldp || !v) return set_error(MLX_ERR_ARGUMENT, "xi, oldp and v are required");
+    parallel_ranges(num_dofs, [&](long long a, long long b) {
+      for (long long i = a; i < b; ++i) v[i] = (xi[i] - oldp[i]) / h;
+    });
+    return MLX_OK;
   });
-  return MLX_OK;
 }
 
 // xpbdLayer2D.contactVelocityUpdate (2d/integrator/xpbdLayer2D.m:577-603):
@@ -117,36 +136,38 @@ int mlx_integrate_end(int32_t num_dofs, double h, const double* xi, const double
 int mlx_contact_velocity_update(int32_t num_contacts, const double* normals, const int32_t* vertex_ids, int32_t dim,
                                 int64_t num_dofs, const double* v, double h, double gravity, double restitution,
                                 double* v_out) {
-  if (num_contacts < 0 || num_dofs < 0) return set_error(MLX_ERR_ARGUMENT, "negative size");
-  if (dim != 2 && dim != 3) return set_error(MLX_ERR_ARGUMENT, "dim must be 2 or 3");
-  if (num_dofs % dim) return set_error(MLX_ERR_ARGUMENT, "num_dofs is not a multiple of dim");
-  if (num_dofs > 0 && (!v || !v_out)) return set_error(MLX_ERR_ARGUMENT, "v and v_out are required");
-  if (num_contacts > 0 && (!normals || !vertex_ids)) return set_error(MLX_ERR_ARGUMENT, "normals and vertex_ids are required");
-  const long long nv = num_dofs / dim, K = num_contacts;
-  for (long long k = 0; k < K; ++k)
-    if (vertex_ids[k] < 1 || vertex_ids[k] > nv) return set_error(MLX_ERR_ARGUMENT, "contact vertex id out of range");
-  std::unique_ptr<double[]> nvel(new double[(size_t)K * dim]);
-  const double thresh = 2 * gravity * h;
-  const bool can_stop = thresh >= 0;  // |vn| <= a negative threshold never holds
-  parallel_ranges(K, [&](long long a, long long b) {
-    for (long long k = a; k < b; ++k) {
-      const double* vk = v + (size_t)(vertex_ids[k] - 1) * dim;
-      double sq = vk[0] * vk[0], vt = normals[k] * vk[0];
-      for (int c = 1; c < dim; ++c) {
-        sq = sq + vk[c] * vk[c];
-        vt = vt + normals[k + c * K] * vk[c];
+  return mlx::guarded([&]() -> int {
+    if (num_contacts < 0 || num_dofs < 0) return set_error(MLX_ERR_ARGUMENT, "negative size");
+    if (dim != 2 && dim != 3) return set_error(MLX_ERR_ARGUMENT, "dim must be 2 or 3");
+    if (num_dofs % dim) return set_error(MLX_ERR_ARGUMENT, "num_dofs is not a multiple of dim");
+    if (num_dofs > 0 && (!v || !v_out)) return set_error(MLX_ERR_ARGUMENT, "v and v_out are required");
+    if (num_contacts > 0 && (!normals || !vertex_ids)) return set_error(MLX_ERR_ARGUMENT, "normals and vertex_ids are required");
+    const long long nv = num_dofs / dim, K = num_contacts;
+    for (long long k = 0; k < K; ++k)
+      if (vertex_ids[k] < 1 || vertex_ids[k] > nv) return set_error(MLX_ERR_ARGUMENT, "contact vertex id out of range");
+    std::unique_ptr<double[]> nvel(new double[(size_t)K * dim]);
+    const double thresh = 2 * gravity * h;
+    const bool can_stop = thresh >= 0;  // |vn| <= a negative threshold never holds
+    parallel_ranges(K, [&](long long a, long long b) {
+      for (long long k = a; k < b; ++k) {
+        const double* vk = v + (size_t)(vertex_ids[k] - 1) * dim;
+        double sq = vk[0] * vk[0], vt = normals[k] * vk[0];
+        for (int c = 1; c < dim; ++c) {
+          sq = sq + vk[c] * vk[c];
+          vt = vt + normals[k + c * K] * vk[c];
+        }
+        const double e = can_stop && std::sqrt(sq) <= thresh ? 0.0 : restitution;
+        const double m = std::min(-e * vt, 0.0);
+        for (int c = 0; c < dim; ++c) nvel[(size_t)k * dim + c] = vk[c] + normals[k + c * K] * (-vk[c] + m);
       }
-      const double e = can_stop && std::sqrt(sq) <= thresh ? 0.0 : restitution;
-      const double m = std::min(-e * vt, 0.0);
-      for (int c = 0; c < dim; ++c) nvel[(size_t)k * dim + c] = vk[c] + normals[k + c * K] * (-vk[c] + m);
+    }, kGrain / 8);  // scattered reads: threads pay off sooner
+    if (v_out != v) std::memcpy(v_out, v, sizeof(double) * (size_t)num_dofs);
+    for (long long k = 0; k < K; ++k) {
+      double* o = v_out + (size_t)(vertex_ids[k] - 1) * dim;
+      for (int c = 0; c < dim; ++c) o[c] = nvel[(size_t)k * dim + c];
     }
-  }, kGrain / 8);  // scattered reads: threads pay off sooner
-  if (v_out != v) std::memcpy(v_out, v, sizeof(double) * (size_t)num_dofs);
-  for (long long k = 0; k < K; ++k) {
-    double* o = v_out + (size_t)(vertex_ids[k] - 1) * dim;
-    for (int c = 0; c < dim; ++c) o[c] = nvel[(size_t)k * dim + c];
-  }
-  return MLX_OK;
+    return MLX_OK;
+  });
 }
 
 }  // extern "C"

@@ -603,109 +603,123 @@ extern "C" {
 
 int mlx_mlp_create(int32_t n_in, int32_t n_hidden, int32_t n_hidden_layers, int32_t n_out, int32_t max_batch,
                    uint64_t seed, int32_t device, mlx_mlp** out) {
-  if (!out) return mlx::set_error(MLX_ERR_ARGUMENT, "null argument");
-  *out = nullptr;
-  mlx_mlp* m = new mlx_mlp();
-  int rc = m->impl.create(n_in, n_hidden, n_hidden_layers, n_out, max_batch, seed, device);
-  if (rc != MLX_OK) {
-    delete m;
-    return rc;
-  }
-  *out = m;
-  return MLX_OK;
+  return mlx::guarded([&]() -> int {
+    if (!out) return mlx::set_error(MLX_ERR_ARGUMENT, "null argument");
+    *out = nullptr;
+    mlx_mlp* m = new mlx_mlp();
+    int rc = m->impl.create(n_in, n_hidden, n_hidden_layers, n_out, max_batch, seed, device);
+    if (rc != MLX_OK) {
+      delete m;
+      return rc;
+    }
+    *out = m;
+    return MLX_OK;
+  });
 }
 
 int mlx_mlp_destroy(mlx_mlp* m) {
-  delete m;
-  return MLX_OK;
+  return mlx::guarded([&]() -> int {
+    delete m;
+    return MLX_OK;
+  });
 }
 
 long long mlx_mlp_num_params(const mlx_mlp* m) { return m ? m->impl.nparams : 0; }
 
 int mlx_mlp_set_params(mlx_mlp* m, const float* params, long long n) {
-  if (!m || !params) return mlx::set_error(MLX_ERR_ARGUMENT, "null argument");
-  cudaSetDevice(m->impl.device);
-  return m->impl.set_params(params, n);
+  return mlx::guarded([&]() -> int {
+    if (!m || !params) return mlx::set_error(MLX_ERR_ARGUMENT, "null argument");
+    cudaSetDevice(m->impl.device);
+    return m->impl.set_params(params, n);
+  });
 }
 
 int mlx_mlp_get_params(mlx_mlp* m, float* params, long long n) {
-  if (!m || !params) return mlx::set_error(MLX_ERR_ARGUMENT, "null argument");
-  if (n != m->impl.nparams) return mlx::set_error(MLX_ERR_ARGUMENT, "parameter count mismatch");
-  cudaSetDevice(m->impl.device);
-  cudaMemcpyAsync(params, m->impl.params, sizeof(float) * n, cudaMemcpyDeviceToHost, m->impl.stream);
-  return cudaStreamSynchronize(m->impl.stream) == cudaSuccess ? MLX_OK : mlx::set_error(MLX_ERR_CUDA, "copy failed");
+  return mlx::guarded([&]() -> int {
+    if (!m || !params) return mlx::set_error(MLX_ERR_ARGUMENT, "null argument");
+    if (n != m->impl.nparams) return mlx::set_error(MLX_ERR_ARGUMENT, "parameter count mismatch");
+    cudaSetDevice(m->impl.device);
+    cudaMemcpyAsync(params, m->impl.params, sizeof(float) * n, cudaMemcpyDeviceToHost, m->impl.stream);
+    return cudaStreamSynchronize(m->impl.stream) == cudaSuccess ? MLX_OK : mlx::set_error(MLX_ERR_CUDA, "copy failed");
+  });
 }
 
 int mlx_mlp_forward(mlx_mlp* m, const float* x, int32_t batch, float* y) {
-  if (!m || !x || !y) return mlx::set_error(MLX_ERR_ARGUMENT, "null argument");
-  Mlp& p = m->impl;
-  cudaSetDevice(p.device);
-  int rc;
-  if ((rc = p.upload(x, nullptr, batch)) || (rc = p.forward_dev(p.xin, batch)) || (rc = p.check_error())) return rc;
-  const int No = p.Np.back();
-  std::vector<float> h((size_t)batch * No);
-  cudaMemcpyAsync(h.data(), p.Y, sizeof(float) * batch * No, cudaMemcpyDeviceToHost, p.stream);
-  if (cudaStreamSynchronize(p.stream) != cudaSuccess) return mlx::set_error(MLX_ERR_CUDA, "copy failed");
-  for (int r = 0; r < batch; ++r)
-    for (int c = 0; c < p.n_out; ++c) y[(size_t)r * p.n_out + c] = h[(size_t)r * No + c];
-  return MLX_OK;
+  return mlx::guarded([&]() -> int {
+    if (!m || !x || !y) return mlx::set_error(MLX_ERR_ARGUMENT, "null argument");
+    Mlp& p = m->impl;
+    cudaSetDevice(p.device);
+    int rc;
+    if ((rc = p.upload(x, nullptr, batch)) || (rc = p.forward_dev(p.xin, batch)) || (rc = p.check_error())) return rc;
+    const int No = p.Np.back();
+    std::vector<float> h((size_t)batch * No);
+    cudaMemcpyAsync(h.data(), p.Y, sizeof(float) * batch * No, cudaMemcpyDeviceToHost, p.stream);
+    if (cudaStreamSynchronize(p.stream) != cudaSuccess) return mlx::set_error(MLX_ERR_CUDA, "copy failed");
+    for (int r = 0; r < batch; ++r)
+      for (int c = 0; c < p.n_out; ++c) y[(size_t)r * p.n_out + c] = h[(size_t)r * No + c];
+    return MLX_OK;
+  });
 }
 
 int mlx_mlp_loss_grad(mlx_mlp* m, const float* x, const float* target, int32_t batch, float* loss, float* grad) {
-  if (!m || !x || !target) return mlx::set_error(MLX_ERR_ARGUMENT, "null argument");
-  Mlp& p = m->impl;
-  cudaSetDevice(p.device);
-  int rc;
-  if ((rc = p.upload(x, target, batch)) || (rc = p.forward_dev(p.xin, batch)) || (rc = p.backward_dev(p.tin, batch)) ||
-      (rc = p.check_error()))
-    return rc;
-  float h[1];
-  cudaMemcpyAsync(h, p.scalar, sizeof(float), cudaMemcpyDeviceToHost, p.stream);
-  if (grad) cudaMemcpyAsync(grad, p.grad, sizeof(float) * p.nparams, cudaMemcpyDeviceToHost, p.stream);
-  if (cudaStreamSynchronize(p.stream) != cudaSuccess) return mlx::set_error(MLX_ERR_CUDA, "copy failed");
-  if (loss) *loss = h[0] / ((float)batch * (float)p.n_out);
-  return MLX_OK;
+  return mlx::guarded([&]() -> int {
+    if (!m || !x || !target) return mlx::set_error(MLX_ERR_ARGUMENT, "null argument");
+    Mlp& p = m->impl;
+    cudaSetDevice(p.device);
+    int rc;
+    if ((rc = p.upload(x, target, batch)) || (rc = p.forward_dev(p.xin, batch)) || (rc = p.backward_dev(p.tin, batch)) ||
+        (rc = p.check_error()))
+      return rc;
+    float h[1];
+    cudaMemcpyAsync(h, p.scalar, sizeof(float), cudaMemcpyDeviceToHost, p.stream);
+    if (grad) cudaMemcpyAsync(grad, p.grad, sizeof(float) * p.nparams, cudaMemcpyDeviceToHost, p.stream);
+    if (cudaStreamSynchronize(p.stream) != cudaSuccess) return mlx::set_error(MLX_ERR_CUDA, "copy failed");
+    if (loss) *loss = h[0] / ((float)batch * (float)p.n_out);
+    return MLX_OK;
+  });
 }
 
 int mlx_mlp_train(mlx_mlp* m, const float* x, const float* target, int32_t n_samples, int32_t batch, int32_t epochs,
                   float lr, uint64_t seed, float* losses) {
-  if (!m || !x || !target) return mlx::set_error(MLX_ERR_ARGUMENT, "null argument");
-  Mlp& p = m->impl;
-  if (batch < 1 || batch > p.max_batch || n_samples < batch)
-    return mlx::set_error(MLX_ERR_ARGUMENT, "need 1 <= batch <= max_batch and batch <= n_samples");
-  cudaSetDevice(p.device);
-  // mini-batches are gathered by a host-side permutation per epoch (fixed seed)
-  std::vector<int> order(n_samples);
-  for (int i = 0; i < n_samples; ++i) order[i] = i;
-  unsigned long long st = seed * 2862933555777941757ull + 3037000493ull;
-  std::vector<float> bx((size_t)batch * p.n_in), bt((size_t)batch * p.n_out);
-  int rc = MLX_OK;
-  const int nb = n_samples / batch;
-  for (int e = 0; e < epochs && rc == MLX_OK; ++e) {
-    for (int i = n_samples - 1; i > 0; --i) {
-      st = st * 6364136223846793005ull + 1442695040888963407ull;
-      const int j = (int)((st >> 33) % (unsigned long long)(i + 1));
-      std::swap(order[i], order[j]);
-    }
-    double esum = 0;
-    for (int b = 0; b < nb && rc == MLX_OK; ++b) {
-      for (int r = 0; r < batch; ++r) {
-        const int k = order[b * batch + r];
-        std::memcpy(&bx[(size_t)r * p.n_in], x + (size_t)k * p.n_in, sizeof(float) * p.n_in);
-        std::memcpy(&bt[(size_t)r * p.n_out], target + (size_t)k * p.n_out, sizeof(float) * p.n_out);
+  return mlx::guarded([&]() -> int {
+    if (!m || !x || !target) return mlx::set_error(MLX_ERR_ARGUMENT, "null argument");
+    Mlp& p = m->impl;
+    if (batch < 1 || batch > p.max_batch || n_samples < batch)
+      return mlx::set_error(MLX_ERR_ARGUMENT, "need 1 <= batch <= max_batch and batch <= n_samples");
+    cudaSetDevice(p.device);
+    // mini-batches are gathered by a host-side permutation per epoch (fixed seed)
+    std::vector<int> order(n_samples);
+    for (int i = 0; i < n_samples; ++i) order[i] = i;
+    unsigned long long st = seed * 2862933555777941757ull + 3037000493ull;
+    std::vector<float> bx((size_t)batch * p.n_in), bt((size_t)batch * p.n_out);
+    int rc = MLX_OK;
+    const int nb = n_samples / batch;
+    for (int e = 0; e < epochs && rc == MLX_OK; ++e) {
+      for (int i = n_samples - 1; i > 0; --i) {
+        st = st * 6364136223846793005ull + 1442695040888963407ull;
+        const int j = (int)((st >> 33) % (unsigned long long)(i + 1));
+        std::swap(order[i], order[j]);
       }
-      if ((rc = p.upload(bx.data(), bt.data(), batch)) || (rc = p.forward_dev(p.xin, batch)) ||
-          (rc = p.backward_dev(p.tin, batch)) || (rc = p.adam(lr)))
-        break;
-      float h = 0;
-      cudaMemcpyAsync(&h, p.scalar, sizeof(float), cudaMemcpyDeviceToHost, p.stream);
-      if (cudaStreamSynchronize(p.stream) != cudaSuccess) rc = mlx::set_error(MLX_ERR_CUDA, "training step failed");
-      esum += h / ((double)batch * p.n_out);
+      double esum = 0;
+      for (int b = 0; b < nb && rc == MLX_OK; ++b) {
+        for (int r = 0; r < batch; ++r) {
+          const int k = order[b * batch + r];
+          std::memcpy(&bx[(size_t)r * p.n_in], x + (size_t)k * p.n_in, sizeof(float) * p.n_in);
+          std::memcpy(&bt[(size_t)r * p.n_out], target + (size_t)k * p.n_out, sizeof(float) * p.n_out);
+        }
+        if ((rc = p.upload(bx.data(), bt.data(), batch)) || (rc = p.forward_dev(p.xin, batch)) ||
+            (rc = p.backward_dev(p.tin, batch)) || (rc = p.adam(lr)))
+          break;
+        float h = 0;
+        cudaMemcpyAsync(&h, p.scalar, sizeof(float), cudaMemcpyDeviceToHost, p.stream);
+        if (cudaStreamSynchronize(p.stream) != cudaSuccess) rc = mlx::set_error(MLX_ERR_CUDA, "training step failed");
+        esum += h / ((double)batch * p.n_out);
+      }
+      if (losses) losses[e] = (float)(esum / nb);
     }
-    if (losses) losses[e] = (float)(esum / nb);
-  }
-  if (rc == MLX_OK) rc = p.check_error();
-  return rc;
+    if (rc == MLX_OK) rc = p.check_error();
+    return rc;
+  });
 }
 
 }  // extern "C"

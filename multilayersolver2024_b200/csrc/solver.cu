@@ -169,7 +169,12 @@ static void host_copy(void* dst, const void* src, size_t bytes) {
   th.reserve(nt - 1);
   for (size_t t = 1; t < nt; ++t) {
     const size_t a = t * chunk, b = std::min(bytes, a + chunk);
-    if (a < b) th.emplace_back([=] { std::memcpy(static_cast<char*>(dst) + a, static_cast<const char*>(src) + a, b - a); });
+    if (a >= b) continue;
+    try {
+      th.emplace_back([=] { std::memcpy(static_cast<char*>(dst) + a, static_cast<const char*>(src) + a, b - a); });
+    } catch (const std::system_error&) {
+      std::memcpy(static_cast<char*>(dst) + a, static_cast<const char*>(src) + a, b - a);  // no thread to be had
+    }
   }
   std::memcpy(dst, src, std::min(bytes, chunk));
   for (std::thread& x : th) x.join();
@@ -3385,174 +3390,216 @@ const char* mlx_last_error(void) { return mlx::g_err.c_str(); }
 int mlx_abi_version(void) { return MLX_ABI_VERSION; }
 
 int mlx_device_count(void) {
-  int n = 0;
-  if (cudaGetDeviceCount(&n) != cudaSuccess) {
-    cudaGetLastError();
-    return 0;
-  }
-  int good = 0;
-  for (int d = 0; d < n; ++d) {
-    cudaDeviceProp pr;
-    if (cudaGetDeviceProperties(&pr, d) == cudaSuccess && pr.major == 10) ++good;
-  }
-  return good;
+  return mlx::guarded([&]() -> int {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    int good = 0;
+    for (int d = 0; d < n; ++d) {
+      cudaDeviceProp pr;
+      if (cudaGetDeviceProperties(&pr, d) == cudaSuccess && pr.major == 10) ++good;
+    }
+    return good;
+  });
 }
 
 int mlx_create(const mlx_mesh_desc* mesh, mlx_solver** out) {
-  if (!mesh || !out) return set_error(MLX_ERR_ARGUMENT, "null argument");
-  *out = nullptr;
-  int n = 0;
-  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
-    cudaGetLastError();
-    return set_error(MLX_ERR_NO_DEVICE, "no CUDA device visible");
-  }
-  if (mesh->device < 0 || mesh->device >= n) return set_error(MLX_ERR_ARGUMENT, "device ordinal out of range");
-  cudaDeviceProp pr;
-  if (cudaGetDeviceProperties(&pr, mesh->device) != cudaSuccess || pr.major != 10)
-    return set_error(MLX_ERR_NO_DEVICE, "this library is built for sm_100a (B200)");
-  int rc = MLX_OK;
-  mlx::SolverBase* impl = mlx::make_solver(mesh, &rc);
-  if (rc != MLX_OK) {
-    delete impl;
-    return rc;
-  }
-  *out = new mlx_solver{mesh->device, impl};
-  return MLX_OK;
+  return mlx::guarded([&]() -> int {
+    if (!mesh || !out) return set_error(MLX_ERR_ARGUMENT, "null argument");
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+      cudaGetLastError();
+      return set_error(MLX_ERR_NO_DEVICE, "no CUDA device visible");
+    }
+    if (mesh->device < 0 || mesh->device >= n) return set_error(MLX_ERR_ARGUMENT, "device ordinal out of range");
+    cudaDeviceProp pr;
+    if (cudaGetDeviceProperties(&pr, mesh->device) != cudaSuccess || pr.major != 10)
+      return set_error(MLX_ERR_NO_DEVICE, "this library is built for sm_100a (B200)");
+    int rc = MLX_OK;
+    mlx::SolverBase* impl = mlx::make_solver(mesh, &rc);
+    if (rc != MLX_OK) {
+      delete impl;
+      return rc;
+    }
+    *out = new mlx_solver{mesh->device, impl};
+    return MLX_OK;
+  });
 }
 
 int mlx_destroy(mlx_solver* s) {
-  if (!s) return MLX_OK;
-  {
-    DeviceGuard g(s->device);
-    delete s->impl;
-  }
-  delete s;
-  return MLX_OK;
+  return mlx::guarded([&]() -> int {
+    if (!s) return MLX_OK;
+    {
+      DeviceGuard g(s->device);
+      delete s->impl;
+    }
+    delete s;
+    return MLX_OK;
+  });
 }
 
 int mlx_layer_solve(mlx_solver* s, const mlx_layer_desc* layers, const mlx_solve_params* params,
                     const mlx_contacts* contacts, const mlx_solve_inputs* in, mlx_solve_outputs* out) {
-  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
-  return s->impl->layer_solve(layers, params, contacts, in, out);
+  return mlx::guarded([&]() -> int {
+    if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+    return s->impl->layer_solve(layers, params, contacts, in, out);
+  });
 }
 
 int mlx_sim_init(mlx_solver* s, const mlx_layer_desc* layers, const mlx_solve_params* params, const double* p0,
                  const double* v0, double air_drag) {
-  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
-  return s->impl->sim_init(layers, params, p0, v0, air_drag);
+  return mlx::guarded([&]() -> int {
+    if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+    return s->impl->sim_init(layers, params, p0, v0, air_drag);
+  });
 }
 
 int mlx_sim_add_velocity(mlx_solver* s, const int32_t* dofs, const double* dv, int32_t n) {
-  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
-  if (n > 0 && (!dofs || !dv)) return set_error(MLX_ERR_ARGUMENT, "null arrays");
-  return s->impl->sim_add_velocity(dofs, dv, n);
+  return mlx::guarded([&]() -> int {
+    if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+    if (n > 0 && (!dofs || !dv)) return set_error(MLX_ERR_ARGUMENT, "null arrays");
+    return s->impl->sim_add_velocity(dofs, dv, n);
+  });
 }
 
 int mlx_sim_step(mlx_solver* s, int32_t nsteps, int32_t use_graph, double* device_ms) {
-  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
-  return s->impl->sim_step(nsteps, use_graph, device_ms);
+  return mlx::guarded([&]() -> int {
+    if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+    return s->impl->sim_step(nsteps, use_graph, device_ms);
+  });
 }
 
 int mlx_sim_get_state(mlx_solver* s, double* p, double* v) {
-  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
-  return s->impl->sim_get_state(p, v);
+  return mlx::guarded([&]() -> int {
+    if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+    return s->impl->sim_get_state(p, v);
+  });
 }
 
 int mlx_sim_sweep_timing(mlx_solver* s, int32_t on) {
-  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
-  return s->impl->enable_sweep_timing(on);
+  return mlx::guarded([&]() -> int {
+    if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+    return s->impl->enable_sweep_timing(on);
+  });
 }
 
 int mlx_sim_sweep_stats(mlx_solver* s, double* ms, double* bytes, long long* launches, int32_t reset) {
-  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
-  return s->impl->sweep_stats(ms, bytes, launches, reset);
+  return mlx::guarded([&]() -> int {
+    if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+    return s->impl->sweep_stats(ms, bytes, launches, reset);
+  });
 }
 
 long long mlx_sim_launches_per_step(const mlx_solver* s) { return s ? s->impl->sim_launches_per_step() : 0; }
 long long mlx_last_call_launches(const mlx_solver* s) { return s ? s->impl->launches_last_call() : 0; }
 int mlx_sim_autotune(mlx_solver* s, int32_t reps, double* before_ms, double* after_ms) {
-  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
-  return s->impl->sim_autotune(reps, before_ms, after_ms);
+  return mlx::guarded([&]() -> int {
+    if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+    return s->impl->sim_autotune(reps, before_ms, after_ms);
+  });
 }
 int mlx_find_contacts(mlx_solver* s, const mlx_obstacle* obstacles, int32_t num_obstacles, const double* p,
                       int32_t max_contacts, int32_t* vertex_ids, double* normals, double* point_colliders,
                       double* compliance, int32_t* num_contacts) {
-  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
-  return s->impl->find_contacts(obstacles, num_obstacles, p, max_contacts, vertex_ids, normals, point_colliders,
-                                compliance, num_contacts);
+  return mlx::guarded([&]() -> int {
+    if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+    return s->impl->find_contacts(obstacles, num_obstacles, p, max_contacts, vertex_ids, normals, point_colliders,
+                                  compliance, num_contacts);
+  });
 }
 int mlx_sim_set_obstacles(mlx_solver* s, const mlx_obstacle* obstacles, int32_t num_obstacles, double restitution) {
-  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
-  return s->impl->sim_set_obstacles(obstacles, num_obstacles, restitution);
+  return mlx::guarded([&]() -> int {
+    if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+    return s->impl->sim_set_obstacles(obstacles, num_obstacles, restitution);
+  });
 }
 int mlx_sim_monitor(mlx_solver* s, double* residuals, int32_t capacity, int32_t* len, int32_t* total_iterations,
                     double* run_until, int32_t* status) {
-  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
-  return s->impl->sim_monitor(residuals, capacity, len, total_iterations, run_until, status);
+  return mlx::guarded([&]() -> int {
+    if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+    return s->impl->sim_monitor(residuals, capacity, len, total_iterations, run_until, status);
+  });
 }
 int mlx_sim_warm_start(mlx_solver* s, int32_t record, int32_t mode, mlx_mlp* net, const float* feature_mean,
                        const float* feature_std, const float* output_mean, const float* output_std,
                        const float* corrections, int32_t* num_clusters) {
-  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
-  return s->impl->ws_configure(record, mode, net, feature_mean, feature_std, output_mean, output_std, corrections,
-                               num_clusters);
+  return mlx::guarded([&]() -> int {
+    if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+    return s->impl->ws_configure(record, mode, net, feature_mean, feature_std, output_mean, output_std, corrections,
+                                 num_clusters);
+  });
 }
 int mlx_sim_warm_start_fetch(mlx_solver* s, float* features, float* targets, int32_t capacity, int32_t* num_clusters) {
-  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
-  return s->impl->ws_fetch(features, targets, capacity, num_clusters);
+  return mlx::guarded([&]() -> int {
+    if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+    return s->impl->ws_fetch(features, targets, capacity, num_clusters);
+  });
 }
 int mlx_build_layers(mlx_solver* s, const double* p, const double* oldp, double h, int32_t ordering,
                      const int32_t* order, const double* DmInv, const double* sorted_layers, int32_t num_layers,
                      const uint8_t* forced_elastic, int32_t* rigid_body_sets, int32_t* num_rigids,
                      uint8_t* is_elastic_element, uint8_t* is_boundary_vertex, uint8_t* is_rigid_vertex,
                      int32_t* vertex_rigid_body) {
-  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
-  return s->impl->build_layers(p, oldp, h, ordering, order, DmInv, sorted_layers, num_layers, forced_elastic,
-                               rigid_body_sets, num_rigids, is_elastic_element, is_boundary_vertex, is_rigid_vertex,
-                               vertex_rigid_body);
+  return mlx::guarded([&]() -> int {
+    if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+    return s->impl->build_layers(p, oldp, h, ordering, order, DmInv, sorted_layers, num_layers, forced_elastic,
+                                 rigid_body_sets, num_rigids, is_elastic_element, is_boundary_vertex, is_rigid_vertex,
+                                 vertex_rigid_body);
+  });
 }
 int mlx_wait_probe(int32_t device, int32_t kind, int64_t limit_ns, int32_t* timed_out) {
-  if (!timed_out) return set_error(MLX_ERR_ARGUMENT, "null argument");
-  if (kind != 0 && kind != 1) return set_error(MLX_ERR_ARGUMENT, "kind must be 0 (grid barrier) or 1 (mbarrier)");
-  limit_ns = std::max<int64_t>(1000000, std::min<int64_t>(limit_ns, 2000000000));
-  *timed_out = 0;
-  if (kind == 1) return mlx::mlp_wait_probe(device, (long long)limit_ns, timed_out);
-  int prev = 0;
-  cudaGetDevice(&prev);
-  if (cudaSetDevice(device) != cudaSuccess) return set_error(MLX_ERR_ARGUMENT, "bad device");
-  unsigned* d = nullptr;
-  cudaError_t e = cudaMalloc(&d, sizeof(unsigned) * 4);
-  if (e == cudaSuccess) {
-    cudaMemset(d, 0, sizeof(unsigned) * 4);
-    k_probe_grid_wait<<<1, 32>>>(d, reinterpret_cast<int*>(d + 1), (unsigned long long)limit_ns,
-                                 reinterpret_cast<int*>(d + 2));
-    e = cudaGetLastError();
-    int r = 0;
-    if (e == cudaSuccess) e = cudaMemcpy(&r, d + 2, sizeof(int), cudaMemcpyDeviceToHost);
-    *timed_out = r;
-    cudaFree(d);
-  }
-  cudaSetDevice(prev);
-  if (e != cudaSuccess) return set_error(MLX_ERR_CUDA, std::string("grid wait probe: ") + cudaGetErrorString(e));
-  return MLX_OK;
+  return mlx::guarded([&]() -> int {
+    if (!timed_out) return set_error(MLX_ERR_ARGUMENT, "null argument");
+    if (kind != 0 && kind != 1) return set_error(MLX_ERR_ARGUMENT, "kind must be 0 (grid barrier) or 1 (mbarrier)");
+    limit_ns = std::max<int64_t>(1000000, std::min<int64_t>(limit_ns, 2000000000));
+    *timed_out = 0;
+    if (kind == 1) return mlx::mlp_wait_probe(device, (long long)limit_ns, timed_out);
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (cudaSetDevice(device) != cudaSuccess) return set_error(MLX_ERR_ARGUMENT, "bad device");
+    unsigned* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, sizeof(unsigned) * 4);
+    if (e == cudaSuccess) {
+      cudaMemset(d, 0, sizeof(unsigned) * 4);
+      k_probe_grid_wait<<<1, 32>>>(d, reinterpret_cast<int*>(d + 1), (unsigned long long)limit_ns,
+                                   reinterpret_cast<int*>(d + 2));
+      e = cudaGetLastError();
+      int r = 0;
+      if (e == cudaSuccess) e = cudaMemcpy(&r, d + 2, sizeof(int), cudaMemcpyDeviceToHost);
+      *timed_out = r;
+      cudaFree(d);
+    }
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) return set_error(MLX_ERR_CUDA, std::string("grid wait probe: ") + cudaGetErrorString(e));
+    return MLX_OK;
+  });
 }
 int mlx_pcg_solve(mlx_solver* s, double h, const double* b, int32_t iterations, double* x, double* resvec) {
-  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
-  return s->impl->pcg_solve(h, b, iterations, x, resvec);
+  return mlx::guarded([&]() -> int {
+    if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+    return s->impl->pcg_solve(h, b, iterations, x, resvec);
+  });
 }
 int mlx_sim_contact_count(mlx_solver* s, int32_t* n) {
-  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
-  return s->impl->sim_contact_count(n);
+  return mlx::guarded([&]() -> int {
+    if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+    return s->impl->sim_contact_count(n);
+  });
 }
 int mlx_launch_path(const mlx_solver* s, char* buf, int32_t n) {
-  if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver"), -1;
-  std::string d = s->impl->launch_path();
-  if (buf && n > 0) {
-    size_t k = std::min<size_t>(d.size(), (size_t)n - 1);
-    std::memcpy(buf, d.data(), k);
-    buf[k] = 0;
-  }
-  return (int)d.size();
+  return mlx::guarded([&]() -> int {
+    if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver"), -1;
+    std::string d = s->impl->launch_path();
+    if (buf && n > 0) {
+      size_t k = std::min<size_t>(d.size(), (size_t)n - 1);
+      std::memcpy(buf, d.data(), k);
+      buf[k] = 0;
+    }
+    return (int)d.size();
+  });
 }
 
 }  // extern "C"

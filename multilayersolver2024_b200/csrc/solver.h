@@ -3,13 +3,34 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <exception>
+#include <new>
 #include <string>
+#include <system_error>
 #include "../../include/mlxpbd.h"
 
 namespace mlx {
 
 extern thread_local std::string g_err;
 int set_error(int code, const std::string& msg);
+
+// The body of a C ABI entry point: a C++ exception (a failed host
+// allocation, a host thread that could not start) becomes a status instead
+// of crossing the C boundary.
+template <typename F>
+int guarded(F&& body) {
+  try {
+    return body();
+  } catch (const std::bad_alloc&) {
+    return set_error(MLX_ERR_ALLOC, "host allocation failed");
+  } catch (const std::system_error& e) {
+    return set_error(MLX_ERR_ALLOC, std::string("host resource: ") + e.what());
+  } catch (const std::exception& e) {
+    return set_error(MLX_ERR_ARGUMENT, e.what());
+  } catch (...) {
+    return set_error(MLX_ERR_ARGUMENT, "unexpected C++ exception");
+  }
+}
 
 struct SolverBase {
   virtual ~SolverBase() {}
