@@ -2,7 +2,8 @@
 config-1 cantilever falling onto a plane and a sphere, against the oracle's
 finders and integrate: positions FP64 <= 1e-9 of the bounding-box diagonal at
 every frame, contact counts equal, and the TimingData log written in
-writeTDcsv's format."""
+writeTDcsv's format.  The single body-free layer runs on the component-group
+path, so this also pins that path's projection of a host contact list."""
 import numpy as np
 import pytest
 
@@ -30,8 +31,10 @@ def test_simulate3d_matches_oracle(gpu, oracle, tmp_path):
     frames = 40
     sc = scenes.config1()
     traj = []
-    td = simulate3d(sc.mesh, _integ(), sc.h, frames, _finders(),
+    integ = _integ()
+    td = simulate3d(sc.mesh, integ, sc.h, frames, _finders(),
                     on_frame=lambda f, m, t: traj.append((m.p.copy(), t.contactCount)))
+    assert "CTAs each owning whole components" in integ.solver(sc.mesh).launch_path
     ref_mesh = scenes.config1().mesh
     it, cache = _integ(), StepCache()
     d = ref_mesh.bbox_diagonal()
