@@ -601,7 +601,12 @@ class XpbdLayer3D:
         # forces and residual velocity (xpbdLayer3D.m:638-643, 662-664) in one
         # native pass; the pinned DOFs get no h f / m term
         n3 = 3 * mesh.N
-        f, resv = np.empty(n3), np.empty(n3)
+        # the residual velocity only feeds layerSolve (which copies it), so
+        # one buffer serves every step: no fresh pages to fault in
+        resv = getattr(self, "_resv_buf", None)
+        if resv is None or resv.size != n3:
+            resv = self._resv_buf = np.empty(n3)
+        f = np.empty(n3)
         cf = self.CustomForce
         cfv = None if np.ndim(cf) == 0 else np.ascontiguousarray(np.broadcast_to(cf, (n3,)), np.float64)
         pins = np.ascontiguousarray(mesh.pinnedDOFs, np.int32)
