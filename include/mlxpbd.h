@@ -397,9 +397,15 @@ int mlx_sim_warm_start_fetch(mlx_solver* solver, float* features, float* targets
  * double.  The call only enqueues work on `stream` (a cudaStream_t, NULL =
  * default stream) and allocates nothing: its scratch is a fixed device array
  * of MLX_NOALLOC_MAX_TETS/256 doubles inside the library, shared by all calls
- * (calls that overlap on the GPU race; serialise them).  The first call on a
- * device looks that array up and should come before any stream capture.
- * More than MLX_NOALLOC_MAX_TETS tets is rejected with MLX_ERR_ARGUMENT. */
+ * (calls that overlap on the GPU race; serialise them).  The first call in a
+ * CUDA context (on a device, and again after cudaDeviceReset) looks that
+ * array up and should come before any stream capture.  Types: d_t is int32
+ * (T x 4, 1-based: int32(mesh.t) in MATLAB, whose mesh.t is double); d_x,
+ * d_DmInv, d_alpha, d_lambda and d_volume are double.  A tet whose vertex
+ * index lies outside [1, num_vertices] is not read and makes the residual
+ * NaN.  An error already pending on entry is reported (MLX_ERR_CUDA) and
+ * nothing is launched.  More than MLX_NOALLOC_MAX_TETS tets is rejected with
+ * MLX_ERR_ARGUMENT. */
 #define MLX_NOALLOC_MAX_TETS 524288
 int mlx_stvk_residual_noalloc(int32_t num_vertices, int32_t num_tets, const double* d_x,
                               const int32_t* d_t, const double* d_DmInv, const double* d_alpha,

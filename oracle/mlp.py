@@ -6,7 +6,9 @@ the device).  `bf16=False` gives the exact FP64 model for finite-difference
 checks.
 
 Parameter layout (flat): per layer W (n_out x n_in, row-major) then b.
-GELU is the tanh form 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))).
+GELU is the tanh form 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))) of
+Hendrycks & Gimpel, "Gaussian Error Linear Units" (arXiv:1606.08415, 2016),
+an approximation of x Phi(x) = 0.5 x (1 + erf(x / sqrt 2)).
 """
 from __future__ import annotations
 

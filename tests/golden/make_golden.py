@@ -1,9 +1,10 @@
 """Generate the golden fixtures of tests/golden from the reference itself.
 
-Run in a tree where the reference is mounted (default /root/reference) and
-oracle/_ref is built (``make -C oracle``):
+Run where the reference tree is mounted and oracle/_ref is built
+(``make -C oracle REF=<tree>``), giving the tree by --ref or the environment
+variable MLX_REFERENCE_TREE:
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <reference tree>
 
 Writes
   stvk_grad.npz   C (6) and gradC (6x12) of the reference's symbolic Green-strain
@@ -24,6 +25,7 @@ The reference sources are read, never copied; only computed numbers are kept.
 from __future__ import annotations
 
 import argparse
+import os
 import re
 import sys
 from pathlib import Path
@@ -220,8 +222,10 @@ def make_layer_solve(ref: Path, out: Path):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("MLX_REFERENCE_TREE"))
     a = ap.parse_args()
+    if not a.ref:
+        ap.error("give the reference tree by --ref or MLX_REFERENCE_TREE")
     out = Path(__file__).resolve().parent
     make_stvk(Path(a.ref), out)
     make_layers(out)

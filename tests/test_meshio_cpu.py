@@ -12,7 +12,7 @@ from multilayersolver2024_b200.meshio import (load_mesh, load_poly, orient_tets,
                                               write_ele, write_node)
 from multilayersolver2024_b200.simulate import TimingData, matlab_d, write_td_csv
 
-REF = Path(os.environ.get("MLX_REFERENCE_TREE", "/root/reference"))
+REF = Path(os.environ["MLX_REFERENCE_TREE"]) if os.environ.get("MLX_REFERENCE_TREE") else None
 
 
 @pytest.mark.parametrize("first", [0, 1])
@@ -55,7 +55,8 @@ def test_medit_mesh_and_orientation(tmp_path):
     assert m.elV[0] > 0 and m.mu[0] == 1e3  # label 2 is the smallest label: first table entry
 
 
-@pytest.mark.skipif(not (REF / "3d/data/cube.node").exists(), reason="reference tree not present")
+@pytest.mark.skipif(REF is None or not (REF / "3d/data/cube.node").exists(),
+                    reason="MLX_REFERENCE_TREE is not set to the reference tree")
 def test_reference_assets():
     cube = load_poly(REF / "3d/data/cube", 1e4, 2e4)
     assert (cube.N, cube.T) == (8, 6) and np.all(cube.elV > 0)

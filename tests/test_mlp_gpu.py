@@ -55,3 +55,23 @@ def test_training_reduces_loss(gpu):
     losses = net.train(x, t, batch=512, epochs=12, lr=2e-3)
     assert np.all(np.isfinite(losses))
     assert losses[-1] < 0.15 * losses[0], losses
+
+
+def test_device_gelu_matches_erf_gelu(gpu):
+    """The hidden activation on the device is GELU: a one-hidden-layer network
+    with identity weights returns GELU(x) of the BF16-rounded inputs, within
+    the BF16 rounding of the stored activation (and the tanh form's 1e-3)."""
+    from scipy.special import erf
+    n = 44
+    net = Mlp(n, n, n_hidden=128, n_hidden_layers=1, max_batch=512, seed=3)
+    W1 = np.zeros((128, n), np.float32)
+    W1[np.arange(n), np.arange(n)] = 1.0
+    W2 = np.zeros((n, 128), np.float32)
+    W2[np.arange(n), np.arange(n)] = 1.0
+    net.set_params(np.concatenate([W1.ravel(), np.zeros(128, np.float32), W2.ravel(), np.zeros(n, np.float32)]))
+    x = np.linspace(-6.0, 6.0, 512 * n, dtype=np.float32).reshape(512, n)
+    y = net.forward(x)
+    xb = M.bf16(x)
+    exact = 0.5 * xb * (1.0 + erf(xb / np.sqrt(2.0)))
+    assert np.all(np.abs(y - exact) <= 1e-3 + 2.0 ** -8 * np.abs(exact))
+    net.close()

@@ -28,3 +28,11 @@ def test_bf16_rounding():
     # 1 + 2^-8 is a tie between 1 and 1 + 2^-7: rounds to even (1.0)
     np.testing.assert_array_equal(r[:3], [1.0, 1.0, 1.0078125])
     assert abs(r[3] + 3.140625) < 1e-12
+
+
+def test_gelu_tanh_form_is_within_1e3_of_erf_gelu():
+    """The tanh GELU (Hendrycks & Gimpel 2016) against x Phi(x) with erf."""
+    from scipy.special import erf
+    x = np.linspace(-10.0, 10.0, 200001)
+    exact = 0.5 * x * (1.0 + erf(x / np.sqrt(2.0)))
+    assert np.max(np.abs(M.gelu(x) - exact)) <= 1e-3
