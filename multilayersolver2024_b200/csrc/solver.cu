@@ -260,6 +260,15 @@ struct WarmStartState {
   }
 };
 
+// Multiplier warm start of the resident stepper (warmstart.cuh): the last
+// two steps' converged multipliers, how many steps they hold, and the first
+// layer's cluster of every tet (colour-sorted order; -1: none).
+struct MultiplierWarmStart {
+  int on = 0, rows = 0;
+  double a = 1.0, b = 0.0;
+  DevBuf d_lam1, d_lam2, d_seen, d_owner;
+};
+
 // Per-call bookkeeping of the layer loop (the scalars layerSolve threads
 // through projectGS, xpbdLayer3D.m:94-232).
 struct RunState {
@@ -420,6 +429,9 @@ struct Solver final : SolverBase {
   int ws_fetch(float* features, float* targets, int cap, int32_t* nb) override;
   int ws_after_make_rigids(const LayerWork& w);
   int ws_after_lamb_reset(const LayerWork& w);
+  MultiplierWarmStart mws;
+  int mws_configure(int on, double a, double b) override;
+  int mws_start();
   int find_contacts(const mlx_obstacle* obs, int nobs, const double* p, int max_contacts, int32_t* vids,
                     double* normals, double* points, double* comp, int32_t* K) override;
   int sim_set_obstacles(const mlx_obstacle* obs, int nobs, double restitution) override;
@@ -1748,6 +1760,10 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
         st.launches += ws.mode == 1 ? 8 : 4;
       }
     }
+    if (&w == &sim_work && layer == 0 && mws.on) {
+      CHECK(mws_start());
+      st.launches += 1 + C;
+    }
     k_release_elastic<R><<<blocks_for(N, 256), 256, 0, stream>>>(p, resv, L.vert_rigid, N, hR);
     CU(cudaGetLastError());
     ++st.launches;
@@ -2539,6 +2555,7 @@ int Solver<R>::sim_setup(const mlx_layer_desc* ld, const mlx_solve_params* P, co
   std::memcpy(hs, p0, sizeof(double) * n3);
   sim_p0.assign(p0, p0 + n3);
   ws.reset();
+  mws.on = 0;
   if (v0) std::memcpy(hs + n3, v0, sizeof(double) * n3);
   else std::memset(hs + n3, 0, sizeof(double) * n3);
   for (size_t i = 0; i < np; ++i) hs[2 * n3 + i] = p0[pinned[i]];
@@ -2803,6 +2820,63 @@ int Solver<R>::sim_monitor(double* ra, int cap, int32_t* len, int32_t* total_it,
   if (run_until) *run_until = ru;
   if (status) *status = err;
   if (ra && cap > 0) std::memcpy(ra, r.data(), sizeof(double) * std::min(cap, n));
+  return MLX_OK;
+}
+
+// Multiplier warm start of the resident stepper: on = 1 carries the
+// converged multipliers of the last steps into the next step's start
+// (coefficients a, b for tets without a perceptron output); every call
+// forgets the steps saved so far.
+template <typename R>
+int Solver<R>::mws_configure(int on, double a, double b) {
+  if (!sim.ready) return set_error(MLX_ERR_ARGUMENT, "mlx_sim_init first");
+  if (!std::isfinite(a) || !std::isfinite(b)) return set_error(MLX_ERR_ARGUMENT, "coefficients must be finite");
+  DeviceGuard g(device);
+  mws.on = on ? 1 : 0;
+  mws.a = a;
+  mws.b = b;
+  mws.rows = mat_kind == MAT_NH ? 2 : 6;
+  if (mws.on) {
+    const size_t bytes = sizeof(R) * (size_t)mws.rows * T;
+    CHECK(mws.d_lam1.ensure(bytes));
+    CHECK(mws.d_lam2.ensure(bytes));
+    CHECK(mws.d_seen.ensure(sizeof(int)));
+    CU(cudaMemsetAsync(mws.d_lam1.p, 0, bytes, stream));
+    CU(cudaMemsetAsync(mws.d_lam2.p, 0, bytes, stream));
+    CU(cudaMemsetAsync(mws.d_seen.p, 0, sizeof(int), stream));
+    CU(cudaStreamSynchronize(stream));
+  }
+  if (sim.graph) { cudaGraphExecDestroy(sim.graph); sim.graph = nullptr; }
+  return MLX_OK;
+}
+
+// Starting multipliers of the step and their position displacement (first
+// layer, after makeRigids and the perceptron, before the elastic release).
+template <typename R>
+int Solver<R>::mws_start() {
+  const bool net = ws.mode == 1 && ws.nb > 0 && mws.d_owner.p;
+  const float* om = ws.d_norm.p ? ws.d_norm.as<float>() + 2 * kWsFeat : nullptr;
+  k_ws_lambda_init<R><<<blocks_for(T, 256), 256, 0, stream>>>(
+      T, mws.rows, d_lambda.as<R>(), mws.d_lam1.as<R>(), mws.d_lam2.as<R>(), net ? mws.d_owner.as<int>() : nullptr,
+      net ? ws.y : nullptr, ws.ld, om, om ? om + kWsOut : nullptr, kWsOut, mws.a, mws.b, mws.d_seen.as<int>(),
+      nullptr);
+  CU(cudaGetLastError());
+  TetData<R> td = tets();
+  const R inv_h = (R)(1.0 / sim.P.h);
+  for (int c = 0; c < C; ++c) {
+    const int begin = color_off[c], count = color_off[c + 1] - color_off[c];
+    if (count <= 0) continue;
+    switch (mat_kind) {
+      case MAT_NH:
+        k_ws_lambda_push<R, MAT_NH><<<blocks_for(count, 256), 256, 0, stream>>>(
+            td, begin, count, pos(), d_resv.as<R4<R>>(), d_pin_mask.as<unsigned char>(), inv_h);
+        break;
+      default:
+        k_ws_lambda_push<R, MAT_STVK_LAME><<<blocks_for(count, 256), 256, 0, stream>>>(
+            td, begin, count, pos(), d_resv.as<R4<R>>(), d_pin_mask.as<unsigned char>(), inv_h);
+    }
+    CU(cudaGetLastError());
+  }
   return MLX_OK;
 }
 
@@ -3234,6 +3308,13 @@ int Solver<R>::sim_issue_step(long long* launches, bool capturing) {
     st.launches += sim.P.contact_coloring ? 8 : 5;
   }
   CHECK(run_layers(&sim.ld, &sim.P, nullptr, cd, st, capturing, sim_work, dc));
+  if (mws.on) {
+    const long long n = (long long)mws.rows * T;
+    k_ws_lambda_save<R><<<(int)((n + 255) / 256), 256, 0, stream>>>(n, d_lambda.as<R>(), mws.d_lam1.as<R>(),
+                                                                   mws.d_lam2.as<R>(), mws.d_seen.as<int>());
+    CU(cudaGetLastError());
+    ++st.launches;
+  }
   if (ws.nb > 0 && ws.record) {
     k_ws_targets<R><<<ws.nb, 256, 0, stream>>>(ws.S, p, d_oldp.as<R4<R>>(), ws.d_rec.as<double>(),
                                                 sim_work.lamB.as<double>(), h, ws.d_target.as<float>());
@@ -3530,6 +3611,12 @@ int mlx_sim_warm_start(mlx_solver* s, int32_t record, int32_t mode, mlx_mlp* net
     if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
     return s->impl->ws_configure(record, mode, net, feature_mean, feature_std, output_mean, output_std, corrections,
                                  num_clusters);
+  });
+}
+int mlx_sim_multiplier_warm_start(mlx_solver* s, int32_t on, double scale, double extrapolation) {
+  return mlx::guarded([&]() -> int {
+    if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+    return s->impl->mws_configure(on, scale, extrapolation);
   });
 }
 int mlx_sim_warm_start_fetch(mlx_solver* s, float* features, float* targets, int32_t capacity, int32_t* num_clusters) {

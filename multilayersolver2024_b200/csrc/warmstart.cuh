@@ -25,6 +25,7 @@
 
 #include "body_kernels.cuh"
 #include "common.cuh"
+#include "tet_kernels.cuh"
 
 namespace mlx {
 
@@ -306,6 +307,115 @@ __global__ void __launch_bounds__(256) k_ws_targets(WsStatic S, const R4<R>* __r
     const int nbv = S.bnd_off[b + 1] - S.bnd_off[b];
     t[6] = (float)(nbv > 0 ? a[9] / nbv : 0.0);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Multiplier warm start.  The reference zeroes every tet's multipliers at the
+// start of a step (xpbdLayer3D.m:666), so projectGS rebuilds them from zero
+// and the stiff tets need most of the iterations to the residual.  Here a
+// step may start from the previous steps' converged multipliers instead,
+//   lambda0 = a lambda_{n-1} + b (lambda_{n-1} - lambda_{n-2}),
+// with (a, b) per rigid cluster of the first layer from the perceptron, or
+// fixed.  XPBD keeps x - x~ = M^-1 grad C^T lambda along its iterations, so
+// starting from lambda0 the positions are moved by M^-1 grad C(x)^T lambda0
+// too: that displacement is added to the residual velocity (divided by h),
+// which the layers release as they do the rest of the step's motion.  The
+// stop rules then decide convergence exactly as in the plain solve.
+
+// lambda0 of every tet (rows: 2 for the Neo-Hookean pair, 6 for StVK).  `y`
+// (network rows, stride ld, denormalised with omean/ostd) gives the
+// coefficients of a tet's cluster (owner >= 0) in output columns col_a and
+// col_a + 1; other tets take (a0, b0).  `gate` (optional) = 0 falls back to
+// the plain start.  `seen` = steps already saved: lambda_{n-1} and
+// lambda_{n-2} exist only after one and two steps.
+template <typename R>
+__global__ void k_ws_lambda_init(int T, int rows, R* __restrict__ lam, const R* __restrict__ lam1,
+                                 const R* __restrict__ lam2, const int* __restrict__ owner,
+                                 const float* __restrict__ y, int ld, const float* __restrict__ omean,
+                                 const float* __restrict__ ostd, int col_a, double a0, double b0,
+                                 const int* __restrict__ seen, const int* __restrict__ gate) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= T) return;
+  const int n = *seen;
+  double a = a0, b = b0;
+  const int c = owner ? owner[s] : -1;
+  if (y && c >= 0) {
+    a = (double)(y[(size_t)ld * c + col_a] * ostd[col_a] + omean[col_a]);
+    b = (double)(y[(size_t)ld * c + col_a + 1] * ostd[col_a + 1] + omean[col_a + 1]);
+  }
+  if ((gate && *gate == 0) || n < 1) a = b = 0.0;
+  else if (n < 2) b = 0.0;
+  for (int q = 0; q < rows; ++q) {
+    const size_t i = (size_t)q * T + s;
+    const double l1 = (double)lam1[i], l2 = (double)lam2[i];
+    lam[i] = (R)(a * l1 + b * (l1 - l2));
+  }
+}
+
+// Position displacement of the starting multipliers, M^-1 grad C(x)^T lambda0,
+// for the tets of one colour (they share no vertex), added to the residual
+// velocity as displacement / h on the unpinned DOFs.
+template <typename R, int MAT>
+__global__ void __launch_bounds__(256) k_ws_lambda_push(TetData<R> td, int begin, int count,
+                                                        const R4<R>* __restrict__ pos, R4<R>* __restrict__ resv,
+                                                        const unsigned char* __restrict__ pin_mask, R inv_h) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const int s = begin + i, T = td.T;
+  int4 v;
+  R G[9], minv[4];
+  V3<R> X[4];
+  load_tet<R>(td, s, pos, v, G, X, minv);
+  V3<R> dx[4];
+  if (MAT == MAT_NH) {
+    NHEval<R> e;
+    nh_eval<R>(X, G, (double)td.mat[s], (double)td.mat[(size_t)T + s], 0.0, e);
+    const R l0 = td.lambda[s], l1 = td.lambda[(size_t)T + s];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const R m = minv[a];
+      dx[a] = {m * (l0 * e.gD[a].x + l1 * e.gH[a].x), m * (l0 * e.gD[a].y + l1 * e.gH[a].y),
+               m * (l0 * e.gD[a].z + l1 * e.gH[a].z)};
+    }
+  } else {
+    StrainKin<R> k;
+    strain_kin<R>(X, G, k);
+    R l[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) l[q] = td.lambda[(size_t)q * T + s];
+    const R half = R(0.5), vol = td.vol[s];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const R c0 = l[0] * k.d[a][0] + half * (l[3] * k.d[a][1] + l[4] * k.d[a][2]);
+      const R c1 = l[1] * k.d[a][1] + half * (l[3] * k.d[a][0] + l[5] * k.d[a][2]);
+      const R c2 = l[2] * k.d[a][2] + half * (l[4] * k.d[a][0] + l[5] * k.d[a][1]);
+      const R sc = minv[a] * vol;
+      const V3<R> d = vaxpy3(c0, k.f[0], c1, k.f[1], c2, k.f[2]);
+      dx[a] = {sc * d.x, sc * d.y, sc * d.z};
+    }
+  }
+  const int vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const unsigned char pm = pin_mask[vv[a]];
+    R4<R> r = resv[vv[a]];
+    if (!(pm & 1)) r.x += dx[a].x * inv_h;
+    if (!(pm & 2)) r.y += dx[a].y * inv_h;
+    if (!(pm & 4)) r.z += dx[a].z * inv_h;
+    resv[vv[a]] = r;
+  }
+}
+
+// End of a step: lambda_{n-2} <- lambda_{n-1} <- lambda (rows x T), and one
+// more step seen (counted up to 2).
+template <typename R>
+__global__ void k_ws_lambda_save(long long n, const R* __restrict__ lam, R* __restrict__ lam1, R* __restrict__ lam2,
+                                 int* __restrict__ seen) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0 && *seen < 2) *seen += 1;
+  if (i >= n) return;
+  lam2[i] = lam1[i];
+  lam1[i] = lam[i];
 }
 
 }  // namespace mlx

@@ -259,6 +259,14 @@ class ResidentSim:
         self._ws_nb = nb.value
         return nb.value
 
+    def multiplier_warm_start(self, on=True, scale=1.0, extrapolation=0.0):
+        """Multiplier warm start (``mlx_sim_multiplier_warm_start``): each
+        step starts from scale * lambda_{n-1} + extrapolation * (lambda_{n-1}
+        - lambda_{n-2}) with the matching position displacement (per cluster
+        coefficients from the perceptron when one is configured)."""
+        check("mlx_sim_multiplier_warm_start", self._lib.mlx_sim_multiplier_warm_start(
+            self.solver.handle, int(bool(on)), float(scale), float(extrapolation)), self._lib)
+
     def warm_start_records(self):
         """Features (clusters x 44) and targets (clusters x 7) of the last step."""
         from ._lib import f32
