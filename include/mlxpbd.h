@@ -389,17 +389,17 @@ int mlx_sim_warm_start_fetch(mlx_solver* solver, float* features, float* targets
 
 /* Multiplier warm start of the resident stepper.  No counterpart in the
  * reference, which zeroes every tet's multipliers at the start of a step
- * (xpbdLayer3D.m:666).  With `on`, a step starts from the converged
- * multipliers of the previous steps,
+ * (xpbdLayer3D.m:666) and rebuilds them in every step's projectGS.  With `on`,
+ * the last layer (the fine layer) starts from the converged multipliers of
+ * the previous steps,
  *   lambda0 = a lambda_{n-1} + b (lambda_{n-1} - lambda_{n-2}),
- * and moves the positions by the displacement those multipliers imply,
- * M^-1 grad C(x)^T lambda0 (added to the residual velocity, which the layers
- * release), so that the solve continues from a consistent XPBD state.  (a, b)
- * come per cluster of the first layer from the perceptron of
- * mlx_sim_warm_start (mode 1) and are `scale` and `extrapolation` elsewhere.
- * The first step after this call starts from zero and the second uses
- * b = 0.  on = 0 restores the reference's zero start.  The stop rules are
- * unchanged. */
+ * and its positions move by the displacement the change of multipliers
+ * implies, M^-1 grad C(x)^T (lambda0 - lambda), so that the layer's
+ * Gauss-Seidel continues from a state with the same fixed point.  (a, b) come
+ * per cluster of the first layer from the perceptron of mlx_sim_warm_start
+ * (mode 1) and are `scale` and `extrapolation` elsewhere.  The first step
+ * after this call starts from the plain state and the second uses b = 0.
+ * on = 0 restores the reference's start.  The stop rules are unchanged. */
 int mlx_sim_multiplier_warm_start(mlx_solver* solver, int32_t on, double scale, double extrapolation);
 
 /* ---- allocation-free residual ------------------------------------------

@@ -1760,10 +1760,6 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
         st.launches += ws.mode == 1 ? 8 : 4;
       }
     }
-    if (&w == &sim_work && layer == 0 && mws.on) {
-      CHECK(mws_start());
-      st.launches += 1 + C;
-    }
     k_release_elastic<R><<<blocks_for(N, 256), 256, 0, stream>>>(p, resv, L.vert_rigid, N, hR);
     CU(cudaGetLastError());
     ++st.launches;
@@ -1794,6 +1790,10 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
         CHECK(ws_after_lamb_reset(w));
         ++st.launches;
       }
+    }
+    if (&w == &sim_work && isLast && mws.on) {
+      CHECK(mws_start());
+      st.launches += C;
     }
     const int* dlist = dint + ls.o_list;
     const bool bodyWork = (ls.nb > 0 && (L.any_boundary || (P->use_rigid_contacts && L.any_rigid_contact))) ||
@@ -2850,31 +2850,27 @@ int Solver<R>::mws_configure(int on, double a, double b) {
   return MLX_OK;
 }
 
-// Starting multipliers of the step and their position displacement (first
-// layer, after makeRigids and the perceptron, before the elastic release).
+// Starting multipliers of the last layer and the position shift they imply
+// (after the layer's elastic release, before its projectGS loop).
 template <typename R>
 int Solver<R>::mws_start() {
   const bool net = ws.mode == 1 && ws.nb > 0 && mws.d_owner.p;
   const float* om = ws.d_norm.p ? ws.d_norm.as<float>() + 2 * kWsFeat : nullptr;
-  k_ws_lambda_init<R><<<blocks_for(T, 256), 256, 0, stream>>>(
-      T, mws.rows, d_lambda.as<R>(), mws.d_lam1.as<R>(), mws.d_lam2.as<R>(), net ? mws.d_owner.as<int>() : nullptr,
-      net ? ws.y : nullptr, ws.ld, om, om ? om + kWsOut : nullptr, kWsOut, mws.a, mws.b, mws.d_seen.as<int>(),
-      nullptr);
-  CU(cudaGetLastError());
+  const int* owner = net ? mws.d_owner.as<int>() : nullptr;
+  const float* y = net ? ws.y : nullptr;
+  const float* os = om ? om + kWsOut : nullptr;
   TetData<R> td = tets();
-  const R inv_h = (R)(1.0 / sim.P.h);
   for (int c = 0; c < C; ++c) {
     const int begin = color_off[c], count = color_off[c + 1] - color_off[c];
     if (count <= 0) continue;
-    switch (mat_kind) {
-      case MAT_NH:
-        k_ws_lambda_push<R, MAT_NH><<<blocks_for(count, 256), 256, 0, stream>>>(
-            td, begin, count, pos(), d_resv.as<R4<R>>(), d_pin_mask.as<unsigned char>(), inv_h);
-        break;
-      default:
-        k_ws_lambda_push<R, MAT_STVK_LAME><<<blocks_for(count, 256), 256, 0, stream>>>(
-            td, begin, count, pos(), d_resv.as<R4<R>>(), d_pin_mask.as<unsigned char>(), inv_h);
-    }
+    if (mat_kind == MAT_NH)
+      k_ws_lambda_shift<R, MAT_NH><<<blocks_for(count, 256), 256, 0, stream>>>(
+          td, begin, count, pos(), d_pin_mask.as<unsigned char>(), mws.d_lam1.as<R>(), mws.d_lam2.as<R>(), owner, y,
+          ws.ld, om, os, kWsOut, mws.a, mws.b, mws.d_seen.as<int>(), nullptr);
+    else
+      k_ws_lambda_shift<R, MAT_STVK_LAME><<<blocks_for(count, 256), 256, 0, stream>>>(
+          td, begin, count, pos(), d_pin_mask.as<unsigned char>(), mws.d_lam1.as<R>(), mws.d_lam2.as<R>(), owner, y,
+          ws.ld, om, os, kWsOut, mws.a, mws.b, mws.d_seen.as<int>(), nullptr);
     CU(cudaGetLastError());
   }
   return MLX_OK;

@@ -310,32 +310,37 @@ __global__ void __launch_bounds__(256) k_ws_targets(WsStatic S, const R4<R>* __r
 }
 
 // ---------------------------------------------------------------------------
-// Multiplier warm start.  The reference zeroes every tet's multipliers at the
-// start of a step (xpbdLayer3D.m:666), so projectGS rebuilds them from zero
-// and the stiff tets need most of the iterations to the residual.  Here a
-// step may start from the previous steps' converged multipliers instead,
+// Multiplier warm start of the last layer.  The reference zeroes every tet's
+// multipliers at the start of a step (xpbdLayer3D.m:666), so projectGS
+// rebuilds them from zero and the stiff tets need most of the iterations to
+// the residual.  Here the last layer (the fine layer, where every tet is
+// elastic) may start from the previous steps' converged multipliers,
 //   lambda0 = a lambda_{n-1} + b (lambda_{n-1} - lambda_{n-2}),
 // with (a, b) per rigid cluster of the first layer from the perceptron, or
-// fixed.  XPBD keeps x - x~ = M^-1 grad C^T lambda along its iterations, so
-// starting from lambda0 the positions are moved by M^-1 grad C(x)^T lambda0
-// too: that displacement is added to the residual velocity (divided by h),
-// which the layers release as they do the rest of the step's motion.  The
-// stop rules then decide convergence exactly as in the plain solve.
+// fixed.  Within one layer XPBD keeps x - x_c = M^-1 grad C^T (lambda -
+// lambda_c) along its iterations (x_c, lambda_c: the state the layer starts
+// from), so replacing lambda_c by lambda0 moves the positions by
+// M^-1 grad C(x)^T (lambda0 - lambda_c): the layer then converges to the same
+// fixed point from a nearer start.  (The coarse layers are not warm-started:
+// they snap boundary vertices to their rigid bodies, which breaks that
+// relation.)  The stop rules decide convergence exactly as in the plain solve.
 
-// lambda0 of every tet (rows: 2 for the Neo-Hookean pair, 6 for StVK).  `y`
-// (network rows, stride ld, denormalised with omean/ostd) gives the
-// coefficients of a tet's cluster (owner >= 0) in output columns col_a and
-// col_a + 1; other tets take (a0, b0).  `gate` (optional) = 0 falls back to
+// lambda0 for the tets of one colour (they share no vertex) and the position
+// shift it implies, on the unpinned DOFs.  Rows: 2 for the Neo-Hookean pair, 6
+// for StVK.  `y` (network rows, stride ld, denormalised with omean/ostd)
+// gives the coefficients of a tet's cluster (owner >= 0) in output columns
+// col_a and col_a + 1; other tets take (a0, b0).  `gate` (optional) = 0 keeps
 // the plain start.  `seen` = steps already saved: lambda_{n-1} and
 // lambda_{n-2} exist only after one and two steps.
-template <typename R>
-__global__ void k_ws_lambda_init(int T, int rows, R* __restrict__ lam, const R* __restrict__ lam1,
-                                 const R* __restrict__ lam2, const int* __restrict__ owner,
-                                 const float* __restrict__ y, int ld, const float* __restrict__ omean,
-                                 const float* __restrict__ ostd, int col_a, double a0, double b0,
-                                 const int* __restrict__ seen, const int* __restrict__ gate) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= T) return;
+template <typename R, int MAT>
+__global__ void __launch_bounds__(256) k_ws_lambda_shift(
+    TetData<R> td, int begin, int count, R4<R>* __restrict__ pos, const unsigned char* __restrict__ pin_mask,
+    const R* __restrict__ lam1, const R* __restrict__ lam2, const int* __restrict__ owner,
+    const float* __restrict__ y, int ld, const float* __restrict__ omean, const float* __restrict__ ostd, int col_a,
+    double a0, double b0, const int* __restrict__ seen, const int* __restrict__ gate) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const int s = begin + i, T = td.T;
   const int n = *seen;
   double a = a0, b = b0;
   const int c = owner ? owner[s] : -1;
@@ -343,25 +348,18 @@ __global__ void k_ws_lambda_init(int T, int rows, R* __restrict__ lam, const R* 
     a = (double)(y[(size_t)ld * c + col_a] * ostd[col_a] + omean[col_a]);
     b = (double)(y[(size_t)ld * c + col_a + 1] * ostd[col_a + 1] + omean[col_a + 1]);
   }
-  if ((gate && *gate == 0) || n < 1) a = b = 0.0;
-  else if (n < 2) b = 0.0;
-  for (int q = 0; q < rows; ++q) {
-    const size_t i = (size_t)q * T + s;
-    const double l1 = (double)lam1[i], l2 = (double)lam2[i];
-    lam[i] = (R)(a * l1 + b * (l1 - l2));
+  if ((gate && *gate == 0) || n < 1) return;  // plain start: lambda and x unchanged
+  if (n < 2) b = 0.0;
+  constexpr int kRows = MAT == MAT_NH ? 2 : 6;
+  R dl[kRows];
+#pragma unroll
+  for (int q = 0; q < kRows; ++q) {
+    const size_t k = (size_t)q * T + s;
+    const double l1 = (double)lam1[k], l2 = (double)lam2[k];
+    const R l0 = (R)(a * l1 + b * (l1 - l2));
+    dl[q] = l0 - td.lambda[k];
+    td.lambda[k] = l0;
   }
-}
-
-// Position displacement of the starting multipliers, M^-1 grad C(x)^T lambda0,
-// for the tets of one colour (they share no vertex), added to the residual
-// velocity as displacement / h on the unpinned DOFs.
-template <typename R, int MAT>
-__global__ void __launch_bounds__(256) k_ws_lambda_push(TetData<R> td, int begin, int count,
-                                                        const R4<R>* __restrict__ pos, R4<R>* __restrict__ resv,
-                                                        const unsigned char* __restrict__ pin_mask, R inv_h) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= count) return;
-  const int s = begin + i, T = td.T;
   int4 v;
   R G[9], minv[4];
   V3<R> X[4];
@@ -370,39 +368,35 @@ __global__ void __launch_bounds__(256) k_ws_lambda_push(TetData<R> td, int begin
   if (MAT == MAT_NH) {
     NHEval<R> e;
     nh_eval<R>(X, G, (double)td.mat[s], (double)td.mat[(size_t)T + s], 0.0, e);
-    const R l0 = td.lambda[s], l1 = td.lambda[(size_t)T + s];
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      const R m = minv[a];
-      dx[a] = {m * (l0 * e.gD[a].x + l1 * e.gH[a].x), m * (l0 * e.gD[a].y + l1 * e.gH[a].y),
-               m * (l0 * e.gD[a].z + l1 * e.gH[a].z)};
+    for (int k = 0; k < 4; ++k) {
+      const R m = minv[k];
+      dx[k] = {m * (dl[0] * e.gD[k].x + dl[1] * e.gH[k].x), m * (dl[0] * e.gD[k].y + dl[1] * e.gH[k].y),
+               m * (dl[0] * e.gD[k].z + dl[1] * e.gH[k].z)};
     }
   } else {
-    StrainKin<R> k;
-    strain_kin<R>(X, G, k);
-    R l[6];
-#pragma unroll
-    for (int q = 0; q < 6; ++q) l[q] = td.lambda[(size_t)q * T + s];
+    StrainKin<R> kin;
+    strain_kin<R>(X, G, kin);
     const R half = R(0.5), vol = td.vol[s];
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      const R c0 = l[0] * k.d[a][0] + half * (l[3] * k.d[a][1] + l[4] * k.d[a][2]);
-      const R c1 = l[1] * k.d[a][1] + half * (l[3] * k.d[a][0] + l[5] * k.d[a][2]);
-      const R c2 = l[2] * k.d[a][2] + half * (l[4] * k.d[a][0] + l[5] * k.d[a][1]);
-      const R sc = minv[a] * vol;
-      const V3<R> d = vaxpy3(c0, k.f[0], c1, k.f[1], c2, k.f[2]);
-      dx[a] = {sc * d.x, sc * d.y, sc * d.z};
+    for (int k = 0; k < 4; ++k) {
+      const R c0 = dl[0] * kin.d[k][0] + half * (dl[3] * kin.d[k][1] + dl[4] * kin.d[k][2]);
+      const R c1 = dl[1] * kin.d[k][1] + half * (dl[3] * kin.d[k][0] + dl[5] * kin.d[k][2]);
+      const R c2 = dl[2] * kin.d[k][2] + half * (dl[4] * kin.d[k][0] + dl[5] * kin.d[k][1]);
+      const R sc = minv[k] * vol;
+      const V3<R> d = vaxpy3(c0, kin.f[0], c1, kin.f[1], c2, kin.f[2]);
+      dx[k] = {sc * d.x, sc * d.y, sc * d.z};
     }
   }
   const int vv[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    const unsigned char pm = pin_mask[vv[a]];
-    R4<R> r = resv[vv[a]];
-    if (!(pm & 1)) r.x += dx[a].x * inv_h;
-    if (!(pm & 2)) r.y += dx[a].y * inv_h;
-    if (!(pm & 4)) r.z += dx[a].z * inv_h;
-    resv[vv[a]] = r;
+  for (int k = 0; k < 4; ++k) {
+    const unsigned char pm = pin_mask[vv[k]];
+    R4<R> r = pos[vv[k]];
+    if (!(pm & 1)) r.x += dx[k].x;
+    if (!(pm & 2)) r.y += dx[k].y;
+    if (!(pm & 4)) r.z += dx[k].z;
+    pos[vv[k]] = r;
   }
 }
 
