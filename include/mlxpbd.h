@@ -395,11 +395,15 @@ int mlx_sim_warm_start_fetch(mlx_solver* solver, float* features, float* targets
  *   lambda0 = a lambda_{n-1} + b (lambda_{n-1} - lambda_{n-2}),
  * and its positions move by the displacement the change of multipliers
  * implies, M^-1 grad C(x)^T (lambda0 - lambda), so that the layer's
- * Gauss-Seidel continues from a state with the same fixed point.  (a, b) come
- * per cluster of the first layer from the perceptron of mlx_sim_warm_start
- * (mode 1) and are `scale` and `extrapolation` elsewhere.  The first step
- * after this call starts from the plain state and the second uses b = 0.
- * on = 0 restores the reference's start.  The stop rules are unchanged. */
+ * Gauss-Seidel continues from a state with the same fixed point to first
+ * order (a = `scale`, b = `extrapolation`).  The first step after this call
+ * starts from the plain state and the second uses b = 0.  on = 0 (the
+ * default) restores the reference's start.  The stop rules are unchanged.
+ * Measured: <= 5 % fewer iterations to residual 1e-4 on the Neo-Hookean
+ * blocks and none on the contact-heavy drop, with positions 3e-4 to 6e-4 of
+ * the bounding-box diagonal away from the plain solve's after one step (the
+ * fixed point of Gauss-Seidel on these nonlinear constraints depends on the
+ * path), so it stays an option. */
 int mlx_sim_multiplier_warm_start(mlx_solver* solver, int32_t on, double scale, double extrapolation);
 
 /* ---- allocation-free residual ------------------------------------------

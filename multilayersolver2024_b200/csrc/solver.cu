@@ -261,12 +261,11 @@ struct WarmStartState {
 };
 
 // Multiplier warm start of the resident stepper (warmstart.cuh): the last
-// two steps' converged multipliers, how many steps they hold, and the first
-// layer's cluster of every tet (colour-sorted order; -1: none).
+// two steps' converged multipliers and how many steps they hold.
 struct MultiplierWarmStart {
   int on = 0, rows = 0;
   double a = 1.0, b = 0.0;
-  DevBuf d_lam1, d_lam2, d_seen, d_owner;
+  DevBuf d_lam1, d_lam2, d_seen;
 };
 
 // Per-call bookkeeping of the layer loop (the scalars layerSolve threads
@@ -2823,10 +2822,9 @@ int Solver<R>::sim_monitor(double* ra, int cap, int32_t* len, int32_t* total_it,
   return MLX_OK;
 }
 
-// Multiplier warm start of the resident stepper: on = 1 carries the
-// converged multipliers of the last steps into the next step's start
-// (coefficients a, b for tets without a perceptron output); every call
-// forgets the steps saved so far.
+// Multiplier warm start of the resident stepper: on = 1 starts the last
+// layer of every step from a lambda_{n-1} + b (lambda_{n-1} - lambda_{n-2});
+// every call forgets the steps saved so far.
 template <typename R>
 int Solver<R>::mws_configure(int on, double a, double b) {
   if (!sim.ready) return set_error(MLX_ERR_ARGUMENT, "mlx_sim_init first");
@@ -2854,23 +2852,18 @@ int Solver<R>::mws_configure(int on, double a, double b) {
 // (after the layer's elastic release, before its projectGS loop).
 template <typename R>
 int Solver<R>::mws_start() {
-  const bool net = ws.mode == 1 && ws.nb > 0 && mws.d_owner.p;
-  const float* om = ws.d_norm.p ? ws.d_norm.as<float>() + 2 * kWsFeat : nullptr;
-  const int* owner = net ? mws.d_owner.as<int>() : nullptr;
-  const float* y = net ? ws.y : nullptr;
-  const float* os = om ? om + kWsOut : nullptr;
   TetData<R> td = tets();
   for (int c = 0; c < C; ++c) {
     const int begin = color_off[c], count = color_off[c + 1] - color_off[c];
     if (count <= 0) continue;
     if (mat_kind == MAT_NH)
       k_ws_lambda_shift<R, MAT_NH><<<blocks_for(count, 256), 256, 0, stream>>>(
-          td, begin, count, pos(), d_pin_mask.as<unsigned char>(), mws.d_lam1.as<R>(), mws.d_lam2.as<R>(), owner, y,
-          ws.ld, om, os, kWsOut, mws.a, mws.b, mws.d_seen.as<int>(), nullptr);
+          td, begin, count, pos(), d_pin_mask.as<unsigned char>(), mws.d_lam1.as<R>(), mws.d_lam2.as<R>(), mws.a,
+          mws.b, mws.d_seen.as<int>());
     else
       k_ws_lambda_shift<R, MAT_STVK_LAME><<<blocks_for(count, 256), 256, 0, stream>>>(
-          td, begin, count, pos(), d_pin_mask.as<unsigned char>(), mws.d_lam1.as<R>(), mws.d_lam2.as<R>(), owner, y,
-          ws.ld, om, os, kWsOut, mws.a, mws.b, mws.d_seen.as<int>(), nullptr);
+          td, begin, count, pos(), d_pin_mask.as<unsigned char>(), mws.d_lam1.as<R>(), mws.d_lam2.as<R>(), mws.a,
+          mws.b, mws.d_seen.as<int>());
     CU(cudaGetLastError());
   }
   return MLX_OK;

@@ -118,19 +118,21 @@ def config1_replicated(copies: int = 16384, per_row: int = 128, energy=_lib.MLX_
     return Scene(f"config1_cantilever_8x2x2_x{copies}", m, 0.01, 200, [0], [20], custom_sets=sets)
 
 
-def config2(seed: int = 2, nx=64, ny=16, nz=16, cluster=8) -> Scene:
+def config2(seed: int = 2, nx=64, ny=16, nz=16, cluster=8, energy=_lib.MLX_ENERGY_NEOHOOKEAN) -> Scene:
     """Plain multi-layer Neo-Hookean block: 64x16x16 cubes (18,785 vertices,
     98,304 tets), per-tet E log-uniform in [1e4, 1e7], nu uniform in
     [0.25, 0.45], coarse layer of fixed 8^3-cube rigid clusters then the fine
     layer, 5 coarse + 10 fine iterations, dt = 1/60, base (z = 0) pinned,
-    seeded random surface impulse at t = 0, 300 steps."""
+    seeded random surface impulse at t = 0, 300 steps.  `energy` swaps the
+    material model (the StVK Voigt constraint: the same scene for the
+    reference's own constraint)."""
     rng = np.random.default_rng(seed)
     V, T, cube = generate_beam(nx, ny, nz, 0.1)
     nt = T.shape[0]
     E = np.exp(rng.uniform(np.log(1e4), np.log(1e7), nt))
     nu = rng.uniform(0.25, 0.45, nt)
     mu, lam = to_lame(nu, E)
-    m = Mesh3D.from_arrays(V, T, mu, lam, rho=1000.0, alpha1=0.0, energy_type=_lib.MLX_ENERGY_NEOHOOKEAN)
+    m = Mesh3D.from_arrays(V, T, mu, lam, rho=1000.0, alpha1=0.0, energy_type=energy)
     m.pin(np.nonzero(np.isclose(V[:, 2], 0.0))[0] + 1)
     forced = np.zeros(nt, dtype=bool)
     forced[m.pinnedTets - 1] = True

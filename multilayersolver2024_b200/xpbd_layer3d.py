@@ -260,10 +260,10 @@ class ResidentSim:
         return nb.value
 
     def multiplier_warm_start(self, on=True, scale=1.0, extrapolation=0.0):
-        """Multiplier warm start (``mlx_sim_multiplier_warm_start``): each
-        step starts from scale * lambda_{n-1} + extrapolation * (lambda_{n-1}
-        - lambda_{n-2}) with the matching position displacement (per cluster
-        coefficients from the perceptron when one is configured)."""
+        """Multiplier warm start (``mlx_sim_multiplier_warm_start``): the
+        last layer of each step starts from scale * lambda_{n-1} +
+        extrapolation * (lambda_{n-1} - lambda_{n-2}) with the matching
+        position shift."""
         check("mlx_sim_multiplier_warm_start", self._lib.mlx_sim_multiplier_warm_start(
             self.solver.handle, int(bool(on)), float(scale), float(extrapolation)), self._lib)
 
