@@ -367,25 +367,31 @@ int mlx_mlp_train(mlx_mlp* mlp, const float* x, const float* target, int32_t n_s
  * COM velocity, angular velocity, COM displacement from the positions given
  * to mlx_sim_init and the rotation vector of its deformation from them (FP64
  * polar decomposition), and for the 4 clusters nearest at rest their
- * relative velocities, COM distance change and mass ratio.  7 outputs act on
- * the layer: a COM-velocity and angular-velocity correction applied before
- * the symplectic rigid step, and the cluster's starting boundary multiplier
- * (0 in the reference).
- *   mode 1: `net` (44 -> 7) maps normalised features
+ * relative velocities, COM distance change and mass ratio.  8 outputs per
+ * cluster: a COM-velocity and angular-velocity correction applied before the
+ * symplectic rigid step (6), the cluster's starting boundary multiplier (0 in
+ * the reference) (1), and the predicted residual of its rigid fit, log10 of
+ * the RMS distance (m) of its vertices' final positions from the best-fit
+ * rigid motion of the step (1).  A cluster whose predicted residual exceeds
+ * `fallback_residual` (m; <= 0: never) gets no correction -- the plain
+ * solve's start -- and is counted (mlx_sim_warm_start_fetch).
+ *   mode 1: `net` (44 -> 8) maps normalised features
  *           ((f - feature_mean) / feature_std) to normalised outputs
  *           (denormalised with output_mean / output_std);
- *   mode 2: `corrections` (num_clusters x 7, output units) are applied;
+ *   mode 2: `corrections` (num_clusters x 8, output units) are applied;
  *   mode 0: nothing is applied.
  * With `record` every step keeps its raw features and the targets -- the
  * corrections that would have put each cluster on the best-fit rigid motion
- * to its final positions, and its mean final boundary multiplier -- for
- * mlx_sim_warm_start_fetch.  The stop rules are unchanged: a warm start
- * changes the iterations needed to reach the residual, not the residual. */
-int mlx_sim_warm_start(mlx_solver* solver, int32_t record, int32_t mode, mlx_mlp* net, const float* feature_mean,
-                       const float* feature_std, const float* output_mean, const float* output_std,
-                       const float* corrections, int32_t* num_clusters);
+ * to its final positions, its mean final boundary multiplier and the log10
+ * RMS residual of that fit -- for mlx_sim_warm_start_fetch, which also
+ * returns how many clusters fell back in the last step.  The stop rules are
+ * unchanged: a warm start changes the iterations needed to reach the
+ * residual, not the residual. */
+int mlx_sim_warm_start(mlx_solver* solver, int32_t record, int32_t mode, mlx_mlp* net, double fallback_residual,
+                       const float* feature_mean, const float* feature_std, const float* output_mean,
+                       const float* output_std, const float* corrections, int32_t* num_clusters);
 int mlx_sim_warm_start_fetch(mlx_solver* solver, float* features, float* targets, int32_t capacity,
-                             int32_t* num_clusters);
+                             int32_t* num_clusters, int32_t* num_fallbacks);
 
 /* Multiplier warm start of the resident stepper.  No counterpart in the
  * reference, which zeroes every tet's multipliers at the start of a step

@@ -153,9 +153,10 @@ SIGNATURES = {
     "mlx_sim_set_obstacles": ([C.c_void_p, C.c_void_p, C.c_int32, C.c_double], C.c_int),
     "mlx_sim_contact_count": ([C.c_void_p, _i32p], C.c_int),
     "mlx_sim_monitor": ([C.c_void_p, _f64p, C.c_int32, _i32p, _i32p, _f64p, _i32p], C.c_int),
-    "mlx_sim_warm_start": ([C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, _f32p, _f32p, _f32p, _f32p, _f32p, _i32p],
+    "mlx_sim_warm_start": ([C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_double, _f32p, _f32p, _f32p, _f32p,
+                            _f32p, _i32p],
                            C.c_int),
-    "mlx_sim_warm_start_fetch": ([C.c_void_p, _f32p, _f32p, C.c_int32, _i32p], C.c_int),
+    "mlx_sim_warm_start_fetch": ([C.c_void_p, _f32p, _f32p, C.c_int32, _i32p, _i32p], C.c_int),
     "mlx_sim_multiplier_warm_start": ([C.c_void_p, C.c_int32, C.c_double, C.c_double], C.c_int),
     "mlx_pcg_solve": ([C.c_void_p, C.c_double, _f64p, C.c_int32, _f64p, _f64p], C.c_int),
     "mlx_wait_probe": ([C.c_int32, C.c_int32, C.c_int64, C.POINTER(C.c_int32)], C.c_int),

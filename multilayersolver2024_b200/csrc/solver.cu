@@ -249,7 +249,8 @@ struct WarmStartState {
   const float* y = nullptr;  // rows of corrections (device) and their stride
   int ld = 0;
   WsStatic S{};
-  DevBuf d_static, d_rest, d_norm, d_own, d_raw, d_feat, d_rec, d_target, d_corr;
+  double gate = 1e-3;        // fall back to the plain start above this predicted fit residual (m)
+  DevBuf d_static, d_rest, d_norm, d_own, d_raw, d_feat, d_rec, d_target, d_corr, d_fallback;
   void reset() {
     record = mode = 0;
     net = nullptr;
@@ -423,9 +424,9 @@ struct Solver final : SolverBase {
   int pcg_setup();
   int pcg_solve(double h, const double* b, int iterations, double* x, double* resvec) override;
   std::vector<double> sim_p0;  // positions given to mlx_sim_init (the rest configuration)
-  int ws_configure(int record, int mode, mlx_mlp* net, const float* fmean, const float* fstd, const float* omean,
+  int ws_configure(int record, int mode, mlx_mlp* net, double gate, const float* fmean, const float* fstd, const float* omean,
                    const float* ostd, const float* corrections, int32_t* nb) override;
-  int ws_fetch(float* features, float* targets, int cap, int32_t* nb) override;
+  int ws_fetch(float* features, float* targets, int cap, int32_t* nb, int32_t* fallbacks) override;
   int ws_after_make_rigids(const LayerWork& w);
   int ws_after_lamb_reset(const LayerWork& w);
   MultiplierWarmStart mws;
@@ -2887,7 +2888,9 @@ int Solver<R>::ws_after_make_rigids(const LayerWork& w) {
     ws.y = ws.d_corr.as<float>();
     ws.ld = kWsOut;
   }
-  k_ws_apply_velocity<<<blocks_for(nb, 128), 128, 0, stream>>>(nb, w.bodies.as<Body>(), ws.y, ws.ld, om, os);
+  CU(cudaMemsetAsync(ws.d_fallback.p, 0, sizeof(int), stream));
+  k_ws_apply_velocity<<<blocks_for(nb, 128), 128, 0, stream>>>(nb, w.bodies.as<Body>(), ws.y, ws.ld, om, os,
+                                                               ws.gate, ws.d_fallback.as<int>());
   CU(cudaGetLastError());
   return MLX_OK;
 }
@@ -2895,18 +2898,18 @@ int Solver<R>::ws_after_make_rigids(const LayerWork& w) {
 template <typename R>
 int Solver<R>::ws_after_lamb_reset(const LayerWork& w) {
   const float* om = ws.d_norm.as<float>() + 2 * kWsFeat;
-  k_ws_apply_lambda<<<ws.nb, 128, 0, stream>>>(ws.S, w.lamB.as<double>(), ws.y, ws.ld, om, om + kWsOut);
+  k_ws_apply_lambda<<<ws.nb, 128, 0, stream>>>(ws.S, w.lamB.as<double>(), ws.y, ws.ld, om, om + kWsOut, ws.gate);
   CU(cudaGetLastError());
   return MLX_OK;
 }
 
 // Sets up the warm start on the first layer of the resident stepper (its
 // rigid clusters): rest data and nearest neighbours of the clusters, the
-// normalisation of features (mean, std: 44 each) and outputs (7 each), the
-// perceptron (mode 1) or fixed corrections (mode 2, clusters x 7 in output
+// normalisation of features (mean, std: 44 each) and outputs (8 each), the
+// perceptron (mode 1) or fixed corrections (mode 2, clusters x 8 in output
 // units), and whether every step keeps its features and targets.
 template <typename R>
-int Solver<R>::ws_configure(int record, int mode, mlx_mlp* net, const float* fmean, const float* fstd,
+int Solver<R>::ws_configure(int record, int mode, mlx_mlp* net, double gate, const float* fmean, const float* fstd,
                             const float* omean, const float* ostd, const float* corrections, int32_t* nb_out) {
   if (!sim.ready) return set_error(MLX_ERR_ARGUMENT, "mlx_sim_init first");
   if (mode < 0 || mode > 2) return set_error(MLX_ERR_ARGUMENT, "warm start mode must be 0, 1 or 2");
@@ -2920,10 +2923,11 @@ int Solver<R>::ws_configure(int record, int mode, mlx_mlp* net, const float* fme
     int ni = 0, no = 0, mb = 0;
     CHECK(mlp_dims(net, &ni, &no, &mb));
     if (ni != kWsFeat || no != kWsOut || mb < nb)
-      return set_error(MLX_ERR_ARGUMENT, "the perceptron must map 44 features to 7 outputs for every cluster");
+      return set_error(MLX_ERR_ARGUMENT, "the perceptron must map 44 features to 8 outputs for every cluster");
     if (!fmean || !fstd || !omean || !ostd) return set_error(MLX_ERR_ARGUMENT, "normalisation arrays are NULL");
   }
   if (mode == 2 && !corrections) return set_error(MLX_ERR_ARGUMENT, "corrections are NULL");
+  if (std::isnan(gate)) return set_error(MLX_ERR_ARGUMENT, "the fallback gate is NaN");
   ws.reset();
   // rest positions and per-cluster rest data
   std::vector<double4> rest(N);
@@ -2986,6 +2990,8 @@ int Solver<R>::ws_configure(int record, int mode, mlx_mlp* net, const float* fme
   CHECK(ws.d_rec.ensure(sizeof(double) * kWsRec * nb));
   CHECK(ws.d_target.ensure(sizeof(float) * kWsOut * nb));
   CHECK(ws.d_corr.ensure(sizeof(float) * kWsOut * nb));
+  CHECK(ws.d_fallback.ensure(sizeof(int)));
+  CU(cudaMemsetAsync(ws.d_fallback.p, 0, sizeof(int), stream));
   CU(cudaMemsetAsync(ws.d_target.p, 0, sizeof(float) * kWsOut * nb, stream));
   if (mode == 2)
     CU(cudaMemcpyAsync(ws.d_corr.p, corrections, sizeof(float) * kWsOut * nb, cudaMemcpyHostToDevice, stream));
@@ -2993,6 +2999,7 @@ int Solver<R>::ws_configure(int record, int mode, mlx_mlp* net, const float* fme
   ws.S = S;
   ws.record = record;
   ws.mode = mode;
+  ws.gate = gate;
   ws.net = net;
   ws.col = col;
   ws.nb = nb;
@@ -3002,7 +3009,7 @@ int Solver<R>::ws_configure(int record, int mode, mlx_mlp* net, const float* fme
 }
 
 template <typename R>
-int Solver<R>::ws_fetch(float* features, float* targets, int cap, int32_t* nb) {
+int Solver<R>::ws_fetch(float* features, float* targets, int cap, int32_t* nb, int32_t* fallbacks) {
   if (ws.nb == 0) return set_error(MLX_ERR_ARGUMENT, "warm start not configured");
   if (nb) *nb = ws.nb;
   if (cap < ws.nb) return set_error(MLX_ERR_LIMIT, "capacity below the number of clusters");
@@ -3011,7 +3018,11 @@ int Solver<R>::ws_fetch(float* features, float* targets, int cap, int32_t* nb) {
     CU(cudaMemcpyAsync(features, ws.d_raw.p, sizeof(float) * kWsFeat * ws.nb, cudaMemcpyDeviceToHost, stream));
   if (targets)
     CU(cudaMemcpyAsync(targets, ws.d_target.p, sizeof(float) * kWsOut * ws.nb, cudaMemcpyDeviceToHost, stream));
+  int fb = 0;
+  if (fallbacks && ws.d_fallback.p)
+    CU(cudaMemcpyAsync(&fb, ws.d_fallback.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
   CU(cudaStreamSynchronize(stream));
+  if (fallbacks) *fallbacks = fb;
   return MLX_OK;
 }
 
@@ -3593,13 +3604,13 @@ int mlx_sim_monitor(mlx_solver* s, double* residuals, int32_t capacity, int32_t*
     return s->impl->sim_monitor(residuals, capacity, len, total_iterations, run_until, status);
   });
 }
-int mlx_sim_warm_start(mlx_solver* s, int32_t record, int32_t mode, mlx_mlp* net, const float* feature_mean,
-                       const float* feature_std, const float* output_mean, const float* output_std,
-                       const float* corrections, int32_t* num_clusters) {
+int mlx_sim_warm_start(mlx_solver* s, int32_t record, int32_t mode, mlx_mlp* net, double fallback_residual,
+                       const float* feature_mean, const float* feature_std, const float* output_mean,
+                       const float* output_std, const float* corrections, int32_t* num_clusters) {
   return mlx::guarded([&]() -> int {
     if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
-    return s->impl->ws_configure(record, mode, net, feature_mean, feature_std, output_mean, output_std, corrections,
-                                 num_clusters);
+    return s->impl->ws_configure(record, mode, net, fallback_residual, feature_mean, feature_std, output_mean,
+                                 output_std, corrections, num_clusters);
   });
 }
 int mlx_sim_multiplier_warm_start(mlx_solver* s, int32_t on, double scale, double extrapolation) {
@@ -3608,10 +3619,11 @@ int mlx_sim_multiplier_warm_start(mlx_solver* s, int32_t on, double scale, doubl
     return s->impl->mws_configure(on, scale, extrapolation);
   });
 }
-int mlx_sim_warm_start_fetch(mlx_solver* s, float* features, float* targets, int32_t capacity, int32_t* num_clusters) {
+int mlx_sim_warm_start_fetch(mlx_solver* s, float* features, float* targets, int32_t capacity, int32_t* num_clusters,
+                             int32_t* num_fallbacks) {
   return mlx::guarded([&]() -> int {
     if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
-    return s->impl->ws_fetch(features, targets, capacity, num_clusters);
+    return s->impl->ws_fetch(features, targets, capacity, num_clusters, num_fallbacks);
   });
 }
 int mlx_build_layers(mlx_solver* s, const double* p, const double* oldp, double h, int32_t ordering,

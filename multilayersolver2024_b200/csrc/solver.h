@@ -53,9 +53,9 @@ struct SolverBase {
   virtual int sim_contact_count(int32_t* n) = 0;
   virtual int sim_monitor(double* ra, int cap, int32_t* len, int32_t* total_it, double* run_until,
                           int32_t* status) = 0;
-  virtual int ws_configure(int record, int mode, mlx_mlp* net, const float* fmean, const float* fstd,
+  virtual int ws_configure(int record, int mode, mlx_mlp* net, double gate, const float* fmean, const float* fstd,
                            const float* omean, const float* ostd, const float* corrections, int32_t* nb) = 0;
-  virtual int ws_fetch(float* features, float* targets, int cap, int32_t* nb) = 0;
+  virtual int ws_fetch(float* features, float* targets, int cap, int32_t* nb, int32_t* fallbacks) = 0;
   virtual int mws_configure(int on, double a, double b) = 0;
   virtual int pcg_solve(double h, const double* b, int iterations, double* x, double* resvec) = 0;
   virtual int build_layers(const double* p, const double* oldp, double h, int ordering, const int32_t* order,

@@ -9,14 +9,19 @@
 //     the 4 clusters nearest at rest (8 each) their COM and angular velocity
 //     relative to this cluster's, the change of their COM distance, and their
 //     mass ratio;
-//   outputs (7): a COM-velocity and angular-velocity correction applied
-//     before the symplectic rigid step (6), and the cluster's starting
-//     boundary multiplier (rigidElasticBoundaryAccumulationConstraints'
-//     lambda, 0 in the reference) (1).
+//   outputs (8): a COM-velocity and angular-velocity correction applied
+//     before the symplectic rigid step (6), the cluster's starting boundary
+//     multiplier (rigidElasticBoundaryAccumulationConstraints' lambda, 0 in
+//     the reference) (1), and the predicted residual of the cluster's rigid
+//     fit, log10 of the RMS distance (m) of its vertices' final positions from
+//     the best-fit rigid motion of the step (1).  A cluster whose predicted
+//     residual exceeds the gate (1e-3 m by default) is not corrected: it falls
+//     back to the plain start.
 // Targets come from the converged step: the best-fit rigid motion of each
 // cluster from its step-start to its final positions (Kabsch: the polar
 // factor of sum m (x* - c*)(x0 - c0)^T), expressed as the velocities that make
-// the rigid step land there, and the mean final boundary multiplier.  The
+// the rigid step land there, the mean final boundary multiplier, and the
+// log10 RMS residual of that fit.  The
 // polar decomposition restates the reference's polarDecomposition.m
 // (2d/tools/math/polarDecomposition.m: C = F'F, eig(C),
 // U^-1 = Q diag(1/sqrt(lambda)) Q', R = F U^-1) in 3D with a cyclic Jacobi
@@ -32,7 +37,8 @@ namespace mlx {
 constexpr int kWsOwn = 12;
 constexpr int kWsNbr = 4;
 constexpr int kWsFeat = kWsOwn + 8 * kWsNbr;  // 44
-constexpr int kWsOut = 7;
+constexpr int kWsOut = 8;
+constexpr int kWsResidualCol = 7;  // log10 of the predicted rigid-fit residual (m)
 constexpr int kWsRec = 9;  // COM, COM velocity, angular velocity at makeRigids
 
 // Eigen-decomposition of a symmetric 3x3 matrix (column-major) by cyclic
@@ -236,12 +242,27 @@ __global__ void k_ws_features(WsStatic S, const float* __restrict__ own, const f
   }
 }
 
+// Whether cluster b falls back to the plain start: its predicted rigid-fit
+// residual (output column kWsResidualCol, denormalised) is above `gate` (m);
+// gate <= 0 applies every correction.
+__device__ __forceinline__ bool ws_gated(const float* __restrict__ y, int ld, int b, const float* __restrict__ omean,
+                                         const float* __restrict__ ostd, double gate) {
+  if (!(gate > 0.0)) return false;
+  const double lg = (double)(y[(size_t)ld * b + kWsResidualCol] * ostd[kWsResidualCol] + omean[kWsResidualCol]);
+  return !(lg <= log10(gate));  // NaN predictions fall back too
+}
+
 // Velocity correction of every cluster from output rows y (stride ld),
-// denormalised as y * std + mean.
+// denormalised as y * std + mean; gated clusters are left alone and counted.
 __global__ void k_ws_apply_velocity(int nb, Body* __restrict__ bodies, const float* __restrict__ y, int ld,
-                                    const float* __restrict__ omean, const float* __restrict__ ostd) {
+                                    const float* __restrict__ omean, const float* __restrict__ ostd, double gate,
+                                    int* __restrict__ fallbacks) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nb) return;
+  if (ws_gated(y, ld, b, omean, ostd, gate)) {
+    atomicAdd(fallbacks, 1);
+    return;
+  }
   Body& B = bodies[b];
   for (int d = 0; d < 3; ++d) {
     B.comdot[d] += (double)(y[(size_t)ld * b + d] * ostd[d] + omean[d]);
@@ -252,8 +273,9 @@ __global__ void k_ws_apply_velocity(int nb, Body* __restrict__ bodies, const flo
 // Starting boundary multipliers: every boundary vertex of cluster b starts
 // at the cluster's predicted multiplier (one CTA per cluster).
 __global__ void k_ws_apply_lambda(WsStatic S, double* __restrict__ lamB, const float* __restrict__ y, int ld,
-                                  const float* __restrict__ omean, const float* __restrict__ ostd) {
+                                  const float* __restrict__ omean, const float* __restrict__ ostd, double gate) {
   const int b = blockIdx.x;
+  if (ws_gated(y, ld, b, omean, ostd, gate)) return;
   const double l = (double)(y[(size_t)ld * b + 6] * ostd[6] + omean[6]);
   for (int i = S.bnd_off[b] + threadIdx.x; i < S.bnd_off[b + 1]; i += blockDim.x) lamB[i] = l;
 }
@@ -293,9 +315,24 @@ __global__ void __launch_bounds__(256) k_ws_targets(WsStatic S, const R4<R>* __r
   }
   for (int i = S.bnd_off[b] + threadIdx.x; i < S.bnd_off[b + 1]; i += blockDim.x) a[9] += lamB[i];
   block_sum<10>(a);
+  __shared__ double sR[9];
+  if (threadIdx.x == 0) polar_rotation(a, sR);
+  __syncthreads();
+  // residual of the fit: sum m |(x - c1) - R (x0 - c0)|^2
+  double q[1] = {0.0};
+  for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+    const int v = S.body_verts[i];
+    const double m = S.vmass[v];
+    const R4<R> p = pos[v], o = x0[v];
+    const D3 x = d3((double)p.x, (double)p.y, (double)p.z) - c1;
+    const D3 y = d3((double)o.x, (double)o.y, (double)o.z) - c0;
+    const D3 e = d3(x.x - (sR[0] * y.x + sR[3] * y.y + sR[6] * y.z), x.y - (sR[1] * y.x + sR[4] * y.y + sR[7] * y.z),
+                    x.z - (sR[2] * y.x + sR[5] * y.y + sR[8] * y.z));
+    q[0] += m * dot(e, e);
+  }
+  block_sum<1>(q);
   if (threadIdx.x == 0) {
-    double Rm[9];
-    polar_rotation(a, Rm);
+    const double* Rm = sR;
     const D3 w = (1.0 / h) * rotation_log(Rm);
     float* t = target + (size_t)kWsOut * b;
     t[0] = (float)((c1.x - c0.x) / h - r[3]);
@@ -306,6 +343,7 @@ __global__ void __launch_bounds__(256) k_ws_targets(WsStatic S, const R4<R>* __r
     t[5] = (float)(w.z - r[8]);
     const int nbv = S.bnd_off[b + 1] - S.bnd_off[b];
     t[6] = (float)(nbv > 0 ? a[9] / nbv : 0.0);
+    t[kWsResidualCol] = (float)log10(fmax(sqrt(q[0] / s[0]), 1e-9));
   }
 }
 

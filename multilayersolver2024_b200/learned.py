@@ -75,7 +75,7 @@ class Mlp:
 
 def collect_warm_start_data(sim, steps, graph=True):
     """Runs `steps` resident steps with recording on (plain solve, mode 0) and
-    returns the stacked features (rows x 44), targets (rows x 7) and the
+    returns the stacked features (rows x 44), targets (rows x 8) and the
     projectGS iterations of every step (when the step monitors residuals)."""
     sim.warm_start(record=True, mode=0)
     feats, tgts, iters = [], [], []
@@ -97,7 +97,7 @@ def normalisation(a, floor=1e-6):
 
 
 def fit_warm_start(features, targets, epochs=200, lr=2e-3, batch=None, seed=0, hidden=128, layers=3, max_batch=4096):
-    """Trains the warm-start perceptron (44 -> 7) on normalised features and
+    """Trains the warm-start perceptron (44 -> 8) on normalised features and
     targets with the library's tensor-core kernels.  Returns the network, the
     feature and output normalisations and the per-epoch losses."""
     fn, on = normalisation(features), normalisation(targets)
@@ -106,7 +106,7 @@ def fit_warm_start(features, targets, epochs=200, lr=2e-3, batch=None, seed=0, h
     n = x.shape[0]
     b = batch or min(max(128, n // 8 // 128 * 128), max_batch)
     b = min(b, n)
-    net = Mlp(44, 7, n_hidden=hidden, n_hidden_layers=layers, max_batch=max(max_batch, b), seed=seed)
+    net = Mlp(44, 8, n_hidden=hidden, n_hidden_layers=layers, max_batch=max(max_batch, b), seed=seed)
     losses = net.train(x, y, batch=b, epochs=epochs, lr=lr, seed=seed)
     return net, fn, on, losses
 

@@ -174,6 +174,49 @@ def config5(seed: int = 5, nx=64, ny=32, nz=32, coarse=8, mid=4) -> Scene:
                  impulse=(dofs, dv.ravel()))
 
 
+def config5_batch(seed: int = 100, n_scenes: int = 16, nx=32, ny=16, nz=16, coarse=8, mid=4,
+                  spacing=1.0) -> Scene:
+    """Training batch of the learned warm start: `n_scenes` blocks of the
+    config-5 scene class (Neo-Hookean, per-tet E log-uniform in [1e4, 1e7],
+    nu uniform in [0.25, 0.45], base pinned, a seeded surface impulse), each
+    with its own seed (seed * 1000 + i), laid out along x `spacing` m apart
+    and merged into one mesh as Mesh3D.mergeMesh does; the three layers of
+    config 5 (coarse^3- and mid^3-cube clusters, then fine)."""
+    meshes, cols_c, cols_m, imp_dofs, imp_dv = [], [], [], [], []
+    x0, nb_c, nb_m, voff = 0.0, 0, 0, 0
+    for i in range(n_scenes):
+        rng = np.random.default_rng(seed * 1000 + i)
+        V, T, cube = generate_beam(nx, ny, nz, 0.1, origin=(x0, 0.0, 0.0))
+        x0 += nx * 0.1 + spacing
+        nt = T.shape[0]
+        E = np.exp(rng.uniform(np.log(1e4), np.log(1e7), nt))
+        mu, lam = to_lame(rng.uniform(0.25, 0.45, nt), E)
+        m = Mesh3D.from_arrays(V, T, mu, lam, rho=1000.0, alpha1=0.0, energy_type=_lib.MLX_ENERGY_NEOHOOKEAN)
+        m.pin(np.nonzero(np.isclose(V[:, 2], 0.0))[0] + 1)
+        forced = np.zeros(nt, dtype=bool)
+        forced[m.pinnedTets - 1] = True
+        sc = cluster_rigid_sets(cube, (nx, ny, nz), coarse, forced)
+        sm = cluster_rigid_sets(cube, (nx, ny, nz), mid, forced)
+        sc[sc > 0] += nb_c
+        sm[sm > 0] += nb_m
+        nb_c, nb_m = int(max(nb_c, sc.max(initial=0))), int(max(nb_m, sm.max(initial=0)))
+        cols_c.append(sc)
+        cols_m.append(sm)
+        patch, dv = _surface_impulse(rng, V, nz * 0.1)
+        g = patch + voff
+        imp_dofs.append(np.stack([g * 3 + 1, g * 3 + 2, g * 3 + 3], 1).ravel())
+        imp_dv.append(dv.ravel())
+        voff += m.N
+        meshes.append(m)
+    mesh = merge_meshes(meshes)
+    sets = np.asfortranarray(np.stack([np.zeros(mesh.T, np.int32), np.concatenate(cols_m).astype(np.int32),
+                                       np.concatenate(cols_c).astype(np.int32)], 1))
+    sc = Scene(f"config5_batch_{n_scenes}x{nx}x{ny}x{nz}_seed{seed}", mesh, 1.0 / 60.0, 300, [50, 25, 0], [5, 5, 10],
+               custom_sets=sets, impulse=(np.concatenate(imp_dofs).astype(np.int32), np.concatenate(imp_dv)))
+    sc.settings["parts"] = meshes
+    return sc
+
+
 def _surface_impulse(rng, V, top_z, radius=0.4):
     """A seeded velocity on a patch of the top surface (0-based vertex ids)."""
     top = np.nonzero(np.isclose(V[:, 2], top_z))[0]

@@ -239,10 +239,13 @@ class ResidentSim:
                                                             C.byref(it), C.byref(ru), C.byref(st)), self._lib)
         return ra[:min(n.value, capacity)].copy(), it.value, ru.value, st.value
 
-    def warm_start(self, record=False, mode=0, net=None, feature_norm=None, output_norm=None, corrections=None):
+    def warm_start(self, record=False, mode=0, net=None, feature_norm=None, output_norm=None, corrections=None,
+                   fallback_residual=1e-3):
         """Learned warm start (``mlx_sim_warm_start``): mode 0 off, 1 the
         perceptron ``net`` with feature / output normalisation ((mean, std)
-        pairs of 44 and 7 values), 2 fixed ``corrections`` (clusters x 7).
+        pairs of 44 and 8 values), 2 fixed ``corrections`` (clusters x 8).
+        Clusters whose predicted rigid-fit residual exceeds
+        ``fallback_residual`` (m; <= 0: never) keep the plain start.
         ``record`` keeps every step's features and targets.  Returns the
         number of clusters."""
         from ._lib import f32
@@ -254,8 +257,8 @@ class ResidentSim:
         self._ws_keep = (net, fm, fs, om, osd, corr)
         nb = C.c_int32(0)
         check("mlx_sim_warm_start", self._lib.mlx_sim_warm_start(
-            self.solver.handle, int(bool(record)), int(mode), net.handle if net is not None else None, f32(fm),
-            f32(fs), f32(om), f32(osd), f32(corr), C.byref(nb)), self._lib)
+            self.solver.handle, int(bool(record)), int(mode), net.handle if net is not None else None,
+            float(fallback_residual), f32(fm), f32(fs), f32(om), f32(osd), f32(corr), C.byref(nb)), self._lib)
         self._ws_nb = nb.value
         return nb.value
 
@@ -268,15 +271,22 @@ class ResidentSim:
             self.solver.handle, int(bool(on)), float(scale), float(extrapolation)), self._lib)
 
     def warm_start_records(self):
-        """Features (clusters x 44) and targets (clusters x 7) of the last step."""
+        """Features (clusters x 44) and targets (clusters x 8) of the last step."""
+        return self._ws_fetch()[:2]
+
+    def warm_start_fallbacks(self):
+        """Clusters that kept the plain start in the last step (gated)."""
+        return self._ws_fetch()[2]
+
+    def _ws_fetch(self):
         from ._lib import f32
         nb = self._ws_nb
         feat = np.zeros((nb, 44), np.float32)
-        tgt = np.zeros((nb, 7), np.float32)
-        n = C.c_int32(0)
+        tgt = np.zeros((nb, 8), np.float32)
+        n, fb = C.c_int32(0), C.c_int32(0)
         check("mlx_sim_warm_start_fetch", self._lib.mlx_sim_warm_start_fetch(self.solver.handle, f32(feat), f32(tgt),
-                                                                              nb, C.byref(n)), self._lib)
-        return feat, tgt
+                                                                              nb, C.byref(n), C.byref(fb)), self._lib)
+        return feat, tgt, fb.value
 
     def contact_count(self):
         """Contact vertices of the last step."""

@@ -95,6 +95,10 @@ def test_features_and_targets_match_numpy(gpu):
             R = _polar(((x1[ids] - c1) * w).T @ (x0[ids] - c0))
             np.testing.assert_allclose(tgt[b, 0:3], (c1 - c0) / h - feat[b, 0:3], rtol=1e-3, atol=1e-4)
             np.testing.assert_allclose(tgt[b, 3:6], _log(R) / h - feat[b, 3:6], rtol=1e-3, atol=2e-3)
+            # predicted-residual target: log10 RMS distance from the fitted rigid motion
+            e = (x1[ids] - c1) - (x0[ids] - c0) @ R.T
+            rms = np.sqrt((w[:, 0] * (e * e).sum(1)).sum() / w.sum())
+            assert abs(tgt[b, 7] - np.log10(max(rms, 1e-9))) <= 2e-2
             checked += 1
     assert checked > 10
 
@@ -104,7 +108,7 @@ def test_zero_corrections_are_the_plain_solve(gpu):
     a, _ = _sim(m, sets, v0, residuals=False)
     b, _ = _sim(m, sets, v0, residuals=False)
     nb = a.warm_start(record=False, mode=0)
-    b.warm_start(record=False, mode=2, corrections=np.zeros((nb, 7), np.float32))
+    b.warm_start(record=False, mode=2, corrections=np.zeros((nb, 8), np.float32), fallback_residual=-1.0)
     for _ in range(3):
         a.step(1, graph=True)
         b.step(1, graph=True)
@@ -134,3 +138,74 @@ def test_trained_network_beats_no_correction(gpu):
         ra, _, _, status = warm.monitor()
         assert status == 0 and abs(ra[-1]) <= 1e-4
         assert np.abs(warm.state()[0] - plain.state()[0]).max() / d <= 1e-3
+
+
+def test_gate_falls_back_to_the_plain_start(gpu):
+    """Corrections whose predicted rigid-fit residual is above the gate are
+    not applied: large corrections with a predicted residual of 1 m leave the
+    solve bit-identical to the plain one, and every cluster is counted."""
+    m, sets, v0 = _scene()
+    a, _ = _sim(m, sets, v0, residuals=False)
+    b, _ = _sim(m, sets, v0, residuals=False)
+    a.warm_start(record=False, mode=0)
+    nb = int(sets[:, 1].max())
+    corr = np.tile(np.array([[0.5, -0.3, 0.2, 1.0, 0.0, -1.0, 10.0, 0.0]], np.float32), (nb, 1))
+    assert b.warm_start(record=False, mode=2, corrections=corr, fallback_residual=1e-3) == nb
+    for _ in range(2):
+        a.step(1, graph=True)
+        b.step(1, graph=True)
+        np.testing.assert_array_equal(a.state()[0], b.state()[0])
+        assert b.warm_start_fallbacks() == nb
+    # below the gate the same corrections change the step
+    c, _ = _sim(m, sets, v0, residuals=False)
+    corr[:, 7] = -6.0
+    c.warm_start(record=False, mode=2, corrections=corr, fallback_residual=1e-3)
+    c.step(1, graph=True)
+    assert c.warm_start_fallbacks() == 0
+    assert np.abs(c.state()[0] - a.state()[0]).max() > 0
+
+
+def _sim_from(m, sets, p0, u0, h=1.0 / 60.0):
+    """A residual-monitored stepper like _sim, started from (p0, u0)."""
+    it = XpbdLayer3D()
+    it.setLayers([50, 0])
+    it.iterations = [3, 6]
+    it.customRigidSets = sets
+    it.precision = _lib.MLX_FP32
+    it.computeResiduals = True
+    it.runUntilResSmallerThan = 1e-4
+    it.hangingStop = 3000
+    ls = find_boundary_vertices(m, sets, [0, int(sets[:, 1].max())])
+    s = Solver(m, precision=_lib.MLX_FP32, material="lame")
+    return ResidentSim(s, it, ls, h, p0=p0, v0=u0)
+
+
+def test_exact_correction_bounds_the_gain(gpu):
+    """Upper bound of a warm start of this form: feeding every cluster the
+    exact correction of the converged step (the recorded targets of the plain
+    solve, as if the network were perfect) from the same state saves few
+    iterations to residual 1e-4, because they are spent in the fine layer's
+    Gauss-Seidel.  Asserts the saving stays below 5 % (so a >= 3x gain in
+    steps/s is out of reach for this warm start) and that the exactly
+    corrected solve reaches the same residual with positions within 1e-4 of
+    the bounding-box diagonal of the plain solve."""
+    m, sets, v0 = _scene(dims=(24, 8, 8), cluster=4)
+    plain, _ = _sim(m, sets, v0)
+    plain.warm_start(record=True, mode=0)
+    d = m.bbox_diagonal()
+    saved, total = 0, 0
+    for _ in range(4):
+        p0, u0 = (a.copy() for a in plain.state()[:2])
+        plain.step(1, graph=True)
+        _, it_plain, _, _ = plain.monitor()
+        _, tgt = plain.warm_start_records()
+        ex = _sim_from(m, sets, p0, u0)
+        ex.warm_start(record=False, mode=2, corrections=tgt, fallback_residual=-1.0)
+        ex.step(1, graph=True)
+        ra, it_exact, _, status = ex.monitor()
+        assert status == 0 and abs(ra[-1]) <= 1e-4
+        assert np.abs(ex.state()[0] - plain.state()[0]).max() / d <= 1e-4
+        saved += it_plain - it_exact
+        total += it_plain
+    assert total > 100
+    assert saved < 0.05 * total, (saved, total)
