@@ -1,22 +1,29 @@
 #!/usr/bin/env python
 """Throughput of the multi-layer XPBD step on B200 (one JSON line on rank 0).
 
-Workload: the plain multi-layer Neo-Hookean block -- 64x16x16 cubes of 0.1 m,
-6 tets per cube (18,785 vertices, 98,304 tets), per-tet E log-uniform in
-[1e4, 1e7] Pa, nu uniform in [0.25, 0.45] (seeded), a coarse layer of fixed
-8^3-cube rigid clusters (5 iterations) then the fine layer (10 iterations),
-dt = 1/60 s, base pinned, seeded surface impulse at t = 0.  Synthetic data.
+Default workload (the metric's configuration, config 5): the learned warm
+start's Neo-Hookean block -- 64x32x32 cubes of 0.1 m, 6 tets per cube (70,785
+vertices, 393,216 tets), per-tet E log-uniform in [1e4, 1e7] Pa, nu uniform in
+[0.25, 0.45] (seeded), three layers (8^3-cube clusters, 4^3-cube clusters,
+fine), dt = 1/60 s, base pinned, seeded surface impulse at t = 0.  Synthetic
+data.  A step is one xpbdLayer3D.integrate step solved to residual 1e-4
+(runUntilResSmallerThan = 1e-4, the stop rules of simpleMonitorError on the
+device).
 
-A step is one xpbdLayer3D.integrate step.  `value` is steps/s of the
-device-resident stepper (state in HBM, one CUDA graph per step) with L2
-flushed between timed steps; `e2e` is steps/s through the public host API
-(XpbdLayer3D.integrate -> mlx_layer_solve with host buffers, every step copies
-its inputs host->device and its positions back).  Multi-GPU runs are
-independent replicas (weak scaling): the step does not shard.
+`value` is steps/s of the learned warm-start solve to residual 1e-4 on the
+device-resident stepper (state in HBM, one CUDA graph per step with the
+monitor as conditional nodes, L2 flushed between timed steps); the plain solve
+of the same steps, both iteration counts and the FP32-vs-FP64 position error
+are in `to_residual`.  `e2e` is steps/s of the plain solve to residual 1e-4
+through the public host API (XpbdLayer3D.integrate -> mlx_layer_solve, host
+buffers in and out every step).  `fixed_iterations` times the same scene at
+the configuration's fixed iteration counts (the colour-sweep roofline).
+Multi-GPU runs are independent replicas (weak scaling).
 
 Other workloads (`--config`): 1 = `--replicas` copies of the 8x2x2
-single-layer cantilever merged into one mesh, 3 = the 256-scene batch, 4 = the
-contact-heavy drop, 5 = the learned warm start's block.
+single-layer cantilever merged into one mesh, 2 = the plain multi-layer block
+64x16x16, 3 = the 256-scene batch, 4 = the contact-heavy drop (2 and 4 also
+run the learned leg, with a network trained in the run).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config C]
 """
@@ -53,7 +60,7 @@ WORKLOADS = {
         "detected on the device every step, 3 layers (4^3-cube clusters 1 it, 2^3-cube clusters 4 it, fine 10 it), "
         "contact resistance 0.9, dt=1/120; timed after the boxes have landed"),
 }
-WORKLOAD = WORKLOADS[2]
+WORKLOAD = WORKLOADS[5]
 REPLICAS = 4096
 
 
@@ -148,7 +155,11 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
-CONFIG = 2
+CONFIG = 5
+# configurations whose line is the metric: the learned warm start vs the
+# plain solve, both to residual 1e-4
+RESIDUAL_CONFIGS = (2, 4, 5)
+RUN_UNTIL = 1e-4
 
 
 def make_scene():
@@ -159,10 +170,12 @@ def make_scene():
 
 
 def make_training_scene():
-    """Another seed of the workload's scene class (other materials and
-    impulse): the warm start's network is trained on its solver records."""
+    """Another seed of the workload's scene class (other materials, impulse
+    or drop): the warm start's network is trained on its solver records when
+    no trained network is shipped for the workload."""
     from multilayersolver2024_b200 import scenes
-    return {2: lambda: scenes.config2(seed=3), 5: lambda: scenes.config5(seed=6)}[CONFIG]()
+    return {2: lambda: scenes.config2(seed=3), 4: lambda: scenes.config4(seed=14),
+            5: lambda: scenes.config5(seed=6)}[CONFIG]()
 
 
 def start_velocity(scene, m):
@@ -171,7 +184,7 @@ def start_velocity(scene, m):
         m.v[scene.impulse[0] - 1] += scene.impulse[1]
 
 
-def make_integrator(scene, precision):
+def make_integrator(scene, precision, residual=False, cap=15000):
     from multilayersolver2024_b200 import XpbdLayer3D
     integ = XpbdLayer3D()
     integ.Gravity = scene.gravity
@@ -180,18 +193,25 @@ def make_integrator(scene, precision):
     integ.customRigidSets = scene.custom_sets
     integ.precision = precision
     integ.contactResistance = scene.settings.get("contactResistance", integ.contactResistance)
+    if residual:
+        integ.computeResiduals = True
+        integ.runUntilResSmallerThan = RUN_UNTIL
+        integ.hangingStop = cap
     return integ
 
 
-def cpu_port_steps_per_s(nsteps, threads, state=None):
+def cpu_port(nsteps, threads, state=None, residual=False, cap=15000, budget_s=None):
     """The oracle (FP64 C++ restatement of the reference path, all given host
-    threads) on the same workload: steps/s over `nsteps` steps, from the
-    scene's t = 0 state or from `state` = (positions, velocities)."""
+    threads) on the same workload from the scene's t = 0 state or from
+    `state` = (positions, velocities): (steps, seconds, projectGS iterations
+    per step).  With `residual` every step runs to residual 1e-4 (at most
+    `cap` iterations); with `budget_s` steps stop once that much time has
+    passed (at least one step)."""
     from oracle import oracle as O
     from multilayersolver2024_b200.xpbd_layer3d import ContactSet, StepCache
     O.load().orc_set_threads(threads)
     sc = make_scene()
-    integ = make_integrator(sc, 1)
+    integ = make_integrator(sc, 1, residual, cap)
     m = sc.mesh
     start_velocity(sc, m)
     if state is not None:
@@ -202,12 +222,15 @@ def cpu_port_steps_per_s(nsteps, threads, state=None):
         # simulate3D's loop: the finders on the step-start positions
         return O.find_contacts(sc.contact_finders, m.p) if sc.contact_finders else ContactSet()
 
-    O.integrate(integ, m, sc.h, contacts(), cache, 1)  # warm-up (frame 1)
     t0 = time.perf_counter()
-    for frame in range(2, nsteps + 2):
-        O.integrate(integ, m, sc.h, contacts(), cache, frame)
-    dt = time.perf_counter() - t0
-    return nsteps / dt, dt
+    iters = []
+    for frame in range(1, nsteps + 1):
+        if residual:
+            integ.runUntilResSmallerThan = RUN_UNTIL
+        iters.append(int(O.integrate(integ, m, sc.h, contacts(), cache, frame)[1]))
+        if budget_s is not None and time.perf_counter() - t0 >= budget_s:
+            break
+    return len(iters), time.perf_counter() - t0, iters
 
 
 # untimed steps of the device stepper that bring a scene into its timed phase
@@ -220,20 +243,25 @@ def run_reference(args, rank, world):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    warm = max(args.warmup, 0)
-    # warm-up steps are part of the same run of the port
-    total = warm + args.steps
-    sps, dt = cpu_port_steps_per_s(total, threads)
-    value = sps
+    if CONFIG in RESIDUAL_CONFIGS:
+        # full steps to residual 1e-4 (the metric's solve), as many as fit a
+        # bounded time; every step is a whole step, none is extrapolated
+        n, dt, iters = cpu_port(max(args.warmup, 0) + args.steps, threads, residual=True, budget_s=args.ref_budget)
+        sample = (f"{n} consecutive steps of the full workload from t = 0, each solved to residual 1e-4 "
+                  f"(projectGS iterations {iters}; oracle restatement, OpenMP over the tets of a colour; stops "
+                  f"once {args.ref_budget:.0f} s have passed; MATLAB, the reference's runtime, is not installed)")
+        solver = "plain multi-layer to residual 1e-4, CPU port"
+    else:
+        n, dt, _ = cpu_port(max(args.warmup, 0) + args.steps, threads)
+        sample = (f"{n} consecutive steps of the full workload (oracle restatement; MATLAB, the reference's "
+                  "runtime, is not installed)")
+        solver = "plain multi-layer, CPU port"
+    value = n / dt
     line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "solver": "plain multi-layer, CPU port"},
-            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "port",
-                             "sample": f"{total} consecutive steps of the full workload (oracle restatement; "
-                                       "MATLAB, the reference's runtime, is not installed)"
-                                       + (", from t = 0 with the oracle contact finders every step" if CONFIG == 4
-                                          else "")},
+            "config": {"workload": WORKLOAD, "solver": solver},
+            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -241,7 +269,7 @@ def run_reference(args, rank, world):
 
 def run_ours(args, rank, world, local):
     import torch
-    from multilayersolver2024_b200 import MLX_ENERGY_NEOHOOKEAN, MLX_FP32, StepCache, XpbdLayer3D, load
+    from multilayersolver2024_b200 import MLX_ENERGY_NEOHOOKEAN, MLX_FP32, MLX_FP64, StepCache, load
     from multilayersolver2024_b200.xpbd_layer3d import ContactSet, ResidentSim, Solver, find_boundary_vertices
 
     torch.cuda.set_device(local)
@@ -257,19 +285,30 @@ def run_ours(args, rank, world, local):
         if dist:
             dist.barrier()
 
-
     sc = make_scene()
     m = sc.mesh
-    integ = make_integrator(sc, MLX_FP32)
+    diag = m.bbox_diagonal()
     sets = sc.custom_sets
     ls = find_boundary_vertices(m, sets, [int(sets[:, c].max(initial=0)) for c in range(sets.shape[1])])
-    solver = Solver(m, precision=MLX_FP32, device=local, material="lame")
-    sim = ResidentSim(solver, integ, ls, sc.h, p0=m.p, v0=np.zeros_like(m.p))
-    if sc.impulse is not None:
-        sim.add_velocity(sc.impulse[0], sc.impulse[1])
-    if sc.contact_finders:
-        sim.set_obstacles(sc.contact_finders, restitution=1e-2)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
     advance = ADVANCE.get(CONFIG, 0) if args.advance is None else args.advance
+
+    def stepper(precision, residual, state=None):
+        integ = make_integrator(sc, precision, residual, args.residual_cap)
+        solver = Solver(m, precision=precision, device=local, material="lame")
+        if state is None:
+            sim = ResidentSim(solver, integ, ls, sc.h, p0=m.p, v0=np.zeros_like(m.p))
+            if sc.impulse is not None:
+                sim.add_velocity(sc.impulse[0], sc.impulse[1])
+        else:
+            sim = ResidentSim(solver, integ, ls, sc.h, p0=state[0], v0=state[1])
+        if sc.contact_finders:
+            sim.set_obstacles(sc.contact_finders, restitution=1e-2)
+        return solver, sim
+
+    # ---- fixed iteration counts (the configuration's own): colour-sweep
+    # roofline and steps/s ----
+    solver, sim = stepper(MLX_FP32, False)
     if advance:
         sim.step(advance, graph=True)
         torch.cuda.synchronize()
@@ -279,52 +318,154 @@ def run_ours(args, rank, world, local):
         before, after = sim.autotune(reps=5)
         tuned = {"step_ms_default_tiles": before, "step_ms_tuned_tiles": after}
     sim.sweep_timing(True)
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
     for _ in range(args.warmup):
         sim.step(1, graph=True)
     torch.cuda.synchronize()
     sim.sweep_stats(reset=True)
     contacts_at_start = sim.contact_count() if sc.contact_finders else None
-
+    residual_metric = CONFIG in RESIDUAL_CONFIGS and not args.no_residual_leg
     clocks = ClockSampler(local)
-    clocks.start()
+    if not residual_metric:
+        clocks.start()
     barrier()
     torch.cuda.synchronize()
-    total_ms = 0.0
+    fixed_ms = 0.0
     for _ in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
-        total_ms += sim.step(1, graph=True, timed=True)
+        fixed_ms += sim.step(1, graph=True, timed=True)
     torch.cuda.synchronize()
     barrier()
-    clocks.stop()
+    if not residual_metric:
+        clocks.stop()
     sweep_ms, sweep_bytes, sweep_launches = sim.sweep_stats(reset=True)
     contacts_at_end = sim.contact_count() if sc.contact_finders else None
-    max_ms = max_over_ranks(total_ms, dist)
-    value = args.steps * world / (max_ms / 1000.0)
-    launches_per_step = sim.launches_per_step
-    p_gpu, _ = sim.state()
-    finite = bool(np.all(np.isfinite(p_gpu)))
+    fixed_max_ms = max_over_ranks(fixed_ms, dist)
+    fixed_value = args.steps * world / (fixed_max_ms / 1000.0)
+    fixed_launches = sim.launches_per_step
+    finite = bool(np.all(np.isfinite(sim.state()[0])))
+    solver_launch_path = solver.launch_path
+    solver.close()
+    state0 = _PHASE.get("state")
+
+    # ---- to residual 1e-4: the plain solve, the learned warm start and the
+    # FP64 plain solve of the same steps ----
+    to_res = None
+    if residual_metric:
+        from multilayersolver2024_b200.learned import collect_warm_start_data, fit_warm_start
+        from multilayersolver2024_b200.warm_start_training import DEFAULT_NET, load_warm_start
+
+        def run_leg(sim3, n, timed, record_clocks=False):
+            iters, ms_steps, finals, fallbacks = [], [], [], []
+            if record_clocks:
+                clocks.start()
+            barrier()
+            for _ in range(n):
+                if timed:
+                    flush.zero_()
+                    torch.cuda.synchronize()
+                ms_steps.append(sim3.step(1, graph=True, timed=True))
+                ra, it_total, _, status = sim3.monitor()
+                iters.append(int(it_total))
+                finals.append(float(ra[-1]))
+                if getattr(sim3, "_ws_nb", 0):
+                    fallbacks.append(sim3.warm_start_fallbacks())
+            barrier()
+            if record_clocks:
+                clocks.stop()
+            return {"iterations_per_step": iters, "ms_per_step": ms_steps,
+                    "steps_per_s": len(ms_steps) / (max_over_ranks(sum(ms_steps), dist) / 1000.0),
+                    "final_residual": finals, "reached": [bool(abs(r) <= RUN_UNTIL) for r in finals],
+                    "clusters_fallen_back_per_step": fallbacks or None}
+
+        # the network: shipped (trained on 20k block-steps by
+        # warm_start_training) for config 5, else trained here on recorded
+        # steps of another seed of the scene class
+        t0 = time.perf_counter()
+        if CONFIG == 5 and DEFAULT_NET.exists() and not args.train_in_bench:
+            net, fn, on, meta = load_warm_start(DEFAULT_NET)
+            training = {"source": f"shipped network {DEFAULT_NET.name} (warm_start_training)", **meta}
+        else:
+            tsc = make_training_scene()
+            integ_t = make_integrator(tsc, MLX_FP32, True, args.residual_cap)
+            ls_t = find_boundary_vertices(tsc.mesh, tsc.custom_sets,
+                                          [int(tsc.custom_sets[:, c].max(initial=0))
+                                           for c in range(tsc.custom_sets.shape[1])])
+            solver_t = Solver(tsc.mesh, precision=MLX_FP32, device=local, material="lame")
+            if advance:
+                solver_a = Solver(tsc.mesh, precision=MLX_FP32, device=local, material="lame")
+                sim_a = ResidentSim(solver_a, make_integrator(tsc, MLX_FP32), ls_t, tsc.h, p0=tsc.mesh.p,
+                                    v0=np.zeros_like(tsc.mesh.p))
+                sim_a.set_obstacles(tsc.contact_finders, restitution=1e-2)
+                sim_a.step(advance, graph=True)
+                pa, va = sim_a.state()
+                solver_a.close()
+                sim_t = ResidentSim(solver_t, integ_t, ls_t, tsc.h, p0=pa, v0=va)
+            else:
+                sim_t = ResidentSim(solver_t, integ_t, ls_t, tsc.h, p0=tsc.mesh.p, v0=np.zeros_like(tsc.mesh.p))
+                if tsc.impulse is not None:
+                    sim_t.add_velocity(tsc.impulse[0], tsc.impulse[1])
+            if tsc.contact_finders:
+                sim_t.set_obstacles(tsc.contact_finders, restitution=1e-2)
+            ftr, ttr, _ = collect_warm_start_data(sim_t, args.learned_train_steps)
+            solver_t.close()
+            net, fn, on, losses = fit_warm_start(ftr, ttr, epochs=300, lr=2e-3, batch=128)
+            training = {"source": f"trained in this run on {args.learned_train_steps} recorded steps of "
+                                  f"{tsc.name}", "rows": int(ftr.shape[0]), "epochs": 300,
+                        "loss_first_last": [float(losses[0]), float(losses[-1])]}
+        training["seconds_in_bench"] = time.perf_counter() - t0
+
+        legs, states = {}, {}
+        for name, precision, warm in (("plain", MLX_FP32, False), ("learned", MLX_FP32, True),
+                                      ("plain_fp64", MLX_FP64, False)):
+            solver3, sim3 = stepper(precision, True, state0)
+            if warm:
+                sim3.warm_start(record=False, mode=1, net=net, feature_norm=fn, output_norm=on,
+                                fallback_residual=args.fallback_residual)
+            run_leg(sim3, args.warmup, timed=False)
+            legs[name] = run_leg(sim3, args.steps if name != "plain_fp64" else args.steps, timed=True,
+                                 record_clocks=(name == "learned"))
+            states[name] = sim3.state()[0]
+            solver3.close()
+        net.close()
+        pl, le = legs["plain"], legs["learned"]
+        it_pl, it_le = sum(pl["iterations_per_step"]), sum(le["iterations_per_step"])
+        to_res = {"run_until": RUN_UNTIL, "hanging_stop": args.residual_cap, "untimed_steps_before": args.warmup,
+                  "steps": args.steps, "plain": pl, "learned_warm_start": {**le, "training": training,
+                                                                            "fallback_residual_m": args.fallback_residual},
+                  "plain_fp64": {k: legs["plain_fp64"][k] for k in ("iterations_per_step", "steps_per_s",
+                                                                      "final_residual")},
+                  "learned_over_plain_steps_per_s": le["steps_per_s"] / pl["steps_per_s"],
+                  "plain_over_learned_iterations": it_pl / max(it_le, 1),
+                  "monitor": "device (layers as conditional IF nodes, projectGS as conditional WHILE nodes)"}
+        parity = {"reference": "FP64 plain solve of the same steps on the GPU (the FP64 path matches the CPU "
+                               "oracle to 1e-9)",
+                  "max_rel_pos_err": float(np.abs(states["learned"] - states["plain_fp64"]).max() / diag),
+                  "max_rel_pos_err_plain_fp32": float(np.abs(states["plain"] - states["plain_fp64"]).max() / diag),
+                  "learned_vs_plain_fp32": float(np.abs(states["learned"] - states["plain"]).max() / diag),
+                  "after_steps": args.warmup + args.steps, "unit": "max |x - x_ref| / bounding-box diagonal"}
 
     # ---- e2e: public host API, host buffers, every step copies in and out ----
     sc2 = make_scene()
     m2 = sc2.mesh
-    integ2 = make_integrator(sc2, MLX_FP32)
+    integ2 = make_integrator(sc2, MLX_FP32, residual_metric, args.residual_cap)
     cache = StepCache()
     start_velocity(sc2, m2)
     if advance:
-        m2.p, m2.v = (a.copy() for a in _PHASE["state"])
+        m2.p, m2.v = (a.copy() for a in state0)
     from multilayersolver2024_b200.contacts import find_contacts
-    contact_bytes = []
+    contact_bytes, e2e_iters = [], []
 
     def e2e_step(frame):
         # simulate3D's step: the finders on the step-start positions (on the
         # device, mlx_find_contacts), then integrate (mlx_layer_solve)
         cs = find_contacts(integ2.solver(m2), sc2.contact_finders, m2.p) if sc2.contact_finders else ContactSet()
         contact_bytes.append(cs.vertex_ids.size)
+        if residual_metric:
+            integ2.runUntilResSmallerThan = RUN_UNTIL
         integ2.integrate(m2, sc2.h, cs, cache, frame)
 
-    e2e_steps = 0 if args.no_e2e else max(3, min(args.steps, {2: 20, 3: 3}.get(CONFIG, 10)))
+    e2e_steps = 0 if args.no_e2e else max(3, min(args.steps, {2: 20, 3: 3, 5: 3}.get(CONFIG, 10)))
     for frame in range(1, 3 if e2e_steps else 1):  # warm-up: solver creation and layer caches
         e2e_step(frame)
     barrier()
@@ -343,105 +484,38 @@ def run_ours(args, rank, world, local):
     # layer solve: xi and v in (2 x 3N; oldp too when the material is
     # damped; lambdai is passed as zeros, NULL), pinned x, contacts (normal,
     # point, compliance, id: 7 x 8 + 4 bytes each); detection: positions in
-    # (3N), contact lists back
+    # (3N), contact lists back; the residual array back when monitored
     damped = m2.energy_type != MLX_ENERGY_NEOHOOKEAN and bool(np.any(np.asarray(m2.alpha1) != 0))
     h2d = (8 * ((3 if damped else 2) * 3 * N + m2.pinnedDOFs.size) + 60 * K
            + (8 * 3 * N if sc2.contact_finders else 0))
     d2h = 8 * 3 * N + (60 * K if sc2.contact_finders else 0)
 
-    # ---- iterations to residual 1e-4: the same workload with the residual
-    # monitor and stop rules on the device (conditional graph nodes) ----
-    to_res = None
-    if not args.no_residual_leg:
-        from multilayersolver2024_b200.learned import collect_warm_start_data, fit_warm_start
-
-        def residual_sim(scene):
-            integ3 = make_integrator(scene, MLX_FP32)
-            integ3.computeResiduals = True
-            integ3.runUntilResSmallerThan = 1e-4
-            integ3.hangingStop = args.residual_cap
-            sets3 = scene.custom_sets
-            ls3 = find_boundary_vertices(scene.mesh, sets3,
-                                         [int(sets3[:, c].max(initial=0)) for c in range(sets3.shape[1])])
-            solver3 = Solver(scene.mesh, precision=MLX_FP32, device=local, material="lame")
-            if advance:
-                p0, v0 = _PHASE["state"]
-            else:
-                p0, v0 = scene.mesh.p, np.zeros_like(scene.mesh.p)
-            sim3 = ResidentSim(solver3, integ3, ls3, scene.h, p0=p0, v0=v0)
-            if scene.impulse is not None and not advance:
-                sim3.add_velocity(scene.impulse[0], scene.impulse[1])
-            if scene.contact_finders:
-                sim3.set_obstacles(scene.contact_finders, restitution=1e-2)
-            return solver3, sim3
-
-        def run_leg(sim3, n):
-            iters, ms_steps, finals = [], [], []
-            for _ in range(n):
-                ms_steps.append(sim3.step(1, graph=True, timed=True))
-                ra, it_total, _, status = sim3.monitor()
-                iters.append(int(it_total))
-                finals.append(float(ra[-1]))
-            return {"iterations_per_step": iters, "ms_per_step": ms_steps,
-                    "steps_per_s": len(ms_steps) / (sum(ms_steps) / 1000.0), "final_residual": finals,
-                    "reached": [bool(abs(r) <= 1e-4) for r in finals]}
-
-        solver_p, sim_p = residual_sim(make_scene())
-        plain_leg = run_leg(sim_p, args.residual_steps)
-        p_plain = sim_p.state()[0]
-        solver_p.close()
-        learned_leg = None
-        if CONFIG in (2, 5) and args.learned_train_steps > 0:
-            # the warm start's network is trained on another seed of the same
-            # scene class, then steps the benchmark scene
-            solver_t, sim_t = residual_sim(make_training_scene())
-            ftr, ttr, _ = collect_warm_start_data(sim_t, args.learned_train_steps)
-            solver_t.close()
-            t0 = time.perf_counter()
-            net, fn, on, losses = fit_warm_start(ftr, ttr, epochs=300, lr=2e-3, batch=128)
-            train_s = time.perf_counter() - t0
-            solver_w, sim_w = residual_sim(make_scene())
-            sim_w.warm_start(record=False, mode=1, net=net, feature_norm=fn, output_norm=on)
-            learned_leg = run_leg(sim_w, args.residual_steps)
-            learned_leg.update({
-                "training": {"samples": int(ftr.shape[0]), "steps_recorded": args.learned_train_steps,
-                             "scene": f"config{CONFIG} seed {3 if CONFIG == 2 else 6}", "epochs": 300,
-                             "seconds": train_s,
-                             "loss_first_last": [float(losses[0]), float(losses[-1])]},
-                "max_position_deviation_from_plain": float(np.abs(sim_w.state()[0] - p_plain).max()
-                                                           / make_scene().mesh.bbox_diagonal())})
-            solver_w.close()
-            net.close()
-        to_res = {"run_until": 1e-4, "hanging_stop": args.residual_cap, "steps": args.residual_steps,
-                  **plain_leg, "learned_warm_start": learned_leg,
-                  "monitor": "device (layers as conditional IF nodes, projectGS as conditional WHILE nodes)"}
-
     # ---- buildLayers for strain-rate layers (the reference's default
     # ordering): on the device against the native host helpers ----
     layer_builder = None
-    if not args.no_e2e:
+    if not args.no_e2e and CONFIG not in (3,):
         from multilayersolver2024_b200.xpbd_layer3d import (build_layers_device, find_boundary_vertices as fbv,
                                                             strain_rate_norms, union_find_layers)
-        sc5 = make_scene()
-        m5 = sc5.mesh
+        solver_b = Solver(m, precision=MLX_FP32, device=local, material="lame")
         rng = np.random.default_rng(0)
-        oldp5 = m5.p + rng.normal(0, 1e-3, m5.p.size)
-        p5 = oldp5 + rng.normal(0, 1e-3, m5.p.size)
-        forced5 = np.zeros(m5.T, np.uint8)
-        forced5[m5.pinnedTets - 1] = 1
+        oldp5 = m.p + rng.normal(0, 1e-3, m.p.size)
+        p5 = oldp5 + rng.normal(0, 1e-3, m.p.size)
+        forced5 = np.zeros(m.T, np.uint8)
+        forced5[m.pinnedTets - 1] = 1
         pct = [0.0, 25.0, 50.0]
-        reps = 5 if m5.T < 1_000_000 else 2
-        build_layers_device(solver, m5, p5, oldp5, sc5.h, pct, forced5)  # warm-up (DmInv copy)
+        reps = 5 if m.T < 1_000_000 else 2
+        build_layers_device(solver_b, m, p5, oldp5, sc.h, pct, forced5)  # warm-up (DmInv copy)
         t0 = time.perf_counter()
         for _ in range(reps):
-            dev = build_layers_device(solver, m5, p5, oldp5, sc5.h, pct, forced5)
+            dev = build_layers_device(solver_b, m, p5, oldp5, sc.h, pct, forced5)
         dev_ms = (time.perf_counter() - t0) * 1000.0 / reps
         t0 = time.perf_counter()
         for _ in range(reps):
-            order5 = np.argsort(strain_rate_norms(m5, p5, oldp5, sc5.h), kind="stable").astype(np.int32) + 1
-            sets5, nr5 = union_find_layers(m5, order5, pct, forced5)
-            host = fbv(m5, sets5, nr5)
+            order5 = np.argsort(strain_rate_norms(m, p5, oldp5, sc.h), kind="stable").astype(np.int32) + 1
+            sets5, nr5 = union_find_layers(m, order5, pct, forced5)
+            host = fbv(m, sets5, nr5)
         host_ms = (time.perf_counter() - t0) * 1000.0 / reps
+        solver_b.close()
         layer_builder = {"layers_pct": pct, "device_ms": dev_ms, "host_ms": host_ms,
                          "identical": bool(np.array_equal(dev.rigidBodySetsPerLayer, host.rigidBodySetsPerLayer)
                                            and np.array_equal(dev.vertexRigidBody, host.vertexRigidBody)),
@@ -451,9 +525,9 @@ def run_ours(args, rank, world, local):
     line = None
     if rank == 0:
         peak, peak_kind = measured_peak_hbm()
-        if solver.launch_path.startswith("cluster"):
+        if solver_launch_path.startswith("cluster"):
             sweep_kernel = "k_layer_cluster (whole projectGS loop of a layer)"
-        elif "CTAs each owning whole components" in solver.launch_path:
+        elif "CTAs each owning whole components" in solver_launch_path:
             sweep_kernel = ("k_layer_groups (whole projectGS loop of each body-free layer; algorithmic bytes without "
                             "vertex records, which stay in shared memory) + k_project_color (layers with bodies)")
         else:
@@ -471,24 +545,55 @@ def run_ours(args, rank, world, local):
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
-            sps, dt = cpu_port_steps_per_s(args.cpu_steps, threads, _PHASE.get("state"))
-            cpu = {"value": sps, "unit": "steps/s", "cores": threads, "kind": "port",
-                   "sample": f"{args.cpu_steps} steps of the full workload after 1 warm-up step "
-                             f"({dt:.1f} s, FP64 oracle restatement, OpenMP over the tets of a colour"
-                             + (", from the same landed state, oracle contact finders every step)" if advance
-                                else ")")}
+            if residual_metric:
+                # a bounded sample: the first step with the monitor on, capped
+                # at cpu_iters iterations, scaled to the plain GPU solve's
+                # iterations per step (same algorithm, same residual rule)
+                n, dt, it = cpu_port(1, threads, state0, residual=True, cap=args.cpu_iters)
+                per_it = dt / max(it[0], 1)
+                gpu_it = float(np.mean(to_res["plain"]["iterations_per_step"]))
+                cpu = {"value": 1.0 / (per_it * gpu_it), "unit": "steps/s", "cores": threads, "kind": "port",
+                       "sample": f"{it[0]} projectGS iterations of one step with the residual monitor on ({dt:.1f} s, "
+                                 f"FP64 oracle restatement, OpenMP over the tets of a colour), scaled to "
+                                 f"{gpu_it:.0f} iterations per step (the plain GPU solve's mean to residual 1e-4)"}
+            else:
+                n, dt, _ = cpu_port(args.cpu_steps + 1, threads, state0)
+                cpu = {"value": n / dt, "unit": "steps/s", "cores": threads, "kind": "port",
+                       "sample": f"{n} steps of the full workload ({dt:.1f} s, FP64 oracle restatement, OpenMP "
+                                 "over the tets of a colour" + (", from the same landed state, oracle contact "
+                                                                 "finders every step)" if advance else ")")}
+        if residual_metric:
+            value = to_res["learned_warm_start"]["steps_per_s"] * world
+            ms_per_step = 1000.0 * world / value
+            solver_desc = "learned warm start (coarse-cluster corrections, BF16 perceptron on tcgen05) to residual 1e-4"
+            iters_le = to_res["learned_warm_start"]["iterations_per_step"]
+            per_iter = fixed_launches / max(sum(sc.iterations), 1)
+            launches = int(sum(it * (per_iter + 2) for it in iters_le))
+            launch_note = ("estimate: iterations of the timed steps x (launches per fixed-count iteration + the "
+                           "monitor's 2)")
+        else:
+            value, ms_per_step = fixed_value, fixed_max_ms / args.steps
+            solver_desc = "plain multi-layer (no warm-start), fixed iteration counts"
+            launches = int(fixed_launches * args.steps)
+            launch_note = "launches of the captured step graph x timed steps"
         line = {
             "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "solver": "plain multi-layer (no warm-start)",
-                       "iterations_per_step": int(sum(sc.iterations)), "precision": "FP32 bulk, FP64 rigid bodies",
+            "config": {"workload": WORKLOAD, "solver": solver_desc,
+                       "fixed_iterations_per_step": int(sum(sc.iterations)),
+                       "precision": "FP32 bulk projection; FP64 rigid bodies, polar decomposition and residual norm; "
+                                    "BF16 perceptron with FP32 accumulation",
                        "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}",
                        "graph": "one CUDA graph per step", "autotune": tuned,
                        "untimed_advance_steps": advance,
                        "contacts_first_last_timed_step": [contacts_at_start, contacts_at_end]},
-            "roofline": {"bound": "hbm", "kernel": sweep_kernel,
-                         "launch_path": solver.launch_path,
+            "to_residual": to_res,
+            "parity": parity if residual_metric else None,
+            "fixed_iterations": {"steps_per_s": fixed_value, "ms_per_step": fixed_max_ms / args.steps,
+                                 "iterations_per_step": int(sum(sc.iterations))},
+            "roofline": {"bound": "hbm", "kernel": sweep_kernel, "measured_on": "fixed_iterations leg",
+                         "launch_path": solver_launch_path,
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None,
                          "traffic": traffic,
@@ -499,12 +604,14 @@ def run_ours(args, rank, world, local):
                          "colour_launches_per_step": sweep_launches / args.steps,
                          "avg_launch_us": 1000.0 * sweep_ms / max(sweep_launches, 1)},
             "cpu_baseline": cpu,
-            "e2e": None if not e2e_steps else {"value": e2e_steps * world / e2e_s, "unit": "steps/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "api": "XpbdLayer3D.integrate -> mlx_layer_solve"
-                    + (" (+ mlx_find_contacts on the step-start positions)" if sc.contact_finders else "")},
-            "to_residual": to_res,
+            "e2e": None if not e2e_steps else {"value": e2e_steps * world / e2e_s, "unit": "steps/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "api": "XpbdLayer3D.integrate -> mlx_layer_solve"
+                    + (" (+ mlx_find_contacts on the step-start positions)" if sc.contact_finders else "")
+                    + (", plain solve to residual 1e-4 with the stop rules on the host (the learned warm start is an "
+                       "option of the device-resident stepper only)" if residual_metric else "")},
             "layer_builder": layer_builder,
-            "gpu_launches": int(launches_per_step * args.steps),
+            "gpu_launches": launches, "gpu_launches_note": launch_note,
             "clocks": clocks.summary(),
             "state_finite": finite,
         }
@@ -512,7 +619,6 @@ def run_ours(args, rank, world, local):
             # independent scenes in the merged mesh
             line["scene_steps_per_s"] = value * (REPLICAS if CONFIG == 1 else 256)
         print(json.dumps(line), flush=True)
-    solver.close()
     if dist:
         dist.destroy_process_group()
     return 0
@@ -533,27 +639,37 @@ def solver_bytes_per_tet(mesh, precision):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=12)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-API leg (profiling runs)")
-    ap.add_argument("--config", type=int, choices=[1, 2, 3, 4, 5], default=2,
-                    help="1: copies of the single-layer cantilever (--replicas); 2: the plain multi-layer block "
-                    "(default); 3: the 256-scene batch; 4: the contact-heavy drop; 5: the learned warm-start "
-                    "workload (64x32x32, 3 layers)")
+    ap.add_argument("--config", type=int, choices=[1, 2, 3, 4, 5], default=5,
+                    help="1: copies of the single-layer cantilever (--replicas); 2: the plain multi-layer block; "
+                    "3: the 256-scene batch; 4: the contact-heavy drop; 5: the learned warm-start workload "
+                    "(64x32x32, 3 layers; default)")
     ap.add_argument("--replicas", type=int, default=4096, help="config 1: copies of the cantilever in the mesh")
     ap.add_argument("--autotune", action="store_true", help="run the per-colour tile autotuner before timing "
                     "(on by default for config 3)")
     ap.add_argument("--no-autotune", action="store_true", help="never run the autotuner (profiling runs)")
     ap.add_argument("--no-residual-leg", action="store_true", help="skip the iterations-to-residual-1e-4 leg")
-    ap.add_argument("--residual-steps", type=int, default=4)
+    ap.add_argument("--cpu-iters", type=int, default=150,
+                    help="projectGS iterations of the CPU-baseline sample on the residual workloads")
+    ap.add_argument("--ref-budget", type=float, default=120.0,
+                    help="--impl reference on the residual workloads: whole steps to residual until this many "
+                    "seconds have passed (at least one)")
+    ap.add_argument("--fallback-residual", type=float, default=1e-3,
+                    help="learned warm start: clusters with a predicted rigid-fit residual above this (m) keep the "
+                    "plain start")
+    ap.add_argument("--train-in-bench", action="store_true",
+                    help="config 5: train the network on recorded steps here instead of loading the shipped one")
     ap.add_argument("--advance", type=int, default=None,
                     help="untimed steps before the warm-up (default: 150 for config 4, which lands the boxes; "
                     "0 for the others)")
-    ap.add_argument("--learned-train-steps", type=int, default=16,
-                    help="recorded steps (another seed) the warm-start network is trained on; 0 skips that leg")
+    ap.add_argument("--learned-train-steps", type=int, default=24,
+                    help="recorded steps (another seed) the warm-start network is trained on when it is trained "
+                    "in the bench")
     ap.add_argument("--residual-cap", type=int, default=15000,
                     help="hangingStop of the residual leg (bounds the iterations of a step)")
     args = ap.parse_args()

@@ -52,7 +52,7 @@ def test_max_over_ranks_gloo():
 def test_reference_arm_two_ranks():
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
            "127.0.0.1", "--master-port", str(_free_port()), "bench.py", "--impl", "reference", "--gpus", "2",
-           "--steps", "1", "--warmup", "0"]
+           "--steps", "1", "--warmup", "0", "--config", "1", "--replicas", "4"]
     r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
