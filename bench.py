@@ -242,6 +242,11 @@ _PHASE = {}
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
+    # the reference arm runs the oracle alone: its scenes are coloured by the
+    # oracle's own first-fit colouring, so the product library is never loaded
+    from oracle import oracle as O
+    from multilayersolver2024_b200 import mesh3d
+    mesh3d.use_coloring(O.greedy_coloring)
     threads = os.cpu_count() or 1
     if CONFIG in RESIDUAL_CONFIGS:
         # full steps to residual 1e-4 (the metric's solve), as many as fit a

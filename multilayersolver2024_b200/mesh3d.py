@@ -28,8 +28,22 @@ def to_lame(nu, E):
     return E / (2 * (1 + nu)), (E * nu) / ((1 + nu) * (1 - 2 * nu))
 
 
+_COLORING = None
+
+
+def use_coloring(fn):
+    """Replace the colouring used by Mesh3D (fn(t, N) -> (colours, count));
+    None restores the native one.  A CPU-only caller that must not load the
+    native library passes its own first-fit colouring here."""
+    global _COLORING
+    _COLORING = fn
+
+
 def greedy_coloring(t: np.ndarray, N: int):
     """naiveGraphColoring via the native first-fit colouring (1-based colours)."""
+    if _COLORING is not None:
+        col, nc = _COLORING(t, N)
+        return np.ascontiguousarray(col, np.int32), int(nc)
     lib = load()
     tf = np.asfortranarray(t, dtype=np.int32)
     T = tf.shape[0]

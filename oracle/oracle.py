@@ -6,7 +6,11 @@ against the headless mx runtime (oracle/_ref/*.so).  Only tests, the smoke
 check and bench.py's CPU-baseline leg import this module; the product never
 does.  ``integrate`` below is an independent restatement of
 xpbdLayer3D.integrate (3d/integrator/xpbdLayer3D.m:621-745) built on the
-oracle's C functions.
+oracle's C functions.  The marshalling to the oracle's C entry points (the
+argument structs of include/mlxpbd.h, contact lists, layer sets, parameters)
+is this module's own, so a layout error in the product's marshalling cannot
+hide in both sides of a comparison; the integrator settings and meshes it
+receives are plain data (attributes are read, no product code is called).
 """
 from __future__ import annotations
 
@@ -37,8 +41,6 @@ def load():
         return _lib
     if not LIB.exists():
         build()
-    from multilayersolver2024_b200._lib import (Contacts, LayerDesc, MeshDesc, SolveInputs, SolveOutputs,
-                                                SolveParams)
     lib = C.CDLL(str(LIB))
     sig = {
         "orc_last_error": ([], C.c_char_p),
@@ -78,7 +80,155 @@ def load():
 
 
 def _p(a, t):
+    if a is None:
+        return C.cast(None, C.POINTER(t))
     return a.ctypes.data_as(C.POINTER(t))
+
+
+# ---- the argument structs of include/mlxpbd.h (layout of the C header) ----
+class MeshDesc(C.Structure):
+    _fields_ = [("num_vertices", C.c_int32), ("num_tets", C.c_int32), ("t", _i32p), ("mass", _f64p),
+                ("DmInv", _f64p), ("volume", _f64p), ("element_color", _i32p), ("num_colors", C.c_int32),
+                ("pinned_dofs", _i32p), ("num_pinned_dofs", C.c_int32), ("energy_type", C.c_int32),
+                ("alpha", _f64p), ("beta", _f64p), ("mu", _f64p), ("lambda_", _f64p), ("alpha1", _f64p),
+                ("precision", C.c_int32), ("device", C.c_int32)]
+
+
+class LayerDesc(C.Structure):
+    _fields_ = [("num_layers", C.c_int32), ("num_columns", C.c_int32), ("layers_map", _i32p),
+                ("iterations", _i32p), ("is_elastic_element", _u8p), ("is_rigid_element", _u8p),
+                ("rigid_body_sets", _i32p), ("vertex_rigid_body", _i32p), ("is_boundary_vertex", _u8p),
+                ("is_rigid_vertex", _u8p), ("num_rigids", _i32p)]
+
+
+class SolveParams(C.Structure):
+    _fields_ = [("h", C.c_double), ("boundary_compliance", C.c_double), ("contact_resistance", C.c_double),
+                ("run_until", C.c_double), ("give_up_threshold", C.c_double), ("gravity_compliance", C.c_double),
+                ("gravity", C.c_double), ("stop_at_improvement_percent", C.c_double),
+                ("compute_residuals", C.c_int32), ("hanging_stop", C.c_int32), ("give_up_enabled", C.c_int32),
+                ("last_layer_give_up_enabled", C.c_int32), ("use_gravity_constraints", C.c_int32),
+                ("use_rigid_contacts", C.c_int32), ("contact_coloring", C.c_int32)]
+
+
+class Contacts(C.Structure):
+    _fields_ = [("num_contacts", C.c_int32), ("normals", _f64p), ("point_colliders", _f64p),
+                ("vertex_ids", _i32p), ("compliance", _f64p)]
+
+
+class SolveInputs(C.Structure):
+    _fields_ = [("xi", _f64p), ("lambdai", _f64p), ("oldp", _f64p), ("old_oldp", _f64p), ("f", _f64p),
+                ("residualv", _f64p), ("pinnedx", _f64p), ("residual_in", _f64p), ("residual_in_len", C.c_int32),
+                ("sum_non_monitored_time", C.c_double)]
+
+
+class SolveOutputs(C.Structure):
+    _fields_ = [("xi", _f64p), ("lambdai", _f64p), ("residual", _f64p), ("residual_capacity", C.c_int32),
+                ("residual_len", C.c_int32), ("run_until", C.c_double), ("sum_non_monitored_time", C.c_double),
+                ("total_iterations", C.c_int32)]
+
+
+ENERGY_NEOHOOKEAN = 1  # mlx_mesh_desc.energy_type of the stable Neo-Hookean pair (include/mlxpbd.h)
+OBSTACLE_PLANE, OBSTACLE_SPHERE, OBSTACLE_BOX = 1, 2, 3  # MLX_OBSTACLE_* of include/mlxpbd.h
+
+
+class ContactList:
+    """One contact list in simulate3D's format: normals and point colliders
+    (K x 3), 1-based vertex ids, compliances."""
+
+    def __init__(self, normals=None, points=None, vertex_ids=None, compliance=None):
+        self.normals = np.zeros((0, 3)) if normals is None else np.asarray(normals, float).reshape(-1, 3)
+        self.points = np.zeros((0, 3)) if points is None else np.asarray(points, float).reshape(-1, 3)
+        self.vertex_ids = np.zeros(0, np.int32) if vertex_ids is None else np.asarray(vertex_ids, np.int32).ravel()
+        self.compliance = np.zeros(0) if compliance is None else np.asarray(compliance, float).ravel()
+
+    @staticmethod
+    def concat(lists):
+        lists = [c for c in lists if c.vertex_ids.size]
+        if not lists:
+            return ContactList()
+        return ContactList(np.concatenate([c.normals for c in lists]), np.concatenate([c.points for c in lists]),
+                           np.concatenate([c.vertex_ids for c in lists]),
+                           np.concatenate([c.compliance for c in lists]))
+
+
+def _mesh_desc(mesh, material, keep):
+    """mlx_mesh_desc of a mesh (FP64 oracle: precision and device unused)."""
+    def k(a, dt):
+        keep.append(np.ascontiguousarray(a, dt) if dt is not None else a)
+        return keep[-1]
+    d = MeshDesc()
+    d.num_vertices, d.num_tets = int(mesh.N), int(mesh.T)
+    d.t = i32(k(np.asfortranarray(mesh.t, np.int32), None))
+    d.mass = f64(k(mesh.mass, np.float64))
+    d.DmInv = f64(k(mesh.DmInv, np.float64))
+    d.volume = f64(k(mesh.elV, np.float64))
+    d.element_color = i32(k(mesh.elementColor, np.int32))
+    d.num_colors = int(mesh.numColors)
+    d.pinned_dofs = i32(k(mesh.pinnedDOFs, np.int32))
+    d.num_pinned_dofs = int(np.asarray(mesh.pinnedDOFs).size)
+    d.energy_type = int(mesh.energy_type)
+    if int(mesh.energy_type) != ENERGY_NEOHOOKEAN and material == "blocks":
+        d.alpha = f64(k(mesh.perElementXPBDalphaMatrix, np.float64))
+        d.beta = f64(k(mesh.perElementXPBDbeta, np.float64))
+    else:
+        d.mu = f64(k(mesh.mu, np.float64))
+        d.lambda_ = f64(k(mesh.lam, np.float64))
+        d.alpha1 = f64(k(mesh.alpha1, np.float64))
+    d.precision, d.device = 1, 0
+    return d
+
+
+def _layer_desc(sets, num_rigids, is_rigid_element, is_elastic, is_boundary, is_rigid_vertex, vertex_body,
+                layersMap, iterations, keep):
+    arrs = [np.asfortranarray(sets, np.int32), np.ascontiguousarray(num_rigids, np.int32),
+            np.asfortranarray(is_rigid_element, np.uint8), np.asfortranarray(is_elastic, np.uint8),
+            np.asfortranarray(is_boundary, np.uint8), np.asfortranarray(is_rigid_vertex, np.uint8),
+            np.asfortranarray(vertex_body, np.int32), np.ascontiguousarray(layersMap, np.int32),
+            np.ascontiguousarray(iterations, np.int32)]
+    keep.extend(arrs)
+    s_, nr, rig, ela, bnd, rv, vb, lm, it = arrs
+    d = LayerDesc()
+    d.num_layers, d.num_columns = lm.size, s_.shape[1]
+    d.layers_map, d.iterations = i32(lm), i32(it)
+    d.is_elastic_element, d.is_rigid_element = u8(ela), u8(rig)
+    d.rigid_body_sets, d.vertex_rigid_body = i32(s_), i32(vb)
+    d.is_boundary_vertex, d.is_rigid_vertex = u8(bnd), u8(rv)
+    d.num_rigids = i32(nr)
+    return d
+
+
+def _contacts(c, keep):
+    out = Contacts()
+    K = int(c.vertex_ids.size)
+    out.num_contacts = K
+    if K:
+        arrs = [np.asfortranarray(c.normals.reshape(K, 3), float), np.asfortranarray(c.points.reshape(K, 3), float),
+                np.ascontiguousarray(c.vertex_ids, np.int32), np.ascontiguousarray(c.compliance, float)]
+        keep.extend(arrs)
+        out.normals, out.point_colliders, out.vertex_ids, out.compliance = (f64(arrs[0]), f64(arrs[1]),
+                                                                              i32(arrs[2]), f64(arrs[3]))
+    return out
+
+
+def params(integ, h):
+    """mlx_solve_params from an integrator's properties (xpbdLayer3D.m:5-40)."""
+    P = SolveParams()
+    P.h = h
+    P.boundary_compliance = integ.boundaryCompliance
+    P.contact_resistance = integ.contactResistance
+    P.run_until = integ.runUntilResSmallerThan
+    P.give_up_threshold = integ.giveUpThreshold
+    P.gravity_compliance = integ.gravityCompliance
+    P.gravity = integ.Gravity
+    P.stop_at_improvement_percent = integ.StopAtImprovementPercent
+    P.compute_residuals = int(bool(integ.computeResiduals))
+    P.hanging_stop = int(integ.hangingStop)
+    P.give_up_enabled = int(bool(integ.giveUpEnabled))
+    P.last_layer_give_up_enabled = int(bool(integ.LastLayerGiveUpEnabled))
+    P.use_gravity_constraints = int(bool(integ.useGravityConstraints))
+    P.use_rigid_contacts = int(bool(integ.useRigidContacts))
+    P.contact_coloring = int(bool(getattr(integ, "contactColoring", False)))
+    return P
 
 
 def f64(a):
@@ -176,33 +326,62 @@ def find_contacts_platform(p, rotation, scale, center, compliance=1e-4):
 
 def find_contacts(finders, p):
     """simulate3D's finder loop (3d/simulate3D.m:156-171) on the oracle's
-    finders: the lists concatenated in finder order."""
-    from multilayersolver2024_b200 import _lib
-    from multilayersolver2024_b200.xpbd_layer3d import ContactSet
-    sets = []
+    finders: the lists concatenated in finder order.  A finder is given by
+    its kind (the MLX_OBSTACLE_* numbers of include/mlxpbd.h) and data."""
+    lists = []
     for f in finders:
-        if f.kind == _lib.MLX_OBSTACLE_PLANE:
-            r = find_contacts_plane(p, f.normal, f.center, f.compliance)
-        elif f.kind == _lib.MLX_OBSTACLE_SPHERE:
+        if f.kind == OBSTACLE_SPHERE:
             r = find_contacts_sphere(p, f.radius, f.center)
-        else:
+        elif f.kind == OBSTACLE_BOX:
             r = find_contacts_platform(p, f.rotation, f.scale, f.center, f.compliance)
-        sets.append(ContactSet(*r))
-    return ContactSet.concat(sets)
+        elif f.kind == OBSTACLE_PLANE:
+            r = find_contacts_plane(p, f.normal, f.center, f.compliance)
+        else:
+            raise ValueError(f"unknown finder kind {f.kind}")
+        lists.append(ContactList(*r))
+    return ContactList.concat(lists)
 
 
-def layer_solve(mesh, ls, layersMap, iterations, params, contacts, xi, lambdai, oldp, oldOldp, f, resv, pinnedx,
+def layer_solve(mesh, ls, layersMap, iterations, P, contacts, xi, lambdai, oldp, oldOldp, f, resv, pinnedx,
                 residual_in, sum_non_monitored_time=0.0, material="blocks", want_lambda=False):
-    """orc_layer_solve with the same marshalling as the product call."""
-    from multilayersolver2024_b200.xpbd_layer3d import call_layer_solve, mesh_desc, pack_layer_desc
+    """orc_layer_solve (xpbdLayer3D.layerSolve restated) on numpy arrays.  `ls`
+    carries the layer masks (rigidBodySetsPerLayer, numRigids,
+    isRigidElement, isElasticElement, isBoundaryVertex, isRigidVertex,
+    vertexRigidBody), `P` is a SolveParams, `contacts` a ContactList.
+    Returns (xi, sumNonMonitoredTime, residualArray, runUntil, lambdai or
+    None, total_iterations)."""
     lib = load()
-    md, keep = mesh_desc(mesh, 1, 0, material)
-    ld, keep2 = pack_layer_desc(ls, layersMap, iterations)
-    rc, res = call_layer_solve(lib.orc_layer_solve, C.byref(md), ld, params, contacts, xi, lambdai, oldp,
-                               oldOldp, f, resv, pinnedx, residual_in, sum_non_monitored_time, want_lambda)
+    keep = []
+    md = _mesh_desc(mesh, material, keep)
+    ld = _layer_desc(ls.rigidBodySetsPerLayer, ls.numRigids, ls.isRigidElement, ls.isElasticElement,
+                     ls.isBoundaryVertex, ls.isRigidVertex, ls.vertexRigidBody, layersMap, iterations, keep)
+    ct = _contacts(contacts, keep)
+    arr = lambda a: keep.append(np.ascontiguousarray(a, np.float64)) or keep[-1]
+    xi_, oldp_, oo_, f_, rv_ = arr(xi), arr(oldp), arr(oldOldp), arr(f), arr(resv)
+    px_ = arr(pinnedx if pinnedx is not None else np.zeros(0))
+    rin = arr(residual_in)
+    lam_ = None if lambdai is None else np.asfortranarray(lambdai, np.float64)
+    inp = SolveInputs()
+    inp.xi, inp.lambdai, inp.oldp, inp.old_oldp, inp.f = f64(xi_), f64(lam_), f64(oldp_), f64(oo_), f64(f_)
+    inp.residualv, inp.pinnedx, inp.residual_in = f64(rv_), f64(px_), f64(rin)
+    inp.residual_in_len = rin.size
+    inp.sum_non_monitored_time = sum_non_monitored_time
+    if not P.compute_residuals:
+        cap = rin.size + 1
+    else:
+        cap = rin.size + 1 + max(0, P.hanging_stop) + int(np.sum(iterations)) + 100000
+    out_xi = np.empty(xi_.size)
+    if want_lambda and lam_ is None:
+        raise ValueError("want_lambda needs lambdai")
+    out_lam = np.zeros(lam_.shape, order="F") if want_lambda else None
+    out_res = np.zeros(cap)
+    out = SolveOutputs()
+    out.xi, out.lambdai, out.residual, out.residual_capacity = f64(out_xi), f64(out_lam), f64(out_res), cap
+    rc = lib.orc_layer_solve(C.byref(md), C.byref(ld), C.byref(P), C.byref(ct), C.byref(inp), C.byref(out))
     if rc != 0:
         raise RuntimeError(f"orc_layer_solve failed ({rc}): {lib.orc_last_error().decode()}")
-    return res
+    return (out_xi, out.sum_non_monitored_time, out_res[:out.residual_len].copy(), out.run_until, out_lam,
+            out.total_iterations)
 
 
 def contact_velocity_update(normals, vids, v, h, gravity, e):
@@ -220,7 +399,6 @@ def integrate(integ, mesh, h, contacts, cache, frame, material="blocks"):
     on the oracle's functions.  ``integ`` provides the integrator properties,
     ``cache`` has oldp/oldOldp; ``mesh.p``/``mesh.v`` are advanced in place.
     Returns the residual array and total iterations."""
-    from multilayersolver2024_b200.xpbd_layer3d import LayerSet, make_params, pack_contacts
     if cache.oldp is None or np.any(np.isnan(cache.oldp)) or frame == 1:
         cache.oldp = mesh.p.copy()
         integ.pinnedx = mesh.p[mesh.pinnedDOFs - 1].copy()
@@ -238,7 +416,11 @@ def integrate(integ, mesh, h, contacts, cache, frame, material="blocks"):
         forced[mesh.pinnedTets - 1] = 1
         sets, nr = union_find_layers(order, integ.sortedLayers, forced, mesh.t, N)
     bnd, ela, rig, vb = find_boundary_vertices(mesh.t, N, sets)
-    ls = LayerSet(sets, nr, np.asfortranarray((sets != 0).astype(np.uint8)), ela, bnd, rig, vb)
+
+    class _Layers:  # buildLayers + findBoundaryVertices output (xpbdLayer3D.m:646-652)
+        rigidBodySetsPerLayer, numRigids = sets, nr
+        isRigidElement = np.asfortranarray((sets != 0).astype(np.uint8))
+        isElasticElement, isBoundaryVertex, isRigidVertex, vertexRigidBody = ela, bnd, rig, vb
     cache.oldOldp = cache.oldp
     cache.oldp = mesh.p.copy()
     xi = mesh.p.copy()
@@ -247,9 +429,9 @@ def integrate(integ, mesh, h, contacts, cache, frame, material="blocks"):
     resv[up] += h * f[up] / mesh.mass[up]
     resv = (1 - integ.airDrag) * resv
     lam = np.zeros((T, 6), order="F")
-    cts, keep = pack_contacts(contacts.normals, contacts.points, contacts.vertex_ids, contacts.compliance)
-    xi, snm, resArr, runUntil, _, iters = layer_solve(mesh, ls, integ.layersMap, integ.iterations,
-                                                      make_params(integ, h), cts, xi, lam, cache.oldp,
+    cl = ContactList(contacts.normals, contacts.points, contacts.vertex_ids, contacts.compliance)
+    xi, snm, resArr, runUntil, _, iters = layer_solve(mesh, _Layers, integ.layersMap, integ.iterations,
+                                                      params(integ, h), cl, xi, lam, cache.oldp,
                                                       cache.oldOldp, f, resv, integ.pinnedx, np.array([0.0]),
                                                       0.0, material)
     integ.runUntilResSmallerThan = runUntil

@@ -80,15 +80,14 @@ class Case:
         _lib.check("mlx_layer_solve", rc, lib)
         return res
 
-    def oracle(self, material="blocks"):
+    def oracle(self, material="blocks", want_lambda=True):
+        """The same call on the CPU oracle, marshalled by the oracle's own code."""
         from oracle import oracle as O
-        import ctypes as C
-        from multilayersolver2024_b200.xpbd_layer3d import mesh_desc
-        lib = O.load()
-        md, keep = mesh_desc(self.mesh, 1, 0, material)
-        rc, res = self.run(lib.orc_layer_solve, C.byref(md))
-        assert rc == 0, lib.orc_last_error()
-        return res
+        c = self.contacts
+        return O.layer_solve(self.mesh, self.ls, self.integ.layersMap, self.integ.iterations,
+                             O.params(self.integ, self.h), O.ContactList(c.normals, c.points, c.vertex_ids, c.compliance),
+                             self.xi, self.lam, self.oldp, self.oldOldp, self.f, self.resv, self.pinnedx,
+                             np.array([0.0]), 0.0, material, want_lambda)
 
 
 def rel_pos_err(a, b, mesh):
