@@ -57,7 +57,8 @@ WORKLOADS = {
         "dt=1/60, base pinned, seeded surface impulse at t=0"),
     4: ("config4: contact-heavy drop, 32 StVK boxes of 12^3 cubes (70304 vertices, 331776 tets), E=5e5, nu=0.3, "
         "seeded rotations and heights 0.5-3 m over a ground plane + 4 analytic spheres (r 0.3-0.6 m), contacts "
-        "detected on the device every step, 3 layers (4^3-cube clusters 1 it, 2^3-cube clusters 4 it, fine 10 it), "
+        "detected on the device every step and coloured together with the elastic constraints, 3 layers "
+        "(4^3-cube clusters 1 it, 2^3-cube clusters 4 it, fine 10 it), "
         "contact resistance 0.9, dt=1/120; timed after the boxes have landed"),
 }
 WORKLOAD = WORKLOADS[5]
@@ -184,7 +185,11 @@ def start_velocity(scene, m):
         m.v[scene.impulse[0] - 1] += scene.impulse[1]
 
 
-def make_integrator(scene, precision, residual=False, cap=15000):
+def make_integrator(scene, precision, residual=False, cap=15000, host_contacts=False):
+    """The scene's integrator settings.  `host_contacts`: the step takes a
+    host contact list (mlx_layer_solve), which keeps the reference's contact
+    order (contacts coloured with the elastic constraints need the contacts
+    detected on the device)."""
     from multilayersolver2024_b200 import XpbdLayer3D
     integ = XpbdLayer3D()
     integ.Gravity = scene.gravity
@@ -193,6 +198,7 @@ def make_integrator(scene, precision, residual=False, cap=15000):
     integ.customRigidSets = scene.custom_sets
     integ.precision = precision
     integ.contactResistance = scene.settings.get("contactResistance", integ.contactResistance)
+    integ.contactColoring = bool(scene.settings.get("contactColoring", False)) and not host_contacts
     if residual:
         integ.computeResiduals = True
         integ.runUntilResSmallerThan = RUN_UNTIL
@@ -352,6 +358,23 @@ def run_ours(args, rank, world, local):
     solver_launch_path = solver.launch_path
     solver.close()
     state0 = _PHASE.get("state")
+    reference_order = None
+    if sc.settings.get("contactColoring"):
+        # the same steps with the reference's contact order (contacts after
+        # the colours, Jacobi), for the cost of colouring the contacts
+        sc.settings["contactColoring"] = False
+        solver_r, sim_r = stepper(MLX_FP32, False, state0)
+        for _ in range(args.warmup):
+            sim_r.step(1, graph=True)
+        ref_ms = 0.0
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ref_ms += sim_r.step(1, graph=True, timed=True)
+        solver_r.close()
+        sc.settings["contactColoring"] = True
+        reference_order = {"steps_per_s": args.steps / (ref_ms / 1000.0),
+                           "note": "fixed iterations, contacts after the colours (xpbdLayer3D.m:330, 422-485)"}
 
     # ---- to residual 1e-4: the plain solve, the learned warm start and the
     # FP64 plain solve of the same steps ----
@@ -466,7 +489,7 @@ def run_ours(args, rank, world, local):
     # ---- e2e: public host API, host buffers, every step copies in and out ----
     sc2 = make_scene()
     m2 = sc2.mesh
-    integ2 = make_integrator(sc2, MLX_FP32, residual_metric, args.residual_cap)
+    integ2 = make_integrator(sc2, MLX_FP32, residual_metric, args.residual_cap, host_contacts=True)
     cache = StepCache()
     start_velocity(sc2, m2)
     if advance:
@@ -609,7 +632,11 @@ def run_ours(args, rank, world, local):
             "to_residual": to_res,
             "parity": parity if residual_metric else None,
             "fixed_iterations": {"steps_per_s": fixed_value, "ms_per_step": fixed_max_ms / args.steps,
-                                 "iterations_per_step": int(sum(sc.iterations))},
+                                 "iterations_per_step": int(sum(sc.iterations)),
+                                 "contacts": ("coloured with the elastic constraints" if sc.settings.get("contactColoring")
+                                              else ("after the colours (reference order)" if sc.contact_finders
+                                                    else None)),
+                                 "reference_contact_order": reference_order},
             "roofline": {"bound": "hbm", "kernel": sweep_kernel, "measured_on": "fixed_iterations leg",
                          "launch_path": solver_launch_path,
                          "achieved": achieved, "peak": peak, "unit": "GB/s",

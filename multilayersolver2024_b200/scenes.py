@@ -280,7 +280,7 @@ def config3(seed: int = 3, n_scenes: int = 256, tmin=2000, tmax=40000, cluster=4
 
 
 def config4(seed: int = 4, n_boxes: int = 32, cubes: int = 12, grid=(8, 4), spacing=2.0, n_spheres: int = 4,
-            coarse: int = 4, mid: int = 2, drop=(0.5, 3.0)) -> Scene:
+            coarse: int = 4, mid: int = 2, drop=(0.5, 3.0), contact_coloring: bool = True) -> Scene:
     """Contact-heavy drop: `n_boxes` StVK boxes of cubes^3 cubes (0.1 m, 6 tets
     per cube; 32 x 10,368 tets by default), E = 5e5 Pa, nu = 0.3, with seeded
     rotations, over a ground plane z = 0 and `n_spheres` analytic spheres
@@ -293,6 +293,10 @@ def config4(seed: int = 4, n_boxes: int = 32, cubes: int = 12, grid=(8, 4), spac
     resistance 0.9 (3d/examples/XPBD/cubeDrop_xpbd.m:27-35) and the finders'
     default contact compliance 1e-4; dt = 1/120, 500 steps.  Boxes sit on a
     grid `spacing` m apart, so they meet the obstacles and not each other.
+    Contacts are coloured together with the elastic constraints (the
+    configuration's definition: each vertex's contacts join the first colour
+    phase whose tets do not touch it); contact_coloring=False keeps the
+    reference's order (contacts after all colours, Jacobi, xpbdLayer3D.m:330).
     Returns the merged mesh; `contact_finders` holds the obstacles."""
     from .contacts import PlaneContactFinder3D, SphereContactFinder, rotation_matrix_degrees
     rng = np.random.default_rng(seed)
@@ -332,4 +336,5 @@ def config4(seed: int = 4, n_boxes: int = 32, cubes: int = 12, grid=(8, 4), spac
                gravity=-9.81, custom_sets=custom, contact_finders=finders)
     sc.settings["parts"] = meshes
     sc.settings["contactResistance"] = 0.9
+    sc.settings["contactColoring"] = bool(contact_coloring)
     return sc

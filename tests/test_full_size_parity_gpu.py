@@ -7,8 +7,10 @@ at full size (max position difference / bounding-box diagonal, worst step):
     (and projectGS iterations within 10 % of the oracle's)
   config 3 (all 256 scenes, 3.35 M tets, 2 layers), 2 steps:      <= 1e-4
   config 4 (32 StVK boxes, 331,776 tets, 3 layers, plane + 4
-    spheres, contacts detected every step), 3 steps from the
-    landed state after 150 steps:                                 <= 1e-4
+    spheres, contacts detected every step and coloured with the
+    elastic constraints; the oracle in the same order), 3 steps
+    from the landed state after 150 steps:                        <= 1e-4
+  config 4 in the reference's contact order, the same steps:      <= 1e-4
   config 5 (393,216 NH tets, 3 layers), 3 steps from t = 0:        <= 1e-4
 
 The oracle runs with every host thread; each case starts both sides from the
@@ -34,6 +36,7 @@ def _integ(scene, precision, residual=False):
     integ.customRigidSets = scene.custom_sets
     integ.precision = precision
     integ.contactResistance = scene.settings.get("contactResistance", integ.contactResistance)
+    integ.contactColoring = bool(scene.settings.get("contactColoring", False))
     if residual:
         integ.computeResiduals = True
         integ.runUntilResSmallerThan = 1e-4
@@ -126,10 +129,12 @@ def test_config3_full_size(gpu, oracle):
     assert worst <= 1e-4
 
 
-def test_config4_full_size_landed(gpu, oracle):
-    (got, _), start = _gpu(scenes.config4(), 3, advance=150)
-    ref, _ = _oracle(scenes.config4(), 3, oracle, state=start)
-    assert _err(scenes.config4(), got, ref, "config4 landed, 3 steps") <= 1e-4
+@pytest.mark.parametrize("coloring", [True, False])
+def test_config4_full_size_landed(gpu, oracle, coloring):
+    (got, _), start = _gpu(scenes.config4(contact_coloring=coloring), 3, advance=150)
+    ref, _ = _oracle(scenes.config4(contact_coloring=coloring), 3, oracle, state=start)
+    name = "config4 landed, 3 steps, contacts " + ("coloured" if coloring else "after the colours")
+    assert _err(scenes.config4(), got, ref, name) <= 1e-4
 
 
 def test_config5_full_size(gpu, oracle):
