@@ -311,6 +311,21 @@ int mlx_sim_contact_count(mlx_solver* solver, int32_t* num_contact_vertices);
  * description. */
 int mlx_pcg_solve(mlx_solver* solver, double h, const double* b, int32_t iterations, double* x, double* resvec);
 
+/* The PCG in the layer solve.  No counterpart in the reference's layerSolve
+ * (its PCG, solvePCG.m, serves the non-XPBD quick solve).  With
+ * pcg_iterations > 0 the last layer of a Neo-Hookean mesh (no rigid bodies)
+ * takes Newton-PCG corrections: the XPBD projection linearised at the current
+ * positions, (M + J^T W J) dx = -J^T (W C + lambda) with W = alpha~^-1 on
+ * the free DOFs, solved by `pcg_iterations` iterations of solvePCG's method
+ * with the 3x3 block-Jacobi preconditioner; then x += dx and
+ * lambda = -W (C + J dx).  One correction comes before the layer's
+ * Gauss-Seidel and one after every `every` of its iterations (0: only the
+ * first).  The stop rules are unchanged.  Applies to mlx_layer_solve and
+ * the resident stepper (also inside its captured step, as a conditional
+ * node); pcg_iterations = 0 (the default) restores the reference's
+ * projectGS.  MLX_ERR_UNSUPPORTED for StVK meshes. */
+int mlx_layer_pcg(mlx_solver* solver, int32_t pcg_iterations, int32_t every);
+
 /* Diagnostic of the bounded device waits (no counterpart in the reference):
  * one thread runs the wait the library's kernels use -- kind 0: the grid
  * barrier of the persistent layer kernel, kind 1: the mbarrier wait of the

@@ -158,6 +158,7 @@ SIGNATURES = {
                            C.c_int),
     "mlx_sim_warm_start_fetch": ([C.c_void_p, _f32p, _f32p, C.c_int32, _i32p, _i32p], C.c_int),
     "mlx_sim_multiplier_warm_start": ([C.c_void_p, C.c_int32, C.c_double, C.c_double], C.c_int),
+    "mlx_layer_pcg": ([C.c_void_p, C.c_int32, C.c_int32], C.c_int),
     "mlx_pcg_solve": ([C.c_void_p, C.c_double, _f64p, C.c_int32, _f64p, _f64p], C.c_int),
     "mlx_wait_probe": ([C.c_int32, C.c_int32, C.c_int64, C.POINTER(C.c_int32)], C.c_int),
     "mlx_build_layers": ([C.c_void_p, _f64p, _f64p, C.c_double, C.c_int32, _i32p, _f64p, _f64p, C.c_int32, _u8p,

@@ -109,4 +109,11 @@ __global__ void k_mon_iter_end(MonState* ms, cudaGraphConditionalHandle loop, in
   mon_iter_end(ms, loop, iterations, is_last, mp);
 }
 
+// Start of projectGS iteration ms->it of the last layer: the Newton-PCG
+// correction (pcg.cuh) runs after every `every` iterations.
+__global__ void k_ns_gate(const MonState* ms, cudaGraphConditionalHandle run, int every) {
+  const long long it = ms->it;
+  cudaGraphSetConditional(run, (it > 1 && (it - 1) % every == 0) ? 1u : 0u);
+}
+
 }  // namespace mlx

@@ -168,7 +168,8 @@ struct PcgScalars {
 // Sums the partials (one block of 256) and updates the scalars:
 // mode 0: rTz = sum0 (set-up); mode 1: dAp = sum0, alpha = rTz / dAp
 // (0 when dAp == 0); mode 2: rTz_new = sum0, beta = rTz_new / rTz,
-// rTz = rTz_new; mode 3: res = sqrt(sum0).
+// rTz = rTz_new; mode 3: res = sqrt(sum0); mode 4: mode 2 with beta = 0
+// when the previous r'z is 0.
 __global__ void __launch_bounds__(256) k_pcg_scalars(const double* __restrict__ partials, int n, int mode,
                                                      PcgScalars* __restrict__ sc, double* __restrict__ resvec, int it) {
   double s[1] = {0.0};
@@ -183,6 +184,10 @@ __global__ void __launch_bounds__(256) k_pcg_scalars(const double* __restrict__ 
   } else if (mode == 2) {
     sc->rTz_new = s[0];
     sc->beta = s[0] / sc->rTz;
+    sc->rTz = s[0];
+  } else if (mode == 4) {  // mode 2 with beta = 0 once r'z is 0 (a converged or zero system)
+    sc->rTz_new = s[0];
+    sc->beta = sc->rTz == 0.0 ? 0.0 : s[0] / sc->rTz;
     sc->rTz = s[0];
   } else {
     sc->res = sqrt(s[0]);
@@ -228,6 +233,174 @@ __global__ void k_pcg_sub(int N, const double4* __restrict__ a, const double4* _
   if (v >= N) return;
   const double4 p = a[v], q = b[v];
   out[v] = make_double4(p.x - q.x, p.y - q.y, p.z - q.z, 0.0);
+}
+
+// ---------------------------------------------------------------------------
+// Newton-PCG correction of a Neo-Hookean layer (the PCG used in the layer
+// solve).  The XPBD projection of a layer solves, constraint by constraint,
+//     C(x) + alpha~ lambda = 0,   M (x - x_c) = J^T (lambda - lambda_c),
+// (x_c, lambda_c: the state the layer started from).  Linearised at the
+// current x with J = dC/dx and W = alpha~^-1 this is
+//     (M + J^T W J) dx = -J^T (W C + lambda),   lambda' = -W (C + J dx),
+// a symmetric positive definite system on the free DOFs, solved here by the
+// iteration of solvePCG (2d/tools/solver/solvePCG.m) with the 3x3
+// block-Jacobi preconditioner; x += dx and lambda = lambda' give a state that
+// keeps M dx = J^T (lambda' - lambda) to the PCG's residual.  The
+// Gauss-Seidel sweeps of projectGS then continue from it.  C = (C_D, C_H) is
+// the library's stable Neo-Hookean pair (tet_kernels.cuh nh_eval), W =
+// (h^2 vol mu, h^2 vol (lambda - mu)) from the stored compliances.
+//
+// Per tet (sorted order, structure of arrays): jac [24][T] = dC_D/dx of the
+// four corners (12) then dC_H/dx (12); w [2][T]; c [2][T]; q [2][T] = W C +
+// lambda (the right-hand side's factor); s [2][T] scratch.
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_ns_jacobian(TetData<R> td, const R4<R>* __restrict__ pos, double h2,
+                                                     R* __restrict__ jac, double* __restrict__ w,
+                                                     double* __restrict__ c, double* __restrict__ q) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int T = td.T;
+  if (s >= T) return;
+  int4 v;
+  R G[9], minv[4];
+  V3<R> X[4];
+  load_tet<R>(td, s, pos, v, G, X, minv);
+  const double cD = (double)td.mat[s], cH = (double)td.mat[(size_t)T + s];
+  NHEval<R> e;
+  nh_eval<R>(X, G, cD, cH, 0.0, e);
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    jac[(size_t)(3 * a + 0) * T + s] = e.gD[a].x;
+    jac[(size_t)(3 * a + 1) * T + s] = e.gD[a].y;
+    jac[(size_t)(3 * a + 2) * T + s] = e.gD[a].z;
+    jac[(size_t)(12 + 3 * a + 0) * T + s] = e.gH[a].x;
+    jac[(size_t)(12 + 3 * a + 1) * T + s] = e.gH[a].y;
+    jac[(size_t)(12 + 3 * a + 2) * T + s] = e.gH[a].z;
+  }
+  const double wD = cD > 0.0 ? h2 / cD : 0.0, wH = e.hasH ? h2 / cH : 0.0;
+  w[s] = wD;
+  w[(size_t)T + s] = wH;
+  c[s] = e.CD;
+  c[(size_t)T + s] = e.CH;
+  q[s] = wD * e.CD + (double)td.lambda[s];
+  q[(size_t)T + s] = e.hasH ? wH * e.CH + (double)td.lambda[(size_t)T + s] : 0.0;
+}
+
+// s_t = W_t (J_t u) for every tet.
+template <typename R>
+__global__ void __launch_bounds__(256) k_ns_tet_apply(int T, const int4* __restrict__ vid, const R* __restrict__ jac,
+                                                      const double* __restrict__ w, const double4* __restrict__ u,
+                                                      double* __restrict__ out) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= T) return;
+  const int4 v = vid[s];
+  const int vv[4] = {v.x, v.y, v.z, v.w};
+  double d0 = 0.0, d1 = 0.0;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const double4 ua = u[vv[a]];
+    d0 += (double)jac[(size_t)(3 * a) * T + s] * ua.x + (double)jac[(size_t)(3 * a + 1) * T + s] * ua.y +
+          (double)jac[(size_t)(3 * a + 2) * T + s] * ua.z;
+    d1 += (double)jac[(size_t)(12 + 3 * a) * T + s] * ua.x + (double)jac[(size_t)(12 + 3 * a + 1) * T + s] * ua.y +
+          (double)jac[(size_t)(12 + 3 * a + 2) * T + s] * ua.z;
+  }
+  out[s] = w[s] * d0;
+  out[(size_t)T + s] = w[(size_t)T + s] * d1;
+}
+
+// y_v = (u ? m_v u_v : 0) + scale * sum over the vertex's (tet, corner) pairs
+// of J_{t,corner}^T f_t, in the CSR's fixed order; pinned components 0.
+template <typename R>
+__global__ void k_ns_vertex_apply(PcgOp op, int T, const R* __restrict__ jac, const double* __restrict__ f,
+                                  double scale, const double4* __restrict__ u, double4* __restrict__ y) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= op.N) return;
+  D3 acc = d3(0.0, 0.0, 0.0);
+  for (int k = op.vt_off[v]; k < op.vt_off[v + 1]; ++k) {
+    const int2 e = op.vt[k];
+    const size_t s = (size_t)e.x;
+    const double f0 = f[s], f1 = f[(size_t)T + s];
+    const int a = e.y;
+    acc = acc + d3(f0 * (double)jac[(size_t)(3 * a) * T + s] + f1 * (double)jac[(size_t)(12 + 3 * a) * T + s],
+                   f0 * (double)jac[(size_t)(3 * a + 1) * T + s] + f1 * (double)jac[(size_t)(12 + 3 * a + 1) * T + s],
+                   f0 * (double)jac[(size_t)(3 * a + 2) * T + s] + f1 * (double)jac[(size_t)(12 + 3 * a + 2) * T + s]);
+  }
+  acc = scale * acc;
+  if (u) {
+    const double m = op.vmass[v];
+    const double4 uv = u[v];
+    acc = acc + d3(m * uv.x, m * uv.y, m * uv.z);
+  }
+  const unsigned char pm = op.pin[v];
+  y[v] = make_double4((pm & 1) ? 0.0 : acc.x, (pm & 2) ? 0.0 : acc.y, (pm & 4) ? 0.0 : acc.z, 0.0);
+}
+
+// Inverse of the 3x3 diagonal block of M + J^T W J at every vertex (pinned
+// rows and columns replaced by the identity).
+template <typename R>
+__global__ void k_ns_block_jacobi(PcgOp op, int T, const R* __restrict__ jac, const double* __restrict__ w,
+                                  double* __restrict__ Pinv) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= op.N) return;
+  const double m = op.vmass[v];
+  double B[9] = {m, 0, 0, 0, m, 0, 0, 0, m};
+  for (int k = op.vt_off[v]; k < op.vt_off[v + 1]; ++k) {
+    const int2 e = op.vt[k];
+    const size_t s = (size_t)e.x;
+    const int a = e.y;
+    const double wD = w[s], wH = w[(size_t)T + s];
+    const double gD[3] = {(double)jac[(size_t)(3 * a) * T + s], (double)jac[(size_t)(3 * a + 1) * T + s],
+                          (double)jac[(size_t)(3 * a + 2) * T + s]};
+    const double gH[3] = {(double)jac[(size_t)(12 + 3 * a) * T + s], (double)jac[(size_t)(12 + 3 * a + 1) * T + s],
+                          (double)jac[(size_t)(12 + 3 * a + 2) * T + s]};
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+      for (int i = 0; i < 3; ++i) B[i + 3 * j] += wD * gD[i] * gD[j] + wH * gH[i] * gH[j];
+  }
+  const unsigned char pm = op.pin[v];
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    if (pm & (1 << d)) {
+      for (int k = 0; k < 3; ++k) B[d + 3 * k] = B[k + 3 * d] = 0.0;
+      B[d + 3 * d] = 1.0;
+    }
+  double inv[9];
+  inverse3(B, inv);
+  for (int i = 0; i < 9; ++i) Pinv[9 * (size_t)v + i] = inv[i];
+}
+
+// lambda = -W (C + J dx) for every tet (rows 0 and 1; an absent C_H keeps 0).
+template <typename R>
+__global__ void __launch_bounds__(256) k_ns_lambda(int T, const int4* __restrict__ vid, const R* __restrict__ jac,
+                                                   const double* __restrict__ w, const double* __restrict__ c,
+                                                   const double4* __restrict__ dx, R* __restrict__ lambda) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= T) return;
+  const int4 v = vid[s];
+  const int vv[4] = {v.x, v.y, v.z, v.w};
+  double d0 = 0.0, d1 = 0.0;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const double4 ua = dx[vv[a]];
+    d0 += (double)jac[(size_t)(3 * a) * T + s] * ua.x + (double)jac[(size_t)(3 * a + 1) * T + s] * ua.y +
+          (double)jac[(size_t)(3 * a + 2) * T + s] * ua.z;
+    d1 += (double)jac[(size_t)(12 + 3 * a) * T + s] * ua.x + (double)jac[(size_t)(12 + 3 * a + 1) * T + s] * ua.y +
+          (double)jac[(size_t)(12 + 3 * a + 2) * T + s] * ua.z;
+  }
+  const double wH = w[(size_t)T + s];
+  lambda[s] = (R)(-w[s] * (c[s] + d0));
+  lambda[(size_t)T + s] = wH > 0.0 ? (R)(-wH * (c[(size_t)T + s] + d1)) : R(0);
+}
+
+// x += dx on every vertex (dx is 0 on the pinned DOFs).
+template <typename R>
+__global__ void k_ns_move(int N, const double4* __restrict__ dx, R4<R>* __restrict__ pos) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= N) return;
+  const double4 d = dx[v];
+  R4<R> p = pos[v];
+  pos[v] = make_r4<R>((R)((double)p.x + d.x), (R)((double)p.y + d.y), (R)((double)p.z + d.z), p.w);
 }
 
 }  // namespace mlx

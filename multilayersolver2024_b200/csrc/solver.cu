@@ -317,6 +317,7 @@ struct Solver final : SolverBase {
     if (hg.exec) cudaGraphExecDestroy(hg.exec);
     if (cs_if) cudaStreamDestroy(cs_if);
     if (cs_while) cudaStreamDestroy(cs_while);
+    if (cs_ns) cudaStreamDestroy(cs_ns);
     if (stream) cudaStreamDestroy(stream);
   }
 
@@ -419,9 +420,19 @@ struct Solver final : SolverBase {
   // PCG on the linearly implicit system (pcg.cuh); host copies of the
   // material kept from create (sorted order), device data built on first use
   std::vector<double> pcg_G, pcg_vol, pcg_lame;
-  bool pcg_ready = false;
+  bool pcg_ready = false, vt_ready = false;
   DevBuf d_pcg_G, d_pcg_vol, d_pcg_lame, d_pcg_vt, d_pcg_pin, d_pcg_vec, d_pcg_P, d_pcg_part, d_pcg_sc, d_pcg_res;
   int pcg_setup();
+  int vt_setup();
+  PcgOp vt_op(double h2);
+  // Newton-PCG corrections of the last layer (pcg.cuh k_ns_*): PCG
+  // iterations per correction (0: off) and Gauss-Seidel iterations between
+  // corrections
+  int ns_iters = 0, ns_every = 0;
+  DevBuf d_ns_jac, d_ns_tet;
+  cudaStream_t cs_ns = nullptr;
+  int ns_configure(int pcg_iterations, int every) override;
+  int ns_correct(double h, long long* launches);
   int pcg_solve(double h, const double* b, int iterations, double* x, double* resvec) override;
   std::vector<double> sim_p0;  // positions given to mlx_sim_init (the rest configuration)
   int ws_configure(int record, int mode, mlx_mlp* net, double gate, const float* fmean, const float* fstd, const float* omean,
@@ -1624,7 +1635,7 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
     cudaStream_t outer;
     bool pdl;
     ~Guard() {
-      for (cudaStream_t b : {s->cs_while, s->cs_if}) {
+      for (cudaStream_t b : {s->cs_ns, s->cs_while, s->cs_if}) {
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
         if (b && cudaStreamIsCapturing(b, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
           cudaGraph_t g = nullptr;
@@ -1640,6 +1651,7 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
     // (same results; ~25 % less time per monitored iteration on config 2)
     if (!cs_if) CU(cudaStreamCreateWithFlags(&cs_if, cudaStreamNonBlocking));
     if (!cs_while) CU(cudaStreamCreateWithFlags(&cs_while, cudaStreamNonBlocking));
+    if (!cs_ns) CU(cudaStreamCreateWithFlags(&cs_ns, cudaStreamNonBlocking));
   }
   MonParams mp{P->stop_at_improvement_percent, P->give_up_threshold, P->give_up_enabled,
                P->last_layer_give_up_enabled, (long long)P->hanging_stop};
@@ -1795,6 +1807,10 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
       CHECK(mws_start());
       st.launches += C;
     }
+    // the PCG in the layer solve: a Newton-PCG correction before the last
+    // layer's Gauss-Seidel and every ns_every of its iterations
+    const bool nsLayer = isLast && ns_iters > 0 && mat_kind == MAT_NH && ls.nb == 0 && ls.n_rigid_elements == 0;
+    if (nsLayer) CHECK(ns_correct(h, &st.launches));
     const int* dlist = dint + ls.o_list;
     const bool bodyWork = (ls.nb > 0 && (L.any_boundary || (P->use_rigid_contacts && L.any_rigid_contact))) ||
                           L.n_ec_groups > 0 || dc.nobs > 0;
@@ -1862,6 +1878,22 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
     }
     long long it = 1;
     while (devmon || it <= ld->iterations[layer] || (!stopSolve && st.runUntil >= 0 && isLast)) {
+      if (nsLayer && ns_every > 0) {
+        if (devmon) {
+          // iteration ms->it of the WHILE body: a correction after every
+          // ns_every iterations, as a conditional node
+          cudaGraphConditionalHandle h_ns;
+          CHECK(cond_handle(&h_ns));
+          k_ns_gate<<<1, 1, 0, stream>>>(mon(), h_ns, ns_every);
+          CU(cudaGetLastError());
+          ++st.launches;
+          CHECK(cond_begin(h_ns, cudaGraphCondTypeIf, cs_ns));
+          CHECK(ns_correct(h, &st.launches));
+          CHECK(cond_end(cs_while));
+        } else if (it > 1 && (it - 1) % ns_every == 0) {
+          CHECK(ns_correct(h, &st.launches));
+        }
+      }
       ++it;
       if (it > kSafetyIterations) return set_error(MLX_ERR_LIMIT, "iteration safety limit reached");
       ++st.totalIterations;
@@ -3030,6 +3062,23 @@ template <typename R>
 int Solver<R>::pcg_setup() {
   if (pcg_ready) return MLX_OK;
   if (pcg_vol.empty()) return set_error(MLX_ERR_UNSUPPORTED, "the PCG system needs mu and lambda in the mesh description");
+  CHECK(vt_setup());
+  CHECK(d_pcg_G.ensure(sizeof(double) * pcg_G.size()));
+  CHECK(d_pcg_vol.ensure(sizeof(double) * T));
+  CHECK(d_pcg_lame.ensure(sizeof(double) * 2 * (size_t)T));
+  CU(cudaMemcpyAsync(d_pcg_G.p, pcg_G.data(), sizeof(double) * pcg_G.size(), cudaMemcpyHostToDevice, stream));
+  CU(cudaMemcpyAsync(d_pcg_vol.p, pcg_vol.data(), sizeof(double) * T, cudaMemcpyHostToDevice, stream));
+  CU(cudaMemcpyAsync(d_pcg_lame.p, pcg_lame.data(), sizeof(double) * 2 * (size_t)T, cudaMemcpyHostToDevice, stream));
+  CU(cudaStreamSynchronize(stream));
+  pcg_ready = true;
+  return MLX_OK;
+}
+
+// The vertex -> (tet, corner) CSR of the matrix-free operators (fixed order:
+// sorted tet id, then corner), the pinned-DOF mask and the PCG's vectors.
+template <typename R>
+int Solver<R>::vt_setup() {
+  if (vt_ready) return MLX_OK;
   std::vector<int> off(N + 1, 0);
   for (int sidx = 0; sidx < T; ++sidx) {
     const int4 q = vid_sorted[sidx];
@@ -3047,14 +3096,8 @@ int Solver<R>::pcg_setup() {
   }
   std::vector<unsigned char> pm(N, 0);
   for (int d : pinned) pm[d / 3] |= (unsigned char)(1u << (d % 3));
-  CHECK(d_pcg_G.ensure(sizeof(double) * pcg_G.size()));
-  CHECK(d_pcg_vol.ensure(sizeof(double) * T));
-  CHECK(d_pcg_lame.ensure(sizeof(double) * 2 * (size_t)T));
   CHECK(d_pcg_vt.ensure(sizeof(int) * (N + 1) + sizeof(int2) * vt.size()));
   CHECK(d_pcg_pin.ensure(N));
-  CU(cudaMemcpyAsync(d_pcg_G.p, pcg_G.data(), sizeof(double) * pcg_G.size(), cudaMemcpyHostToDevice, stream));
-  CU(cudaMemcpyAsync(d_pcg_vol.p, pcg_vol.data(), sizeof(double) * T, cudaMemcpyHostToDevice, stream));
-  CU(cudaMemcpyAsync(d_pcg_lame.p, pcg_lame.data(), sizeof(double) * 2 * (size_t)T, cudaMemcpyHostToDevice, stream));
   // CSR: vt pairs first (8-byte aligned), then the offsets
   CU(cudaMemcpyAsync(d_pcg_vt.p, vt.data(), sizeof(int2) * vt.size(), cudaMemcpyHostToDevice, stream));
   CU(cudaMemcpyAsync(static_cast<char*>(d_pcg_vt.p) + sizeof(int2) * vt.size(), off.data(), sizeof(int) * (N + 1),
@@ -3065,7 +3108,90 @@ int Solver<R>::pcg_setup() {
   CHECK(d_pcg_part.ensure(sizeof(double) * 2 * 296));
   CHECK(d_pcg_sc.ensure(sizeof(PcgScalars)));
   CU(cudaStreamSynchronize(stream));
-  pcg_ready = true;
+  vt_ready = true;
+  return MLX_OK;
+}
+
+template <typename R>
+PcgOp Solver<R>::vt_op(double h2) {
+  const size_t npairs = (d_pcg_vt.bytes - sizeof(int) * (N + 1)) / sizeof(int2);
+  PcgOp op;
+  op.N = N;
+  op.vt = d_pcg_vt.as<int2>();
+  op.vt_off = reinterpret_cast<const int*>(static_cast<const char*>(d_pcg_vt.p) + sizeof(int2) * npairs);
+  op.vid = d_vid.as<int4>();
+  op.G = d_pcg_G.as<double>();
+  op.vol = d_pcg_vol.as<double>();
+  op.lame = d_pcg_lame.as<double>();
+  op.vmass = d_vmass.as<double>();
+  op.pin = d_pcg_pin.as<unsigned char>();
+  op.h2 = h2;
+  return op;
+}
+
+// The PCG in the layer solve of a Neo-Hookean mesh: `pcg_iterations` PCG
+// iterations per Newton correction of the last layer (0 turns it off),
+// before its Gauss-Seidel and after every `every` of its iterations (0: only
+// before).  Set-up (buffers, the vertex CSR) happens here, outside any
+// capture; cached step graphs are dropped.
+template <typename R>
+int Solver<R>::ns_configure(int pcg_iterations, int every) {
+  if (pcg_iterations < 0 || every < 0) return set_error(MLX_ERR_ARGUMENT, "iterations and interval must be >= 0");
+  if (pcg_iterations > 0 && mat_kind != MAT_NH)
+    return set_error(MLX_ERR_UNSUPPORTED, "the layer PCG covers the Neo-Hookean constraint pair");
+  DeviceGuard g(device);
+  if (pcg_iterations > 0) {
+    CHECK(vt_setup());
+    CHECK(d_ns_jac.ensure(sizeof(R) * 24 * (size_t)T));
+    CHECK(d_ns_tet.ensure(sizeof(double) * 8 * (size_t)T));
+  }
+  ns_iters = pcg_iterations;
+  ns_every = every;
+  if (sim.graph) { cudaGraphExecDestroy(sim.graph); sim.graph = nullptr; }
+  drop_host_graph();
+  return MLX_OK;
+}
+
+// One Newton-PCG correction of the current positions and multipliers
+// (pcg.cuh): stream work only, so it can be captured.
+template <typename R>
+int Solver<R>::ns_correct(double h, long long* launches) {
+  const PcgOp op = vt_op(h * h);
+  const int nb = blocks_for(N, 256), tb = blocks_for(T, 256), nred = std::min(nb, 296);
+  R* jac = d_ns_jac.as<R>();
+  double* tw = d_ns_tet.as<double>();
+  double *w = tw, *c = tw + 2 * (size_t)T, *q = tw + 4 * (size_t)T, *sv = tw + 6 * (size_t)T;
+  double4* V = d_pcg_vec.as<double4>();
+  double4 *db = V, *dx = V + N, *dr = V + 2 * (size_t)N, *dz = V + 3 * (size_t)N, *dd = V + 4 * (size_t)N,
+          *dAp = V + 5 * (size_t)N;
+  double* P = d_pcg_P.as<double>();
+  double* part = d_pcg_part.as<double>();
+  PcgScalars* sc = d_pcg_sc.as<PcgScalars>();
+  const int4* vid = d_vid.as<int4>();
+  k_ns_jacobian<R><<<tb, 256, 0, stream>>>(tets(), pos(), h * h, jac, w, c, q);
+  k_ns_vertex_apply<R><<<nb, 256, 0, stream>>>(op, T, jac, q, -1.0, nullptr, db);  // b = -J^T (W C + lambda)
+  CU(cudaMemsetAsync(dx, 0, sizeof(double4) * N, stream));
+  CU(cudaMemcpyAsync(dr, db, sizeof(double4) * N, cudaMemcpyDeviceToDevice, stream));
+  k_ns_block_jacobi<R><<<nb, 256, 0, stream>>>(op, T, jac, w, P);
+  k_pcg_precond<<<nb, 256, 0, stream>>>(N, P, op.pin, dr, dz);
+  CU(cudaMemcpyAsync(dd, dz, sizeof(double4) * N, cudaMemcpyDeviceToDevice, stream));
+  k_pcg_dot2<<<nred, 256, 0, stream>>>(N, dr, dz, nullptr, nullptr, part);
+  k_pcg_scalars<<<1, 256, 0, stream>>>(part, nred, 0, sc, nullptr, 0);
+  for (int i = 0; i < ns_iters; ++i) {
+    k_ns_tet_apply<R><<<tb, 256, 0, stream>>>(T, vid, jac, w, dd, sv);
+    k_ns_vertex_apply<R><<<nb, 256, 0, stream>>>(op, T, jac, sv, 1.0, dd, dAp);  // Ap = A d
+    k_pcg_dot2<<<nred, 256, 0, stream>>>(N, dd, dAp, nullptr, nullptr, part);
+    k_pcg_scalars<<<1, 256, 0, stream>>>(part, nred, 1, sc, nullptr, 0);
+    k_pcg_step<<<nb, 256, 0, stream>>>(N, sc, dd, dAp, dx, dr);
+    k_pcg_precond<<<nb, 256, 0, stream>>>(N, P, op.pin, dr, dz);
+    k_pcg_dot2<<<nred, 256, 0, stream>>>(N, dr, dz, nullptr, nullptr, part);
+    k_pcg_scalars<<<1, 256, 0, stream>>>(part, nred, 4, sc, nullptr, 0);
+    k_pcg_direction<<<nb, 256, 0, stream>>>(N, sc, dz, dd);
+  }
+  k_ns_lambda<R><<<tb, 256, 0, stream>>>(T, vid, jac, w, c, dx, d_lambda.as<R>());
+  k_ns_move<R><<<nb, 256, 0, stream>>>(N, dx, pos());
+  CU(cudaGetLastError());
+  if (launches) *launches += 7 + 9LL * ns_iters;
   return MLX_OK;
 }
 
@@ -3078,18 +3204,7 @@ int Solver<R>::pcg_solve(double h, const double* b, int iterations, double* x, d
   if (iterations < 0 || !(h > 0)) return set_error(MLX_ERR_ARGUMENT, "need iterations >= 0 and h > 0");
   DeviceGuard g(device);
   CHECK(pcg_setup());
-  const size_t npairs = (d_pcg_vt.bytes - sizeof(int) * (N + 1)) / sizeof(int2);
-  PcgOp op;
-  op.N = N;
-  op.vt = d_pcg_vt.as<int2>();
-  op.vt_off = reinterpret_cast<const int*>(static_cast<const char*>(d_pcg_vt.p) + sizeof(int2) * npairs);
-  op.vid = d_vid.as<int4>();
-  op.G = d_pcg_G.as<double>();
-  op.vol = d_pcg_vol.as<double>();
-  op.lame = d_pcg_lame.as<double>();
-  op.vmass = d_vmass.as<double>();
-  op.pin = d_pcg_pin.as<unsigned char>();
-  op.h2 = h * h;
+  const PcgOp op = vt_op(h * h);
   double4* V = d_pcg_vec.as<double4>();
   double4 *db = V, *dx = V + N, *dr = V + 2 * (size_t)N, *dz = V + 3 * (size_t)N, *dd = V + 4 * (size_t)N,
           *dAp = V + 5 * (size_t)N, *dtmp = V + 6 * (size_t)N;
@@ -3611,6 +3726,12 @@ int mlx_sim_warm_start(mlx_solver* s, int32_t record, int32_t mode, mlx_mlp* net
     if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
     return s->impl->ws_configure(record, mode, net, fallback_residual, feature_mean, feature_std, output_mean,
                                  output_std, corrections, num_clusters);
+  });
+}
+int mlx_layer_pcg(mlx_solver* s, int32_t pcg_iterations, int32_t every) {
+  return mlx::guarded([&]() -> int {
+    if (!s) return set_error(MLX_ERR_ARGUMENT, "null solver");
+    return s->impl->ns_configure(pcg_iterations, every);
   });
 }
 int mlx_sim_multiplier_warm_start(mlx_solver* s, int32_t on, double scale, double extrapolation) {

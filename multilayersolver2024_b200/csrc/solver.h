@@ -57,6 +57,7 @@ struct SolverBase {
                            const float* omean, const float* ostd, const float* corrections, int32_t* nb) = 0;
   virtual int ws_fetch(float* features, float* targets, int cap, int32_t* nb, int32_t* fallbacks) = 0;
   virtual int mws_configure(int on, double a, double b) = 0;
+  virtual int ns_configure(int pcg_iterations, int every) = 0;
   virtual int pcg_solve(double h, const double* b, int iterations, double* x, double* resvec) = 0;
   virtual int build_layers(const double* p, const double* oldp, double h, int ordering, const int32_t* order,
                            const double* dminv, const double* sorted_layers, int L, const uint8_t* forced,

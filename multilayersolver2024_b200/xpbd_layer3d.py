@@ -154,6 +154,13 @@ class Solver:
         check("mlx_create", lib.mlx_create(C.byref(d), C.byref(h)), lib)
         self.handle = h
 
+    def layer_pcg(self, pcg_iterations=100, every=50):
+        """The PCG in the layer solve (``mlx_layer_pcg``): Newton-PCG
+        corrections of the last layer, ``pcg_iterations`` PCG iterations each,
+        before its Gauss-Seidel and after every ``every`` iterations;
+        pcg_iterations = 0 turns them off."""
+        check("mlx_layer_pcg", self._lib.mlx_layer_pcg(self.handle, int(pcg_iterations), int(every)), self._lib)
+
     @property
     def launch_path(self) -> str:
         """How fixed-iteration layers are launched (``mlx_launch_path``)."""

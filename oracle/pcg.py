@@ -82,3 +82,63 @@ def solve_pcg(iterations, A, b, x0, preconditioner):
         d = z + beta * d
         resvec[i] = np.linalg.norm(A @ x - b)
     return x, resvec
+
+
+def nh_linearized_step(mesh, x, h, lam_c, free):
+    """The XPBD layer step of a Neo-Hookean mesh linearised at x (test
+    infrastructure: the predictor experiment).  With J the Jacobian of the
+    per-tet constraints C = (C_D, C_H) = (sqrt(B), det F - 1) (the pair the
+    library projects), W = alpha~^-1 = diag(h^2 vol mu, h^2 vol (lambda - mu))
+    and lam_c (2T) the multipliers the layer starts from, the linear system
+        [M  -J^T] [dx]   [0            ]
+        [J  W^-1] [dl] = [-C - W^-1 lam_c]
+    reduces to (M + J^T W J) dx = -J^T (W C + lam_c) on the free DOFs, and the
+    multipliers become lam = -W (C + J dx).  Returns (A_free, b_free,
+    preconditioner, J, W, C): the system, its 3x3 block-Jacobi
+    preconditioner, and the pieces that give lam."""
+    t = np.asarray(mesh.t, np.int64) - 1
+    nt, N = t.shape[0], mesh.N
+    X = np.asarray(x, float).reshape(-1, 3)
+    Gm = np.asarray(mesh.DmInv, float).reshape(nt, 3, 3).transpose(0, 2, 1)  # Gm[e, r, c] = DmInv(r, c)
+    Ds = np.stack([X[t[:, k]] - X[t[:, 0]] for k in (1, 2, 3)], 2)
+    F = Ds @ Gm
+    f0, f1, f2 = F[:, :, 0], F[:, :, 1], F[:, :, 2]
+    cf = np.stack([np.cross(f1, f2), np.cross(f2, f0), np.cross(f0, f1)], 2)
+    Jd = np.einsum("ei,ei->e", f0, cf[:, :, 0])
+    B = (F ** 2).sum((1, 2)) + Jd * Jd - 4 * Jd
+    CD = np.sqrt(np.maximum(B, 0.0))
+    mu, lam = np.asarray(mesh.mu, float), np.asarray(mesh.lam, float)
+    hasH = lam > mu
+    CH = np.where(hasH, Jd - 1.0, 0.0)
+    dD = (F + (Jd - 2.0)[:, None, None] * cf) / np.where(CD > 1e-12, CD, np.inf)[:, None, None]
+    dH = cf * hasH[:, None, None]
+
+    def grad_x(dF):
+        g = np.einsum("erc,ekc->ekr", dF, Gm)
+        return np.concatenate([-g.sum(1, keepdims=True), g], 1)
+
+    rows, cols, vals = [], [], []
+    for q, g in enumerate((grad_x(dD), grad_x(dH))):
+        for k in range(4):
+            for d in range(3):
+                rows.append(2 * np.arange(nt) + q)
+                cols.append(3 * t[:, k] + d)
+                vals.append(g[:, k, d])
+    J = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(2 * nt, 3 * N))
+    vol = np.asarray(mesh.elV, float)
+    W = sp.diags(np.stack([h * h * vol * mu, np.where(hasH, h * h * vol * (lam - mu), 0.0)], 1).ravel())
+    C = np.stack([CD, CH], 1).ravel()
+    A = (sp.diags(np.asarray(mesh.mass, float)) + J.T @ W @ J).tocsr()[free][:, free].tocsr()
+    b = -(J.T @ (W @ C + np.asarray(lam_c, float)))[free]
+    # 3x3 block-Jacobi on the free DOFs of every vertex
+    blocks = {}
+    for k, dof in enumerate(free):
+        blocks.setdefault(int(dof) // 3, []).append(k)
+    P = sp.lil_matrix(A.shape)
+    for ks in blocks.values():
+        inv = np.linalg.inv(A[ks][:, ks].toarray())
+        for i, ki in enumerate(ks):
+            for j, kj in enumerate(ks):
+                P[ki, kj] = inv[i, j]
+    P = P.tocsr()
+    return A, b, (lambda r: P @ r), J, W, C
