@@ -443,16 +443,24 @@ def run_ours(args, rank, world, local):
                         "loss_first_last": [float(losses[0]), float(losses[-1])]}
         training["seconds_in_bench"] = time.perf_counter() - t0
 
+        # the PCG in the layer solve (Newton-PCG corrections of the last
+        # layer) covers the Neo-Hookean pair
+        use_pcg = m.energy_type == MLX_ENERGY_NEOHOOKEAN and args.layer_pcg > 0
+        full = "learned_pcg" if use_pcg else "learned"
+        plan = [("plain", MLX_FP32, False, False), ("learned", MLX_FP32, True, False)]
+        if use_pcg:
+            plan += [("layer_pcg", MLX_FP32, False, True), ("learned_pcg", MLX_FP32, True, True)]
+        plan.append(("plain_fp64", MLX_FP64, False, False))
         legs, states = {}, {}
-        for name, precision, warm in (("plain", MLX_FP32, False), ("learned", MLX_FP32, True),
-                                      ("plain_fp64", MLX_FP64, False)):
+        for name, precision, warm, pcg in plan:
             solver3, sim3 = stepper(precision, True, state0)
             if warm:
                 sim3.warm_start(record=False, mode=1, net=net, feature_norm=fn, output_norm=on,
                                 fallback_residual=args.fallback_residual)
+            if pcg:
+                solver3.layer_pcg(args.layer_pcg, args.layer_pcg_every)
             run_leg(sim3, args.warmup, timed=False)
-            legs[name] = run_leg(sim3, args.steps if name != "plain_fp64" else args.steps, timed=True,
-                                 record_clocks=(name == "learned"))
+            legs[name] = run_leg(sim3, args.steps, timed=True, record_clocks=(name == full))
             states[name] = sim3.state()[0]
             if name == "plain":
                 states["plain_state"] = sim3.state()[:2]
@@ -466,19 +474,29 @@ def run_ours(args, rank, world, local):
             sim3.step(1, graph=True)
             one[name] = sim3.state()[0]
             solver3.close()
-        pl, le = legs["plain"], legs["learned"]
-        it_pl, it_le = sum(pl["iterations_per_step"]), sum(le["iterations_per_step"])
+        pl, le, fu = legs["plain"], legs["learned"], legs[full]
+        it_pl, it_fu = sum(pl["iterations_per_step"]), sum(fu["iterations_per_step"])
         to_res = {"run_until": RUN_UNTIL, "hanging_stop": args.residual_cap, "untimed_steps_before": args.warmup,
-                  "steps": args.steps, "plain": pl, "learned_warm_start": {**le, "training": training,
-                                                                            "fallback_residual_m": args.fallback_residual},
+                  "steps": args.steps, "value_leg": full, "plain": pl,
+                  "learned_warm_start": {**le, "training": training, "fallback_residual_m": args.fallback_residual},
                   "plain_fp64": {k: legs["plain_fp64"][k] for k in ("iterations_per_step", "steps_per_s",
                                                                       "final_residual")},
-                  "learned_over_plain_steps_per_s": le["steps_per_s"] / pl["steps_per_s"],
-                  "plain_over_learned_iterations": it_pl / max(it_le, 1),
+                  "value_over_plain_steps_per_s": fu["steps_per_s"] / pl["steps_per_s"],
+                  "plain_over_value_iterations": it_pl / max(it_fu, 1),
+                  "ablation_steps_per_s": {k: legs[k]["steps_per_s"] for k in legs},
                   "monitor": "device (layers as conditional IF nodes, projectGS as conditional WHILE nodes)"}
+        if use_pcg:
+            to_res["layer_pcg"] = {**legs["layer_pcg"], "pcg_iterations": args.layer_pcg,
+                                   "gs_iterations_between": args.layer_pcg_every}
+            to_res["learned_pcg"] = {**legs["learned_pcg"], "pcg_iterations": args.layer_pcg,
+                                     "gs_iterations_between": args.layer_pcg_every}
         parity = {"reference": "FP64 plain solve of the same steps on the GPU (the FP64 path matches the CPU "
                                "oracle to 1e-9)",
-                  "max_rel_pos_err": float(np.abs(states["learned"] - states["plain_fp64"]).max() / diag),
+                  "max_rel_pos_err": float(np.abs(states[full] - states["plain_fp64"]).max() / diag),
+                  "max_rel_pos_err_of": full,
+                  "max_rel_pos_err_learned": float(np.abs(states["learned"] - states["plain_fp64"]).max() / diag),
+                  "max_rel_pos_err_layer_pcg": (float(np.abs(states["layer_pcg"] - states["plain_fp64"]).max() / diag)
+                                                if use_pcg else None),
                   "max_rel_pos_err_plain_fp32": float(np.abs(states["plain"] - states["plain_fp64"]).max() / diag),
                   "learned_vs_plain_fp32": float(np.abs(states["learned"] - states["plain"]).max() / diag),
                   "after_steps": args.warmup + args.steps,
@@ -506,7 +524,10 @@ def run_ours(args, rank, world, local):
             integ2.runUntilResSmallerThan = RUN_UNTIL
         integ2.integrate(m2, sc2.h, cs, cache, frame)
 
-    e2e_steps = 0 if args.no_e2e else max(3, min(args.steps, {2: 20, 3: 3, 5: 3}.get(CONFIG, 10)))
+    e2e_pcg = residual_metric and m2.energy_type == MLX_ENERGY_NEOHOOKEAN and args.layer_pcg > 0
+    if e2e_pcg:
+        integ2.solver(m2).layer_pcg(args.layer_pcg, args.layer_pcg_every)
+    e2e_steps = 0 if args.no_e2e else max(3, min(args.steps, {2: 20, 3: 3, 5: 5}.get(CONFIG, 10)))
     for frame in range(1, 3 if e2e_steps else 1):  # warm-up: solver creation and layer caches
         e2e_step(frame)
     barrier()
@@ -604,10 +625,15 @@ def run_ours(args, rank, world, local):
                                  "over the tets of a colour" + (", from the same landed state, oracle contact "
                                                                  "finders every step)" if advance else ")")}
         if residual_metric:
-            value = to_res["learned_warm_start"]["steps_per_s"] * world
+            fleg = to_res[to_res["value_leg"]] if to_res["value_leg"] != "learned" else to_res["learned_warm_start"]
+            value = fleg["steps_per_s"] * world
             ms_per_step = 1000.0 * world / value
-            solver_desc = "learned warm start (coarse-cluster corrections, BF16 perceptron on tcgen05) to residual 1e-4"
-            iters_le = to_res["learned_warm_start"]["iterations_per_step"]
+            solver_desc = ("learned warm start (coarse-cluster corrections, BF16 perceptron on tcgen05)"
+                           + (f" with the PCG in the layer solve (Newton-PCG corrections of the fine layer, "
+                              f"{args.layer_pcg} PCG iterations after every {args.layer_pcg_every} Gauss-Seidel "
+                              f"iterations)" if to_res["value_leg"] == "learned_pcg" else "")
+                           + " to residual 1e-4")
+            iters_le = fleg["iterations_per_step"]
             per_iter = fixed_launches / max(sum(sc.iterations), 1)
             launches = int(sum(it * (per_iter + 2) for it in iters_le))
             launch_note = ("estimate: iterations of the timed steps x (launches per fixed-count iteration + the "
@@ -653,8 +679,10 @@ def run_ours(args, rank, world, local):
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "api": "XpbdLayer3D.integrate -> mlx_layer_solve"
                     + (" (+ mlx_find_contacts on the step-start positions)" if sc.contact_finders else "")
-                    + (", plain solve to residual 1e-4 with the stop rules on the host (the learned warm start is an "
-                       "option of the device-resident stepper only)" if residual_metric else "")},
+                    + ((", to residual 1e-4 with the stop rules on the host and the PCG in the layer solve "
+                        "(mlx_layer_pcg; the learned warm start is an option of the device-resident stepper only)")
+                       if e2e_pcg else (", plain solve to residual 1e-4 with the stop rules on the host"
+                                        if residual_metric else ""))},
             "layer_builder": layer_builder,
             "gpu_launches": launches, "gpu_launches_note": launch_note,
             "clocks": clocks.summary(),
@@ -707,6 +735,11 @@ def main():
     ap.add_argument("--fallback-residual", type=float, default=1e-3,
                     help="learned warm start: clusters with a predicted rigid-fit residual above this (m) keep the "
                     "plain start")
+    ap.add_argument("--layer-pcg", type=int, default=50,
+                    help="PCG iterations of each Newton-PCG correction of the fine layer (Neo-Hookean residual "
+                    "workloads; 0: none)")
+    ap.add_argument("--layer-pcg-every", type=int, default=50,
+                    help="Gauss-Seidel iterations between the Newton-PCG corrections")
     ap.add_argument("--train-in-bench", action="store_true",
                     help="config 5: train the network on recorded steps here instead of loading the shipped one")
     ap.add_argument("--advance", type=int, default=None,
