@@ -451,6 +451,9 @@ def run_ours(args, rank, world, local):
         if use_pcg:
             plan += [("layer_pcg", MLX_FP32, False, True), ("learned_pcg", MLX_FP32, True, True)]
         plan.append(("plain_fp64", MLX_FP64, False, False))
+        if args.legs:
+            # profiling runs: only the named legs (each leg's work is unchanged)
+            plan = [x for x in plan if x[0] in args.legs.split(",") or x[0] == full]
         legs, states = {}, {}
         for name, precision, warm, pcg in plan:
             solver3, sim3 = stepper(precision, True, state0)
@@ -469,38 +472,45 @@ def run_ours(args, rank, world, local):
         # one step from the same state (the plain FP32 leg's last): the
         # kernels' own error, apart from any divergence of the trajectories
         one = {}
-        for name, precision in (("plain", MLX_FP32), ("plain_fp64", MLX_FP64)):
-            solver3, sim3 = stepper(precision, True, states["plain_state"])
-            sim3.step(1, graph=True)
-            one[name] = sim3.state()[0]
-            solver3.close()
-        pl, le, fu = legs["plain"], legs["learned"], legs[full]
-        it_pl, it_fu = sum(pl["iterations_per_step"]), sum(fu["iterations_per_step"])
+        if "plain_state" in states and "plain_fp64" in legs:
+            for name, precision in (("plain", MLX_FP32), ("plain_fp64", MLX_FP64)):
+                solver3, sim3 = stepper(precision, True, states["plain_state"])
+                sim3.step(1, graph=True)
+                one[name] = sim3.state()[0]
+                solver3.close()
+        fu = legs[full]
+        pl = legs.get("plain")
         to_res = {"run_until": RUN_UNTIL, "hanging_stop": args.residual_cap, "untimed_steps_before": args.warmup,
                   "steps": args.steps, "value_leg": full, "plain": pl,
-                  "learned_warm_start": {**le, "training": training, "fallback_residual_m": args.fallback_residual},
-                  "plain_fp64": {k: legs["plain_fp64"][k] for k in ("iterations_per_step", "steps_per_s",
-                                                                      "final_residual")},
-                  "value_over_plain_steps_per_s": fu["steps_per_s"] / pl["steps_per_s"],
-                  "plain_over_value_iterations": it_pl / max(it_fu, 1),
+                  "learned_warm_start": ({**legs["learned"], "training": training,
+                                          "fallback_residual_m": args.fallback_residual} if "learned" in legs
+                                         else {"training": training}),
+                  "plain_fp64": ({k: legs["plain_fp64"][k] for k in ("iterations_per_step", "steps_per_s",
+                                                                       "final_residual")}
+                                 if "plain_fp64" in legs else None),
+                  "value_over_plain_steps_per_s": fu["steps_per_s"] / pl["steps_per_s"] if pl else None,
+                  "plain_over_value_iterations": (sum(pl["iterations_per_step"]) /
+                                                  max(sum(fu["iterations_per_step"]), 1)) if pl else None,
                   "ablation_steps_per_s": {k: legs[k]["steps_per_s"] for k in legs},
                   "monitor": "device (layers as conditional IF nodes, projectGS as conditional WHILE nodes)"}
-        if use_pcg:
-            to_res["layer_pcg"] = {**legs["layer_pcg"], "pcg_iterations": args.layer_pcg,
-                                   "gs_iterations_between": args.layer_pcg_every}
-            to_res["learned_pcg"] = {**legs["learned_pcg"], "pcg_iterations": args.layer_pcg,
-                                     "gs_iterations_between": args.layer_pcg_every}
+        for name in ("layer_pcg", "learned_pcg"):
+            if name in legs:
+                to_res[name] = {**legs[name], "pcg_iterations": args.layer_pcg,
+                                "gs_iterations_between": args.layer_pcg_every}
+
+        def err(a, b):
+            return float(np.abs(states[a] - states[b]).max() / diag) if a in states and b in states else None
+
         parity = {"reference": "FP64 plain solve of the same steps on the GPU (the FP64 path matches the CPU "
                                "oracle to 1e-9)",
-                  "max_rel_pos_err": float(np.abs(states[full] - states["plain_fp64"]).max() / diag),
-                  "max_rel_pos_err_of": full,
-                  "max_rel_pos_err_learned": float(np.abs(states["learned"] - states["plain_fp64"]).max() / diag),
-                  "max_rel_pos_err_layer_pcg": (float(np.abs(states["layer_pcg"] - states["plain_fp64"]).max() / diag)
-                                                if use_pcg else None),
-                  "max_rel_pos_err_plain_fp32": float(np.abs(states["plain"] - states["plain_fp64"]).max() / diag),
-                  "learned_vs_plain_fp32": float(np.abs(states["learned"] - states["plain"]).max() / diag),
+                  "max_rel_pos_err": err(full, "plain_fp64"), "max_rel_pos_err_of": full,
+                  "max_rel_pos_err_learned": err("learned", "plain_fp64"),
+                  "max_rel_pos_err_layer_pcg": err("layer_pcg", "plain_fp64"),
+                  "max_rel_pos_err_plain_fp32": err("plain", "plain_fp64"),
+                  "learned_vs_plain_fp32": err("learned", "plain"),
                   "after_steps": args.warmup + args.steps,
-                  "one_step_plain_fp32": float(np.abs(one["plain"] - one["plain_fp64"]).max() / diag),
+                  "one_step_plain_fp32": (float(np.abs(one["plain"] - one["plain_fp64"]).max() / diag)
+                                          if one else None),
                   "one_step_note": "FP32 and FP64 plain solves to residual 1e-4, one step from the same state",
                   "unit": "max |x - x_ref| / bounding-box diagonal"}
 
@@ -613,7 +623,7 @@ def run_ours(args, rank, world, local):
                 # iterations per step (same algorithm, same residual rule)
                 n, dt, it = cpu_port(1, threads, state0, residual=True, cap=args.cpu_iters)
                 per_it = dt / max(it[0], 1)
-                gpu_it = float(np.mean(to_res["plain"]["iterations_per_step"]))
+                gpu_it = float(np.mean((to_res["plain"] or fleg_of(to_res))["iterations_per_step"]))
                 cpu = {"value": 1.0 / (per_it * gpu_it), "unit": "steps/s", "cores": threads, "kind": "port",
                        "sample": f"{it[0]} projectGS iterations of one step with the residual monitor on ({dt:.1f} s, "
                                  f"FP64 oracle restatement, OpenMP over the tets of a colour), scaled to "
@@ -625,7 +635,7 @@ def run_ours(args, rank, world, local):
                                  "over the tets of a colour" + (", from the same landed state, oracle contact "
                                                                  "finders every step)" if advance else ")")}
         if residual_metric:
-            fleg = to_res[to_res["value_leg"]] if to_res["value_leg"] != "learned" else to_res["learned_warm_start"]
+            fleg = fleg_of(to_res)
             value = fleg["steps_per_s"] * world
             ms_per_step = 1000.0 * world / value
             solver_desc = ("learned warm start (coarse-cluster corrections, BF16 perceptron on tcgen05)"
@@ -697,6 +707,11 @@ def run_ours(args, rank, world, local):
     return 0
 
 
+def fleg_of(to_res):
+    """The value leg's record of a to_residual block."""
+    return to_res[to_res["value_leg"]] if to_res["value_leg"] != "learned" else to_res["learned_warm_start"]
+
+
 def solver_bytes_per_tet(mesh, precision):
     """Algorithmic bytes of one tet projection in the device layout: vertex
     ids (16), DmInv (9 r), volume (r, StVK only), material (2 r for the
@@ -740,6 +755,8 @@ def main():
                     "workloads; 0: none)")
     ap.add_argument("--layer-pcg-every", type=int, default=50,
                     help="Gauss-Seidel iterations between the Newton-PCG corrections")
+    ap.add_argument("--legs", default="",
+                    help="comma-separated residual legs to run (profiling; the value leg always runs)")
     ap.add_argument("--train-in-bench", action="store_true",
                     help="config 5: train the network on recorded steps here instead of loading the shipped one")
     ap.add_argument("--advance", type=int, default=None,
