@@ -392,7 +392,7 @@ def run_ours(args, rank, world, local):
                 if timed:
                     flush.zero_()
                     torch.cuda.synchronize()
-                ms_steps.append(sim3.step(1, graph=True, timed=True))
+                ms_steps.append(sim3.step(1, graph=not args.host_monitor, timed=True))
                 ra, it_total, _, status = sim3.monitor()
                 iters.append(int(it_total))
                 finals.append(float(ra[-1]))
@@ -755,6 +755,9 @@ def main():
                     "workloads; 0: none)")
     ap.add_argument("--layer-pcg-every", type=int, default=50,
                     help="Gauss-Seidel iterations between the Newton-PCG corrections")
+    ap.add_argument("--host-monitor", action="store_true",
+                    help="residual legs without the step graph: the same kernels with the stop rules on the host "
+                    "(ncu cannot profile kernels of graphs with conditional nodes)")
     ap.add_argument("--legs", default="",
                     help="comma-separated residual legs to run (profiling; the value leg always runs)")
     ap.add_argument("--train-in-bench", action="store_true",
