@@ -250,14 +250,18 @@ __global__ void k_pcg_sub(int N, const double4* __restrict__ a, const double4* _
 // the library's stable Neo-Hookean pair (tet_kernels.cuh nh_eval), W =
 // (h^2 vol mu, h^2 vol (lambda - mu)) from the stored compliances.
 //
-// Per tet (sorted order, structure of arrays): jac [24][T] = dC_D/dx of the
-// four corners (12) then dC_H/dx (12); w [2][T]; c [2][T]; q [2][T] = W C +
-// lambda (the right-hand side's factor); s [2][T] scratch.
+// Storage.  The Jacobian is kept twice: tet-major jt[T][4 corners][6]
+// (corner a: dC_D/dx_a then dC_H/dx_a) for the per-tet products, and in the
+// order of the vertex -> (tet, corner) CSR, jv[pairs][6], for the per-vertex
+// gathers (each vertex then reads its pairs contiguously).  vtpos[4 s + a] is
+// the CSR position of corner a of tet s.  Per tet, double2: w = (W_D, W_H),
+// c = (C_D, C_H), q = W C + lambda (the right-hand side's factor), s scratch.
 
 template <typename R>
 __global__ void __launch_bounds__(256) k_ns_jacobian(TetData<R> td, const R4<R>* __restrict__ pos, double h2,
-                                                     R* __restrict__ jac, double* __restrict__ w,
-                                                     double* __restrict__ c, double* __restrict__ q) {
+                                                     const int* __restrict__ vtpos, R* __restrict__ jt,
+                                                     R* __restrict__ jv, double2* __restrict__ w,
+                                                     double2* __restrict__ c, double2* __restrict__ q) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   const int T = td.T;
   if (s >= T) return;
@@ -270,93 +274,138 @@ __global__ void __launch_bounds__(256) k_ns_jacobian(TetData<R> td, const R4<R>*
   nh_eval<R>(X, G, cD, cH, 0.0, e);
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
-    jac[(size_t)(3 * a + 0) * T + s] = e.gD[a].x;
-    jac[(size_t)(3 * a + 1) * T + s] = e.gD[a].y;
-    jac[(size_t)(3 * a + 2) * T + s] = e.gD[a].z;
-    jac[(size_t)(12 + 3 * a + 0) * T + s] = e.gH[a].x;
-    jac[(size_t)(12 + 3 * a + 1) * T + s] = e.gH[a].y;
-    jac[(size_t)(12 + 3 * a + 2) * T + s] = e.gH[a].z;
+    const R g[6] = {e.gD[a].x, e.gD[a].y, e.gD[a].z, e.gH[a].x, e.gH[a].y, e.gH[a].z};
+    R* t = jt + (size_t)24 * s + 6 * a;
+    R* u = jv + (size_t)6 * vtpos[4 * (size_t)s + a];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      t[k] = g[k];
+      u[k] = g[k];
+    }
   }
   const double wD = cD > 0.0 ? h2 / cD : 0.0, wH = e.hasH ? h2 / cH : 0.0;
-  w[s] = wD;
-  w[(size_t)T + s] = wH;
-  c[s] = e.CD;
-  c[(size_t)T + s] = e.CH;
-  q[s] = wD * e.CD + (double)td.lambda[s];
-  q[(size_t)T + s] = e.hasH ? wH * e.CH + (double)td.lambda[(size_t)T + s] : 0.0;
+  w[s] = make_double2(wD, wH);
+  c[s] = make_double2(e.CD, e.CH);
+  q[s] = make_double2(wD * e.CD + (double)td.lambda[s],
+                      e.hasH ? wH * e.CH + (double)td.lambda[(size_t)T + s] : 0.0);
 }
 
-// s_t = W_t (J_t u) for every tet.
+// (J_t u) for tet s: the two constraint rows against the corners' u.
 template <typename R>
-__global__ void __launch_bounds__(256) k_ns_tet_apply(int T, const int4* __restrict__ vid, const R* __restrict__ jac,
-                                                      const double* __restrict__ w, const double4* __restrict__ u,
-                                                      double* __restrict__ out) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= T) return;
-  const int4 v = vid[s];
+__device__ __forceinline__ double2 ns_ju(const R* __restrict__ jt, int s, int4 v, const double4* __restrict__ u) {
   const int vv[4] = {v.x, v.y, v.z, v.w};
+  const R* t = jt + (size_t)24 * s;
   double d0 = 0.0, d1 = 0.0;
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
     const double4 ua = u[vv[a]];
-    d0 += (double)jac[(size_t)(3 * a) * T + s] * ua.x + (double)jac[(size_t)(3 * a + 1) * T + s] * ua.y +
-          (double)jac[(size_t)(3 * a + 2) * T + s] * ua.z;
-    d1 += (double)jac[(size_t)(12 + 3 * a) * T + s] * ua.x + (double)jac[(size_t)(12 + 3 * a + 1) * T + s] * ua.y +
-          (double)jac[(size_t)(12 + 3 * a + 2) * T + s] * ua.z;
+    d0 += (double)t[6 * a] * ua.x + (double)t[6 * a + 1] * ua.y + (double)t[6 * a + 2] * ua.z;
+    d1 += (double)t[6 * a + 3] * ua.x + (double)t[6 * a + 4] * ua.y + (double)t[6 * a + 5] * ua.z;
   }
-  out[s] = w[s] * d0;
-  out[(size_t)T + s] = w[(size_t)T + s] * d1;
+  return make_double2(d0, d1);
 }
 
-// y_v = (u ? m_v u_v : 0) + scale * sum over the vertex's (tet, corner) pairs
-// of J_{t,corner}^T f_t, in the CSR's fixed order; pinned components 0.
+// s_t = W_t (J_t u) for every tet.
 template <typename R>
-__global__ void k_ns_vertex_apply(PcgOp op, int T, const R* __restrict__ jac, const double* __restrict__ f,
-                                  double scale, const double4* __restrict__ u, double4* __restrict__ y) {
-  const int v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= op.N) return;
+__global__ void __launch_bounds__(256) k_ns_tet_apply(int T, const int4* __restrict__ vid, const R* __restrict__ jt,
+                                                      const double2* __restrict__ w, const double4* __restrict__ u,
+                                                      double2* __restrict__ out) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= T) return;
+  const double2 ju = ns_ju<R>(jt, s, vid[s], u);
+  const double2 ws = w[s];
+  out[s] = make_double2(ws.x * ju.x, ws.y * ju.y);
+}
+
+// sum over the vertex's (tet, corner) pairs of J_{t,corner}^T f_t, in the
+// CSR's fixed order.
+template <typename R>
+__device__ __forceinline__ D3 ns_jtf(const PcgOp& op, const R* __restrict__ jv, const double2* __restrict__ f,
+                                     int v) {
   D3 acc = d3(0.0, 0.0, 0.0);
   for (int k = op.vt_off[v]; k < op.vt_off[v + 1]; ++k) {
-    const int2 e = op.vt[k];
-    const size_t s = (size_t)e.x;
-    const double f0 = f[s], f1 = f[(size_t)T + s];
-    const int a = e.y;
-    acc = acc + d3(f0 * (double)jac[(size_t)(3 * a) * T + s] + f1 * (double)jac[(size_t)(12 + 3 * a) * T + s],
-                   f0 * (double)jac[(size_t)(3 * a + 1) * T + s] + f1 * (double)jac[(size_t)(12 + 3 * a + 1) * T + s],
-                   f0 * (double)jac[(size_t)(3 * a + 2) * T + s] + f1 * (double)jac[(size_t)(12 + 3 * a + 2) * T + s]);
+    const double2 fk = f[op.vt[k].x];
+    const R* g = jv + (size_t)6 * k;
+    acc = acc + d3(fk.x * (double)g[0] + fk.y * (double)g[3], fk.x * (double)g[1] + fk.y * (double)g[4],
+                   fk.x * (double)g[2] + fk.y * (double)g[5]);
   }
-  acc = scale * acc;
-  if (u) {
+  return acc;
+}
+
+// y = -J^T q on the unpinned DOFs (the right-hand side).
+template <typename R>
+__global__ void k_ns_rhs(PcgOp op, const R* __restrict__ jv, const double2* __restrict__ q, double4* __restrict__ y) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= op.N) return;
+  const D3 a = ns_jtf<R>(op, jv, q, v);
+  const unsigned char pm = op.pin[v];
+  y[v] = make_double4((pm & 1) ? 0.0 : -a.x, (pm & 2) ? 0.0 : -a.y, (pm & 4) ? 0.0 : -a.z, 0.0);
+}
+
+// y = M u + J^T f on the unpinned DOFs, and the partial sums of u'y (one per
+// block, at partials[2 b]; grid-stride over the vertices, fixed order).
+template <typename R>
+__global__ void __launch_bounds__(256) k_ns_vertex_apply(PcgOp op, const R* __restrict__ jv,
+                                                         const double2* __restrict__ f, const double4* __restrict__ u,
+                                                         double4* __restrict__ y, double* __restrict__ partials) {
+  double dot[1] = {0.0};
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < op.N; v += gridDim.x * blockDim.x) {
+    const D3 a = ns_jtf<R>(op, jv, f, v);
     const double m = op.vmass[v];
     const double4 uv = u[v];
-    acc = acc + d3(m * uv.x, m * uv.y, m * uv.z);
+    const unsigned char pm = op.pin[v];
+    const double4 yv = make_double4((pm & 1) ? 0.0 : a.x + m * uv.x, (pm & 2) ? 0.0 : a.y + m * uv.y,
+                                    (pm & 4) ? 0.0 : a.z + m * uv.z, 0.0);
+    y[v] = yv;
+    dot[0] += uv.x * yv.x + uv.y * yv.y + uv.z * yv.z;
   }
-  const unsigned char pm = op.pin[v];
-  y[v] = make_double4((pm & 1) ? 0.0 : acc.x, (pm & 2) ? 0.0 : acc.y, (pm & 4) ? 0.0 : acc.z, 0.0);
+  block_sum<1>(dot);
+  if (threadIdx.x == 0) partials[2 * blockIdx.x] = dot[0];
+}
+
+// x += alpha d, r -= alpha Ap, z = P r, and the partial sums of r'z (one per
+// block at partials[2 b]; grid-stride, fixed order).
+__global__ void __launch_bounds__(256) k_ns_step(int N, const PcgScalars* __restrict__ sc,
+                                                 const double4* __restrict__ d, const double4* __restrict__ Ap,
+                                                 double4* __restrict__ x, double4* __restrict__ r,
+                                                 const double* __restrict__ Pinv,
+                                                 const unsigned char* __restrict__ pin, double4* __restrict__ z,
+                                                 double* __restrict__ partials) {
+  const double alpha = sc->alpha;
+  double dot[1] = {0.0};
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < N; v += gridDim.x * blockDim.x) {
+    const double4 dv = d[v], av = Ap[v], xv = x[v], rv = r[v];
+    x[v] = make_double4(xv.x + alpha * dv.x, xv.y + alpha * dv.y, xv.z + alpha * dv.z, 0.0);
+    const D3 rn = d3(rv.x - alpha * av.x, rv.y - alpha * av.y, rv.z - alpha * av.z);
+    r[v] = make_double4(rn.x, rn.y, rn.z, 0.0);
+    const D3 b = mv3(Pinv + 9 * (size_t)v, rn);
+    const unsigned char pm = pin[v];
+    const D3 zn = d3((pm & 1) ? 0.0 : b.x, (pm & 2) ? 0.0 : b.y, (pm & 4) ? 0.0 : b.z);
+    z[v] = make_double4(zn.x, zn.y, zn.z, 0.0);
+    dot[0] += rn.x * zn.x + rn.y * zn.y + rn.z * zn.z;
+  }
+  block_sum<1>(dot);
+  if (threadIdx.x == 0) partials[2 * blockIdx.x] = dot[0];
 }
 
 // Inverse of the 3x3 diagonal block of M + J^T W J at every vertex (pinned
 // rows and columns replaced by the identity).
 template <typename R>
-__global__ void k_ns_block_jacobi(PcgOp op, int T, const R* __restrict__ jac, const double* __restrict__ w,
+__global__ void k_ns_block_jacobi(PcgOp op, const R* __restrict__ jv, const double2* __restrict__ w,
                                   double* __restrict__ Pinv) {
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= op.N) return;
   const double m = op.vmass[v];
   double B[9] = {m, 0, 0, 0, m, 0, 0, 0, m};
   for (int k = op.vt_off[v]; k < op.vt_off[v + 1]; ++k) {
-    const int2 e = op.vt[k];
-    const size_t s = (size_t)e.x;
-    const int a = e.y;
-    const double wD = w[s], wH = w[(size_t)T + s];
-    const double gD[3] = {(double)jac[(size_t)(3 * a) * T + s], (double)jac[(size_t)(3 * a + 1) * T + s],
-                          (double)jac[(size_t)(3 * a + 2) * T + s]};
-    const double gH[3] = {(double)jac[(size_t)(12 + 3 * a) * T + s], (double)jac[(size_t)(12 + 3 * a + 1) * T + s],
-                          (double)jac[(size_t)(12 + 3 * a + 2) * T + s]};
+    const double2 wk = w[op.vt[k].x];
+    const R* g = jv + (size_t)6 * k;
+    const double gD[3] = {(double)g[0], (double)g[1], (double)g[2]};
+    const double gH[3] = {(double)g[3], (double)g[4], (double)g[5]};
 #pragma unroll
     for (int j = 0; j < 3; ++j)
 #pragma unroll
-      for (int i = 0; i < 3; ++i) B[i + 3 * j] += wD * gD[i] * gD[j] + wH * gH[i] * gH[j];
+      for (int i = 0; i < 3; ++i) B[i + 3 * j] += wk.x * gD[i] * gD[j] + wk.y * gH[i] * gH[j];
   }
   const unsigned char pm = op.pin[v];
 #pragma unroll
@@ -372,25 +421,15 @@ __global__ void k_ns_block_jacobi(PcgOp op, int T, const R* __restrict__ jac, co
 
 // lambda = -W (C + J dx) for every tet (rows 0 and 1; an absent C_H keeps 0).
 template <typename R>
-__global__ void __launch_bounds__(256) k_ns_lambda(int T, const int4* __restrict__ vid, const R* __restrict__ jac,
-                                                   const double* __restrict__ w, const double* __restrict__ c,
+__global__ void __launch_bounds__(256) k_ns_lambda(int T, const int4* __restrict__ vid, const R* __restrict__ jt,
+                                                   const double2* __restrict__ w, const double2* __restrict__ c,
                                                    const double4* __restrict__ dx, R* __restrict__ lambda) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= T) return;
-  const int4 v = vid[s];
-  const int vv[4] = {v.x, v.y, v.z, v.w};
-  double d0 = 0.0, d1 = 0.0;
-#pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    const double4 ua = dx[vv[a]];
-    d0 += (double)jac[(size_t)(3 * a) * T + s] * ua.x + (double)jac[(size_t)(3 * a + 1) * T + s] * ua.y +
-          (double)jac[(size_t)(3 * a + 2) * T + s] * ua.z;
-    d1 += (double)jac[(size_t)(12 + 3 * a) * T + s] * ua.x + (double)jac[(size_t)(12 + 3 * a + 1) * T + s] * ua.y +
-          (double)jac[(size_t)(12 + 3 * a + 2) * T + s] * ua.z;
-  }
-  const double wH = w[(size_t)T + s];
-  lambda[s] = (R)(-w[s] * (c[s] + d0));
-  lambda[(size_t)T + s] = wH > 0.0 ? (R)(-wH * (c[(size_t)T + s] + d1)) : R(0);
+  const double2 jd = ns_ju<R>(jt, s, vid[s], dx);
+  const double2 ws = w[s], cs = c[s];
+  lambda[s] = (R)(-ws.x * (cs.x + jd.x));
+  lambda[(size_t)T + s] = ws.y > 0.0 ? (R)(-ws.y * (cs.y + jd.y)) : R(0);
 }
 
 // x += dx on every vertex (dx is 0 on the pinned DOFs).

@@ -429,7 +429,7 @@ struct Solver final : SolverBase {
   // iterations per correction (0: off) and Gauss-Seidel iterations between
   // corrections
   int ns_iters = 0, ns_every = 0;
-  DevBuf d_ns_jac, d_ns_tet;
+  DevBuf d_ns_jac, d_ns_tet, d_vtpos;
   cudaStream_t cs_ns = nullptr;
   int ns_configure(int pcg_iterations, int every) override;
   int ns_correct(double h, long long* launches);
@@ -3086,14 +3086,20 @@ int Solver<R>::vt_setup() {
   }
   for (int v = 0; v < N; ++v) off[v + 1] += off[v];
   std::vector<int2> vt(off[N]);
+  std::vector<int> vtpos(4 * (size_t)T);
   {
     std::vector<int> f(off.begin(), off.end() - 1);
     for (int sidx = 0; sidx < T; ++sidx) {
       const int4 q = vid_sorted[sidx];
       const int vv[4] = {q.x, q.y, q.z, q.w};
-      for (int k = 0; k < 4; ++k) vt[f[vv[k]]++] = make_int2(sidx, k);
+      for (int k = 0; k < 4; ++k) {
+        vtpos[4 * (size_t)sidx + k] = f[vv[k]];
+        vt[f[vv[k]]++] = make_int2(sidx, k);
+      }
     }
   }
+  CHECK(d_vtpos.ensure(sizeof(int) * vtpos.size()));
+  CU(cudaMemcpyAsync(d_vtpos.p, vtpos.data(), sizeof(int) * vtpos.size(), cudaMemcpyHostToDevice, stream));
   std::vector<unsigned char> pm(N, 0);
   for (int d : pinned) pm[d / 3] |= (unsigned char)(1u << (d % 3));
   CHECK(d_pcg_vt.ensure(sizeof(int) * (N + 1) + sizeof(int2) * vt.size()));
@@ -3142,8 +3148,8 @@ int Solver<R>::ns_configure(int pcg_iterations, int every) {
   DeviceGuard g(device);
   if (pcg_iterations > 0) {
     CHECK(vt_setup());
-    CHECK(d_ns_jac.ensure(sizeof(R) * 24 * (size_t)T));
-    CHECK(d_ns_tet.ensure(sizeof(double) * 8 * (size_t)T));
+    CHECK(d_ns_jac.ensure(sizeof(R) * 48 * (size_t)T));      // tet-major and CSR-order copies
+    CHECK(d_ns_tet.ensure(sizeof(double2) * 4 * (size_t)T));  // w, c, q, scratch
   }
   ns_iters = pcg_iterations;
   ns_every = every;
@@ -3158,9 +3164,10 @@ template <typename R>
 int Solver<R>::ns_correct(double h, long long* launches) {
   const PcgOp op = vt_op(h * h);
   const int nb = blocks_for(N, 256), tb = blocks_for(T, 256), nred = std::min(nb, 296);
-  R* jac = d_ns_jac.as<R>();
-  double* tw = d_ns_tet.as<double>();
-  double *w = tw, *c = tw + 2 * (size_t)T, *q = tw + 4 * (size_t)T, *sv = tw + 6 * (size_t)T;
+  R* jt = d_ns_jac.as<R>();
+  R* jv = jt + (size_t)24 * T;
+  double2* tw = d_ns_tet.as<double2>();
+  double2 *w = tw, *c = tw + T, *q = tw + 2 * (size_t)T, *sv = tw + 3 * (size_t)T;
   double4* V = d_pcg_vec.as<double4>();
   double4 *db = V, *dx = V + N, *dr = V + 2 * (size_t)N, *dz = V + 3 * (size_t)N, *dd = V + 4 * (size_t)N,
           *dAp = V + 5 * (size_t)N;
@@ -3168,30 +3175,27 @@ int Solver<R>::ns_correct(double h, long long* launches) {
   double* part = d_pcg_part.as<double>();
   PcgScalars* sc = d_pcg_sc.as<PcgScalars>();
   const int4* vid = d_vid.as<int4>();
-  k_ns_jacobian<R><<<tb, 256, 0, stream>>>(tets(), pos(), h * h, jac, w, c, q);
-  k_ns_vertex_apply<R><<<nb, 256, 0, stream>>>(op, T, jac, q, -1.0, nullptr, db);  // b = -J^T (W C + lambda)
+  k_ns_jacobian<R><<<tb, 256, 0, stream>>>(tets(), pos(), h * h, d_vtpos.as<int>(), jt, jv, w, c, q);
+  k_ns_rhs<R><<<nb, 256, 0, stream>>>(op, jv, q, db);  // b = -J^T (W C + lambda)
   CU(cudaMemsetAsync(dx, 0, sizeof(double4) * N, stream));
   CU(cudaMemcpyAsync(dr, db, sizeof(double4) * N, cudaMemcpyDeviceToDevice, stream));
-  k_ns_block_jacobi<R><<<nb, 256, 0, stream>>>(op, T, jac, w, P);
+  k_ns_block_jacobi<R><<<nb, 256, 0, stream>>>(op, jv, w, P);
   k_pcg_precond<<<nb, 256, 0, stream>>>(N, P, op.pin, dr, dz);
   CU(cudaMemcpyAsync(dd, dz, sizeof(double4) * N, cudaMemcpyDeviceToDevice, stream));
   k_pcg_dot2<<<nred, 256, 0, stream>>>(N, dr, dz, nullptr, nullptr, part);
   k_pcg_scalars<<<1, 256, 0, stream>>>(part, nred, 0, sc, nullptr, 0);
   for (int i = 0; i < ns_iters; ++i) {
-    k_ns_tet_apply<R><<<tb, 256, 0, stream>>>(T, vid, jac, w, dd, sv);
-    k_ns_vertex_apply<R><<<nb, 256, 0, stream>>>(op, T, jac, sv, 1.0, dd, dAp);  // Ap = A d
-    k_pcg_dot2<<<nred, 256, 0, stream>>>(N, dd, dAp, nullptr, nullptr, part);
-    k_pcg_scalars<<<1, 256, 0, stream>>>(part, nred, 1, sc, nullptr, 0);
-    k_pcg_step<<<nb, 256, 0, stream>>>(N, sc, dd, dAp, dx, dr);
-    k_pcg_precond<<<nb, 256, 0, stream>>>(N, P, op.pin, dr, dz);
-    k_pcg_dot2<<<nred, 256, 0, stream>>>(N, dr, dz, nullptr, nullptr, part);
-    k_pcg_scalars<<<1, 256, 0, stream>>>(part, nred, 4, sc, nullptr, 0);
+    k_ns_tet_apply<R><<<tb, 256, 0, stream>>>(T, vid, jt, w, dd, sv);
+    k_ns_vertex_apply<R><<<nred, 256, 0, stream>>>(op, jv, sv, dd, dAp, part);  // Ap = A d, d'Ap
+    k_pcg_scalars<<<1, 256, 0, stream>>>(part, nred, 1, sc, nullptr, 0);         // alpha
+    k_ns_step<<<nred, 256, 0, stream>>>(N, sc, dd, dAp, dx, dr, P, op.pin, dz, part);  // x, r, z, r'z
+    k_pcg_scalars<<<1, 256, 0, stream>>>(part, nred, 4, sc, nullptr, 0);         // beta
     k_pcg_direction<<<nb, 256, 0, stream>>>(N, sc, dz, dd);
   }
-  k_ns_lambda<R><<<tb, 256, 0, stream>>>(T, vid, jac, w, c, dx, d_lambda.as<R>());
+  k_ns_lambda<R><<<tb, 256, 0, stream>>>(T, vid, jt, w, c, dx, d_lambda.as<R>());
   k_ns_move<R><<<nb, 256, 0, stream>>>(N, dx, pos());
   CU(cudaGetLastError());
-  if (launches) *launches += 7 + 9LL * ns_iters;
+  if (launches) *launches += 7 + 6LL * ns_iters;
   return MLX_OK;
 }
 
