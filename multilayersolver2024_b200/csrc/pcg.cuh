@@ -250,10 +250,11 @@ __global__ void k_pcg_sub(int N, const double4* __restrict__ a, const double4* _
 // the library's stable Neo-Hookean pair (tet_kernels.cuh nh_eval), W =
 // (h^2 vol mu, h^2 vol (lambda - mu)) from the stored compliances.
 //
-// Storage.  The Jacobian is kept twice: tet-major jt[T][4 corners][6]
-// (corner a: dC_D/dx_a then dC_H/dx_a) for the per-tet products, and in the
-// order of the vertex -> (tet, corner) CSR, jv[pairs][6], for the per-vertex
-// gathers (each vertex then reads its pairs contiguously).  vtpos[4 s + a] is
+// Storage.  The Jacobian is kept twice: structure of arrays jt[24][T] (row
+// 6a + k: corner a, k < 3 dC_D/dx_a, k >= 3 dC_H/dx_a) for the per-tet
+// products, whose warps then read consecutive words, and in the order of the
+// vertex -> (tet, corner) CSR, jv[pairs][6], for the per-vertex gathers (each
+// vertex then reads its pairs contiguously).  vtpos[4 s + a] is
 // the CSR position of corner a of tet s.  Per tet, double2: w = (W_D, W_H),
 // c = (C_D, C_H), q = W C + lambda (the right-hand side's factor), s scratch.
 
@@ -275,11 +276,10 @@ __global__ void __launch_bounds__(256) k_ns_jacobian(TetData<R> td, const R4<R>*
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
     const R g[6] = {e.gD[a].x, e.gD[a].y, e.gD[a].z, e.gH[a].x, e.gH[a].y, e.gH[a].z};
-    R* t = jt + (size_t)24 * s + 6 * a;
     R* u = jv + (size_t)6 * vtpos[4 * (size_t)s + a];
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
-      t[k] = g[k];
+      jt[(size_t)(6 * a + k) * T + s] = g[k];
       u[k] = g[k];
     }
   }
@@ -292,15 +292,16 @@ __global__ void __launch_bounds__(256) k_ns_jacobian(TetData<R> td, const R4<R>*
 
 // (J_t u) for tet s: the two constraint rows against the corners' u.
 template <typename R>
-__device__ __forceinline__ double2 ns_ju(const R* __restrict__ jt, int s, int4 v, const double4* __restrict__ u) {
+__device__ __forceinline__ double2 ns_ju(const R* __restrict__ jt, int T, int s, int4 v,
+                                         const double4* __restrict__ u) {
   const int vv[4] = {v.x, v.y, v.z, v.w};
-  const R* t = jt + (size_t)24 * s;
   double d0 = 0.0, d1 = 0.0;
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
     const double4 ua = u[vv[a]];
-    d0 += (double)t[6 * a] * ua.x + (double)t[6 * a + 1] * ua.y + (double)t[6 * a + 2] * ua.z;
-    d1 += (double)t[6 * a + 3] * ua.x + (double)t[6 * a + 4] * ua.y + (double)t[6 * a + 5] * ua.z;
+    const R* t = jt + (size_t)(6 * a) * T + s;
+    d0 += (double)t[0] * ua.x + (double)t[(size_t)T] * ua.y + (double)t[2 * (size_t)T] * ua.z;
+    d1 += (double)t[3 * (size_t)T] * ua.x + (double)t[4 * (size_t)T] * ua.y + (double)t[5 * (size_t)T] * ua.z;
   }
   return make_double2(d0, d1);
 }
@@ -312,7 +313,7 @@ __global__ void __launch_bounds__(256) k_ns_tet_apply(int T, const int4* __restr
                                                       double2* __restrict__ out) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= T) return;
-  const double2 ju = ns_ju<R>(jt, s, vid[s], u);
+  const double2 ju = ns_ju<R>(jt, T, s, vid[s], u);
   const double2 ws = w[s];
   out[s] = make_double2(ws.x * ju.x, ws.y * ju.y);
 }
@@ -426,7 +427,7 @@ __global__ void __launch_bounds__(256) k_ns_lambda(int T, const int4* __restrict
                                                    const double4* __restrict__ dx, R* __restrict__ lambda) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= T) return;
-  const double2 jd = ns_ju<R>(jt, s, vid[s], dx);
+  const double2 jd = ns_ju<R>(jt, T, s, vid[s], dx);
   const double2 ws = w[s], cs = c[s];
   lambda[s] = (R)(-ws.x * (cs.x + jd.x));
   lambda[(size_t)T + s] = ws.y > 0.0 ? (R)(-ws.y * (cs.y + jd.y)) : R(0);
