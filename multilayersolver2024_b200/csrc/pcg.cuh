@@ -364,15 +364,27 @@ __global__ void __launch_bounds__(256) k_ns_vertex_apply(PcgOp op, const R* __re
   if (threadIdx.x == 0) partials[2 * blockIdx.x] = dot[0];
 }
 
+// Sum of the n partials of a fixed-order reduction (the same order in every
+// block, so every block obtains the same value).
+__device__ __forceinline__ double ns_sum_partials(const double* __restrict__ partials, int n) {
+  double s[1] = {0.0};
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s[0] += partials[2 * i];
+  block_sum<1>(s);
+  return s[0];
+}
+
+// alpha = rTz[cur] / d'Ap (0 when d'Ap = 0) from the partials of d'Ap; then
 // x += alpha d, r -= alpha Ap, z = P r, and the partial sums of r'z (one per
-// block at partials[2 b]; grid-stride, fixed order).
-__global__ void __launch_bounds__(256) k_ns_step(int N, const PcgScalars* __restrict__ sc,
+// block at partials2[2 b]; grid-stride, fixed order).
+__global__ void __launch_bounds__(256) k_ns_step(int N, const double* __restrict__ rTz, int cur,
+                                                 const double* __restrict__ partials, int nparts,
                                                  const double4* __restrict__ d, const double4* __restrict__ Ap,
                                                  double4* __restrict__ x, double4* __restrict__ r,
                                                  const double* __restrict__ Pinv,
                                                  const unsigned char* __restrict__ pin, double4* __restrict__ z,
-                                                 double* __restrict__ partials) {
-  const double alpha = sc->alpha;
+                                                 double* __restrict__ partials2) {
+  const double dAp = ns_sum_partials(partials, nparts);
+  const double alpha = dAp == 0.0 ? 0.0 : rTz[cur] / dAp;
   double dot[1] = {0.0};
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < N; v += gridDim.x * blockDim.x) {
     const double4 dv = d[v], av = Ap[v], xv = x[v], rv = r[v];
@@ -386,7 +398,23 @@ __global__ void __launch_bounds__(256) k_ns_step(int N, const PcgScalars* __rest
     dot[0] += rn.x * zn.x + rn.y * zn.y + rn.z * zn.z;
   }
   block_sum<1>(dot);
-  if (threadIdx.x == 0) partials[2 * blockIdx.x] = dot[0];
+  if (threadIdx.x == 0) partials2[2 * blockIdx.x] = dot[0];
+}
+
+// rTz_new from the partials of r'z; beta = rTz_new / rTz[cur] (0 when
+// rTz[cur] = 0); d = z + beta d; block 0 stores rTz_new in rTz[1 - cur] for
+// the next iteration (r'z is double-buffered: every block reads rTz[cur]).
+__global__ void __launch_bounds__(256) k_ns_direction(int N, double* __restrict__ rTz, int cur,
+                                                      const double* __restrict__ partials, int nparts,
+                                                      const double4* __restrict__ z, double4* __restrict__ d) {
+  const double rtz_new = ns_sum_partials(partials, nparts);
+  const double old = rTz[cur];
+  const double beta = old == 0.0 ? 0.0 : rtz_new / old;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < N; v += gridDim.x * blockDim.x) {
+    const double4 zv = z[v], dv = d[v];
+    d[v] = make_double4(zv.x + beta * dv.x, zv.y + beta * dv.y, zv.z + beta * dv.z, 0.0);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) rTz[1 - cur] = rtz_new;
 }
 
 // Inverse of the 3x3 diagonal block of M + J^T W J at every vertex (pinned

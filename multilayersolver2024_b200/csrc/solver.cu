@@ -3111,7 +3111,7 @@ int Solver<R>::vt_setup() {
   CU(cudaMemcpyAsync(d_pcg_pin.p, pm.data(), N, cudaMemcpyHostToDevice, stream));
   CHECK(d_pcg_vec.ensure(sizeof(double4) * 7 * (size_t)N));
   CHECK(d_pcg_P.ensure(sizeof(double) * 9 * (size_t)N));
-  CHECK(d_pcg_part.ensure(sizeof(double) * 2 * 296));
+  CHECK(d_pcg_part.ensure(sizeof(double) * 4 * 296));  // two sets of partials
   CHECK(d_pcg_sc.ensure(sizeof(PcgScalars)));
   CU(cudaStreamSynchronize(stream));
   vt_ready = true;
@@ -3182,20 +3182,24 @@ int Solver<R>::ns_correct(double h, long long* launches) {
   k_ns_block_jacobi<R><<<nb, 256, 0, stream>>>(op, jv, w, P);
   k_pcg_precond<<<nb, 256, 0, stream>>>(N, P, op.pin, dr, dz);
   CU(cudaMemcpyAsync(dd, dz, sizeof(double4) * N, cudaMemcpyDeviceToDevice, stream));
+  // r'z double-buffered in the first two doubles of the scalars (rTz, then
+  // the alpha slot, which this loop does not use); the start's r'z goes to
+  // rTz[0]
+  double* rTz = reinterpret_cast<double*>(sc);
+  double* part2 = part + 2 * 296;
   k_pcg_dot2<<<nred, 256, 0, stream>>>(N, dr, dz, nullptr, nullptr, part);
   k_pcg_scalars<<<1, 256, 0, stream>>>(part, nred, 0, sc, nullptr, 0);
   for (int i = 0; i < ns_iters; ++i) {
+    const int cur = i & 1;
     k_ns_tet_apply<R><<<tb, 256, 0, stream>>>(T, vid, jt, w, dd, sv);
-    k_ns_vertex_apply<R><<<nred, 256, 0, stream>>>(op, jv, sv, dd, dAp, part);  // Ap = A d, d'Ap
-    k_pcg_scalars<<<1, 256, 0, stream>>>(part, nred, 1, sc, nullptr, 0);         // alpha
-    k_ns_step<<<nred, 256, 0, stream>>>(N, sc, dd, dAp, dx, dr, P, op.pin, dz, part);  // x, r, z, r'z
-    k_pcg_scalars<<<1, 256, 0, stream>>>(part, nred, 4, sc, nullptr, 0);         // beta
-    k_pcg_direction<<<nb, 256, 0, stream>>>(N, sc, dz, dd);
+    k_ns_vertex_apply<R><<<nred, 256, 0, stream>>>(op, jv, sv, dd, dAp, part);           // Ap = A d, d'Ap
+    k_ns_step<<<nred, 256, 0, stream>>>(N, rTz, cur, part, nred, dd, dAp, dx, dr, P, op.pin, dz, part2);
+    k_ns_direction<<<nred, 256, 0, stream>>>(N, rTz, cur, part2, nred, dz, dd);           // beta, d
   }
   k_ns_lambda<R><<<tb, 256, 0, stream>>>(T, vid, jt, w, c, dx, d_lambda.as<R>());
   k_ns_move<R><<<nb, 256, 0, stream>>>(N, dx, pos());
   CU(cudaGetLastError());
-  if (launches) *launches += 7 + 6LL * ns_iters;
+  if (launches) *launches += 7 + 4LL * ns_iters;
   return MLX_OK;
 }
 
