@@ -320,11 +320,30 @@ __global__ void __launch_bounds__(256) k_ns_tet_apply(int T, const int4* __restr
 
 // sum over the vertex's (tet, corner) pairs of J_{t,corner}^T f_t, in the
 // CSR's fixed order.
+// Pairs go four at a time with their loads issued together (the sum keeps
+// the CSR order).
 template <typename R>
 __device__ __forceinline__ D3 ns_jtf(const PcgOp& op, const R* __restrict__ jv, const double2* __restrict__ f,
                                      int v) {
   D3 acc = d3(0.0, 0.0, 0.0);
-  for (int k = op.vt_off[v]; k < op.vt_off[v + 1]; ++k) {
+  const int k0 = op.vt_off[v], k1 = op.vt_off[v + 1];
+  int k = k0;
+  for (; k + 4 <= k1; k += 4) {
+    double2 fk[4];
+    R g[4][6];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) fk[q] = f[op.vt[k + q].x];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int c = 0; c < 6; ++c) g[q][c] = jv[(size_t)6 * (k + q) + c];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      acc = acc + d3(fk[q].x * (double)g[q][0] + fk[q].y * (double)g[q][3],
+                     fk[q].x * (double)g[q][1] + fk[q].y * (double)g[q][4],
+                     fk[q].x * (double)g[q][2] + fk[q].y * (double)g[q][5]);
+  }
+  for (; k < k1; ++k) {
     const double2 fk = f[op.vt[k].x];
     const R* g = jv + (size_t)6 * k;
     acc = acc + d3(fk.x * (double)g[0] + fk.y * (double)g[3], fk.x * (double)g[1] + fk.y * (double)g[4],
