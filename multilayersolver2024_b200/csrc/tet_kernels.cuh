@@ -285,29 +285,6 @@ __device__ __forceinline__ double stvk_residual(const V3<R> X[4], const R G[9], 
 // F + (J - 2) cof(F) of dC_D/dF cancel to O(strain) near rest, so they are
 // formed in FP64 from F; since B is stationary at rotations, rounding F to R
 // moves B only by O(strain * eps_R).  The 2x2 solve is FP64.
-// Reciprocal square root and reciprocal in FP64 by Newton-Raphson refinement
-// of an FP32 seed (y <- y (3 - b y^2) / 2 for b^-1/2, y <- y (2 - d y) for
-// d^-1; each step about doubles the correct bits, so two steps take the
-// seed's ~2^-22 to the double's rounding).  The projection's dependent chain
-// then carries no IEEE division or square root.  Arguments outside the range
-// where the float seed is accurate (|x| in [1e-36, 1e36]) take the exact
-// operation.
-__device__ __forceinline__ double nr_rsqrt(double b) {
-  if (!(b >= 1e-36 && b <= 1e36)) return 1.0 / sqrt(b);
-  double y = (double)rsqrtf((float)b);
-  y = y * (1.5 - 0.5 * b * y * y);
-  y = y * (1.5 - 0.5 * b * y * y);
-  return y;
-}
-__device__ __forceinline__ double nr_rcp(double d) {
-  const double a = fabs(d);
-  if (!(a >= 1e-36 && a <= 1e36)) return 1.0 / d;
-  double y = (double)__frcp_rn((float)d);
-  y = y * (2.0 - d * y);
-  y = y * (2.0 - d * y);
-  return y;
-}
-
 template <typename R> struct NHEval {
   double CD, CH, aD, aH;
   bool hasH;
@@ -327,18 +304,12 @@ __device__ __forceinline__ void nh_eval(const V3<R> X[4], const R G[9], double c
   double J = dot(f[0], cf[0]);
   double IC = dot(f[0], f[0]) + dot(f[1], f[1]) + dot(f[2], f[2]);
   double B = IC + J * J - 4.0 * J;
-  // C_D = sqrt(B) and 1 / C_D (0 when C_D <= 1e-12, i.e. B <= 1e-24)
-  double invCD = 0.0;
-  if (B > 1e-24) {
-    invCD = nr_rsqrt(B);
-    e.CD = B * invCD;
-  } else {
-    e.CD = sqrt(fmax(B, 0.0));
-  }
+  e.CD = sqrt(fmax(B, 0.0));
   e.hasH = cH > 0.0;
   e.CH = e.hasH ? J - 1.0 : 0.0;
   e.aD = inv_h2 * cD;
   e.aH = e.hasH ? inv_h2 * cH : 0.0;
+  const double invCD = e.CD > 1e-12 ? 1.0 / e.CD : 0.0;
   V3<R> pd[3], cr[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
@@ -376,11 +347,11 @@ __device__ __forceinline__ void nh_project(V3<R> X[4], const R minv[4], const R 
   if (e.hasH) {
     const double a11 = (double)wD + e.aD, a22 = (double)wH + e.aH, a12 = (double)wDH;
     const double b2 = -e.CH - e.aH * lam[1];
-    const double rdet = nr_rcp(a11 * a22 - a12 * a12);
+    const double rdet = 1.0 / (a11 * a22 - a12 * a12);
     dl[0] = (b1 * a22 - a12 * b2) * rdet;
     dl[1] = (a11 * b2 - a12 * b1) * rdet;
   } else {
-    dl[0] = b1 * nr_rcp((double)wD + e.aD);
+    dl[0] = b1 / ((double)wD + e.aD);
     dl[1] = 0.0;
   }
   const R d0 = (R)dl[0], d1 = (R)dl[1];
