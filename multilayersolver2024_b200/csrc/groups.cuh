@@ -29,6 +29,7 @@
 // colour launches.
 #pragma once
 
+#include "cluster.cuh"
 #include "common.cuh"
 #include "contacts.cuh"
 #include "persistent.cuh"
@@ -212,6 +213,119 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
     }
   }
   for (int i = tid; i < nv; i += nthr) stcg_r4(pos + v0 + i, rec[i]);
+}
+
+// ---------------------------------------------------------------------------
+// The same loop when a group is too large for one CTA's pass of a colour:
+// group g runs on thread-block cluster g of CS CTAs.  The group's vertex
+// range [v0, v1) is split into CS contiguous spans of ceil(nv / CS) records,
+// span r in the shared memory of rank r; a tet's corners are addressed by
+// code (rank << 24 | slot, in GroupArgs.tloc) through distributed shared
+// memory (mapa), the
+// tets of (colour, group) are split across the ranks, and colours are
+// separated by the hardware cluster barrier (release on arrive, acquire on
+// wait), between whose two halves every thread loads its tet of the next
+// colour.  Body-free layers without contacts (the batch of independent
+// scenes).  Every vertex sees the same sequence of updates as with the colour
+// launches, so results are bit-identical.
+template <typename R, int MAT, bool DAMP>
+__device__ __forceinline__ void project_cgroup(const TetData<R>& td, const TetRest<R, MAT>& r, const uint32_t a[4],
+                                               const R4<R>* __restrict__ oldp, R inv_h2, R inv_h) {
+  R4<R> p[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) dsm_ld(a[k], p[k]);
+  V3<R> X[4] = {{p[0].x, p[0].y, p[0].z}, {p[1].x, p[1].y, p[1].z}, {p[2].x, p[2].y, p[2].z},
+                {p[3].x, p[3].y, p[3].z}};
+  R minv[4] = {p[0].w, p[1].w, p[2].w, p[3].w};
+  R lnew[num_lambda<MAT>()];
+  tet_update<R, MAT, DAMP>(r, X, minv, oldp, inv_h2, inv_h, lnew);
+#pragma unroll
+  for (int q = 0; q < num_lambda<MAT>(); ++q) td.lambda[(size_t)q * td.T + r.s] = lnew[q];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) dsm_st(a[k], make_r4<R>(X[k].x, X[k].y, X[k].z, minv[k]));
+}
+
+template <typename R, int MAT, bool DAMP>
+__global__ void __launch_bounds__(kGroupThreads, 1)
+    k_layer_cgroups(TetData<R> td, GroupArgs ga, R4<R>* __restrict__ pos, const R4<R>* __restrict__ oldp,
+                    R inv_h2, R inv_h, const R* __restrict__ pin_vals) {
+  extern __shared__ __align__(32) unsigned char cg_smem[];
+  R4<R>* rec = reinterpret_cast<R4<R>*>(cg_smem);
+  const int rank = (int)cluster_rank(), CS = (int)cluster_size();
+  const int g = (int)blockIdx.x / CS;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int v0 = ga.gv0[g], nv = ga.gv0[g + 1] - v0;
+  const int span = (nv + CS - 1) / CS;
+  const int my0 = min(nv, rank * span), my1 = min(nv, (rank + 1) * span);
+  for (int i = my0 + tid; i < my1; i += nthr) rec[i - my0] = ldcg_r4(pos + v0 + i);
+  const uint32_t base = smem_u32(rec), rb = (uint32_t)sizeof(R4<R>);
+  TetRest<R, MAT> cur;
+  uint32_t ca[4] = {0, 0, 0, 0};
+  bool have = false;
+  // ga.tloc holds the corner codes (rank << 24 | slot) on this path
+  auto load = [&](int i, TetRest<R, MAT>& t, uint32_t* a) {
+    int4 c;
+    load_group_rest<R, MAT, DAMP>(td, ga, i, t, c);
+    a[0] = vcode_addr(base, c.x, rb);
+    a[1] = vcode_addr(base, c.y, rb);
+    a[2] = vcode_addr(base, c.z, rb);
+    a[3] = vcode_addr(base, c.w, rb);
+  };
+  auto fetch = [&](int c) {
+    have = false;
+    if (c >= ga.C) return;
+    const int beg = ga.off[c * ga.G + g], cnt = ga.off[c * ga.G + g + 1] - beg;
+    const int q = rank * nthr + tid;
+    if (q < cnt) {
+      load(beg + q, cur, ca);
+      have = true;
+    }
+  };
+  // colours with no tet of this group are skipped (the same for every rank)
+  auto next_colour = [&](int c) {
+    ++c;
+    while (c < ga.C && ga.off[c * ga.G + g + 1] == ga.off[c * ga.G + g]) ++c;
+    return c;
+  };
+  __syncthreads();
+  cluster_arrive();
+  if (ga.one_per_thread) fetch(next_colour(-1));
+  cluster_wait();
+  for (int it = 0; it < ga.iterations; ++it) {
+    for (int c = next_colour(-1); c < ga.C; c = next_colour(c)) {
+      if (ga.one_per_thread) {
+        if (have) project_cgroup<R, MAT, DAMP>(td, cur, ca, oldp, inv_h2, inv_h);
+      } else {
+        const int beg = ga.off[c * ga.G + g], end = ga.off[c * ga.G + g + 1];
+        for (int i = beg + rank * nthr + tid; i < end; i += CS * nthr) {
+          TetRest<R, MAT> t;
+          uint32_t a[4];
+          load(i, t, a);
+          project_cgroup<R, MAT, DAMP>(td, t, a, oldp, inv_h2, inv_h);
+        }
+      }
+      cluster_arrive();
+      if (ga.one_per_thread) {
+        const int nc = next_colour(c);
+        fetch(nc < ga.C ? nc : (it + 1 < ga.iterations ? next_colour(-1) : ga.C));
+      }
+      cluster_wait();
+    }
+    const int p0 = ga.pin_off[g], p1 = ga.pin_off[g + 1];
+    if (p1 > p0) {
+      for (int i = p0 + rank * nthr + tid; i < p1; i += CS * nthr) {
+        const int d = ga.pin_dofs[i];
+        const int off = d / 3 - v0;
+        const uint32_t a = mapa_rank(base + (uint32_t)(off % span) * rb + (uint32_t)((d % 3) * sizeof(R)),
+                                     (unsigned)(off / span));
+        dsm_st1(a, pin_vals[i]);
+      }
+      cluster_arrive();
+      cluster_wait();
+    }
+  }
+  // every remote access ended at the last barrier: write this rank's span back
+  for (int i = my0 + tid; i < my1; i += nthr) stcg_r4(pos + v0 + i, rec[i - my0]);
 }
 
 }  // namespace mlx

@@ -481,6 +481,7 @@ struct Solver final : SolverBase {
   // skips the estimate.
   bool groups_ok = false;
   int gr_G = 0;
+  int gr_cs = 1;  // CTAs per group (a thread-block cluster when > 1)
   size_t gr_smem = 0;
   std::vector<int> tgroup_sorted;  // group of each tet, sorted order
   DevBuf d_gv0, d_tloc, d_gpin;
@@ -541,6 +542,10 @@ struct Solver final : SolverBase {
   long long sim_launches_per_step() const override { return sim.launches_per_step; }
   std::string launch_path() const override {
     if (persistent) return "persistent cooperative kernel per layer (" + std::to_string(persist_ctas) + " CTAs)";
+    if (groups_ok && !cluster_ok && gr_cs > 1)
+      return "body-free layers: one launch, " + std::to_string(gr_G) + " clusters of " + std::to_string(gr_cs) +
+             " CTAs each owning whole components (records in distributed shared memory); other layers: one launch "
+             "per colour (programmatic dependent launches)";
     if (groups_ok && !cluster_ok)
       return "body-free layers: one launch, " + std::to_string(gr_G) + " CTAs each owning whole components "
              "(records in shared memory); other layers: one launch per colour (programmatic dependent launches)";
@@ -889,6 +894,20 @@ static const void* group_kernel(int mat_kind, bool damp, int mode = 0) {
 // sweep is estimated shorter than the colour launches' (one dependent launch
 // per colour, ~2.6 us, plus the colour's bytes at ~6.5 TB/s).
 template <typename R>
+static const void* cgroup_kernel(int mat_kind, bool damp) {
+  switch (mat_kind) {
+    case MAT_NH:
+      return (const void*)k_layer_cgroups<R, MAT_NH, false>;
+    case MAT_STVK_BLOCKS:
+      return damp ? (const void*)k_layer_cgroups<R, MAT_STVK_BLOCKS, true>
+                  : (const void*)k_layer_cgroups<R, MAT_STVK_BLOCKS, false>;
+    default:
+      return damp ? (const void*)k_layer_cgroups<R, MAT_STVK_LAME, true>
+                  : (const void*)k_layer_cgroups<R, MAT_STVK_LAME, false>;
+  }
+}
+
+template <typename R>
 int Solver<R>::plan_groups(const mlx_mesh_desc* md) {
   groups_ok = false;
   const char* env = std::getenv("MLXPBD_GROUPS");
@@ -941,50 +960,108 @@ int Solver<R>::plan_groups(const mlx_mesh_desc* md) {
   int optin = 0, sms = 0;
   CU(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
   CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-  const void* fn = group_kernel<R>(mat_kind, damp);
-  cudaFuncAttributes fa;
-  CU(cudaFuncGetAttributes(&fa, fn));
-  const long long budget = (long long)optin - (long long)fa.sharedSizeBytes - 1024;
-  const long long vmax = budget / (long long)sizeof(R4<R>);
-  std::vector<int> gv0{0}, acc(C, 0);
-  long long gv = 0, max_gv = 0, max_passes = 0, gt = 0;
-  // a group closes once it holds T / SMs tets, so many small components
-  // spread over all SMs instead of filling fewer CTAs to the colour limit
-  const long long target = ((long long)T + sms - 1) / sms;
-  auto passes = [&]() {
-    long long n = 0;
-    for (int q = 0; q < C; ++q) n += (acc[q] + kGroupThreads - 1) / kGroupThreads;
-    return n;
+  // Groups for cs CTAs each (cs = 1: one CTA; cs > 1: a thread-block cluster
+  // whose CTAs hold contiguous spans of the group's vertex records).  A group
+  // takes components while every colour still fits one pass of its cs CTAs
+  // and closes once it holds cs * T / SMs tets, so many small components
+  // spread over all SMs.  Returns the estimated sweep (us), or < 0.
+  struct Plan {
+    std::vector<int> gv0;
+    long long max_span = 0;
+    double t = -1;
   };
-  for (int c = 0; c < ncomp; ++c) {
-    const long long nv = cv0[c + 1] - cv0[c];
-    if (nv > vmax) return MLX_OK;
-    bool fits = gv + nv <= vmax;
-    for (int q = 0; q < C && fits; ++q) fits = acc[q] + ccol[(size_t)c * C + q] <= kGroupThreads;
-    if (gv > 0 && (!fits || gt >= target)) {
-      gv0.push_back(cv0[c]);
+  auto form = [&](int cs, Plan& pl) -> double {
+    const void* fn = cs == 1 ? group_kernel<R>(mat_kind, damp) : cgroup_kernel<R>(mat_kind, damp);
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, fn) != cudaSuccess) { cudaGetLastError(); return -1; }
+    const long long budget = (long long)optin - (long long)fa.sharedSizeBytes - 1024;
+    const long long vmax = budget / (long long)sizeof(R4<R>) * cs;  // records of one group
+    const long long cap = (long long)cs * kGroupThreads;
+    std::vector<int> gv0{0}, acc(C, 0);
+    long long gv = 0, max_gv = 0, max_passes = 0, gt = 0, max_span = 0;
+    const long long target = ((long long)T * cs + sms - 1) / sms;
+    auto passes = [&]() {
+      long long n = 0;
+      for (int q = 0; q < C; ++q) n += (acc[q] + cap - 1) / cap;
+      return n;
+    };
+    auto close = [&]() {
       max_gv = std::max(max_gv, gv);
+      max_span = std::max(max_span, (gv + cs - 1) / cs);
       max_passes = std::max(max_passes, passes());
-      std::fill(acc.begin(), acc.end(), 0);
-      gv = 0;
-      gt = 0;
+    };
+    for (int c = 0; c < ncomp; ++c) {
+      const long long nv = cv0[c + 1] - cv0[c];
+      if (nv > vmax) return -1;
+      bool fits = gv + nv <= vmax;
+      for (int q = 0; q < C && fits; ++q) fits = acc[q] + ccol[(size_t)c * C + q] <= cap;
+      if (gv > 0 && (!fits || gt >= target)) {
+        gv0.push_back(cv0[c]);
+        close();
+        std::fill(acc.begin(), acc.end(), 0);
+        gv = 0;
+        gt = 0;
+      }
+      for (int q = 0; q < C; ++q) {
+        acc[q] += ccol[(size_t)c * C + q];
+        gt += ccol[(size_t)c * C + q];
+      }
+      gv += nv;
     }
-    for (int q = 0; q < C; ++q) {
-      acc[q] += ccol[(size_t)c * C + q];
-      gt += ccol[(size_t)c * C + q];
+    gv0.push_back(N);
+    close();
+    const long long G = (long long)gv0.size() - 1;
+    long long resident = sms;  // groups in flight at once
+    double per_phase = 2.0;    // us: the dependent chain of one projection
+    if (cs > 1) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3((unsigned)(cs * std::min<long long>(G, 1 << 16)));
+      cfg.blockDim = dim3(kGroupThreads);
+      cfg.dynamicSmemBytes = (size_t)max_span * sizeof(R4<R>);
+      cudaLaunchAttribute a;
+      a.id = cudaLaunchAttributeClusterDimension;
+      a.val.clusterDim.x = cs;
+      a.val.clusterDim.y = 1;
+      a.val.clusterDim.z = 1;
+      cfg.attrs = &a;
+      cfg.numAttrs = 1;
+      int ncl = 0;
+      if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)std::max<size_t>(cfg.dynamicSmemBytes, 16)) != cudaSuccess ||
+          cudaOccupancyMaxActiveClusters(&ncl, fn, &cfg) != cudaSuccess || ncl < 1) {
+        cudaGetLastError();
+        return -1;
+      }
+      resident = ncl;
+      per_phase = 2.7;  // + the cluster barrier after remote stores
     }
-    gv += nv;
-  }
-  gv0.push_back(N);
-  max_gv = std::max(max_gv, gv);
-  max_passes = std::max(max_passes, passes());
-  const int G = (int)gv0.size() - 1;
-  // estimated sweeps (us); one CTA per SM, so more groups than SMs run in waves
-  const double t_groups = 2.0 * (double)max_passes * (double)((G + sms - 1) / sms);
+    pl.gv0 = gv0;
+    pl.max_span = max_span;
+    pl.t = per_phase * (double)max_passes * (double)((G + resident - 1) / resident);
+    return pl.t;
+  };
   double t_colours = 0;
   for (int q = 0; q < C; ++q)
     if (colcount[q]) t_colours += 2.6 + (double)colcount[q] * (double)bytes_per_tet() / 6.5e6;
-  if (!force && t_groups >= t_colours) return MLX_OK;
+  int cs_force = 0;
+  if (const char* f = std::getenv("MLXPBD_GROUP_CS")) cs_force = std::atoi(f);
+  Plan best;
+  int best_cs = 0;
+  for (int cs : {1, 2, 4, 8}) {
+    if (cs_force > 0 && cs != cs_force) continue;
+    Plan pl;
+    const double t = form(cs, pl);
+    if (t < 0) continue;
+    if (best_cs == 0 || t < best.t) {
+      best = pl;
+      best_cs = cs;
+    }
+  }
+  if (best_cs == 0) return MLX_OK;
+  if (!force && cs_force <= 0 && best.t >= t_colours) return MLX_OK;
+  const std::vector<int>& gv0 = best.gv0;
+  const int G = (int)gv0.size() - 1;
+  const int cs = best_cs;
   // each group's pins must be one range of the pinned list, in group order
   // (true when the list is ascending); a group applies its range in order
   std::vector<int> gpin(G + 1, 0);
@@ -998,7 +1075,8 @@ int Solver<R>::plan_groups(const mlx_mesh_desc* md) {
     }
     for (int q = 0; q < G; ++q) gpin[q + 1] += gpin[q];
   }
-  // group of every tet (sorted order) and its corner slots
+  // group of every tet (sorted order) and its corner slots (cs = 1: vertex -
+  // v0; cs > 1: rank << 24 | slot in that rank's span of ceil(nv / cs))
   tgroup_sorted.assign(T, 0);
   std::vector<int4> tloc(T);
   for (int sidx = 0; sidx < T; ++sidx) {
@@ -1006,13 +1084,25 @@ int Solver<R>::plan_groups(const mlx_mesh_desc* md) {
     const int g = (int)(std::upper_bound(gv0.begin(), gv0.end(), v.x) - gv0.begin()) - 1;
     tgroup_sorted[sidx] = g;
     const int b = gv0[g];
-    tloc[sidx] = make_int4(v.x - b, v.y - b, v.z - b, v.w - b);
+    if (cs == 1) {
+      tloc[sidx] = make_int4(v.x - b, v.y - b, v.z - b, v.w - b);
+    } else {
+      const int span = (gv0[g + 1] - b + cs - 1) / cs;
+      auto code = [&](int u) { return (((u - b) / span) << 24) | ((u - b) % span); };
+      tloc[sidx] = make_int4(code(v.x), code(v.y), code(v.z), code(v.w));
+    }
   }
-  gr_smem = (size_t)max_gv * sizeof(R4<R>);
-  CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(gr_smem, 16)));
-  for (int mode = 1; mode <= 2; ++mode)
-    CU(cudaFuncSetAttribute(group_kernel<R>(mat_kind, damp, mode), cudaFuncAttributeMaxDynamicSharedMemorySize,
+  gr_smem = (size_t)best.max_span * sizeof(R4<R>);
+  if (cs == 1) {
+    CU(cudaFuncSetAttribute(group_kernel<R>(mat_kind, damp), cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)std::max<size_t>(gr_smem, 16)));
+    for (int mode = 1; mode <= 2; ++mode)
+      CU(cudaFuncSetAttribute(group_kernel<R>(mat_kind, damp, mode), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)std::max<size_t>(gr_smem, 16)));
+  } else {
+    CU(cudaFuncSetAttribute(cgroup_kernel<R>(mat_kind, damp), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)std::max<size_t>(gr_smem, 16)));
+  }
   CHECK(d_gv0.ensure(sizeof(int) * gv0.size()));
   CHECK(d_tloc.ensure(sizeof(int4) * (size_t)T));
   CHECK(d_gpin.ensure(sizeof(int) * gpin.size()));
@@ -1021,6 +1111,7 @@ int Solver<R>::plan_groups(const mlx_mesh_desc* md) {
   CU(cudaMemcpyAsync(d_gpin.p, gpin.data(), sizeof(int) * gpin.size(), cudaMemcpyHostToDevice, stream));
   CU(cudaStreamSynchronize(stream));
   gr_G = G;
+  gr_cs = cs;
   groups_ok = true;
   return MLX_OK;
 }
@@ -1072,6 +1163,37 @@ int Solver<R>::launch_groups(const LayerStatic& ls, const int* dint, const mlx_s
   const R4<R>* oldp = d_oldp.as<R4<R>>();
   const R* pv = d_pinx.as<R>();
   const double h = P->h, cr = P->contact_resistance;
+  if (gr_cs > 1) {
+    // a cluster of gr_cs CTAs per group (no contact phase on this path)
+    cfg.gridDim = dim3(gr_G * gr_cs);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = gr_cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e;
+    switch (mat_kind) {
+      case MAT_NH:
+        e = cudaLaunchKernelEx(&cfg, k_layer_cgroups<R, MAT_NH, false>, td, ga, pos(), oldp, inv_h2, inv_h, pv);
+        break;
+      case MAT_STVK_BLOCKS:
+        e = damp ? cudaLaunchKernelEx(&cfg, k_layer_cgroups<R, MAT_STVK_BLOCKS, true>, td, ga, pos(), oldp, inv_h2,
+                                      inv_h, pv)
+                 : cudaLaunchKernelEx(&cfg, k_layer_cgroups<R, MAT_STVK_BLOCKS, false>, td, ga, pos(), oldp, inv_h2,
+                                      inv_h, pv);
+        break;
+      default:
+        e = damp ? cudaLaunchKernelEx(&cfg, k_layer_cgroups<R, MAT_STVK_LAME, true>, td, ga, pos(), oldp, inv_h2,
+                                      inv_h, pv)
+                 : cudaLaunchKernelEx(&cfg, k_layer_cgroups<R, MAT_STVK_LAME, false>, td, ga, pos(), oldp, inv_h2,
+                                      inv_h, pv);
+    }
+    if (e != cudaSuccess)
+      return set_error(MLX_ERR_CUDA, std::string("cluster group layer launch: ") + cudaGetErrorString(e));
+    return MLX_OK;
+  }
   HostContactGroups none{};
   const HostContactGroups& hg_ = hc ? *hc : none;
   const cudaError_t e =
@@ -1372,7 +1494,7 @@ int Solver<R>::build_static(const mlx_layer_desc* ld, int col, LayerStatic& ls, 
         }
       }
       goff[(size_t)C * G] = ls.identity_list ? T : (int)list.size();
-      ls.gr_one = maxr <= kGroupThreads ? 1 : 0;
+      ls.gr_one = maxr <= gr_cs * kGroupThreads ? 1 : 0;
       ls.o_goff = put(goff);
       ls.gr_ok = true;
     }
@@ -1845,7 +1967,7 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
       }
       continue;
     }
-    if (groups_ok && ls.gr_ok && ls.nb == 0 && !P->compute_residuals) {
+    if (groups_ok && ls.gr_ok && ls.nb == 0 && !P->compute_residuals && (gr_cs == 1 || (!dc.nobs && nK == 0))) {
       // a body-free layer with a fixed iteration count: one launch, a CTA per
       // group of components
       const int iters = std::max(ld->iterations[layer], 0);

@@ -12,7 +12,10 @@ the colour launches: positions bit-identical at every step, for
     FP32 and FP64;
   * the single-component cantilever of config 1 with the path forced, FP64,
     which also matches the oracle;
-  * 64 copies of that cantilever in one mesh, FP32.
+  * 64 copies of that cantilever in one mesh, FP32;
+  * batches of blocks on clusters of 2 and 4 CTAs per group (records in
+    distributed shared memory), with colours that fit one pass of the
+    cluster and colours that need several, FP32 and FP64.
 """
 import numpy as np
 import pytest
@@ -177,3 +180,18 @@ def test_host_layer_solve_graph_replay_is_bit_identical(gpu, monkeypatch):
     a, b = run("1"), run("0")
     for k in range(len(a)):
         np.testing.assert_array_equal(a[k], b[k], err_msg=f"frame {k + 1}")
+
+
+@pytest.mark.parametrize("cs,precision,dims", [
+    (2, _lib.MLX_FP32, (1500, 6000)),
+    (4, _lib.MLX_FP32, (1500, 6000)),
+    (2, _lib.MLX_FP32, (30000, 40000)),   # colours of a group exceed one pass of the cluster
+    (4, _lib.MLX_FP64, (1500, 6000)),
+])
+def test_batch_on_thread_block_clusters(gpu, monkeypatch, cs, precision, dims):
+    monkeypatch.setenv("MLXPBD_GROUP_CS", str(cs))
+    got = _same(monkeypatch, lambda: scenes.config3(seed=7, n_scenes=5, tmin=dims[0], tmax=dims[1]), 3, precision)
+    _, path = _run(monkeypatch, lambda: scenes.config3(seed=7, n_scenes=5, tmin=dims[0], tmax=dims[1]), "1", 1,
+                   precision)
+    assert f"clusters of {cs} CTAs" in path, path
+    assert np.all(np.isfinite(got[-1]))
