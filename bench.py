@@ -651,10 +651,10 @@ def run_ours(args, rank, world, local):
             if to_res["value_leg"] == "learned_pcg":
                 # each Newton-PCG correction: 7 launches + 4 per PCG iteration, one before the fine layer
                 # and one after every `every` of its iterations (the fine layer holds most iterations)
-                per_corr = 7 + 4 * args.layer_pcg
+                per_corr = 7 + 2 * args.layer_pcg
                 launches += int(sum((1 + max(it - 1, 0) // max(args.layer_pcg_every, 1)) * per_corr
                                     for it in iters_le))
-                launch_note += " + Newton-PCG corrections x (7 + 4 x PCG iterations)"
+                launch_note += " + Newton-PCG corrections x (7 + 2 x PCG iterations)"
         else:
             value, ms_per_step = fixed_value, fixed_max_ms / args.steps
             solver_desc = "plain multi-layer (no warm-start), fixed iteration counts"

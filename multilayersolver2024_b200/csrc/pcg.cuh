@@ -163,6 +163,7 @@ struct PcgScalars {
   double dAp;    // d'Ap
   double rTz_new;
   double res;    // ||A x - b||
+  unsigned int count[2];  // last-block counts of the Newton-PCG grid reductions (0 between launches)
 };
 
 // Sums the partials (one block of 256) and updates the scalars:
@@ -306,16 +307,12 @@ __device__ __forceinline__ double2 ns_ju(const R* __restrict__ jt, int T, int s,
   return make_double2(d0, d1);
 }
 
-// s_t = W_t (J_t u) for every tet.
-template <typename R>
-__global__ void __launch_bounds__(256) k_ns_tet_apply(int T, const int4* __restrict__ vid, const R* __restrict__ jt,
-                                                      const double2* __restrict__ w, const double4* __restrict__ u,
-                                                      double2* __restrict__ out) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= T) return;
-  const double2 ju = ns_ju<R>(jt, T, s, vid[s], u);
-  const double2 ws = w[s];
-  out[s] = make_double2(ws.x * ju.x, ws.y * ju.y);
+// The search direction at vertex v for this iteration: d_k = z_k + beta d_{k-1}
+// (beta from the previous iteration's r'z; beta = 0 and d = 0 at the start).
+// Every row that reads vertex v evaluates it with the same fused
+// multiply-add, so all see the bits that v's own row stores.
+__device__ __forceinline__ double4 ns_dir(const double4 z, const double4 d, double beta) {
+  return make_double4(__fma_rn(beta, d.x, z.x), __fma_rn(beta, d.y, z.y), __fma_rn(beta, d.z, z.z), 0.0);
 }
 
 // sum over the vertex's (tet, corner) pairs of J_{t,corner}^T f_t, in the
@@ -362,48 +359,228 @@ __global__ void k_ns_rhs(PcgOp op, const R* __restrict__ jv, const double2* __re
   y[v] = make_double4((pm & 1) ? 0.0 : -a.x, (pm & 2) ? 0.0 : -a.y, (pm & 4) ? 0.0 : -a.z, 0.0);
 }
 
-// y = M u + J^T f on the unpinned DOFs, and the partial sums of u'y (one per
-// block, at partials[2 b]; grid-stride over the vertices, fixed order).
+// Lanes per row in the blocked product: a vertex of a tet mesh shares tets
+// with ~14 others; eight lanes take two blocks each, so the pass has eight
+// times the threads (and loads in flight) of one lane per row.
+constexpr int kNsTeam = 8;
+// Largest grid of a Newton-PCG grid reduction (one partial sum per block).
+constexpr int kNsMaxPartials = 2048;
+
+// The block's partial sum of a grid reduction goes to partials[blockIdx.x];
+// the last block to finish (an atomic count, after a fence) sums all of them
+// in index order, which does not depend on which block that is, and resets
+// the count for the next launch.  Returns true in that block, with the sum in
+// `total` (all its threads).
+__device__ __forceinline__ bool ns_last_block(double mine, double* __restrict__ partials,
+                                              unsigned int* __restrict__ count, double& total) {
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = mine;
+    __threadfence();
+    last = atomicAdd(count, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+  double s[1] = {0.0};
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) s[0] += __ldcg(partials + i);
+  block_sum<1>(s);
+  total = s[0];
+  if (threadIdx.x == 0) *count = 0u;
+  return true;
+}
+
+// J^T W J assembled into 3x3 blocks per (vertex, neighbour) once per
+// correction, so that each PCG iteration reads one blocked sparse matrix
+// (~15 blocks per vertex) instead of passing twice over the Jacobian.
+// Row v lists the vertices sharing a tet with v (itself included), in
+// increasing order: nb_off[N+1], nb_col[nnz]; block j of the matrix is
+// K[9 j + r + 3 c] (column-major) = sum over the tets t holding v (corner a)
+// and nb_col[j] (corner b) of wD gD_a gD_b' + wH gH_a gH_b'.
+// pslot[k] holds, for pair k = (t, a) of the vertex CSR, the row slot of each
+// corner b of t (byte b).
+struct NsBlocks {
+  const int* nb_off;         // [N+1]
+  const int* nb_col;         // [nnz]
+  const unsigned int* pslot; // [pairs] four row slots, one byte per corner
+  const int* vtpos;          // [4T] CSR position of pair (t, b)
+};
+
+// One warp per row (grid-stride over the rows), 32 pairs at a time: lane p
+// stages pair p (its tet's four corner gradients from the CSR-order
+// Jacobian, the tet's weights, the corners' row slots) in shared memory;
+// then lane l, the owner of slots l, l + 32, ..., sums the staged pairs'
+// contributions to its slots in CSR order -- the same order every run, no
+// atomics.  The owner of the row's diagonal block also writes the inverse of
+// M + K_vv (pinned rows and columns replaced by the identity): the
+// block-Jacobi preconditioner.
+constexpr int kNsAsmWarps = 4;
+
+struct NsStage {
+  double g[32][4][6];     // corner b's two gradient rows (D: 0..2, H: 3..5)
+  double2 w[32];          // (wD, wH)
+  unsigned int slot[32];  // byte b: row slot of corner b
+  int corner[32];         // the row's own corner a
+};
+
 template <typename R>
-__global__ void __launch_bounds__(256) k_ns_vertex_apply(PcgOp op, const R* __restrict__ jv,
-                                                         const double2* __restrict__ f, const double4* __restrict__ u,
-                                                         double4* __restrict__ y, double* __restrict__ partials) {
+__global__ void __launch_bounds__(32 * kNsAsmWarps) k_ns_assemble(PcgOp op, NsBlocks nb, const R* __restrict__ jv,
+                                                                  const double2* __restrict__ w,
+                                                                  R* __restrict__ K, double* __restrict__ Pinv) {
+  __shared__ NsStage stage[kNsAsmWarps];
+  NsStage& st = stage[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const int nwarps = gridDim.x * kNsAsmWarps;
+  for (int v = blockIdx.x * kNsAsmWarps + (threadIdx.x >> 5); v < op.N; v += nwarps) {
+    const int k0 = op.vt_off[v], k1 = op.vt_off[v + 1];
+    const int r0 = nb.nb_off[v], rn = nb.nb_off[v + 1] - r0;
+    for (int base = 0; base < rn; base += 32) {
+      const int mine = base + lane;
+      // every byte of the pattern is this lane's slot (slots are < 255)
+      const unsigned int rep = mine < rn ? (unsigned int)mine * 0x01010101u : 0xffffffffu;
+      double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (int p0 = k0; p0 < k1; p0 += 32) {
+        const int np = min(32, k1 - p0);
+        __syncwarp();
+        if (lane < np) {
+          const int k = p0 + lane;
+          const int2 tk = op.vt[k];
+          const int4 pos4 = *reinterpret_cast<const int4*>(nb.vtpos + 4 * (size_t)tk.x);
+          const int pk[4] = {pos4.x, pos4.y, pos4.z, pos4.w};
+#pragma unroll
+          for (int b = 0; b < 4; ++b)
+#pragma unroll
+            for (int c = 0; c < 6; ++c) st.g[lane][b][c] = (double)jv[(size_t)6 * pk[b] + c];
+          st.w[lane] = w[tk.x];
+          st.slot[lane] = nb.pslot[k];
+          st.corner[lane] = tk.y;
+        }
+        __syncwarp();
+        // bit 4 q + b of word wd: corner b of staged pair 8 wd + q lies in
+        // this lane's slot (a byte compare, then the four match bits of a
+        // word gathered by one multiply: byte b's bit lands on bit 24 + b)
+        unsigned int mw[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+        for (int wd = 0; wd < 4; ++wd)
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const int p = 8 * wd + q;
+            if (p < np) {
+              const unsigned int x = __vcmpeq4(st.slot[p], rep) & 0x01010101u;
+              mw[wd] |= ((x * 0x01020408u) >> 24) << (4 * q);
+            }
+          }
+        // the matches in pair order, then corner order
+#pragma unroll
+        for (int wd = 0; wd < 4; ++wd) {
+          unsigned int m = mw[wd];
+          while (m) {
+            const int bit = __ffs(m) - 1;
+            m &= m - 1u;
+            const int p = 8 * wd + (bit >> 2), b = bit & 3;
+            const double* ga = st.g[p][st.corner[p]];
+            const double* gb = st.g[p][b];
+            const double2 wk = st.w[p];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              const double bD = wk.x * gb[c], bH = wk.y * gb[3 + c];
+#pragma unroll
+              for (int r = 0; r < 3; ++r) acc[r + 3 * c] += ga[r] * bD + ga[3 + r] * bH;
+            }
+          }
+        }
+      }
+      if (mine < rn) {
+        R* kb = K + (size_t)9 * (r0 + mine);
+#pragma unroll
+        for (int q = 0; q < 9; ++q) kb[q] = (R)acc[q];
+        if (nb.nb_col[r0 + mine] == v) {
+          const double m = op.vmass[v];
+          double B[9];
+#pragma unroll
+          for (int q = 0; q < 9; ++q) B[q] = acc[q];
+          B[0] += m;
+          B[4] += m;
+          B[8] += m;
+          const unsigned char pm = op.pin[v];
+#pragma unroll
+          for (int d = 0; d < 3; ++d)
+            if (pm & (1 << d)) {
+              for (int k = 0; k < 3; ++k) B[d + 3 * k] = B[k + 3 * d] = 0.0;
+              B[d + 3 * d] = 1.0;
+            }
+          double inv[9];
+          inverse3(B, inv);
+#pragma unroll
+          for (int q = 0; q < 9; ++q) Pinv[9 * (size_t)v + q] = inv[q];
+        }
+      }
+    }
+  }
+}
+
+// Ap = M d_k + K d_k on the unpinned DOFs, with d_k = z + beta d_{k-1} formed
+// at every column (d_{k-1} from `dprev`) and stored for the row in `dnext`
+// (the two direction buffers alternate between iterations, so no row reads a
+// direction another row has already replaced).  A team of kNsTeam lanes per
+// row, each lane every kNsTeam-th block, a fixed butterfly over the team
+// (lane 0's sum), d_k'Ap summed per block; the last block sets alpha.
+template <typename R>
+__global__ void __launch_bounds__(256) k_ns_spmv(PcgOp op, NsBlocks nb, const R* __restrict__ K,
+                                                 const double4* __restrict__ z, const double4* __restrict__ dprev,
+                                                 double4* __restrict__ dnext, double4* __restrict__ Ap,
+                                                 PcgScalars* __restrict__ sc, double* __restrict__ partials,
+                                                 unsigned int* __restrict__ count) {
+  const double beta = sc->beta;
+  const int lane = threadIdx.x & (kNsTeam - 1);
+  const unsigned mask = ((1u << kNsTeam) - 1u) << ((threadIdx.x & 31) & ~(kNsTeam - 1));
+  const int nteams = gridDim.x * (blockDim.x / kNsTeam);
   double dot[1] = {0.0};
-  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < op.N; v += gridDim.x * blockDim.x) {
-    const D3 a = ns_jtf<R>(op, jv, f, v);
-    const double m = op.vmass[v];
-    const double4 uv = u[v];
-    const unsigned char pm = op.pin[v];
-    const double4 yv = make_double4((pm & 1) ? 0.0 : a.x + m * uv.x, (pm & 2) ? 0.0 : a.y + m * uv.y,
-                                    (pm & 4) ? 0.0 : a.z + m * uv.z, 0.0);
-    y[v] = yv;
-    dot[0] += uv.x * yv.x + uv.y * yv.y + uv.z * yv.z;
+  for (int v = blockIdx.x * (blockDim.x / kNsTeam) + threadIdx.x / kNsTeam; v < op.N; v += nteams) {
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    const int j1 = nb.nb_off[v + 1];
+    for (int j = nb.nb_off[v] + lane; j < j1; j += kNsTeam) {
+      const int c = nb.nb_col[j];
+      const double4 u = ns_dir(z[c], dprev[c], beta);
+      const R* kb = K + (size_t)9 * j;
+      ax += (double)kb[0] * u.x + (double)kb[3] * u.y + (double)kb[6] * u.z;
+      ay += (double)kb[1] * u.x + (double)kb[4] * u.y + (double)kb[7] * u.z;
+      az += (double)kb[2] * u.x + (double)kb[5] * u.y + (double)kb[8] * u.z;
+    }
+#pragma unroll
+    for (int o = kNsTeam / 2; o > 0; o >>= 1) {
+      ax += __shfl_xor_sync(mask, ax, o);
+      ay += __shfl_xor_sync(mask, ay, o);
+      az += __shfl_xor_sync(mask, az, o);
+    }
+    if (lane == 0) {
+      const double4 dk = ns_dir(z[v], dprev[v], beta);
+      dnext[v] = dk;
+      const double m = op.vmass[v];
+      const unsigned char pm = op.pin[v];
+      const double4 yv = make_double4((pm & 1) ? 0.0 : ax + m * dk.x, (pm & 2) ? 0.0 : ay + m * dk.y,
+                                      (pm & 4) ? 0.0 : az + m * dk.z, 0.0);
+      Ap[v] = yv;
+      dot[0] += dk.x * yv.x + dk.y * yv.y + dk.z * yv.z;
+    }
   }
   block_sum<1>(dot);
-  if (threadIdx.x == 0) partials[2 * blockIdx.x] = dot[0];
+  double dAp;
+  if (ns_last_block(dot[0], partials, count, dAp) && threadIdx.x == 0) {
+    sc->dAp = dAp;
+    sc->alpha = dAp == 0.0 ? 0.0 : sc->rTz / dAp;
+  }
 }
 
-// Sum of the n partials of a fixed-order reduction (the same order in every
-// block, so every block obtains the same value).
-__device__ __forceinline__ double ns_sum_partials(const double* __restrict__ partials, int n) {
-  double s[1] = {0.0};
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s[0] += partials[2 * i];
-  block_sum<1>(s);
-  return s[0];
-}
-
-// alpha = rTz[cur] / d'Ap (0 when d'Ap = 0) from the partials of d'Ap; then
-// x += alpha d, r -= alpha Ap, z = P r, and the partial sums of r'z (one per
-// block at partials2[2 b]; grid-stride, fixed order).
-__global__ void __launch_bounds__(256) k_ns_step(int N, const double* __restrict__ rTz, int cur,
-                                                 const double* __restrict__ partials, int nparts,
-                                                 const double4* __restrict__ d, const double4* __restrict__ Ap,
-                                                 double4* __restrict__ x, double4* __restrict__ r,
-                                                 const double* __restrict__ Pinv,
+// x += alpha d_k, r -= alpha Ap, z = P r (grid-stride, fixed order), and r'z:
+// the last block sets beta = r'z / rTz (0 when rTz = 0) and rTz = r'z for the
+// next iteration.
+__global__ void __launch_bounds__(256) k_ns_step(int N, PcgScalars* __restrict__ sc, const double4* __restrict__ d,
+                                                 const double4* __restrict__ Ap, double4* __restrict__ x,
+                                                 double4* __restrict__ r, const double* __restrict__ Pinv,
                                                  const unsigned char* __restrict__ pin, double4* __restrict__ z,
-                                                 double* __restrict__ partials2) {
-  const double dAp = ns_sum_partials(partials, nparts);
-  const double alpha = dAp == 0.0 ? 0.0 : rTz[cur] / dAp;
+                                                 double* __restrict__ partials, unsigned int* __restrict__ count) {
+  const double alpha = sc->alpha;
   double dot[1] = {0.0};
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < N; v += gridDim.x * blockDim.x) {
     const double4 dv = d[v], av = Ap[v], xv = x[v], rv = r[v];
@@ -417,54 +594,12 @@ __global__ void __launch_bounds__(256) k_ns_step(int N, const double* __restrict
     dot[0] += rn.x * zn.x + rn.y * zn.y + rn.z * zn.z;
   }
   block_sum<1>(dot);
-  if (threadIdx.x == 0) partials2[2 * blockIdx.x] = dot[0];
-}
-
-// rTz_new from the partials of r'z; beta = rTz_new / rTz[cur] (0 when
-// rTz[cur] = 0); d = z + beta d; block 0 stores rTz_new in rTz[1 - cur] for
-// the next iteration (r'z is double-buffered: every block reads rTz[cur]).
-__global__ void __launch_bounds__(256) k_ns_direction(int N, double* __restrict__ rTz, int cur,
-                                                      const double* __restrict__ partials, int nparts,
-                                                      const double4* __restrict__ z, double4* __restrict__ d) {
-  const double rtz_new = ns_sum_partials(partials, nparts);
-  const double old = rTz[cur];
-  const double beta = old == 0.0 ? 0.0 : rtz_new / old;
-  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < N; v += gridDim.x * blockDim.x) {
-    const double4 zv = z[v], dv = d[v];
-    d[v] = make_double4(zv.x + beta * dv.x, zv.y + beta * dv.y, zv.z + beta * dv.z, 0.0);
+  double rtz;
+  if (ns_last_block(dot[0], partials, count, rtz) && threadIdx.x == 0) {
+    sc->rTz_new = rtz;
+    sc->beta = sc->rTz == 0.0 ? 0.0 : rtz / sc->rTz;
+    sc->rTz = rtz;
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) rTz[1 - cur] = rtz_new;
-}
-
-// Inverse of the 3x3 diagonal block of M + J^T W J at every vertex (pinned
-// rows and columns replaced by the identity).
-template <typename R>
-__global__ void k_ns_block_jacobi(PcgOp op, const R* __restrict__ jv, const double2* __restrict__ w,
-                                  double* __restrict__ Pinv) {
-  const int v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= op.N) return;
-  const double m = op.vmass[v];
-  double B[9] = {m, 0, 0, 0, m, 0, 0, 0, m};
-  for (int k = op.vt_off[v]; k < op.vt_off[v + 1]; ++k) {
-    const double2 wk = w[op.vt[k].x];
-    const R* g = jv + (size_t)6 * k;
-    const double gD[3] = {(double)g[0], (double)g[1], (double)g[2]};
-    const double gH[3] = {(double)g[3], (double)g[4], (double)g[5]};
-#pragma unroll
-    for (int j = 0; j < 3; ++j)
-#pragma unroll
-      for (int i = 0; i < 3; ++i) B[i + 3 * j] += wk.x * gD[i] * gD[j] + wk.y * gH[i] * gH[j];
-  }
-  const unsigned char pm = op.pin[v];
-#pragma unroll
-  for (int d = 0; d < 3; ++d)
-    if (pm & (1 << d)) {
-      for (int k = 0; k < 3; ++k) B[d + 3 * k] = B[k + 3 * d] = 0.0;
-      B[d + 3 * d] = 1.0;
-    }
-  double inv[9];
-  inverse3(B, inv);
-  for (int i = 0; i < 9; ++i) Pinv[9 * (size_t)v + i] = inv[i];
 }
 
 // lambda = -W (C + J dx) for every tet (rows 0 and 1; an absent C_H keeps 0).

@@ -428,8 +428,10 @@ struct Solver final : SolverBase {
   // Newton-PCG corrections of the last layer (pcg.cuh k_ns_*): PCG
   // iterations per correction (0: off) and Gauss-Seidel iterations between
   // corrections
-  int ns_iters = 0, ns_every = 0;
-  DevBuf d_ns_jac, d_ns_tet, d_vtpos;
+  int ns_iters = 0, ns_every = 0, ns_vertex_blocks = 1;
+  DevBuf d_ns_jac, d_ns_tet, d_vtpos, d_ns_nb, d_ns_pslot, d_ns_K;
+  int ns_topology();
+  NsBlocks ns_blocks() const;
   cudaStream_t cs_ns = nullptr;
   int ns_configure(int pcg_iterations, int every) override;
   int ns_correct(double h, long long* launches);
@@ -3243,6 +3245,74 @@ int Solver<R>::vt_setup() {
   return MLX_OK;
 }
 
+// The rows of the assembled J^T W J (pcg.cuh k_ns_assemble): for every
+// vertex the vertices sharing a tet with it, in increasing order, and for
+// every pair of the vertex CSR the row slots of its tet's four corners.
+// Fixed by the mesh, built once.
+template <typename R>
+int Solver<R>::ns_topology() {
+  if (d_ns_K.p) return MLX_OK;
+  std::vector<int> off(N + 1, 0);
+  for (int sidx = 0; sidx < T; ++sidx) {
+    const int4 q = vid_sorted[sidx];
+    for (int v : {q.x, q.y, q.z, q.w}) ++off[v + 1];
+  }
+  for (int v = 0; v < N; ++v) off[v + 1] += off[v];
+  std::vector<int> pt(off[N]);  // the vertex CSR's tets, in the order vt_setup stores them
+  {
+    std::vector<int> f(off.begin(), off.end() - 1);
+    for (int sidx = 0; sidx < T; ++sidx) {
+      const int4 q = vid_sorted[sidx];
+      for (int v : {q.x, q.y, q.z, q.w}) pt[f[v]++] = sidx;
+    }
+  }
+  std::vector<int> nb_off(N + 1, 0), nb_col;
+  std::vector<unsigned int> pslot(off[N]);
+  nb_col.reserve((size_t)N * 16);
+  std::vector<int> row;
+  for (int v = 0; v < N; ++v) {
+    row.clear();
+    for (int k = off[v]; k < off[v + 1]; ++k) {
+      const int4 q = vid_sorted[pt[k]];
+      row.insert(row.end(), {q.x, q.y, q.z, q.w});
+    }
+    std::sort(row.begin(), row.end());
+    row.erase(std::unique(row.begin(), row.end()), row.end());
+    if (row.size() > 255)
+      return set_error(MLX_ERR_UNSUPPORTED, "a vertex shares tets with more than 254 other vertices");
+    for (int k = off[v]; k < off[v + 1]; ++k) {
+      const int4 q = vid_sorted[pt[k]];
+      unsigned int sl = 0;
+      int b = 0;
+      for (int c : {q.x, q.y, q.z, q.w})
+        sl |= (unsigned int)(std::lower_bound(row.begin(), row.end(), c) - row.begin()) << (8 * b++);
+      pslot[k] = sl;
+    }
+    nb_col.insert(nb_col.end(), row.begin(), row.end());
+    nb_off[v + 1] = (int)nb_col.size();
+  }
+  CHECK(d_ns_nb.ensure(sizeof(int) * (N + 1 + nb_col.size())));
+  CHECK(d_ns_pslot.ensure(sizeof(unsigned int) * pslot.size()));
+  CHECK(d_ns_K.ensure(sizeof(R) * 9 * nb_col.size()));
+  CU(cudaMemcpyAsync(d_ns_nb.p, nb_off.data(), sizeof(int) * (N + 1), cudaMemcpyHostToDevice, stream));
+  CU(cudaMemcpyAsync(d_ns_nb.as<int>() + N + 1, nb_col.data(), sizeof(int) * nb_col.size(), cudaMemcpyHostToDevice,
+                     stream));
+  CU(cudaMemcpyAsync(d_ns_pslot.p, pslot.data(), sizeof(unsigned int) * pslot.size(), cudaMemcpyHostToDevice,
+                     stream));
+  CU(cudaStreamSynchronize(stream));
+  return MLX_OK;
+}
+
+template <typename R>
+NsBlocks Solver<R>::ns_blocks() const {
+  NsBlocks b;
+  b.nb_off = d_ns_nb.as<int>();
+  b.nb_col = d_ns_nb.as<int>() + N + 1;
+  b.pslot = d_ns_pslot.as<unsigned int>();
+  b.vtpos = d_vtpos.as<int>();
+  return b;
+}
+
 template <typename R>
 PcgOp Solver<R>::vt_op(double h2) {
   const size_t npairs = (d_pcg_vt.bytes - sizeof(int) * (N + 1)) / sizeof(int2);
@@ -3273,8 +3343,16 @@ int Solver<R>::ns_configure(int pcg_iterations, int every) {
   DeviceGuard g(device);
   if (pcg_iterations > 0) {
     CHECK(vt_setup());
+    CHECK(ns_topology());
     CHECK(d_ns_jac.ensure(sizeof(R) * 48 * (size_t)T));      // tet-major and CSR-order copies
-    CHECK(d_ns_tet.ensure(sizeof(double2) * 4 * (size_t)T));  // w, c, q, scratch
+    CHECK(d_ns_tet.ensure(sizeof(double2) * 3 * (size_t)T));  // w, c, q
+    CHECK(d_pcg_part.ensure(sizeof(double) * 2 * kNsMaxPartials));
+    // the vertex pass's grid: the blocks resident at once, at most one
+    // partial sum each
+    int per_sm = 0, sms = 0;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ns_spmv<R>, 256, 0));
+    CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    ns_vertex_blocks = std::max(1, std::min(per_sm * sms, kNsMaxPartials));
   }
   ns_iters = pcg_iterations;
   ns_every = every;
@@ -3292,7 +3370,7 @@ int Solver<R>::ns_correct(double h, long long* launches) {
   R* jt = d_ns_jac.as<R>();
   R* jv = jt + (size_t)24 * T;
   double2* tw = d_ns_tet.as<double2>();
-  double2 *w = tw, *c = tw + T, *q = tw + 2 * (size_t)T, *sv = tw + 3 * (size_t)T;
+  double2 *w = tw, *c = tw + T, *q = tw + 2 * (size_t)T;
   double4* V = d_pcg_vec.as<double4>();
   double4 *db = V, *dx = V + N, *dr = V + 2 * (size_t)N, *dz = V + 3 * (size_t)N, *dd = V + 4 * (size_t)N,
           *dAp = V + 5 * (size_t)N;
@@ -3304,27 +3382,29 @@ int Solver<R>::ns_correct(double h, long long* launches) {
   k_ns_rhs<R><<<nb, 256, 0, stream>>>(op, jv, q, db);  // b = -J^T (W C + lambda)
   CU(cudaMemsetAsync(dx, 0, sizeof(double4) * N, stream));
   CU(cudaMemcpyAsync(dr, db, sizeof(double4) * N, cudaMemcpyDeviceToDevice, stream));
-  k_ns_block_jacobi<R><<<nb, 256, 0, stream>>>(op, jv, w, P);
+  const NsBlocks nbk = ns_blocks();
+  R* K = d_ns_K.as<R>();
+  k_ns_assemble<R><<<blocks_for(N, kNsAsmWarps), 32 * kNsAsmWarps, 0, stream>>>(op, nbk, jv, w, K, P);  // K, P
   k_pcg_precond<<<nb, 256, 0, stream>>>(N, P, op.pin, dr, dz);
-  CU(cudaMemcpyAsync(dd, dz, sizeof(double4) * N, cudaMemcpyDeviceToDevice, stream));
-  // r'z double-buffered in the first two doubles of the scalars (rTz, then
-  // the alpha slot, which this loop does not use); the start's r'z goes to
-  // rTz[0]
-  double* rTz = reinterpret_cast<double*>(sc);
-  double* part2 = part + 2 * 296;
+  // beta = 0, d = 0 (the first direction is z) and the last-block counts 0;
+  // then rTz = r'z of the start
+  CU(cudaMemsetAsync(dd, 0, sizeof(double4) * N, stream));
+  CU(cudaMemsetAsync(sc, 0, sizeof(PcgScalars), stream));
   k_pcg_dot2<<<nred, 256, 0, stream>>>(N, dr, dz, nullptr, nullptr, part);
   k_pcg_scalars<<<1, 256, 0, stream>>>(part, nred, 0, sc, nullptr, 0);
+  const int vb = std::max(1, std::min(blocks_for((long long)N * kNsTeam, 256), ns_vertex_blocks));
+  double* part2 = part + kNsMaxPartials;
+  double4* D[2] = {dd, V + 6 * (size_t)N};  // the direction, alternating
   for (int i = 0; i < ns_iters; ++i) {
-    const int cur = i & 1;
-    k_ns_tet_apply<R><<<tb, 256, 0, stream>>>(T, vid, jt, w, dd, sv);
-    k_ns_vertex_apply<R><<<nred, 256, 0, stream>>>(op, jv, sv, dd, dAp, part);           // Ap = A d, d'Ap
-    k_ns_step<<<nred, 256, 0, stream>>>(N, rTz, cur, part, nred, dd, dAp, dx, dr, P, op.pin, dz, part2);
-    k_ns_direction<<<nred, 256, 0, stream>>>(N, rTz, cur, part2, nred, dz, dd);           // beta, d
+    k_ns_spmv<R><<<vb, 256, 0, stream>>>(op, nbk, K, dz, D[i & 1], D[(i + 1) & 1], dAp, sc, part,
+                                         &sc->count[0]);  // d, Ap = A d, alpha
+    k_ns_step<<<nred, 256, 0, stream>>>(N, sc, D[(i + 1) & 1], dAp, dx, dr, P, op.pin, dz, part2,
+                                        &sc->count[1]);  // x, r, z, beta
   }
   k_ns_lambda<R><<<tb, 256, 0, stream>>>(T, vid, jt, w, c, dx, d_lambda.as<R>());
   k_ns_move<R><<<nb, 256, 0, stream>>>(N, dx, pos());
   CU(cudaGetLastError());
-  if (launches) *launches += 7 + 4LL * ns_iters;
+  if (launches) *launches += 7 + 2LL * ns_iters;
   return MLX_OK;
 }
 
