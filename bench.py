@@ -760,7 +760,7 @@ def main():
     ap.add_argument("--layer-pcg", type=int, default=50,
                     help="PCG iterations of each Newton-PCG correction of the fine layer (Neo-Hookean residual "
                     "workloads; 0: none)")
-    ap.add_argument("--layer-pcg-every", type=int, default=50,
+    ap.add_argument("--layer-pcg-every", type=int, default=35,
                     help="Gauss-Seidel iterations between the Newton-PCG corrections")
     ap.add_argument("--host-monitor", action="store_true",
                     help="residual legs without the step graph: the same kernels with the stop rules on the host "

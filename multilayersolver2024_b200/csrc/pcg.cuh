@@ -360,9 +360,8 @@ __global__ void k_ns_rhs(PcgOp op, const R* __restrict__ jv, const double2* __re
 }
 
 // Lanes per row in the blocked product: a vertex of a tet mesh shares tets
-// with ~14 others; eight lanes take two blocks each, so the pass has eight
-// times the threads (and loads in flight) of one lane per row.
-constexpr int kNsTeam = 8;
+// with ~14 others; four lanes take ~4 blocks each, eight rows to a warp.
+constexpr int kNsTeam = 4;
 // Largest grid of a Newton-PCG grid reduction (one partial sum per block).
 constexpr int kNsMaxPartials = 2048;
 
@@ -538,6 +537,16 @@ __global__ void __launch_bounds__(256) k_ns_spmv(PcgOp op, NsBlocks nb, const R*
   double dot[1] = {0.0};
   for (int v = blockIdx.x * (blockDim.x / kNsTeam) + threadIdx.x / kNsTeam; v < op.N; v += nteams) {
     double ax = 0.0, ay = 0.0, az = 0.0;
+    // the row's own data, loaded while the blocks are gathered
+    double4 zv = make_double4(0, 0, 0, 0), dv = zv;
+    double m = 0.0;
+    unsigned char pm = 0;
+    if (lane == 0) {
+      zv = z[v];
+      dv = dprev[v];
+      m = op.vmass[v];
+      pm = op.pin[v];
+    }
     const int j1 = nb.nb_off[v + 1];
     for (int j = nb.nb_off[v] + lane; j < j1; j += kNsTeam) {
       const int c = nb.nb_col[j];
@@ -554,10 +563,8 @@ __global__ void __launch_bounds__(256) k_ns_spmv(PcgOp op, NsBlocks nb, const R*
       az += __shfl_xor_sync(mask, az, o);
     }
     if (lane == 0) {
-      const double4 dk = ns_dir(z[v], dprev[v], beta);
+      const double4 dk = ns_dir(zv, dv, beta);
       dnext[v] = dk;
-      const double m = op.vmass[v];
-      const unsigned char pm = op.pin[v];
       const double4 yv = make_double4((pm & 1) ? 0.0 : ax + m * dk.x, (pm & 2) ? 0.0 : ay + m * dk.y,
                                       (pm & 4) ? 0.0 : az + m * dk.z, 0.0);
       Ap[v] = yv;

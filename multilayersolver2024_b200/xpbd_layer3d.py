@@ -154,11 +154,15 @@ class Solver:
         check("mlx_create", lib.mlx_create(C.byref(d), C.byref(h)), lib)
         self.handle = h
 
-    def layer_pcg(self, pcg_iterations=100, every=50):
+    def layer_pcg(self, pcg_iterations=50, every=35):
         """The PCG in the layer solve (``mlx_layer_pcg``): Newton-PCG
         corrections of the last layer, ``pcg_iterations`` PCG iterations each,
         before its Gauss-Seidel and after every ``every`` iterations;
-        pcg_iterations = 0 turns them off."""
+        pcg_iterations = 0 turns them off.  The defaults are the fastest
+        setting to residual 1e-4 on a 393 k-tet Neo-Hookean block that stays
+        as close to the plain solve as 50 or 100 iterations every 50 sweeps
+        (fewer PCG iterations per correction move the converged positions
+        further from it)."""
         check("mlx_layer_pcg", self._lib.mlx_layer_pcg(self.handle, int(pcg_iterations), int(every)), self._lib)
 
     @property
