@@ -649,7 +649,7 @@ def run_ours(args, rank, world, local):
             launch_note = ("estimate: iterations of the timed steps x (launches per fixed-count iteration + the "
                            "monitor's 2)")
             if to_res["value_leg"] == "learned_pcg":
-                # each Newton-PCG correction: 7 launches + 4 per PCG iteration, one before the fine layer
+                # each Newton-PCG correction: 7 launches + 2 per PCG iteration, one before the fine layer
                 # and one after every `every` of its iterations (the fine layer holds most iterations)
                 per_corr = 7 + 2 * args.layer_pcg
                 launches += int(sum((1 + max(it - 1, 0) // max(args.layer_pcg_every, 1)) * per_corr

@@ -69,8 +69,12 @@ __global__ void k_mon_loop_begin(MonState* ms, cudaGraphConditionalHandle loop, 
 
 // End of one projectGS iteration: append the residual and apply
 // simpleMonitorError's rules (xpbdLayer3D.m:515-544), then the loop test.
+// With ns_every > 0 it also sets `ns`, the condition of the Newton-PCG
+// correction (pcg.cuh) that closes the iteration: after every ns_every
+// iterations of the last layer, when the loop goes on.
 __device__ __forceinline__ void mon_iter_end(MonState* ms, cudaGraphConditionalHandle loop, int iterations,
-                                             int is_last, const MonParams& mp) {
+                                             int is_last, const MonParams& mp, cudaGraphConditionalHandle ns = 0,
+                                             int ns_every = 0) {
   ms->it += 1;
   ms->total_iterations += 1;
   const double newRes = ms->res;
@@ -102,18 +106,12 @@ __device__ __forceinline__ void mon_iter_end(MonState* ms, cudaGraphConditionalH
   const bool go = !(ms->end_layer || ms->stop) &&
                   (ms->it <= iterations || (!ms->stop && ms->run_until >= 0 && is_last));
   cudaGraphSetConditional(loop, go ? 1u : 0u);
+  if (ns_every > 0) cudaGraphSetConditional(ns, (go && (ms->it - 1) % ns_every == 0) ? 1u : 0u);
 }
 
 __global__ void k_mon_iter_end(MonState* ms, cudaGraphConditionalHandle loop, int iterations, int is_last,
-                               MonParams mp) {
-  mon_iter_end(ms, loop, iterations, is_last, mp);
-}
-
-// Start of projectGS iteration ms->it of the last layer: the Newton-PCG
-// correction (pcg.cuh) runs after every `every` iterations.
-__global__ void k_ns_gate(const MonState* ms, cudaGraphConditionalHandle run, int every) {
-  const long long it = ms->it;
-  cudaGraphSetConditional(run, (it > 1 && (it - 1) % every == 0) ? 1u : 0u);
+                               MonParams mp, cudaGraphConditionalHandle ns, int ns_every) {
+  mon_iter_end(ms, loop, iterations, is_last, mp, ns, ns_every);
 }
 
 }  // namespace mlx

@@ -315,55 +315,42 @@ __device__ __forceinline__ double4 ns_dir(const double4 z, const double4 d, doub
   return make_double4(__fma_rn(beta, d.x, z.x), __fma_rn(beta, d.y, z.y), __fma_rn(beta, d.z, z.z), 0.0);
 }
 
-// sum over the vertex's (tet, corner) pairs of J_{t,corner}^T f_t, in the
-// CSR's fixed order.
-// Pairs go four at a time with their loads issued together (the sum keeps
-// the CSR order).
-template <typename R>
-__device__ __forceinline__ D3 ns_jtf(const PcgOp& op, const R* __restrict__ jv, const double2* __restrict__ f,
-                                     int v) {
-  D3 acc = d3(0.0, 0.0, 0.0);
-  const int k0 = op.vt_off[v], k1 = op.vt_off[v + 1];
-  int k = k0;
-  for (; k + 4 <= k1; k += 4) {
-    double2 fk[4];
-    R g[4][6];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) fk[q] = f[op.vt[k + q].x];
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-#pragma unroll
-      for (int c = 0; c < 6; ++c) g[q][c] = jv[(size_t)6 * (k + q) + c];
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-      acc = acc + d3(fk[q].x * (double)g[q][0] + fk[q].y * (double)g[q][3],
-                     fk[q].x * (double)g[q][1] + fk[q].y * (double)g[q][4],
-                     fk[q].x * (double)g[q][2] + fk[q].y * (double)g[q][5]);
-  }
-  for (; k < k1; ++k) {
-    const double2 fk = f[op.vt[k].x];
-    const R* g = jv + (size_t)6 * k;
-    acc = acc + d3(fk.x * (double)g[0] + fk.y * (double)g[3], fk.x * (double)g[1] + fk.y * (double)g[4],
-                   fk.x * (double)g[2] + fk.y * (double)g[5]);
-  }
-  return acc;
-}
-
-// y = -J^T q on the unpinned DOFs (the right-hand side).
-template <typename R>
-__global__ void k_ns_rhs(PcgOp op, const R* __restrict__ jv, const double2* __restrict__ q, double4* __restrict__ y) {
-  const int v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= op.N) return;
-  const D3 a = ns_jtf<R>(op, jv, q, v);
-  const unsigned char pm = op.pin[v];
-  y[v] = make_double4((pm & 1) ? 0.0 : -a.x, (pm & 2) ? 0.0 : -a.y, (pm & 4) ? 0.0 : -a.z, 0.0);
-}
-
 // Lanes per row in the blocked product: a vertex of a tet mesh shares tets
 // with ~14 others; four lanes take ~4 blocks each, eight rows to a warp.
 constexpr int kNsTeam = 4;
 // Largest grid of a Newton-PCG grid reduction (one partial sum per block).
 constexpr int kNsMaxPartials = 2048;
+
+// y = -J^T q on the unpinned DOFs (the right-hand side): kNsTeam lanes per
+// vertex, each lane every kNsTeam-th (tet, corner) pair of the vertex's CSR
+// range, a fixed butterfly over the team (lane 0 stores).
+template <typename R>
+__global__ void __launch_bounds__(256) k_ns_rhs(PcgOp op, const R* __restrict__ jv, const double2* __restrict__ q,
+                                                double4* __restrict__ y) {
+  const int lane = threadIdx.x & (kNsTeam - 1);
+  const unsigned mask = ((1u << kNsTeam) - 1u) << ((threadIdx.x & 31) & ~(kNsTeam - 1));
+  const int v = (blockIdx.x * blockDim.x + threadIdx.x) / kNsTeam;
+  if (v >= op.N) return;  // whole teams leave together
+  double ax = 0.0, ay = 0.0, az = 0.0;
+  const int k1 = op.vt_off[v + 1];
+  for (int k = op.vt_off[v] + lane; k < k1; k += kNsTeam) {
+    const double2 fk = q[op.vt[k].x];
+    const R* g = jv + (size_t)6 * k;
+    ax += fk.x * (double)g[0] + fk.y * (double)g[3];
+    ay += fk.x * (double)g[1] + fk.y * (double)g[4];
+    az += fk.x * (double)g[2] + fk.y * (double)g[5];
+  }
+#pragma unroll
+  for (int o = kNsTeam / 2; o > 0; o >>= 1) {
+    ax += __shfl_xor_sync(mask, ax, o);
+    ay += __shfl_xor_sync(mask, ay, o);
+    az += __shfl_xor_sync(mask, az, o);
+  }
+  if (lane == 0) {
+    const unsigned char pm = op.pin[v];
+    y[v] = make_double4((pm & 1) ? 0.0 : -ax, (pm & 2) ? 0.0 : -ay, (pm & 4) ? 0.0 : -az, 0.0);
+  }
+}
 
 // The block's partial sum of a grid reduction goes to partials[blockIdx.x];
 // the last block to finish (an atomic count, after a fence) sums all of them
@@ -433,10 +420,38 @@ __global__ void __launch_bounds__(32 * kNsAsmWarps) k_ns_assemble(PcgOp op, NsBl
   for (int v = blockIdx.x * kNsAsmWarps + (threadIdx.x >> 5); v < op.N; v += nwarps) {
     const int k0 = op.vt_off[v], k1 = op.vt_off[v + 1];
     const int r0 = nb.nb_off[v], rn = nb.nb_off[v + 1] - r0;
+    if (rn == 0) {  // a vertex of no tet: the preconditioner block is M alone
+      if (lane == 0) {
+        const double m = op.vmass[v];
+        const unsigned char pm = op.pin[v];
+        double* pv = Pinv + 9 * (size_t)v;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) pv[q] = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) pv[4 * d] = (pm & (1 << d)) ? 1.0 : 1.0 / m;
+      }
+      continue;
+    }
+    // the row's diagonal slot (the vertex itself)
+    int dslot = -1;
+    for (int b0 = 0; b0 < rn; b0 += 32) {
+      const unsigned bal = __ballot_sync(0xffffffffu, b0 + lane < rn && nb.nb_col[r0 + b0 + lane] == v);
+      if (bal) dslot = b0 + __ffs(bal) - 1;
+    }
     for (int base = 0; base < rn; base += 32) {
       const int mine = base + lane;
-      // every byte of the pattern is this lane's slot (slots are < 255)
-      const unsigned int rep = mine < rn ? (unsigned int)mine * 0x01010101u : 0xffffffffu;
+      // every pair adds one product to the diagonal block (its own corner),
+      // ~22 against ~6 for the other blocks: when this round has two or
+      // more lanes without a slot, they split the diagonal's pairs (helper
+      // h takes the pairs p = h mod nh) and the diagonal's owner sums their
+      // parts in helper order
+      const int nh = base + 32 > rn ? base + 32 - rn : 0;
+      const bool split = nh >= 2 && dslot >= base && dslot < base + 32;
+      const int hi = mine - rn;  // helper index (split rounds, lanes without a slot)
+      // every byte of the pattern is this lane's slot (slots are < 255); no
+      // match for lanes without a slot and for a split diagonal's owner
+      const unsigned int rep =
+          (mine < rn && !(split && mine == dslot)) ? (unsigned int)mine * 0x01010101u : 0xffffffffu;
       double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
       for (int p0 = k0; p0 < k1; p0 += 32) {
         const int np = min(32, k1 - p0);
@@ -469,6 +484,13 @@ __global__ void __launch_bounds__(32 * kNsAsmWarps) k_ns_assemble(PcgOp op, NsBl
               mw[wd] |= ((x * 0x01020408u) >> 24) << (4 * q);
             }
           }
+        // a helper's diagonal pairs of this chunk
+        if (split && hi >= 0) {
+          for (int p = ((hi - (p0 - k0)) % nh + nh) % nh; p < np; p += nh) {
+            const int b = st.corner[p];
+            mw[p >> 3] |= 1u << (4 * (p & 7) + b);
+          }
+        }
         // the matches in pair order, then corner order
 #pragma unroll
         for (int wd = 0; wd < 4; ++wd) {
@@ -489,11 +511,21 @@ __global__ void __launch_bounds__(32 * kNsAsmWarps) k_ns_assemble(PcgOp op, NsBl
           }
         }
       }
+      if (split) {
+#pragma unroll 1
+        for (int hh = 0; hh < nh; ++hh) {
+#pragma unroll
+          for (int q = 0; q < 9; ++q) {
+            const double t = __shfl_sync(0xffffffffu, acc[q], rn - base + hh);
+            if (mine == dslot) acc[q] += t;
+          }
+        }
+      }
       if (mine < rn) {
         R* kb = K + (size_t)9 * (r0 + mine);
 #pragma unroll
         for (int q = 0; q < 9; ++q) kb[q] = (R)acc[q];
-        if (nb.nb_col[r0 + mine] == v) {
+        if (mine == dslot) {
           const double m = op.vmass[v];
           double B[9];
 #pragma unroll

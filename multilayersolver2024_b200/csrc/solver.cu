@@ -1719,7 +1719,7 @@ __global__ void __launch_bounds__(256) k_residual_monitor(TetData<R> td, const R
                                                           R inv_h, double inv_h2_d, double* __restrict__ partials,
                                                           unsigned* __restrict__ ticket, MonState* ms,
                                                           cudaGraphConditionalHandle loop, int iterations, int is_last,
-                                                          MonParams mp) {
+                                                          MonParams mp, cudaGraphConditionalHandle ns, int ns_every) {
   double acc[1] = {residual_tets<R, MAT>(td, pos, inv_h2, inv_h, inv_h2_d, blockIdx.x * blockDim.x + threadIdx.x,
                                          gridDim.x * blockDim.x)};
   block_sum<1>(acc);
@@ -1738,7 +1738,7 @@ __global__ void __launch_bounds__(256) k_residual_monitor(TetData<R> td, const R
   if (threadIdx.x == 0) {
     ms->res = sqrt(sum[0]);
     *ticket = 0;
-    mon_iter_end(ms, loop, iterations, is_last, mp);
+    mon_iter_end(ms, loop, iterations, is_last, mp, ns, ns_every);
   }
 }
 
@@ -2005,22 +2005,10 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
     }
     long long it = 1;
     while (devmon || it <= ld->iterations[layer] || (!stopSolve && st.runUntil >= 0 && isLast)) {
-      if (nsLayer && ns_every > 0) {
-        if (devmon) {
-          // iteration ms->it of the WHILE body: a correction after every
-          // ns_every iterations, as a conditional node
-          cudaGraphConditionalHandle h_ns;
-          CHECK(cond_handle(&h_ns));
-          k_ns_gate<<<1, 1, 0, stream>>>(mon(), h_ns, ns_every);
-          CU(cudaGetLastError());
-          ++st.launches;
-          CHECK(cond_begin(h_ns, cudaGraphCondTypeIf, cs_ns));
-          CHECK(ns_correct(h, &st.launches));
-          CHECK(cond_end(cs_while));
-        } else if (it > 1 && (it - 1) % ns_every == 0) {
-          CHECK(ns_correct(h, &st.launches));
-        }
-      }
+      // (in the device-monitored loop the correction closes the WHILE body
+      // instead, below)
+      if (nsLayer && ns_every > 0 && !devmon && it > 1 && (it - 1) % ns_every == 0)
+        CHECK(ns_correct(h, &st.launches));
       ++it;
       if (it > kSafetyIterations) return set_error(MLX_ERR_LIMIT, "iteration safety limit reached");
       ++st.totalIterations;
@@ -2061,6 +2049,21 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
         ++st.launches;
       }
       bool endLayer = false;
+      // device-monitored last layer with corrections: the iteration's
+      // monitor also sets the condition of the correction that closes the
+      // WHILE body (after every ns_every iterations, when the loop goes on)
+      const bool nsGate = devmon && nsLayer && ns_every > 0;
+      cudaGraphConditionalHandle h_ns = 0;
+      if (nsGate) CHECK(cond_handle(&h_ns));
+      const int nsEvery = nsGate ? ns_every : 0;
+      auto close_body = [&]() -> int {
+        if (nsGate) {
+          CHECK(cond_begin(h_ns, cudaGraphCondTypeIf, cs_ns));
+          CHECK(ns_correct(h, &st.launches));
+          CHECK(cond_end(cs_while));
+        }
+        return cond_end(cs_if);  // end of the WHILE body
+      };
       if (devmon && !dc.nobs) {
         // residual, its norm and the stop rules in one launch
         const int tb = std::min(blocks_for(T, 256), 592);
@@ -2073,28 +2076,32 @@ int Solver<R>::run_layers(const mlx_layer_desc* ld, const mlx_solve_params* P, c
         switch (mat_kind) {
           case MAT_NH:
             k_residual_monitor<R, MAT_NH><<<tb, 256, 0, stream>>>(td, pos(), ih2, ih, 1.0 / (h * h), parts, ticket, ms,
-                                                                  h_while_cur, its, il, mp);
+                                                                  h_while_cur, its, il, mp, h_ns,
+                                                                  nsEvery);
             break;
           case MAT_STVK_BLOCKS:
             k_residual_monitor<R, MAT_STVK_BLOCKS><<<tb, 256, 0, stream>>>(td, pos(), ih2, ih, 1.0 / (h * h), parts,
-                                                                           ticket, ms, h_while_cur, its, il, mp);
+                                                                           ticket, ms, h_while_cur, its, il, mp, h_ns,
+                                                                  nsEvery);
             break;
           default:
             k_residual_monitor<R, MAT_STVK_LAME><<<tb, 256, 0, stream>>>(td, pos(), ih2, ih, 1.0 / (h * h), parts,
-                                                                         ticket, ms, h_while_cur, its, il, mp);
+                                                                         ticket, ms, h_while_cur, its, il, mp, h_ns,
+                                                                  nsEvery);
         }
         CU(cudaGetLastError());
         ++st.launches;
-        CHECK(cond_end(cs_if));  // end of the WHILE body
+        CHECK(close_body());
         break;
       }
       if (devmon) {
         CHECK(residual_dev(&mon()->res, dc));
         if (dc.nobs) ++st.launches;
-        k_mon_iter_end<<<1, 1, 0, stream>>>(mon(), h_while_cur, ld->iterations[layer], isLast ? 1 : 0, mp);
+        k_mon_iter_end<<<1, 1, 0, stream>>>(mon(), h_while_cur, ld->iterations[layer], isLast ? 1 : 0, mp, h_ns,
+                                            nsEvery);
         CU(cudaGetLastError());
         st.launches += 3;
-        CHECK(cond_end(cs_if));  // end of the WHILE body
+        CHECK(close_body());
         break;
       }
       if (P->compute_residuals) {
@@ -3379,7 +3386,7 @@ int Solver<R>::ns_correct(double h, long long* launches) {
   PcgScalars* sc = d_pcg_sc.as<PcgScalars>();
   const int4* vid = d_vid.as<int4>();
   k_ns_jacobian<R><<<tb, 256, 0, stream>>>(tets(), pos(), h * h, d_vtpos.as<int>(), jt, jv, w, c, q);
-  k_ns_rhs<R><<<nb, 256, 0, stream>>>(op, jv, q, db);  // b = -J^T (W C + lambda)
+  k_ns_rhs<R><<<blocks_for((long long)N * kNsTeam, 256), 256, 0, stream>>>(op, jv, q, db);  // b = -J^T (W C + lambda)
   CU(cudaMemsetAsync(dx, 0, sizeof(double4) * N, stream));
   CU(cudaMemcpyAsync(dr, db, sizeof(double4) * N, cudaMemcpyDeviceToDevice, stream));
   const NsBlocks nbk = ns_blocks();
