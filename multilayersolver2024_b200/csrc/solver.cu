@@ -402,9 +402,12 @@ struct Solver final : SolverBase {
   }
   int detect_contacts(const R4<R>* x0);  // stream work only (captured in the step)
   // device residual monitor (monitor.cuh): conditional graph nodes
-  DevBuf d_mon;
+  // (d_mon: the resident stepper's, whose run-until persists across steps;
+  // d_mon_ls: a layer solve replayed as a graph)
+  DevBuf d_mon, d_mon_ls;
+  const DevBuf* mon_active = &d_mon;
   cudaStream_t cs_if = nullptr, cs_while = nullptr;
-  MonState* mon() const { return d_mon.as<MonState>(); }
+  MonState* mon() const { return mon_active->as<MonState>(); }
   int cond_handle(cudaGraphConditionalHandle* h);
   int cond_begin(cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type, cudaStream_t body);
   int cond_end(cudaStream_t parent);
@@ -450,6 +453,7 @@ struct Solver final : SolverBase {
   int sim_set_obstacles(const mlx_obstacle* obs, int nobs, double restitution) override;
   int sim_contact_count(int32_t* n) override;
   PinnedBuf h_gsync;
+  PinnedBuf h_mon;  // the device monitor's state, staged for a layer solve replayed as a graph
   long long last_launches = 0;
   // Fixed-iteration layers run as one launch per colour, each launched as a
   // programmatic dependent of the previous (off with MLXPBD_PDL=0).  The
@@ -2551,7 +2555,13 @@ int Solver<R>::layer_solve(const mlx_layer_desc* ld, const mlx_solve_params* P, 
   st.runUntil = P->run_until;
   st.sumNonMon = in->sum_non_monitored_time;
   CHECK(reset_gsync());
-  const bool graphable = host_graph_on && !P->compute_residuals && cd.K == 0 && !sweep_timing;
+  // A call of the same shape as the previous one replays it as a graph; with
+  // residual monitoring the stop rules then run on the device (monitor.cuh:
+  // the same rules and residual bits as the host loop), the residual array
+  // going in and out through the device monitor's state.  The time spent on
+  // residuals is not measured there (sum_non_monitored_time passes through).
+  const bool monDev = P->compute_residuals && in->residual_in_len < kMonCapacity;
+  const bool graphable = host_graph_on && (!P->compute_residuals || monDev) && cd.K == 0 && !sweep_timing;
   std::vector<int> lkey;
   std::vector<unsigned char> pkey;
   if (graphable) {
@@ -2562,14 +2572,20 @@ int Solver<R>::layer_solve(const mlx_layer_desc* ld, const mlx_solve_params* P, 
     }
     pkey.assign(reinterpret_cast<const unsigned char*>(P), reinterpret_cast<const unsigned char*>(P) + sizeof(*P));
   }
+  bool replayed = false;
   if (graphable && lkey == hg.lkey && pkey == hg.pkey && statics_hit(ld, work)) {
+    replayed = true;
+    // the monitor's state lives at a fixed address the graph records
+    if (P->compute_residuals) CHECK(d_mon_ls.ensure(sizeof(MonState)));
     // the same shape as the previous call, whose uncaptured run built every
     // layer static: record the loop once, then replay it
     if (!hg.exec) {
       cudaGraph_t graph = nullptr;
       CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
       RunState cs = st;
+      mon_active = &d_mon_ls;
       const int rc = run_layers(ld, P, K, cd, cs, true, work);
+      mon_active = &d_mon;
       const cudaError_t e = cudaStreamEndCapture(stream, &graph);
       if (rc != MLX_OK) {
         if (graph) cudaGraphDestroy(graph);
@@ -2585,9 +2601,25 @@ int Solver<R>::layer_solve(const mlx_layer_desc* ld, const mlx_solve_params* P, 
       hg.launches = cs.launches - st.launches;
       hg.iterations = cs.totalIterations - st.totalIterations;
     }
+    if (P->compute_residuals) {
+      // the monitor's state for this call: the caller's residual array and
+      // run-until, the rest cleared as at the start of the host loop
+      CHECK(h_mon.ensure(sizeof(MonState)));
+      MonState* hm = h_mon.as<MonState>();
+      const size_t head = offsetof(MonState, ra);
+      std::memset(static_cast<void*>(hm), 0, head);
+      hm->run_until = P->run_until;
+      hm->ra_len = in->residual_in_len;
+      std::memcpy(hm->ra, in->residual_in, sizeof(double) * in->residual_in_len);
+      CU(cudaMemcpyAsync(d_mon_ls.p, hm, head + sizeof(double) * in->residual_in_len, cudaMemcpyHostToDevice,
+                         stream));
+    }
     CU(cudaGraphLaunch(hg.exec, stream));
     st.launches += hg.launches;
-    st.totalIterations += hg.iterations;
+    if (P->compute_residuals)
+      CU(cudaMemcpyAsync(h_mon.p, d_mon_ls.p, sizeof(MonState), cudaMemcpyDeviceToHost, stream));
+    else
+      st.totalIterations += hg.iterations;
   } else {
     drop_host_graph();
     CHECK(run_layers(ld, P, K, cd, st, false, work));
@@ -2603,6 +2635,15 @@ int Solver<R>::layer_solve(const mlx_layer_desc* ld, const mlx_solve_params* P, 
   CU(cudaStreamSynchronize(stream));
   cpack_used = 0;  // no copy of the contact lists is in flight now
   CHECK(check_gsync());
+  if (P->compute_residuals && replayed) {
+    // replayed with the stop rules on the device
+    const MonState* hm = h_mon.as<MonState>();
+    if (hm->error == 1) return set_error(MLX_ERR_LIMIT, "a layer reached the device monitor's iteration cap");
+    if (hm->error == 2) return set_error(MLX_ERR_LIMIT, "the residual array reached the device monitor's capacity");
+    st.residualArray.assign(hm->ra, hm->ra + hm->ra_len);
+    st.runUntil = hm->run_until;
+    st.totalIterations = hm->total_iterations;
+  }
   host_copy(out->xi, hs, sizeof(double) * n3);
   if (out->lambdai) host_copy(out->lambdai, hs + n3, sizeof(double) * n6);
   int n = (int)st.residualArray.size();
