@@ -696,10 +696,12 @@ def run_ours(args, rank, world, local):
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "api": "XpbdLayer3D.integrate -> mlx_layer_solve"
                     + (" (+ mlx_find_contacts on the step-start positions)" if sc.contact_finders else "")
-                    + ((", to residual 1e-4 with the stop rules on the host and the PCG in the layer solve "
-                        "(mlx_layer_pcg; the learned warm start is an option of the device-resident stepper only)")
-                       if e2e_pcg else (", plain solve to residual 1e-4 with the stop rules on the host"
-                                        if residual_metric else ""))},
+                    + ((", to residual 1e-4 with the PCG in the layer solve (mlx_layer_pcg; the learned warm "
+                        "start is an option of the device-resident stepper only)")
+                       if e2e_pcg else (", plain solve to residual 1e-4" if residual_metric else ""))
+                    + ("; from the second step on each call replays the recorded loop with the stop rules on "
+                       "the device" if residual_metric and not sc.contact_finders else
+                       ("; stop rules on the host (host contact list)" if residual_metric else ""))},
             "layer_builder": layer_builder,
             "gpu_launches": launches, "gpu_launches_note": launch_note,
             "clocks": clocks.summary(),

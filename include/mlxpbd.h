@@ -165,7 +165,10 @@ typedef struct mlx_solve_outputs {
   int32_t residual_capacity;
   int32_t residual_len;                /* written                             */
   double run_until;                    /* written                             */
-  double sum_non_monitored_time;       /* written                             */
+  double sum_non_monitored_time;       /* written (host stop rules add their
+                                          residual time; a replayed call,
+                                          whose rules run on the device,
+                                          passes the input through)           */
   int32_t total_iterations;            /* written: projectGS iterations run   */
 } mlx_solve_outputs;
 
@@ -184,7 +187,12 @@ int mlx_destroy(mlx_solver* solver);
 
 /* xpbdLayer3D.layerSolve (xpbdLayer3D.m:44-232) with host buffers: uploads
  * the per-step vectors, runs every layer on the device, downloads xi.  The
- * outputs mirror [xi, sumNonMonitoredTime, residualArray, runUntil]. */
+ * outputs mirror [xi, sumNonMonitoredTime, residualArray, runUntil].  A call
+ * with the same layers and params as the previous one and no host contacts
+ * replays the loop recorded once as a CUDA graph; with compute_residuals the
+ * stop rules then run on the device (the same results bit for bit; the
+ * residual array may hold up to 16,384 entries on entry, else the call keeps
+ * the host rules). */
 int mlx_layer_solve(mlx_solver* solver,
                     const mlx_layer_desc* layers,
                     const mlx_solve_params* params,
