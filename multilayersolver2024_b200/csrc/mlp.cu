@@ -102,6 +102,7 @@ enum Epilogue : int {
   EPI_BIAS_GELU = 1,   // Z = C + bias (FP32), H = GELU(Z) as BF16 row-major and transposed
   EPI_BIAS = 2,        // Y = C + bias (FP32)
   EPI_GELU_GRAD = 3,   // dZ = C * GELU'(Z) as BF16 row-major and transposed
+  EPI_BIAS_GELU_FWD = 4,  // inference: H = GELU(C + bias) as BF16 row-major only
 };
 
 struct GemmArgs {
@@ -206,6 +207,37 @@ __global__ void __launch_bounds__(128, 1) k_umma_gemm(GemmArgs g) {
           : "r"(taddr));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       if (!live) continue;
+      if (g.epi == EPI_BIAS || g.epi == EPI_BIAS_GELU_FWD) {
+        // the thread's 16 consecutive columns of its row, in 16-byte stores
+        // (ldo and n0 are multiples of 16)
+        float v[16];
+#pragma unroll
+        for (int j = 0; j < 16; j += 4) {
+          const float4 b4 = *reinterpret_cast<const float4*>(g.bias + n0 + j);
+          const float bb[4] = {b4.x, b4.y, b4.z, b4.w};
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            v[j + i] = n0 + j + i >= g.n_valid ? 0.f : __uint_as_float(r[j + i]) + bb[i];
+        }
+        if (g.epi == EPI_BIAS) {
+          float4* o = reinterpret_cast<float4*>(g.outF + (size_t)row * g.ldo + n0);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) o[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+        } else {
+          uint4 h[2];
+          __nv_bfloat162* hp = reinterpret_cast<__nv_bfloat162*>(h);
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const int a = 2 * j, b = 2 * j + 1;
+            hp[j] = __floats2bfloat162_rn(n0 + a >= g.n_valid ? 0.f : gelu(v[a]),
+                                          n0 + b >= g.n_valid ? 0.f : gelu(v[b]));
+          }
+          uint4* o = reinterpret_cast<uint4*>(g.outH + (size_t)row * g.ldo + n0);
+          o[0] = h[0];
+          o[1] = h[1];
+        }
+        continue;
+      }
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
         const int n = n0 + j;
@@ -215,11 +247,6 @@ __global__ void __launch_bounds__(128, 1) k_umma_gemm(GemmArgs g) {
           case EPI_STORE_F32:
             g.outF[(size_t)row * g.ldo + n] = pad ? 0.f : v;
             break;
-          case EPI_BIAS: {
-            v = pad ? 0.f : v + g.bias[n];
-            g.outF[(size_t)row * g.ldo + n] = v;
-            break;
-          }
           case EPI_BIAS_GELU: {
             const float z = pad ? 0.f : v + g.bias[n];
             const __nv_bfloat16 hb = __float2bfloat16_rn(pad ? 0.f : gelu(z));
@@ -483,15 +510,20 @@ struct Mlp {
     return cudaGetLastError() == cudaSuccess ? MLX_OK : set_error(MLX_ERR_CUDA, "tensor-core GEMM launch failed");
   }
 
-  // forward on device inputs x [B x n_in] (FP32); output Y [Bp x Np_last]
-  int forward_dev(const float* x, int B) {
+  // forward on device inputs x [B x n_in] (FP32); output Y [Bp x Np_last].
+  // `train` keeps what the backward pass reads (pre-activations, transposed
+  // activations); inference writes the activations only.
+  int forward_dev(const float* x, int B, bool train = true) {
     if (B < 1 || B > max_batch) return set_error(MLX_ERR_ARGUMENT, "batch size out of [1, max_batch]");
     const int Bp = pad_to(B, kTileM), L = layers();
     const int n0 = Bp * Kp[0];
     k_stage_input<<<(n0 + 255) / 256, 256, 0, stream>>>(x, B, n_in, Bp, Kp[0], H[0], HT[0]);
     int rc;
     for (int l = 0; l < L; ++l) {
-      if (l < L - 1) {
+      if (l < L - 1 && !train) {
+        rc = gemm(H[l], Kp[l], wb[l], Kp[l], Bp, Np[l], Kp[l], EPI_BIAS_GELU_FWD, bias[l], nullptr, 0, nullptr,
+                  H[l + 1], nullptr, Np[l], 0, dout[l]);
+      } else if (l < L - 1) {
         rc = gemm(H[l], Kp[l], wb[l], Kp[l], Bp, Np[l], Kp[l], EPI_BIAS_GELU, bias[l], nullptr, 0, Z[l], H[l + 1],
                   HT[l + 1], Np[l], Bp, dout[l]);
       } else {
@@ -571,7 +603,7 @@ int mlp_forward_on_stream(mlx_mlp* m, const float* d_x, int batch, cudaStream_t 
   Mlp& p = m->impl;
   cudaStream_t own = p.stream;
   p.stream = s;
-  const int rc = p.forward_dev(d_x, batch);
+  const int rc = p.forward_dev(d_x, batch, false);
   p.stream = own;
   if (y) *y = p.Y;
   if (ld) *ld = p.Np.back();
@@ -656,7 +688,8 @@ int mlx_mlp_forward(mlx_mlp* m, const float* x, int32_t batch, float* y) {
     Mlp& p = m->impl;
     cudaSetDevice(p.device);
     int rc;
-    if ((rc = p.upload(x, nullptr, batch)) || (rc = p.forward_dev(p.xin, batch)) || (rc = p.check_error())) return rc;
+    if ((rc = p.upload(x, nullptr, batch)) || (rc = p.forward_dev(p.xin, batch, false)) || (rc = p.check_error()))
+      return rc;
     const int No = p.Np.back();
     std::vector<float> h((size_t)batch * No);
     cudaMemcpyAsync(h.data(), p.Y, sizeof(float) * batch * No, cudaMemcpyDeviceToHost, p.stream);
