@@ -1692,8 +1692,29 @@ int Solver<R>::upload_contacts(const mlx_contacts* K, ContactData& cd) {
     return set_error(MLX_ERR_ARGUMENT, "contact arrays are NULL");
   for (int k = 0; k < nK; ++k)
     if (K->vertex_ids[k] < 1 || K->vertex_ids[k] > N) return set_error(MLX_ERR_ARGUMENT, "contact vertex id out of range");
-  CHECK(h_cstage.ensure(sizeof(double) * 7 * nK + sizeof(int) * nK, true));
-  CHECK(d_contacts.ensure(sizeof(double) * 7 * nK, true));
+  // the distinct compliances and their counts (the residual's K x K term)
+  double cv[kMaxCompliances];
+  int cn[kMaxCompliances];
+  int nc = 0;
+  for (int k = 0; k < nK && nc >= 0; ++k) {
+    const double a = K->compliance[k];
+    int g = 0;
+    while (g < nc && !(cv[g] == a)) ++g;
+    if (g == nc) {
+      if (nc == kMaxCompliances) {
+        nc = -1;
+        break;
+      }
+      cv[nc] = a;
+      cn[nc++] = 0;
+    }
+    ++cn[g];
+  }
+  // host staging: 7 nK doubles, nK ids (rounded up to whole doubles), the
+  // compliance values, their counts
+  const size_t o_cv = 7 * (size_t)nK + (nK + 1) / 2;
+  CHECK(h_cstage.ensure(sizeof(double) * (o_cv + kMaxCompliances) + sizeof(int) * kMaxCompliances, true));
+  CHECK(d_contacts.ensure(sizeof(double) * (7 * nK + kMaxCompliances) + sizeof(int) * kMaxCompliances, true));
   CHECK(d_cvid.ensure(sizeof(int) * nK, true));
   CHECK(d_clam.ensure(sizeof(double) * nK, true));
   double* hc = h_cstage.as<double>();
@@ -1702,7 +1723,17 @@ int Solver<R>::upload_contacts(const mlx_contacts* K, ContactData& cd) {
   host_copy(hc + 6 * nK, K->compliance, sizeof(double) * nK);
   int* hv = reinterpret_cast<int*>(hc + 7 * nK);
   for (int k = 0; k < nK; ++k) hv[k] = K->vertex_ids[k] - 1;
+  double* hcv = hc + o_cv;
+  int* hcn = reinterpret_cast<int*>(hcv + kMaxCompliances);
+  for (int g = 0; g < std::max(nc, 0); ++g) {
+    hcv[g] = cv[g];
+    hcn[g] = cn[g];
+  }
   CU(cudaMemcpyAsync(d_contacts.p, hc, sizeof(double) * 7 * nK, cudaMemcpyHostToDevice, stream));
+  double* dcv = d_contacts.as<double>() + 7 * (size_t)nK;
+  if (nc > 0)
+    CU(cudaMemcpyAsync(dcv, hcv, sizeof(double) * kMaxCompliances + sizeof(int) * kMaxCompliances,
+                       cudaMemcpyHostToDevice, stream));
   CU(cudaMemcpyAsync(d_cvid.p, hv, sizeof(int) * nK, cudaMemcpyHostToDevice, stream));
   CU(cudaMemsetAsync(d_clam.p, 0, sizeof(double) * nK, stream));
   cd.normal = d_contacts.as<double>();
@@ -1710,6 +1741,9 @@ int Solver<R>::upload_contacts(const mlx_contacts* K, ContactData& cd) {
   cd.compliance = cd.normal + 6 * nK;
   cd.vid = d_cvid.as<int>();
   cd.lambda = d_clam.as<double>();
+  cd.ncomp = std::max(nc, 0);
+  cd.comp_vals = dcv;
+  cd.comp_counts = reinterpret_cast<const int*>(dcv + kMaxCompliances);
   return MLX_OK;
 }
 

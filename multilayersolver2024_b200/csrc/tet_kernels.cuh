@@ -540,7 +540,13 @@ struct ContactData {
   const double* compliance; // [K]
   const int* vid;           // [K] 0-based
   double* lambda;           // [K]
+  // the distinct compliance values and how many contacts carry each (first
+  // occurrence order; ncomp = 0 when there are more than kMaxCompliances)
+  int ncomp;
+  const double* comp_vals;  // [ncomp]
+  const int* comp_counts;   // [ncomp]
 };
+constexpr int kMaxCompliances = 32;
 
 // Residual partial sums over all tets (blocks [0, tetBlocks)) and all
 // contacts (the remaining blocks), one double per block
@@ -593,7 +599,10 @@ __global__ void __launch_bounds__(256) k_residual_partials(TetData<R> td, const 
   } else {
     // contacts: the reference's correction term is the K x 1 x K implicit
     // expansion of (compliance/h^2) (1x1xK) times lambda (Kx1)
-    // (xpbdLayer3D.m:581-583), so contact k meets every compliance j
+    // (xpbdLayer3D.m:581-583), so contact k meets every compliance j; the
+    // contacts sharing a compliance give equal terms, so with few distinct
+    // compliances each is taken once, times its count (O(K) instead of
+    // O(K^2))
     int cb = blockIdx.x - tetBlocks, ncb = gridDim.x - tetBlocks;
     for (int k = cb * blockDim.x + threadIdx.x; k < cd.K; k += ncb * blockDim.x) {
       R4<R> p = ldcg_r4(pos + cd.vid[k]);
@@ -603,10 +612,17 @@ __global__ void __launch_bounds__(256) k_residual_partials(TetData<R> td, const 
       if (phi > 0) phi = 0;
       double a = fabs(contact_resistance * phi);
       double lk = cd.lambda[k];
-      for (int j = 0; j < cd.K; ++j) {
-        double c = fabs((cd.compliance[j] * inv_h2_d) * lk);
-        double r = a - fmin(a, c);
-        acc[0] += r * r;
+      if (cd.ncomp > 0) {
+        for (int g = 0; g < cd.ncomp; ++g) {
+          const double r = a - fmin(a, fabs((cd.comp_vals[g] * inv_h2_d) * lk));
+          acc[0] += (double)cd.comp_counts[g] * (r * r);
+        }
+      } else {
+        for (int j = 0; j < cd.K; ++j) {
+          double c = fabs((cd.compliance[j] * inv_h2_d) * lk);
+          double r = a - fmin(a, c);
+          acc[0] += r * r;
+        }
       }
     }
   }

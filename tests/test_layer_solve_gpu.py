@@ -78,6 +78,33 @@ def test_residual_monitor_and_stop_rules_fp64(gpu):
     np.testing.assert_allclose(got[3], ref[3], rtol=1e-9)
 
 
+@pytest.mark.parametrize("spread", ["three_values", "all_distinct"])
+def test_contact_residual_term_with_mixed_compliances_fp64(gpu, spread):
+    """The residual's contact term meets every contact's compliance (the
+    reference's K x 1 x K expansion, xpbdLayer3D.m:581-583).  With up to 32
+    distinct compliances the device takes each once, times its count; with
+    more it runs the K x K loop.  Both give the oracle's residual array."""
+    m = block_mesh(dims=(8, 4, 4), seed=4)  # 49 contacts
+    case = Case(m, [60, 0], [3, 6], seed=5)
+    integ = case.integ
+    integ.computeResiduals = True
+    integ.runUntilResSmallerThan = 0.0
+    integ.hangingStop = 30
+    integ.contactResistance = 0.9
+    c = _contacts(case)
+    K = c.vertex_ids.size
+    assert K > 32
+    rng = np.random.default_rng(11)
+    if spread == "three_values":
+        c.compliance = rng.choice(np.array([1e-4, 5e-5, 2e-4]), K)
+    else:
+        c.compliance = rng.uniform(5e-5, 2e-4, K)
+    case.contacts = c
+    got, ref = _compare(case)
+    assert got[5] == ref[5], (got[5], ref[5])
+    np.testing.assert_allclose(got[2], ref[2], rtol=1e-9, atol=1e-14)
+
+
 def test_lame_material_form_matches_blocks_fp64(gpu):
     m = block_mesh(alpha1=0.02, seed=6)
     case = Case(m, [40, 0], [3, 6], seed=7)
