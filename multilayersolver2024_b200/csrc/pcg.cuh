@@ -253,11 +253,15 @@ __global__ void k_pcg_sub(int N, const double4* __restrict__ a, const double4* _
 //
 // Storage.  The Jacobian is kept twice: structure of arrays jt[24][T] (row
 // 6a + k: corner a, k < 3 dC_D/dx_a, k >= 3 dC_H/dx_a) for the per-tet
-// products, whose warps then read consecutive words, and in the order of the
-// vertex -> (tet, corner) CSR, jv[pairs][6], for the per-vertex gathers (each
-// vertex then reads its pairs contiguously).  vtpos[4 s + a] is
-// the CSR position of corner a of tet s.  Per tet, double2: w = (W_D, W_H),
-// c = (C_D, C_H), q = W C + lambda (the right-hand side's factor), s scratch.
+// product of the new multipliers, whose warps then read consecutive words,
+// and in the order of the vertex -> (tet, corner) CSR, jv[pairs][6], for the
+// right-hand side and the assembly (each vertex then reads its pairs
+// contiguously).  vtpos[4 s + a] is the CSR position of corner a of tet s.
+// Per tet, double2: w = (W_D, W_H), c = (C_D, C_H), q = W C + lambda (the
+// right-hand side's factor).  The PCG iterations read neither: J^T W J is
+// assembled once per correction into 3x3 blocks per (vertex, neighbour)
+// (k_ns_assemble), and an iteration is one blocked product (k_ns_spmv) and
+// one vector step (k_ns_step).
 
 template <typename R>
 __global__ void __launch_bounds__(256) k_ns_jacobian(TetData<R> td, const R4<R>* __restrict__ pos, double h2,
